@@ -1,0 +1,269 @@
+"""cg3m -- Python face of the B200-native cgemm3m library (libcg3m.so).
+
+The compute path is the C-ABI library built from ``../csrc`` for sm_100a; this
+module only binds it with ctypes and passes device pointers from torch tensors.
+There is no CPU or PyTorch fallback: if the library is missing, importing this
+module raises.
+
+Matrices follow the reference's conventions (ops-blas/include/cann_ops_blas.h
+:497-500): column-major complex64, op in {N, T, C}, leading dimensions in
+complex elements, alpha/beta complex scalars.  A column-major m x n matrix with
+leading dimension ld is stored here as a torch complex64 tensor of shape
+(n, ld) (row j = column j), or passed as any flat complex64 device buffer.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcg3m.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"libcg3m.so not found at {LIB_PATH}; build it with "
+        "`python ascend-open-source-contributions_b200/build_cg3m.py` (nvcc, sm_100a)")
+
+_lib = ctypes.CDLL(LIB_PATH)
+
+# ---- constants (include/cg3m.h) ------------------------------------------------
+SUCCESS, HANDLE_IS_NULLPTR, INVALID_VALUE, INVALID_ENUM, ALLOC_FAILED, INTERNAL_ERROR, EXECUTION_FAILED, \
+    NOT_SUPPORTED = range(8)
+STATUS_NAMES = {0: "SUCCESS", 1: "HANDLE_IS_NULLPTR", 2: "INVALID_VALUE", 3: "INVALID_ENUM", 4: "ALLOC_FAILED",
+                5: "INTERNAL_ERROR", 6: "EXECUTION_FAILED", 7: "NOT_SUPPORTED"}
+OP = {"N": 0, "T": 1, "C": 2, "R": 3}
+FORM = {"fp32": 0, "tf32x3": 1, "bf16x6": 2, "bf16x9": 3}
+ROUNDING = {"auto": 0, "off": 1}
+
+
+class cg3mComplex(ctypes.Structure):
+    _fields_ = [("real", ctypes.c_float), ("imag", ctypes.c_float)]
+
+
+class cg3mOptions(ctypes.Structure):
+    _fields_ = [("form", ctypes.c_int), ("rounding", ctypes.c_int), ("k_partitions", ctypes.c_int),
+                ("reserved", ctypes.c_int * 5)]
+
+
+class cg3mCallInfo(ctypes.Structure):
+    _fields_ = [("path", ctypes.c_int), ("form", ctypes.c_int), ("tile_m", ctypes.c_int), ("tile_n", ctypes.c_int),
+                ("k_partitions", ctypes.c_int), ("k_span", ctypes.c_int), ("rounding", ctypes.c_int),
+                ("kernels", ctypes.c_int), ("workspace_bytes", ctypes.c_size_t)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class cg3mProblem(ctypes.Structure):
+    _fields_ = [("transa", ctypes.c_int), ("transb", ctypes.c_int), ("m", ctypes.c_int), ("n", ctypes.c_int),
+                ("k", ctypes.c_int), ("alpha", cg3mComplex), ("beta", cg3mComplex), ("A", ctypes.c_void_p),
+                ("lda", ctypes.c_int), ("B", ctypes.c_void_p), ("ldb", ctypes.c_int), ("C", ctypes.c_void_p),
+                ("ldc", ctypes.c_int)]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_CP = ctypes.POINTER(cg3mComplex)
+
+SIGNATURES = {
+    "cg3mCreate": [ctypes.POINTER(_P)],
+    "cg3mDestroy": [_P],
+    "cg3mSetStream": [_P, _P],
+    "cg3mGetStream": [_P, ctypes.POINTER(_P)],
+    "cg3mSetWorkspace": [_P, _P, ctypes.c_size_t],
+    "cg3mGetVersion": [_P, ctypes.POINTER(_I)],
+    "cg3mCgemm3m": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I],
+    "cg3mCgemm3mEx": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I, ctypes.POINTER(cg3mOptions),
+                      ctypes.POINTER(cg3mCallInfo)],
+    "cg3mCgemm3mStridedBatched": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, ctypes.c_int64, _P, _I, ctypes.c_int64, _CP,
+                                  _P, _I, ctypes.c_int64, _I],
+    "cg3mBatchPlanCreate": [_P, ctypes.POINTER(cg3mProblem), _I, _I, ctypes.POINTER(_P), ctypes.POINTER(_I)],
+    "cg3mBatchPlanExecute": [_P, _P, _I],
+    "cg3mBatchPlanDestroy": [_P],
+    "cg3mBatchPlanDescribe": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
+    "cg3mGetDeviceStatus": [_P, ctypes.POINTER(_I)],
+    "cg3mSetStageEvents": [_P, ctypes.POINTER(_P), _I],
+    "cg3mValidate": [_I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I, _I, ctypes.POINTER(_I)],
+    "cg3mPlan": [_I, _I, _I, _I, _I, _CP, _I, _I, _CP, _I, ctypes.POINTER(cg3mOptions), _I,
+                 ctypes.POINTER(cg3mCallInfo)],
+    "cg3mZgemmReference": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I, _P],
+    "cg3mErrorReport": [_P, _I, _I, _P, _I, _P, ctypes.POINTER(ctypes.c_double)],
+    "aclblasCreate": [ctypes.POINTER(_P)],
+    "aclblasDestroy": [_P],
+    "aclblasSetStream": [_P, _P],
+    "aclblasGetStream": [_P, ctypes.POINTER(_P)],
+    "aclblasSetWorkspace": [_P, _P, ctypes.c_size_t],
+    "aclblasGetVersion": [_P, ctypes.POINTER(_I)],
+    "aclblasCgemm3m": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I],
+    "aclblasCgemm3mStridedBatched": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, ctypes.c_int64, _P, _I, ctypes.c_int64,
+                                     _CP, _P, _I, ctypes.c_int64, _I],
+}
+
+for _name, _args in SIGNATURES.items():
+    _fn = getattr(_lib, _name)
+    _fn.argtypes = _args
+    _fn.restype = ctypes.c_int
+
+lib = _lib
+
+
+def cx(z) -> cg3mComplex:
+    z = complex(z)
+    return cg3mComplex(z.real, z.imag)
+
+
+def _op(o):
+    return OP[o] if isinstance(o, str) else int(o)
+
+
+class Cg3mError(RuntimeError):
+    def __init__(self, status, what=""):
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}")
+        self.status = status
+
+
+def _check(status, what):
+    if status != SUCCESS:
+        raise Cg3mError(status, what)
+
+
+def ptr(t):
+    """Device (or host) address of a torch tensor / None."""
+    if t is None:
+        return None
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Handle:
+    """Owns one cg3m handle bound to a CUDA stream (default: torch's current)."""
+
+    def __init__(self, stream=None):
+        self.h = ctypes.c_void_p()
+        _check(_lib.cg3mCreate(ctypes.byref(self.h)), "cg3mCreate")
+        if stream is not None:
+            self.set_stream(stream)
+
+    def set_stream(self, stream):
+        s = stream if isinstance(stream, int) else getattr(stream, "cuda_stream", stream)
+        _check(_lib.cg3mSetStream(self.h, ctypes.c_void_p(s)), "cg3mSetStream")
+
+    def close(self):
+        if self.h:
+            _lib.cg3mDestroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stage_events(self, events):
+        """Record the given torch.cuda.Event objects around each kernel of later calls."""
+        arr = (ctypes.c_void_p * max(1, len(events)))(*[ctypes.c_void_p(e.cuda_event) for e in events])
+        _check(_lib.cg3mSetStageEvents(self.h, arr, len(events)), "cg3mSetStageEvents")
+
+    def device_status(self):
+        f = ctypes.c_int()
+        _check(_lib.cg3mGetDeviceStatus(self.h, ctypes.byref(f)), "cg3mGetDeviceStatus")
+        return f.value
+
+    def cgemm3m(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, form="fp32", rounding="auto",
+                k_partitions=0, raw=False):
+        """C <- alpha*op(A)*op(B) + beta*C on device buffers; returns the call info.
+
+        ``raw=True`` calls the drop-in cg3mCgemm3m (FP32 form only) and returns
+        the status instead of raising."""
+        al, be = cx(alpha), cx(beta)
+        if raw:
+            return _lib.cg3mCgemm3m(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda, ptr(B),
+                                    ldb, ctypes.byref(be), ptr(C), ldc)
+        opts = cg3mOptions(FORM[form] if isinstance(form, str) else form,
+                           ROUNDING[rounding] if isinstance(rounding, str) else rounding, k_partitions)
+        info = cg3mCallInfo()
+        st = _lib.cg3mCgemm3mEx(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda, ptr(B), ldb,
+                                ctypes.byref(be), ptr(C), ldc, ctypes.byref(opts), ctypes.byref(info))
+        _check(st, "cg3mCgemm3mEx")
+        return info.as_dict()
+
+    def zgemm_reference(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, out64):
+        al, be = cx(alpha), cx(beta)
+        _check(_lib.cg3mZgemmReference(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda,
+                                       ptr(B), ldb, ctypes.byref(be), ptr(C), ldc, ptr(out64)), "cg3mZgemmReference")
+
+    def error_report(self, m, n, C, ldc, out64):
+        rep = (ctypes.c_double * 5)()
+        _check(_lib.cg3mErrorReport(self.h, m, n, ptr(C), ldc, ptr(out64), rep), "cg3mErrorReport")
+        return {"normwise": rep[0], "comp_re": rep[1], "comp_im": rep[2], "abs_re": rep[3], "abs_im": rep[4]}
+
+
+def validate(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, allow_conj_only=False):
+    """Host-only validation (no device access): (status, action)."""
+    act = ctypes.c_int()
+    al = ctypes.byref(cx(alpha)) if alpha is not None else None
+    be = ctypes.byref(cx(beta)) if beta is not None else None
+    st = _lib.cg3mValidate(_op(transa), _op(transb), m, n, k, al, A, lda, B, ldb, be, C, ldc, int(allow_conj_only),
+                           ctypes.byref(act))
+    return st, act.value
+
+
+def plan(transa, transb, m, n, k, alpha=1, beta=0, lda=None, ldb=None, ldc=None, form="fp32", rounding="auto",
+         k_partitions=0, sm_count=148):
+    """The planner's decision (host only)."""
+    ta, tb = _op(transa), _op(transb)
+    lda = lda or (m if ta in (0, 3) else k)
+    ldb = ldb or (k if tb in (0, 3) else n)
+    ldc = ldc or m
+    opts = cg3mOptions(FORM[form], ROUNDING[rounding], k_partitions)
+    info = cg3mCallInfo()
+    _check(_lib.cg3mPlan(ta, tb, m, n, k, ctypes.byref(cx(alpha)), lda, ldb, ctypes.byref(cx(beta)), ldc,
+                         ctypes.byref(opts), sm_count, ctypes.byref(info)), "cg3mPlan")
+    return info.as_dict()
+
+
+_default_handles = {}
+
+
+def default_handle():
+    """A per-process handle following torch's current stream."""
+    import torch
+
+    dev = torch.cuda.current_device()
+    h = _default_handles.get(dev)
+    if h is None:
+        h = _default_handles[dev] = Handle()
+    h.set_stream(torch.cuda.current_stream().cuda_stream)
+    return h
+
+
+def cgemm3m(A, B, transa="N", transb="N", alpha=1.0, beta=0.0, C=None, form="fp32", rounding="auto"):
+    """Convenience wrapper on torch complex64 tensors in *row-major torch* shape.
+
+    ``A`` holds op-stored matrix X as a torch (rows, cols) tensor; it is handed
+    to the library as the column-major matrix X^T (no copy), so this computes
+    the same product torch would: result = alpha*opt(A) @ opt(B) + beta*C where
+    opt() applies ``transa``/``transb`` to the torch matrices.  Returns C.
+    """
+    import torch
+
+    if not (A.is_cuda and B.is_cuda):
+        raise ValueError("cg3m runs on CUDA tensors only")
+    A = A.contiguous()
+    B = B.contiguous()
+    ta, tb = _op(transa), _op(transb)
+    ar, ac = A.shape
+    br, bc = B.shape
+    m, k = (ar, ac) if ta in (0, 3) else (ac, ar)
+    k2, n = (br, bc) if tb in (0, 3) else (bc, br)
+    if k != k2:
+        raise ValueError("inner dimensions differ")
+    # torch row-major (rows, cols) == column-major (cols, rows): compute
+    # C^T = op(B)^T op(A)^T, i.e. swap the operands (the reference's C^T
+    # convention, gemm_host_common.h:69-74).
+    if C is None:
+        C = torch.zeros((m, n), dtype=torch.complex64, device=A.device)
+    else:
+        C = C.contiguous()
+    h = default_handle()
+    h.cgemm3m(tb, ta, n, m, k, alpha, B, bc, A, ac, beta, C, n, form=form, rounding=rounding)
+    return C

@@ -1,0 +1,523 @@
+// api.cpp -- the C ABI (include/cg3m.h, include/cg3m_aclblas.h).
+//
+// Reference: aclblasCgemm3m (blas/gemm/arch35/cgemm3m_host.cpp:17-23) ->
+// LaunchComplexGemm (cgemm_host.cpp:701-730) -> LaunchCgemmKernel (:553-587)
+// -> HandleCgemmAlphaZero (:636-663) or LaunchGeneralCgemm (:503-551); handle
+// API cann_ops_blas.h:31-110.  Every launch goes to the handle's stream and
+// nothing here synchronizes except Destroy and GetDeviceStatus.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "../../include/cg3m_aclblas.h"
+#include "cg3m_internal.h"
+
+using namespace cg3m;
+
+namespace {
+
+constexpr int kVersion = 10000;  // 1.0.0
+
+bool log_enabled()
+{
+    static const bool on = std::getenv("CG3M_LOG") != nullptr;
+    return on;
+}
+
+void log_call(const char* what, const Plan& plan, const Problem& p)
+{
+    if (!log_enabled()) {
+        return;
+    }
+    std::fprintf(stderr,
+                 "{\"cg3m\":\"%s\",\"m\":%d,\"n\":%d,\"k\":%d,\"transa\":%d,\"transb\":%d,\"form\":%d,"
+                 "\"tile\":[%d,%d],\"parts\":%d,\"span\":%d,\"rounding\":%d,\"workspace\":%zu}\n",
+                 what, p.m, p.n, p.k, p.transa, p.transb, plan.form, plan.tile_m, plan.tile_n, plan.parts, plan.span,
+                 plan.rounding ? 1 : 0, plan.total);
+}
+
+cg3mStatus_t bind_device(cg3mContext* h)
+{
+    if (h->device >= 0) {
+        return CG3M_STATUS_SUCCESS;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        return CG3M_STATUS_INTERNAL_ERROR;
+    }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+        return CG3M_STATUS_INTERNAL_ERROR;
+    }
+    int* status = nullptr;
+    if (cudaMalloc(&status, 64) != cudaSuccess) {
+        return CG3M_STATUS_ALLOC_FAILED;
+    }
+    if (cudaMemset(status, 0, 64) != cudaSuccess) {
+        cudaFree(status);
+        return CG3M_STATUS_INTERNAL_ERROR;
+    }
+    void* ws = nullptr;
+    if (cudaMalloc(&ws, kDefaultWorkspaceBytes) != cudaSuccess) {
+        cudaFree(status);
+        return CG3M_STATUS_ALLOC_FAILED;
+    }
+    h->device = dev;
+    h->sm_count = sms;
+    h->status = status;
+    h->default_ws = ws;
+    h->default_ws_bytes = kDefaultWorkspaceBytes;
+    return CG3M_STATUS_SUCCESS;
+}
+
+// Effective workspace of at least `bytes` (EnsureDefaultWorkspace /
+// GetEffectiveWorkspace in the reference): the borrowed one when large enough,
+// else the library's own, grown on demand.
+cg3mStatus_t workspace(cg3mContext* h, size_t bytes, void** out)
+{
+    if (h->user_ws != nullptr && h->user_ws_bytes >= bytes) {
+        *out = h->user_ws;
+        return CG3M_STATUS_SUCCESS;
+    }
+    if (h->default_ws_bytes < bytes) {
+        // Work already queued may still read the old buffer; cudaFree waits for it.
+        if (h->default_ws != nullptr) {
+            cudaFree(h->default_ws);
+            h->default_ws = nullptr;
+            h->default_ws_bytes = 0;
+        }
+        const size_t grow = align_up(bytes, size_t(2) << 20);
+        if (cudaMalloc(&h->default_ws, grow) != cudaSuccess) {
+            h->default_ws = nullptr;
+            return CG3M_STATUS_ALLOC_FAILED;
+        }
+        h->default_ws_bytes = grow;
+    }
+    *out = h->default_ws;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t to_status(cudaError_t e)
+{
+    if (e == cudaSuccess) {
+        return CG3M_STATUS_SUCCESS;
+    }
+    if (e == cudaErrorMemoryAllocation) {
+        return CG3M_STATUS_ALLOC_FAILED;
+    }
+    return CG3M_STATUS_EXECUTION_FAILED;
+}
+
+cg3mStatus_t run_one(cg3mContext* h, int transa, int transb, int m, int n, int k, const cg3mComplex* alpha,
+                     const cg3mComplex* A, int lda, const cg3mComplex* B, int ldb, const cg3mComplex* beta,
+                     cg3mComplex* C, int ldc, const cg3mOptions& opts, bool allow_conj_only, cg3mCallInfo* info)
+{
+    int action = 0;
+    const cg3mStatus_t st =
+        validate(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, allow_conj_only, &action);
+    if (info != nullptr) {
+        std::memset(info, 0, sizeof(*info));
+        info->form = opts.form;
+    }
+    if (st != CG3M_STATUS_SUCCESS || action == 0) {
+        return st;
+    }
+    if (opts.form < CG3M_FORM_FP32 || opts.form > CG3M_FORM_BF16X9 || opts.rounding < CG3M_ROUNDING_AUTO ||
+        opts.rounding > CG3M_ROUNDING_OFF || opts.k_partitions < 0) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    const cg3mStatus_t bs = bind_device(h);
+    if (bs != CG3M_STATUS_SUCCESS) {
+        return bs;
+    }
+    if (action == 1) {
+        if (info != nullptr) {
+            info->path = 1;
+            info->kernels = 1;
+        }
+        return to_status(launch_beta_scale(h->stream, m, n, beta->real, beta->imag, C, ldc));
+    }
+    Problem p{transa, transb, m, n, k, alpha->real, alpha->imag, beta->real, beta->imag, A, lda, B, ldb, C, ldc};
+    Plan plan;
+    if (!make_plan(p, opts, h->sm_count, &plan)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    void* ws = nullptr;
+    const cg3mStatus_t wst = workspace(h, plan.total, &ws);
+    if (wst != CG3M_STATUS_SUCCESS) {
+        return wst;
+    }
+    log_call("cgemm3m", plan, p);
+    int kernels = 0;
+    const cudaError_t err = enqueue(h->stream, p, plan, ws, h->status, &kernels, h->stage_events,
+                                    h->stage_event_count);
+    if (info != nullptr) {
+        info->path = plan.parts > 1 ? 3 : 2;
+        info->tile_m = plan.tile_m;
+        info->tile_n = plan.tile_n;
+        info->k_partitions = plan.parts;
+        info->k_span = plan.span;
+        info->rounding = plan.rounding ? 1 : 0;
+        info->kernels = kernels;
+        info->workspace_bytes = plan.total;
+    }
+    return to_status(err);
+}
+
+}  // namespace
+
+namespace cg3m {
+
+cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status, int* kernels,
+                    const cudaEvent_t* events, int nevents)
+{
+    int count = 0;
+    auto mark = [&](int i) {
+        if (events != nullptr && i < nevents && events[i] != nullptr) {
+            cudaEventRecord(events[i], s);
+        }
+    };
+    mark(0);
+    cudaError_t err = launch_pack(s, p, plan, ws);
+    mark(++count);
+    if (err == cudaSuccess) {
+        err = plan.form == CG3M_FORM_FP32 ? launch_gemm_fp32(s, p, plan, ws, status)
+                                          : launch_gemm_tc(s, p, plan, ws, status);
+        mark(++count);
+    }
+    if (err == cudaSuccess && plan.parts > 1) {
+        err = launch_merge(s, p, plan, ws);
+        mark(++count);
+    }
+    if (err == cudaSuccess && plan.rounding) {
+        int launched = 0;
+        err = launch_rounding(s, p, plan, ws, status, &launched);
+        count += launched;
+        mark(count);
+    }
+    if (kernels != nullptr) {
+        *kernels = count;
+    }
+    return err;
+}
+
+}  // namespace cg3m
+
+extern "C" {
+
+cg3mStatus_t cg3mCreate(cg3mHandle_t* handle)
+{
+    if (handle == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (*handle != nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    cg3mContext* h = new (std::nothrow) cg3mContext();
+    if (h == nullptr) {
+        return CG3M_STATUS_ALLOC_FAILED;
+    }
+    *handle = h;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mDestroy(cg3mHandle_t h)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    cg3mStatus_t st = CG3M_STATUS_SUCCESS;
+    if (h->device >= 0) {
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+            st = CG3M_STATUS_EXECUTION_FAILED;
+        }
+        cudaFree(h->default_ws);
+        cudaFree(h->status);
+    }
+    delete h;
+    return st;
+}
+
+cg3mStatus_t cg3mSetStream(cg3mHandle_t h, void* stream)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    h->stream = static_cast<cudaStream_t>(stream);
+    h->user_ws = nullptr;  // back to the default workspace (cann_ops_blas.h:63-71)
+    h->user_ws_bytes = 0;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mGetStream(cg3mHandle_t h, void** stream)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (stream == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    *stream = h->stream;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mSetWorkspace(cg3mHandle_t h, void* ws, size_t bytes)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (ws == nullptr || bytes == 0) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (bytes > h->user_ws_bytes) {  // grow-only (cann_ops_blas.h:86-98)
+        h->user_ws = ws;
+        h->user_ws_bytes = bytes;
+    }
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mGetVersion(cg3mHandle_t, int* version)
+{
+    if (version == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    *version = kVersion;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mCgemm3m(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                         const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B, int ldb,
+                         const cg3mComplex* beta, cg3mComplex* C, int ldc)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    const cg3mOptions opts{};
+    return run_one(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, opts, false, nullptr);
+}
+
+cg3mStatus_t cg3mCgemm3mEx(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                           const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B, int ldb,
+                           const cg3mComplex* beta, cg3mComplex* C, int ldc, const cg3mOptions* opts,
+                           cg3mCallInfo* info)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    const cg3mOptions o = opts != nullptr ? *opts : cg3mOptions{};
+    return run_one(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, o, true, info);
+}
+
+cg3mStatus_t cg3mCgemm3mStridedBatched(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m,
+                                       int n, int k, const cg3mComplex* alpha, const cg3mComplex* A, int lda,
+                                       int64_t strideA, const cg3mComplex* B, int ldb, int64_t strideB,
+                                       const cg3mComplex* beta, cg3mComplex* C, int ldc, int64_t strideC,
+                                       int batch_count)
+{
+    // Statuses of the strided API (blas/gemm/README.md:850-858): enum errors stay INVALID_ENUM.
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    auto op_ok = [](int op) { return op == CG3M_OP_N || op == CG3M_OP_T || op == CG3M_OP_C; };
+    if (!op_ok(transa) || !op_ok(transb)) {
+        return CG3M_STATUS_INVALID_ENUM;
+    }
+    if (batch_count < 0) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    int action = 0;
+    // Shape / ld / scalar checks as the single call; an empty batch needs no
+    // matrices at all (blas/gemm/README.md:850-851).
+    const void* any = reinterpret_cast<const void*>(1);
+    const bool empty = batch_count == 0;
+    const cg3mStatus_t st = validate(transa, transb, m, n, k, alpha, empty ? any : A, lda, empty ? any : B, ldb, beta,
+                                     empty ? any : C, ldc, false, &action);
+    if (st != CG3M_STATUS_SUCCESS || action == 0 || batch_count == 0) {
+        return st;
+    }
+    const cg3mOptions opts{};
+    for (int i = 0; i < batch_count; ++i) {
+        const cg3mStatus_t r = run_one(h, transa, transb, m, n, k, alpha, A == nullptr ? nullptr : A + i * strideA,
+                                       lda, B == nullptr ? nullptr : B + i * strideB, ldb, beta, C + i * strideC, ldc,
+                                       opts, false, nullptr);
+        if (r != CG3M_STATUS_SUCCESS) {
+            return r;
+        }
+    }
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mSetStageEvents(cg3mHandle_t h, void* const* events, int count)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (count < 0 || count > 16 || (count > 0 && events == nullptr)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    for (int i = 0; i < 16; ++i) {
+        h->stage_events[i] = i < count ? static_cast<cudaEvent_t>(events[i]) : nullptr;
+    }
+    h->stage_event_count = count;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t h, int* flags)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (flags == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    *flags = 0;
+    if (h->device < 0) {
+        return CG3M_STATUS_SUCCESS;
+    }
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        return CG3M_STATUS_EXECUTION_FAILED;
+    }
+    int v = 0;
+    if (cudaMemcpy(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemset(h->status, 0, sizeof(int)) != cudaSuccess) {
+        return CG3M_STATUS_EXECUTION_FAILED;
+    }
+    *flags = v;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mValidate(cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                          const cg3mComplex* alpha, const void* A, int lda, const void* B, int ldb,
+                          const cg3mComplex* beta, const void* C, int ldc, int allow_conj_only, int* action)
+{
+    int a = 0;
+    const cg3mStatus_t st =
+        validate(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, allow_conj_only != 0, &a);
+    if (action != nullptr) {
+        *action = a;
+    }
+    return st;
+}
+
+cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k, const cg3mComplex* alpha,
+                      int lda, int ldb, const cg3mComplex* beta, int ldc, const cg3mOptions* opts, int sm_count,
+                      cg3mCallInfo* info)
+{
+    if (info == nullptr || alpha == nullptr || beta == nullptr || m <= 0 || n <= 0 || k <= 0) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    const cg3mOptions o = opts != nullptr ? *opts : cg3mOptions{};
+    Problem p{transa, transb, m, n, k, alpha->real, alpha->imag, beta->real, beta->imag,
+              nullptr, lda, nullptr, ldb, nullptr, ldc};
+    Plan plan;
+    if (!make_plan(p, o, sm_count, &plan)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    std::memset(info, 0, sizeof(*info));
+    info->path = plan.parts > 1 ? 3 : 2;
+    info->form = plan.form;
+    info->tile_m = plan.tile_m;
+    info->tile_n = plan.tile_n;
+    info->k_partitions = plan.parts;
+    info->k_span = plan.span;
+    info->rounding = plan.rounding ? 1 : 0;
+    info->kernels = 2 + (plan.parts > 1 ? 1 : 0) + (plan.rounding ? 4 : 0);
+    info->workspace_bytes = plan.total;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mZgemmReference(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                                const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B,
+                                int ldb, const cg3mComplex* beta, const cg3mComplex* C, int ldc, void* out64)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    int action = 0;
+    const cg3mStatus_t st = validate(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, true, &action);
+    if (st != CG3M_STATUS_SUCCESS || m == 0 || n == 0) {
+        return st;
+    }
+    if (out64 == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    const cg3mStatus_t bs = bind_device(h);
+    if (bs != CG3M_STATUS_SUCCESS) {
+        return bs;
+    }
+    Problem p{transa, transb, m, n, k, alpha->real, alpha->imag, beta->real, beta->imag, A, lda, B, ldb,
+              const_cast<cg3mComplex*>(C), ldc};
+    return to_status(launch_zgemm_ref(h->stream, p, C, out64));
+}
+
+cg3mStatus_t cg3mErrorReport(cg3mHandle_t h, int m, int n, const cg3mComplex* C, int ldc, const void* out64,
+                             double* report)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (m <= 0 || n <= 0 || ldc < m || C == nullptr || out64 == nullptr || report == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    const cg3mStatus_t bs = bind_device(h);
+    if (bs != CG3M_STATUS_SUCCESS) {
+        return bs;
+    }
+    double* dev = nullptr;
+    if (cudaMalloc(&dev, 8 * sizeof(double)) != cudaSuccess) {
+        return CG3M_STATUS_ALLOC_FAILED;
+    }
+    cudaError_t err = launch_error_report(h->stream, m, n, C, ldc, out64, dev);
+    double host[8] = {0};
+    if (err == cudaSuccess) {
+        err = cudaMemcpyAsync(host, dev, sizeof(host), cudaMemcpyDeviceToHost, h->stream);
+    }
+    if (err == cudaSuccess) {
+        err = cudaStreamSynchronize(h->stream);
+    }
+    cudaFree(dev);
+    if (err != cudaSuccess) {
+        return CG3M_STATUS_EXECUTION_FAILED;
+    }
+    // host: [0] sum |d|^2, [1] sum |x|^2, [2] max rel re, [3] max rel im, [4] max abs re, [5] max abs im
+    report[0] = host[1] > 0 ? __builtin_sqrt(host[0] / host[1]) : __builtin_sqrt(host[0]);
+    report[1] = host[2];
+    report[2] = host[3];
+    report[3] = host[4];
+    report[4] = host[5];
+    return CG3M_STATUS_SUCCESS;
+}
+
+// ---- aclblas-named entry points (drop-in link compatibility) -----------------
+
+aclblasStatus_t aclblasCreate(aclblasHandle_t* handle) { return cg3mCreate(handle); }
+aclblasStatus_t aclblasDestroy(aclblasHandle_t handle) { return cg3mDestroy(handle); }
+aclblasStatus_t aclblasSetStream(aclblasHandle_t handle, aclrtStream stream) { return cg3mSetStream(handle, stream); }
+aclblasStatus_t aclblasGetStream(aclblasHandle_t handle, aclrtStream* stream) { return cg3mGetStream(handle, stream); }
+aclblasStatus_t aclblasSetWorkspace(aclblasHandle_t handle, void* workspace, size_t bytes)
+{
+    return cg3mSetWorkspace(handle, workspace, bytes);
+}
+aclblasStatus_t aclblasGetVersion(aclblasHandle_t handle, int* version) { return cg3mGetVersion(handle, version); }
+
+aclblasStatus_t aclblasCgemm3m(aclblasHandle_t handle, aclblasOperation_t transa, aclblasOperation_t transb, int m,
+                               int n, int k, const aclblasComplex* alpha, const aclblasComplex* A, int lda,
+                               const aclblasComplex* B, int ldb, const aclblasComplex* beta, aclblasComplex* C,
+                               int ldc)
+{
+    return cg3mCgemm3m(handle, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+aclblasStatus_t aclblasCgemm3mStridedBatched(aclblasHandle_t handle, aclblasOperation_t transa,
+                                             aclblasOperation_t transb, int m, int n, int k,
+                                             const aclblasComplex* alpha, const aclblasComplex* A, int lda,
+                                             int64_t strideA, const aclblasComplex* B, int ldb, int64_t strideB,
+                                             const aclblasComplex* beta, aclblasComplex* C, int ldc, int64_t strideC,
+                                             int batchCount)
+{
+    return cg3mCgemm3mStridedBatched(handle, transa, transb, m, n, k, alpha, A, lda, strideA, B, ldb, strideB, beta,
+                                     C, ldc, strideC, batchCount);
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// cg3m_internal.h -- host-side types shared by the C ABI, the planner and the
+// kernel launchers.  No torch types anywhere: plain CUDA runtime only.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/cg3m.h"
+
+struct cg3mContext {
+    cudaStream_t stream = nullptr;
+    int device = -1;             // bound on first launch
+    int sm_count = 0;
+    void* default_ws = nullptr;  // library-owned workspace (grown on demand)
+    size_t default_ws_bytes = 0;
+    void* user_ws = nullptr;     // borrowed (cg3mSetWorkspace), never freed here
+    size_t user_ws_bytes = 0;
+    int* status = nullptr;       // device status word (bounded-wait failures)
+    cudaEvent_t stage_events[16] = {};
+    int stage_event_count = 0;
+};
+
+namespace cg3m {
+
+constexpr size_t kDefaultWorkspaceBytes = size_t(32) << 20;  // cann_ops_blas.h:33-35
+constexpr size_t kRegionAlign = 512;                          // cgemm_host.cpp:33 (16 x 32 B)
+
+// Which plane layout a GEMM kernel consumes.
+enum class Layout { MnMajor, KMajor };
+
+// One planned cgemm3m call.
+struct Plan {
+    int action = 0;   // 0 nothing, 1 beta-scale only, 2 product path
+    int form = CG3M_FORM_FP32;
+    int tile_m = 128, tile_n = 64;
+    int parts = 1;
+    int span = 0;
+    bool unit = false;       // alpha == 1, beta == 0
+    bool beta_zero = false;
+    bool rounding = false;
+    // workspace layout (byte offsets from the workspace base)
+    size_t planes_a_off = 0, planes_b_off = 0, partial_off = 0, round_off = 0, total = 0;
+    int pitch_a = 0, pitch_b = 0;  // elements per plane row
+    int planes = 3;                // planes per operand
+    size_t plane_a_elems = 0, plane_b_elems = 0;
+    size_t partial_plane_elems = 0;
+    int partial_pitch = 0;
+};
+
+struct Problem {
+    int transa, transb, m, n, k;
+    float ar, ai, br, bi;
+    const void* A;
+    int lda;
+    const void* B;
+    int ldb;
+    void* C;
+    int ldc;
+};
+
+cg3mStatus_t validate(int transa, int transb, int m, int n, int k, const cg3mComplex* alpha, const void* A, int lda,
+                      const void* B, int ldb, const cg3mComplex* beta, const void* C, int ldc, bool allow_conj_only,
+                      int* action);
+
+bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* plan);
+
+// Tensor-map encoding through the driver entry point (no -lcuda needed).
+bool encode_tensor_map(CUtensorMap* map, CUtensorMapDataType type, int rank, const uint64_t* dims,
+                       const uint64_t* strides_bytes, const uint32_t* box, CUtensorMapSwizzle swizzle,
+                       const void* base);
+
+// ---- kernel launchers (return cudaSuccess or the launch error) -------------
+cudaError_t launch_beta_scale(cudaStream_t s, int m, int n, float br, float bi, void* C, int ldc);
+cudaError_t launch_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws);
+cudaError_t launch_gemm_fp32(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
+cudaError_t launch_gemm_tc(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
+cudaError_t launch_merge(cudaStream_t s, const Problem& p, const Plan& plan, void* ws);
+cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status, int* launched);
+cudaError_t launch_zgemm_ref(cudaStream_t s, const Problem& p, const void* Cin, void* out64);
+cudaError_t launch_error_report(cudaStream_t s, int m, int n, const void* C, int ldc, const void* out64,
+                                double* dev_report);
+
+// Enqueue a fully planned call (pack + GEMM [+ merge] [+ rounding]); when
+// `events` is non-null, events[0] is recorded before the first launch and
+// events[i] after the i-th (i < nevents).
+cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status, int* kernels,
+                    const cudaEvent_t* events = nullptr, int nevents = 0);
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace cg3m

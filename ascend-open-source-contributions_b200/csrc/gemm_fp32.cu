@@ -1,0 +1,354 @@
+// gemm_fp32.cu -- plain FP32 3M GEMM (the drop-in form), its split-K merge and
+// the beta-only scaling kernel.
+//
+// Reference counterparts:
+//   products  gemm_cgemm_products_kernel  blas/gemm/arch35/cgemm_compute_kernel.cpp:350-366
+//   fused     gemm_cgemm_fused_kernel                         cgemm_compute_kernel.cpp:879-896
+//   epilogue  gemm_cgemm_epilogue_kernel / CgemmEpilogueVf     cgemm_epilogue_kernel.cpp:232-332
+//   alpha=0   HandleCgemmAlphaZero                            cgemm_host.cpp:636-663
+//
+// B200 design.  One CTA owns a BM x BN tile of complex outputs and computes all
+// three real products of it on the CUDA cores with FFMA, so the epilogue
+// (Re = P0-P1, Im = (P2-P0)-P1, alpha, beta, interleave, ldc store) runs from
+// registers with no workspace round trip -- the reference's "fused" kernel for
+// every alpha/beta.  Operand planes (Ar, Ai, Ar+Ai / Br, Bi, Br+Bi, MN-major)
+// are staged by TMA: one 3-D box per operand per K-tile carries all three
+// planes, into a STAGES-deep ring guarded by full/empty mbarriers.  A producer
+// warp issues the copies; the consumer warps each own a 32x32 sub-tile, every
+// thread an 8 x 4 complex micro-tile (96 FP32 accumulators).  Each output's
+// K terms are accumulated by one thread in increasing k -- a fixed order, so
+// results are bitwise reproducible.  For long-K, few-tile shapes the K range is
+// split into partitions (grid.y); each writes (Re_p, Im_p) planes and a merge
+// kernel sums them in partition order before alpha/beta.
+#include "cg3m_internal.h"
+#include "ptx.cuh"
+
+namespace cg3m {
+
+struct EpiParams {
+    float ar, ai, br, bi;
+    int unit, beta_zero;
+};
+
+// alpha*(re,im) [+ beta*c]; one rounding per operation (no contraction).
+__device__ __forceinline__ float2 epilogue_value(float re, float im, const EpiParams& e, const float2* cptr)
+{
+    if (e.unit) {
+        return make_float2(re, im);
+    }
+    float xr = __fsub_rn(__fmul_rn(e.ar, re), __fmul_rn(e.ai, im));
+    float xi = __fadd_rn(__fmul_rn(e.ar, im), __fmul_rn(e.ai, re));
+    if (!e.beta_zero) {
+        const float2 c = *cptr;
+        xr = __fadd_rn(xr, __fsub_rn(__fmul_rn(e.br, c.x), __fmul_rn(e.bi, c.y)));
+        xi = __fadd_rn(xi, __fadd_rn(__fmul_rn(e.br, c.y), __fmul_rn(e.bi, c.x)));
+    }
+    return make_float2(xr, xi);
+}
+
+namespace {
+
+struct Fp32Params {
+    int m, n, k;
+    int span, parts;
+    int tiles_m, tiles_n;
+    EpiParams epi;
+    float2* C;
+    int ldc;
+    float* partial;  // [part][2][n][ppitch]
+    int ppitch;
+    size_t pplane;
+    int* status;
+};
+
+template <int BM, int BN>
+struct Fp32Cfg {
+    static constexpr int BK = 16;
+    static constexpr int STAGES = 4;
+    static constexpr int WARPS_M = BM / 32;
+    static constexpr int WARPS_N = BN / 32;
+    static constexpr int CONSUMER_WARPS = WARPS_M * WARPS_N;
+    static constexpr int THREADS = (CONSUMER_WARPS + 1) * 32;
+    static constexpr int A_STAGE = 3 * BK * BM;  // floats
+    static constexpr int B_STAGE = 3 * BK * BN;
+    static constexpr size_t SMEM = size_t(STAGES) * (A_STAGE + B_STAGE) * 4 + 2 * STAGES * 8 + 1024;
+};
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(Fp32Cfg<BM, BN>::THREADS, 1)
+    gemm3m_fp32_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                       const Fp32Params p)
+{
+    using Cfg = Fp32Cfg<BM, BN>;
+    constexpr int BK = Cfg::BK, STAGES = Cfg::STAGES;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    float* sA = reinterpret_cast<float*>(base);
+    float* sB = sA + STAGES * Cfg::A_STAGE;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * Cfg::B_STAGE);
+    uint64_t* empty = full + STAGES;
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+
+    // Grouped rasterisation: 8 row-tiles per group keeps the operand panels of
+    // concurrently running CTAs resident in L2.
+    constexpr int GM = 8;
+    const int pid = blockIdx.x;
+    const int in_group = GM * p.tiles_n;
+    const int first_m = (pid / in_group) * GM;
+    const int gsz = min(p.tiles_m - first_m, GM);
+    const int tm = first_m + (pid % in_group) % gsz;
+    const int tn = (pid % in_group) / gsz;
+    const int m0 = tm * BM, n0 = tn * BN;
+    const int part = blockIdx.y;
+    const int kbeg = part * p.span;
+    const int kend = min(p.k, kbeg + p.span);
+    const int ktiles = (kend - kbeg + BK - 1) / BK;
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], Cfg::CONSUMER_WARPS);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    if (warp == Cfg::CONSUMER_WARPS) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            tma_prefetch_desc(&tmA);
+            tma_prefetch_desc(&tmB);
+            int issued = 0;
+            for (int kt = 0; kt < ktiles; ++kt) {
+                const int s = kt % STAGES;
+                if (kt >= STAGES && !mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1, p.status)) {
+                    break;
+                }
+                mbar_arrive_expect_tx(&full[s], (Cfg::A_STAGE + Cfg::B_STAGE) * 4);
+                tma_load_3d(sA + s * Cfg::A_STAGE, &tmA, &full[s], m0, kbeg + kt * BK, 0);
+                tma_load_3d(sB + s * Cfg::B_STAGE, &tmB, &full[s], n0, kbeg + kt * BK, 0);
+                ++issued;
+            }
+            // Drain: the last STAGES copies may still be landing in shared memory.
+            for (int kt = issued > STAGES ? issued - STAGES : 0; kt < issued; ++kt) {
+                mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1, p.status);
+            }
+        }
+    } else {
+        // ---------------- consumers ----------------
+        const int wm = warp % Cfg::WARPS_M, wn = warp / Cfg::WARPS_M;
+        const int lm = lane & 3, ln = lane >> 2;
+        const int tm0 = wm * 32 + lm * 8;  // 8 rows
+        const int tn0 = wn * 32 + ln * 4;  // 4 columns
+        float p0[8][4], p1[8][4], p2[8][4];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                p0[i][j] = 0.0f;
+                p1[i][j] = 0.0f;
+                p2[i][j] = 0.0f;
+            }
+        }
+        bool ok = true;
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const int s = kt % STAGES;
+            if (!mbar_wait(&full[s], (kt / STAGES) & 1, p.status)) {
+                ok = false;
+                break;
+            }
+            const float* a = sA + s * Cfg::A_STAGE + tm0;
+            const float* b = sB + s * Cfg::B_STAGE + tn0;
+#pragma unroll
+            for (int kk = 0; kk < BK; ++kk) {
+                float x[8], y[4];
+                // plane 0: Ar * Br
+                *reinterpret_cast<float4*>(&x[0]) = *reinterpret_cast<const float4*>(a + kk * BM);
+                *reinterpret_cast<float4*>(&x[4]) = *reinterpret_cast<const float4*>(a + kk * BM + 4);
+                *reinterpret_cast<float4*>(&y[0]) = *reinterpret_cast<const float4*>(b + kk * BN);
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) p0[i][j] = __fmaf_rn(x[i], y[j], p0[i][j]);
+                // plane 1: Ai * Bi
+                *reinterpret_cast<float4*>(&x[0]) = *reinterpret_cast<const float4*>(a + (BK + kk) * BM);
+                *reinterpret_cast<float4*>(&x[4]) = *reinterpret_cast<const float4*>(a + (BK + kk) * BM + 4);
+                *reinterpret_cast<float4*>(&y[0]) = *reinterpret_cast<const float4*>(b + (BK + kk) * BN);
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) p1[i][j] = __fmaf_rn(x[i], y[j], p1[i][j]);
+                // plane 2: (Ar+Ai) * (Br+Bi)
+                *reinterpret_cast<float4*>(&x[0]) = *reinterpret_cast<const float4*>(a + (2 * BK + kk) * BM);
+                *reinterpret_cast<float4*>(&x[4]) = *reinterpret_cast<const float4*>(a + (2 * BK + kk) * BM + 4);
+                *reinterpret_cast<float4*>(&y[0]) = *reinterpret_cast<const float4*>(b + (2 * BK + kk) * BN);
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) p2[i][j] = __fmaf_rn(x[i], y[j], p2[i][j]);
+            }
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&empty[s]);
+            }
+        }
+        if (ok) {
+            const int row0 = m0 + tm0, col0 = n0 + tn0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int col = col0 + j;
+                if (col >= p.n) {
+                    continue;
+                }
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int row = row0 + i;
+                    if (row >= p.m) {
+                        continue;
+                    }
+                    const float re = __fsub_rn(p0[i][j], p1[i][j]);
+                    const float im = __fsub_rn(__fsub_rn(p2[i][j], p0[i][j]), p1[i][j]);
+                    if (p.parts == 1) {
+                        float2* cp = p.C + (size_t)col * p.ldc + row;
+                        *cp = epilogue_value(re, im, p.epi, cp);
+                    } else {
+                        const size_t o = (size_t)col * p.ppitch + row;
+                        p.partial[(size_t)(2 * part) * p.pplane + o] = re;
+                        p.partial[(size_t)(2 * part + 1) * p.pplane + o] = im;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();  // no CTA retires while its copies may still land
+}
+
+// Sum of the partition partials in increasing partition order, then alpha/beta.
+__global__ void merge_kernel(int m, int n, int parts, const float* __restrict__ partial, int ppitch, size_t pplane,
+                             EpiParams e, float2* C, int ldc)
+{
+    const size_t total = (size_t)m * n;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int col = (int)(idx / m), row = (int)(idx - (size_t)col * m);
+        const size_t o = (size_t)col * ppitch + row;
+        float re = partial[o], im = partial[pplane + o];
+        for (int q = 1; q < parts; ++q) {
+            re = __fadd_rn(re, partial[(size_t)(2 * q) * pplane + o]);
+            im = __fadd_rn(im, partial[(size_t)(2 * q + 1) * pplane + o]);
+        }
+        float2* cp = C + (size_t)col * ldc + row;
+        *cp = epilogue_value(re, im, e, cp);
+    }
+}
+
+// k == 0 or alpha == 0: C = beta*C (beta == 0: C = 0 without reading C).
+__global__ void beta_scale_kernel(int m, int n, float br, float bi, float2* C, int ldc)
+{
+    const size_t total = (size_t)m * n;
+    const bool zero = br == 0.0f && bi == 0.0f;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int col = (int)(idx / m), row = (int)(idx - (size_t)col * m);
+        float2* cp = C + (size_t)col * ldc + row;
+        if (zero) {
+            *cp = make_float2(0.0f, 0.0f);
+        } else {
+            const float2 c = *cp;
+            *cp = make_float2(__fsub_rn(__fmul_rn(br, c.x), __fmul_rn(bi, c.y)),
+                              __fadd_rn(__fmul_rn(br, c.y), __fmul_rn(bi, c.x)));
+        }
+    }
+}
+
+int elementwise_blocks(size_t total)
+{
+    const size_t blocks = (total + 255) / 256;
+    return (int)(blocks < 148 * 16 ? (blocks == 0 ? 1 : blocks) : 148 * 16);
+}
+
+template <int BM, int BN>
+cudaError_t launch_fp32_tile(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
+{
+    using Cfg = Fp32Cfg<BM, BN>;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    CUtensorMap ta, tb;
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.m, (uint64_t)pr.k, 3};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_a * 4, (uint64_t)plan.plane_a_elems * 4};
+        const uint32_t box[3] = {BM, Cfg::BK, 3};
+        if (!encode_tensor_map(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, dims, strides, box,
+                               CU_TENSOR_MAP_SWIZZLE_NONE, w + plan.planes_a_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.n, (uint64_t)pr.k, 3};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_b * 4, (uint64_t)plan.plane_b_elems * 4};
+        const uint32_t box[3] = {BN, Cfg::BK, 3};
+        if (!encode_tensor_map(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, dims, strides, box,
+                               CU_TENSOR_MAP_SWIZZLE_NONE, w + plan.planes_b_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    Fp32Params p{};
+    p.m = pr.m;
+    p.n = pr.n;
+    p.k = pr.k;
+    p.span = plan.span;
+    p.parts = plan.parts;
+    p.tiles_m = ceil_div(pr.m, BM);
+    p.tiles_n = ceil_div(pr.n, BN);
+    p.epi = EpiParams{pr.ar, pr.ai, pr.br, pr.bi, plan.unit ? 1 : 0, plan.beta_zero ? 1 : 0};
+    p.C = static_cast<float2*>(pr.C);
+    p.ldc = pr.ldc;
+    p.partial = reinterpret_cast<float*>(w + plan.partial_off);
+    p.ppitch = plan.partial_pitch;
+    p.pplane = plan.partial_plane_elems;
+    p.status = status;
+    auto kernel = gemm3m_fp32_kernel<BM, BN>;
+    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    const dim3 grid((unsigned)(p.tiles_m * p.tiles_n), (unsigned)plan.parts);
+    kernel<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(ta, tb, p);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_gemm_fp32(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
+{
+    if (plan.tile_m == 128 && plan.tile_n == 64) {
+        return launch_fp32_tile<128, 64>(stream, pr, plan, ws, status);
+    }
+    if (plan.tile_m == 64 && plan.tile_n == 64) {
+        return launch_fp32_tile<64, 64>(stream, pr, plan, ws, status);
+    }
+    if (plan.tile_m == 64 && plan.tile_n == 32) {
+        return launch_fp32_tile<64, 32>(stream, pr, plan, ws, status);
+    }
+    return launch_fp32_tile<32, 32>(stream, pr, plan, ws, status);
+}
+
+cudaError_t launch_merge(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws)
+{
+    const float* partial = reinterpret_cast<const float*>(static_cast<uint8_t*>(ws) + plan.partial_off);
+    const EpiParams e{pr.ar, pr.ai, pr.br, pr.bi, plan.unit ? 1 : 0, plan.beta_zero ? 1 : 0};
+    merge_kernel<<<elementwise_blocks((size_t)pr.m * pr.n), 256, 0, stream>>>(
+        pr.m, pr.n, plan.parts, partial, plan.partial_pitch, plan.partial_plane_elems, e, static_cast<float2*>(pr.C),
+        pr.ldc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_beta_scale(cudaStream_t stream, int m, int n, float br, float bi, void* C, int ldc)
+{
+    beta_scale_kernel<<<elementwise_blocks((size_t)m * n), 256, 0, stream>>>(m, n, br, bi, static_cast<float2*>(C),
+                                                                             ldc);
+    return cudaGetLastError();
+}
+
+}  // namespace cg3m

@@ -1,0 +1,174 @@
+// pack.cu -- deinterleave / pack kernel (north-star item (a)).
+//
+// Reference: gemm_cgemm_deinterleave_kernel, blas/gemm/arch35/cgemm_kernel.cpp
+// :137-157 and DeinterleaveElement, cgemm_deinterleave_common.h:18-52.  The
+// reference splits interleaved complex A and B into FP32 planes Ar, Ai, Ar+Ai
+// (and the B counterparts) for the standard 3M products, applying the
+// conjugation of op 'C' to the imaginary part, and keeps the stored shape.
+//
+// B200 design: one launch packs both operands (blockIdx.z selects A or B).
+// Unlike the reference, op() is resolved here: each plane is written in the
+// one layout its GEMM consumes, so every GEMM kernel has a single layout.
+//   MN-major (FP32 FFMA GEMM):  A plane [k][pitch] holds op(A)(i,p) at p*pitch+i,
+//                               B plane [k][pitch] holds op(B)(p,j) at p*pitch+j.
+//   K-major  (tensor-core GEMM): A plane [m][pitch] holds op(A)(i,p) at i*pitch+p,
+//                               B plane [n][pitch] holds op(B)(p,j) at j*pitch+p.
+// Each plane element is written once; 32x32 complex tiles are staged through
+// shared memory when the source's contiguous dimension is not the plane's.
+// Components: re, im (conjugated), sum = fl(re + im).  Tensor-core forms split
+// every component into TF32 hi/lo or three BF16 terms after the sum is formed
+// in FP32, so the split never changes the 3M identity.
+#include <cuda_bf16.h>
+
+#include "cg3m_internal.h"
+
+namespace cg3m {
+namespace {
+
+struct PackSide {
+    const float2* src;  // stored matrix, column-major
+    int rows, cols, ld; // stored shape
+    int trans;          // 1: plane rows follow source rows (transpose through smem)
+    float conj;         // -1 for op C / R, else +1
+    void* out;          // plane 0; plane q at out + q*plane_elems elements
+    int pitch;
+    size_t plane_elems;
+};
+
+__device__ __forceinline__ float tf32_rna(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// Writes the planes of one component value v (component c in 0..2).
+template <int FORM>
+__device__ __forceinline__ void put(const PackSide& s, int c, size_t idx, float v)
+{
+    if constexpr (FORM == CG3M_FORM_FP32) {
+        static_cast<float*>(s.out)[c * s.plane_elems + idx] = v;
+    } else if constexpr (FORM == CG3M_FORM_TF32X3) {
+        const float hi = tf32_rna(v);
+        const float lo = tf32_rna(v - hi);
+        float* o = static_cast<float*>(s.out);
+        o[(2 * c) * s.plane_elems + idx] = hi;
+        o[(2 * c + 1) * s.plane_elems + idx] = lo;
+    } else {
+        const __nv_bfloat16 b0 = __float2bfloat16_rn(v);
+        const float r1 = v - __bfloat162float(b0);
+        const __nv_bfloat16 b1 = __float2bfloat16_rn(r1);
+        const float r2 = r1 - __bfloat162float(b1);
+        const __nv_bfloat16 b2 = __float2bfloat16_rn(r2);
+        __nv_bfloat16* o = static_cast<__nv_bfloat16*>(s.out);
+        o[(3 * c) * s.plane_elems + idx] = b0;
+        o[(3 * c + 1) * s.plane_elems + idx] = b1;
+        o[(3 * c + 2) * s.plane_elems + idx] = b2;
+    }
+}
+
+template <int FORM>
+__device__ __forceinline__ void put_all(const PackSide& s, size_t idx, float2 v)
+{
+    const float re = v.x;
+    const float im = v.y * s.conj;
+    put<FORM>(s, 0, idx, re);
+    put<FORM>(s, 1, idx, im);
+    put<FORM>(s, 2, idx, __fadd_rn(re, im));
+}
+
+constexpr int TILE = 32;
+constexpr int ROWS = 8;
+
+template <int FORM>
+__global__ void __launch_bounds__(TILE* ROWS) pack_kernel(PackSide a, PackSide b)
+{
+    __shared__ float2 tile[TILE][TILE + 1];
+    const PackSide& s = blockIdx.z == 0 ? a : b;
+    const int r0 = blockIdx.x * TILE;
+    const int c0 = blockIdx.y * TILE;
+    if (r0 >= s.rows || c0 >= s.cols) {
+        return;
+    }
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    if (!s.trans) {
+        // Plane row = source column, plane column = source row: both contiguous.
+        const int r = r0 + tx;
+        if (r < s.rows) {
+#pragma unroll
+            for (int q = 0; q < TILE / ROWS; ++q) {
+                const int c = c0 + ty + q * ROWS;
+                if (c < s.cols) {
+                    const float2 v = __ldg(&s.src[(size_t)c * s.ld + r]);
+                    put_all<FORM>(s, (size_t)c * s.pitch + r, v);
+                }
+            }
+        }
+        return;
+    }
+    // Plane row = source row, plane column = source column: transpose the tile.
+    {
+        const int r = r0 + tx;
+#pragma unroll
+        for (int q = 0; q < TILE / ROWS; ++q) {
+            const int c = c0 + ty + q * ROWS;
+            if (r < s.rows && c < s.cols) {
+                tile[ty + q * ROWS][tx] = __ldg(&s.src[(size_t)c * s.ld + r]);
+            }
+        }
+    }
+    __syncthreads();
+    const int c = c0 + tx;
+    if (c < s.cols) {
+#pragma unroll
+        for (int q = 0; q < TILE / ROWS; ++q) {
+            const int r = r0 + ty + q * ROWS;
+            if (r < s.rows) {
+                put_all<FORM>(s, (size_t)r * s.pitch + c, tile[tx][ty + q * ROWS]);
+            }
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_pack(cudaStream_t stream, const Problem& p, const Plan& plan, void* ws)
+{
+    const bool kmajor = plan.form != CG3M_FORM_FP32;
+    auto side = [&](bool isA) {
+        PackSide s{};
+        const int op = isA ? p.transa : p.transb;
+        const bool normal = op == CG3M_OP_N || op == CG3M_OP_R;
+        const int opr = isA ? p.m : p.k;  // rows of op(X)
+        const int opc = isA ? p.k : p.n;  // cols of op(X)
+        s.src = static_cast<const float2*>(isA ? p.A : p.B);
+        s.rows = normal ? opr : opc;
+        s.cols = normal ? opc : opr;
+        s.ld = isA ? p.lda : p.ldb;
+        s.conj = (op == CG3M_OP_C || op == CG3M_OP_R) ? -1.0f : 1.0f;
+        // MN-major planes are indexed [k][mn]: A wants source rows on the plane's
+        // columns when op(A) is N (no transpose); B when op(B) is T/C.
+        // K-major planes are indexed [mn][k]: the opposite.
+        const bool plane_cols_are_src_rows = isA ? (normal != kmajor) : (normal == kmajor);
+        s.trans = plane_cols_are_src_rows ? 0 : 1;
+        s.out = static_cast<uint8_t*>(ws) + (isA ? plan.planes_a_off : plan.planes_b_off);
+        s.pitch = isA ? plan.pitch_a : plan.pitch_b;
+        s.plane_elems = isA ? plan.plane_a_elems : plan.plane_b_elems;
+        return s;
+    };
+    const PackSide a = side(true), b = side(false);
+    const int gx = ceil_div(a.rows > b.rows ? a.rows : b.rows, TILE);
+    const int gy = ceil_div(a.cols > b.cols ? a.cols : b.cols, TILE);
+    if (gy > 65535) {
+        return cudaErrorInvalidConfiguration;
+    }
+    const dim3 grid(gx, gy, 2), block(TILE, ROWS);
+    switch (plan.form) {
+        case CG3M_FORM_FP32: pack_kernel<CG3M_FORM_FP32><<<grid, block, 0, stream>>>(a, b); break;
+        case CG3M_FORM_TF32X3: pack_kernel<CG3M_FORM_TF32X3><<<grid, block, 0, stream>>>(a, b); break;
+        default: pack_kernel<CG3M_FORM_BF16X6><<<grid, block, 0, stream>>>(a, b); break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace cg3m

@@ -1,0 +1,233 @@
+// planner.cpp -- argument validation and path / tile / K-split selection.
+//
+// Reference: ValidateCgemmParams and ValidateCgemmPointers
+// (blas/gemm/arch35/cgemm_host.cpp:589-634,687-699), LaunchComplexGemm
+// (:701-730), CalculateCgemmWorkspaceSizes (:228-285) with
+// SelectCgemmAccumulationTile (:130), EstimateCgemmCoreWork (:145),
+// SelectCgemmProductTile (:157), SelectCgemm3mDecomposition (:174) and the
+// rounding gate (:234-238), AllocateCgemmWorkspace (:326-360).
+//
+// The validation order, statuses and quick returns are the reference's.  The
+// tile/K-split policy keeps the reference's structure -- a joint search over
+// output tile x K partitions that minimises the busiest core's work times
+// (span + 16), with a forced deeper split for narrow long-K outputs -- but its
+// capacities are the B200's: the "cores" are SM slots (148 SMs x resident CTAs
+// of the tile), the tiles are this kernel's, and the partition bound scales
+// with how few tiles there are, since a 148-SM part needs far more
+// independent tasks than a 1-4-way split of a handful of tiles provides.
+#include <algorithm>
+#include <cstring>
+#include <limits>
+
+#include "cg3m_internal.h"
+
+namespace cg3m {
+
+static bool is_op(int op, bool allow_conj_only)
+{
+    return op == CG3M_OP_N || op == CG3M_OP_T || op == CG3M_OP_C || (allow_conj_only && op == CG3M_OP_R);
+}
+
+cg3mStatus_t validate(int transa, int transb, int m, int n, int k, const cg3mComplex* alpha, const void* A, int lda,
+                      const void* B, int ldb, const cg3mComplex* beta, const void* C, int ldc, bool allow_conj_only,
+                      int* action)
+{
+    *action = 0;
+    // Enum errors are reported as INVALID_VALUE by the 3m entry (cgemm_host.cpp:713).
+    if (!is_op(transa, allow_conj_only) || !is_op(transb, allow_conj_only)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (m < 0 || n < 0 || k < 0) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    const bool normal_a = transa == CG3M_OP_N || transa == CG3M_OP_R;
+    const bool normal_b = transb == CG3M_OP_N || transb == CG3M_OP_R;
+    if (lda < std::max(1, normal_a ? m : k)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (ldb < std::max(1, normal_b ? k : n)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (ldc < std::max(1, m)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (alpha == nullptr || beta == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (m == 0 || n == 0) {
+        return CG3M_STATUS_SUCCESS;  // quick return after validation (cgemm_host.cpp:715)
+    }
+    const bool alpha_zero = alpha->real == 0.0f && alpha->imag == 0.0f;
+    if (C == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (!alpha_zero && k > 0 && (A == nullptr || B == nullptr)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (k == 0 || alpha_zero) {
+        const bool beta_one = beta->real == 1.0f && beta->imag == 0.0f;
+        *action = beta_one ? 0 : 1;  // cgemm_host.cpp:639
+        return CG3M_STATUS_SUCCESS;
+    }
+    *action = 2;
+    return CG3M_STATUS_SUCCESS;
+}
+
+namespace {
+
+// The rounding-correction kernels (rounding.cu) are wired into the gate below.
+constexpr bool kRoundingImplemented = false;
+
+struct TileChoice {
+    int bm, bn;
+    int slots_per_sm;  // resident CTAs per SM of this tile's kernel
+};
+
+// FP32 FFMA kernel tiles (gemm_fp32.cu) and how many fit on one SM.
+const TileChoice kFp32Tiles[] = {{128, 64, 1}, {64, 64, 2}, {64, 32, 3}, {32, 32, 6}};
+// Tensor-core kernel tile (gemm_tc.cu): 128 x 128, one CTA per SM (TMEM).
+const TileChoice kTcTiles[] = {{128, 128, 1}};
+
+// Busiest-SM work for `tiles` output tiles split into `parts` K partitions
+// (EstimateCgemmCoreWork, cgemm_host.cpp:145-156, with SM slots as cores).
+uint64_t core_work(const TileChoice& t, int m, int n, int parts, int sm_count)
+{
+    const uint64_t tiles = (uint64_t)ceil_div(m, t.bm) * ceil_div(n, t.bn);
+    const uint64_t slots = (uint64_t)sm_count * t.slots_per_sm;
+    const uint64_t waves = (tiles * parts + slots - 1) / slots;
+    // Work per wave: one tile's multiply-adds per K term, scaled by how many of
+    // the SM's slots share its FP32 pipe.
+    const uint64_t rows = std::min(m, t.bm), cols = std::min(n, t.bn);
+    return waves * rows * cols * (uint64_t)t.slots_per_sm;
+}
+
+int k_span(int k, int parts)
+{
+    // kSpan = ceil(ceil(k/16)/parts)*16 (cgemm_host.cpp:274-275).
+    return ceil_div(ceil_div(k, 16), parts) * 16;
+}
+
+}  // namespace
+
+bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* plan)
+{
+    Plan out{};
+    out.action = 2;
+    out.form = opts.form;
+    out.unit = p.ar == 1.0f && p.ai == 0.0f && p.br == 0.0f && p.bi == 0.0f;
+    out.beta_zero = p.br == 0.0f && p.bi == 0.0f;
+    if (sm_count <= 0) {
+        sm_count = 148;
+    }
+    const bool tc = opts.form != CG3M_FORM_FP32;
+
+    // Rounding-correction gate (cgemm_host.cpp:234-238).
+    out.rounding = kRoundingImplemented && opts.rounding == CG3M_ROUNDING_AUTO && out.unit && p.m == p.n && p.n == p.k && p.k >= 2048 &&
+                   p.k <= 4096 && p.lda == p.m && p.ldb == p.m && p.ldc == p.m;
+
+    // ---- tile x K-partition search -------------------------------------------
+    const TileChoice* tiles = tc ? kTcTiles : kFp32Tiles;
+    const int ntiles = tc ? 1 : 4;
+    const uint64_t default_tiles = (uint64_t)ceil_div(p.m, tiles[0].bm) * ceil_div(p.n, tiles[0].bn);
+    TileChoice best_tile = tiles[0];
+    int best_parts = 1;
+    if (opts.k_partitions > 0) {
+        best_parts = std::min(opts.k_partitions, 64);
+    } else if (default_tiles < (uint64_t)sm_count * tiles[0].slots_per_sm && !out.rounding) {
+        // Few tiles: search jointly (SelectCgemm3mDecomposition, :174-200).
+        // Partitions are bounded by what can still fill the machine: at most
+        // 4-way as in the reference when tiles are plentiful, deeper only while
+        // tiles x parts stays within two waves of SM slots and every partition
+        // keeps >= 256 K terms.
+        uint64_t best = std::numeric_limits<uint64_t>::max();
+        for (int t = 0; t < ntiles; ++t) {
+            const uint64_t nt = (uint64_t)ceil_div(p.m, tiles[t].bm) * ceil_div(p.n, tiles[t].bn);
+            const uint64_t slots = (uint64_t)sm_count * tiles[t].slots_per_sm;
+            int max_parts = (int)std::max<uint64_t>(4, (2 * slots) / std::max<uint64_t>(nt, 1));
+            max_parts = std::min(max_parts, 64);
+            for (int parts = 1; parts <= max_parts; ++parts) {
+                const int span = k_span(p.k, parts);
+                if ((parts - 1) * span >= p.k) {
+                    continue;
+                }
+                if (parts > 4 && span < 256) {
+                    continue;
+                }
+                const uint64_t work = core_work(tiles[t], p.m, p.n, parts, sm_count) * (uint64_t)(span + 16);
+                // Charge the partial-output traffic of the merge: 2 planes per part.
+                const uint64_t merge = parts > 1 ? (uint64_t)parts * p.m * p.n / sm_count : 0;
+                if (work + merge < best) {
+                    best = work + merge;
+                    best_tile = tiles[t];
+                    best_parts = parts;
+                }
+            }
+        }
+    }
+    // Narrow long-K outputs force >= 8 partitions (cgemm_host.cpp:269-273).
+    if (opts.k_partitions <= 0 && !tc && p.k >= 1024 && std::min(p.m, p.n) <= 16 && std::max(p.m, p.n) <= 32) {
+        best_parts = std::max(best_parts, 8);
+    }
+    out.tile_m = best_tile.bm;
+    out.tile_n = best_tile.bn;
+    out.parts = best_parts;
+    out.span = k_span(p.k, best_parts);
+    while (out.parts > 1 && (out.parts - 1) * out.span >= p.k) {
+        --out.parts;
+        out.span = k_span(p.k, out.parts);
+    }
+    if (out.parts == 1) {
+        out.span = p.k;
+    }
+
+    // ---- workspace layout -----------------------------------------------------
+    const bool kmajor = tc;
+    int splits = 1;
+    size_t elem = 4;
+    if (opts.form == CG3M_FORM_TF32X3) {
+        splits = 2;
+    } else if (opts.form == CG3M_FORM_BF16X6 || opts.form == CG3M_FORM_BF16X9) {
+        splits = 3;
+        elem = 2;
+    }
+    out.planes = 3 * splits;
+    if (kmajor) {
+        // [mn][k] planes: K padded so every row starts on a 128-byte boundary.
+        const int kp = (int)align_up((size_t)p.k, 128 / elem);
+        out.pitch_a = kp;
+        out.pitch_b = kp;
+        out.plane_a_elems = (size_t)p.m * kp;
+        out.plane_b_elems = (size_t)p.n * kp;
+    } else {
+        out.pitch_a = (int)align_up((size_t)p.m, 32);
+        out.pitch_b = (int)align_up((size_t)p.n, 32);
+        out.plane_a_elems = (size_t)out.pitch_a * p.k;
+        out.plane_b_elems = (size_t)out.pitch_b * p.k;
+    }
+    size_t off = 0;
+    out.planes_a_off = off;
+    off = align_up(off + out.plane_a_elems * elem * out.planes, kRegionAlign);
+    out.planes_b_off = off;
+    off = align_up(off + out.plane_b_elems * elem * out.planes, kRegionAlign);
+    out.partial_pitch = (int)align_up((size_t)p.m, 32);
+    out.partial_plane_elems = (size_t)out.partial_pitch * p.n;
+    out.partial_off = off;
+    if (out.parts > 1) {
+        off = align_up(off + out.partial_plane_elems * 4 * 2 * out.parts, kRegionAlign);
+    }
+    out.round_off = off;
+    if (out.rounding) {
+        // risk plane n^2 floats, energies 2n floats, selected list n^2 u32,
+        // counters: see rounding.cu for the layout.
+        const size_t n = (size_t)p.n;
+        off = align_up(off + n * n * 4, kRegionAlign);
+        off = align_up(off + 2 * n * 4, kRegionAlign);
+        off = align_up(off + n * n * 4, kRegionAlign);
+        off = align_up(off + 4096, kRegionAlign);
+    }
+    out.total = off;
+    *plan = out;
+    return true;
+}
+
+}  // namespace cg3m

@@ -1,0 +1,373 @@
+"""Benchmark of the cgemm3m hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form tf32x3|bf16x6|fp32]
+
+Workload (one step = one cgemm3m call): C <- A*B, complex64, M = N = K = 4096,
+column-major, op N/N, alpha = 1, beta = 0, contiguous; Re(A), Re(B) ~ N(0,1),
+Im ~ N(0,1)*2^e with an integer e in [-8, 8] drawn per column; seeded
+synthetic data (the reference publishes no dataset).  Rounding-correction pass
+per the reference's gate (this shape qualifies).  Metric: c64 TFLOP/s counted
+as 8*M*N*K per call.  Under torchrun every rank runs its own independent
+problem on its own GPU (no data-path collective; weak scaling) and the value is
+the whole job's throughput over the max-over-ranks time.
+
+--impl reference times the reference's CPU algorithm (the oracle restatement of
+reference-BLAS cgemm, scalar C) on all host cores on a bounded column sample of
+the same workload; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "ascend-open-source-contributions_b200")
+for _p in (PKG, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "c64 TFLOP/s (8MNK) at 4096^3: tensor-core 3M vs FP32 3M, same err vs FP64"
+UNIT = "TFLOP/s"
+SIZE = 4096
+SEED_A, SEED_B = 20261203, 20261204
+WORKLOAD = "cgemm3m 4096x4096x4096 complex64 NN alpha=1 beta=0, precision-form data"
+PASSES = {"fp32": 1, "tf32x3": 3, "bf16x6": 6, "bf16x9": 9}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="fp32", choices=["fp32", "tf32x3", "bf16x6", "bf16x9"])
+    ap.add_argument("--size", type=int, default=SIZE)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- peaks
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def pipe_peak(form, sm_count):
+    pk, src = peaks()
+    if form == "fp32":
+        mhz = pk.get("sm_max_mhz", 1965.0)
+        return sm_count * 128 * 2 * mhz * 1e6 / 1e12, f"nominal: {sm_count} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz"
+    if form == "tf32x3":
+        return pk["bf16_tflops"] / 2.0, f"{src} bf16 burst / 2 (dense TF32 = half of dense BF16)"
+    return pk["bf16_tflops"], f"{src} bf16 burst"
+
+
+# ----------------------------------------------------------------------------- data
+
+def host_operands(n):
+    import oracle as O
+
+    a = O.precision_matrix(n, n, SEED_A)
+    b = O.precision_matrix(n, n, SEED_B)
+    return a, b
+
+
+def cpu_sample(cols, n, seed_offset=0):
+    """Reference-order FP32 cgemm (the oracle) on op(A) (n x n) times the first
+    `cols` columns of B: (seconds, flops8)."""
+    import numpy as np
+
+    import oracle as O
+
+    a = O.precision_matrix(n, n, SEED_A)
+    b = O.precision_matrix(n, n, SEED_B)[: n * cols]
+    c = np.zeros(n * cols, np.complex64)
+    t0 = time.perf_counter()
+    O.cgemm("N", "N", n, cols, n, 1 + 0j, a, n, b, n, 0j, c, n)
+    dt = time.perf_counter() - t0
+    return dt, 8.0 * n * cols * n
+
+
+def _cpu_worker(args):
+    cols, n = args
+    return cpu_sample(cols, n)
+
+
+# ----------------------------------------------------------------------------- reference arm
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    n = args.size
+    cores = os.cpu_count() or 1
+    cols_per_worker = 8
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(cores) as pool:
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_worker, [(cols_per_worker, n)] * cores)
+            dt = time.perf_counter() - t0
+            if step >= args.warmup:
+                times.append(dt)
+    flops = 8.0 * n * n * cols_per_worker * cores
+    t = statistics.median(times)
+    value = flops / t / 1e12
+    sample = f"{n}x{cols_per_worker * cores}x{n} column sample of the {n}^3 workload per step ({cores} processes)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "form": "reference-BLAS order FP32 (oracle port)", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- our arm
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    # CPU baseline sample first: its processes must not fork after CUDA is up.
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        dt, fl = cpu_sample(96, args.size)
+        cpu = {"value": fl / dt / 1e12, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{args.size}x96x{args.size} column sample, reference-BLAS order FP32 (oracle), 1 thread"}
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    import cg3m
+
+    n = args.size
+    a_host, b_host = host_operands(n)
+    A = torch.from_numpy(a_host).to(dev)
+    B = torch.from_numpy(b_host).to(dev)
+    C = torch.zeros(n * n, dtype=torch.complex64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    h = cg3m.Handle(stream=stream.cuda_stream)
+    sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+
+    def call(form):
+        return h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form)
+
+    def timed(form, steps, warmup):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                info = call(form)
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                info = call(form)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, info
+
+    def stage_times(form, steps):
+        """Per-kernel durations from events the library records between its launches."""
+        info = call(form)
+        nk = info["kernels"]
+        per = []
+        with torch.cuda.stream(stream):
+            for _ in range(steps):
+                evs = [torch.cuda.Event(enable_timing=True) for _ in range(nk + 1)]
+                h.set_stage_events(evs)
+                call(form)
+                per.append(evs)
+            h.set_stage_events([])
+            torch.cuda.synchronize()
+        out = []
+        for i in range(nk):
+            out.append(sum(e[i].elapsed_time(e[i + 1]) for e in per) / steps)
+        return out, info
+
+    flops8 = 8.0 * n ** 3
+    flops6 = 6.0 * n ** 3
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms, info = timed(args.form, args.steps, args.warmup)
+    clocks = sampler.stop()
+    value = world * flops8 / (ms * 1e-3) / 1e12
+
+    # per-kernel times of the same call (instrumented, separate loop)
+    stages, _ = stage_times(args.form, max(3, min(args.steps, 10)))
+    gemm_ms = stages[1]
+    p = PASSES[args.form]
+    peak, peak_src = pipe_peak(args.form, sm_count)
+    achieved = flops6 * p / (gemm_ms * 1e-3) / 1e12
+    roofline = {"bound": "tensor" if args.form != "fp32" else "fp32-pipe", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "kernel": "gemm",
+                "peak_source": peak_src, "flops_per_launch": flops6 * p, "kernel_ms": gemm_ms,
+                "stage_ms": stages}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            roofline["traffic"] = json.load(f).get(f"gemm_{args.form}_{n}")
+
+    # end to end through the public API with host buffers
+    a_pin = torch.from_numpy(a_host).pin_memory()
+    b_pin = torch.from_numpy(b_host).pin_memory()
+    c_pin = torch.empty(n * n, dtype=torch.complex64).pin_memory()
+    with torch.cuda.stream(stream):
+        for it in range(args.warmup + args.steps):
+            if it == args.warmup:
+                torch.cuda.synchronize()
+                if world > 1:
+                    dist.barrier()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            A.copy_(a_pin, non_blocking=True)
+            B.copy_(b_pin, non_blocking=True)
+            call(args.form)
+            c_pin.copy_(C, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * flops8 / (e2e_ms * 1e-3) / 1e12, "unit": UNIT, "h2d_bytes_per_step": 2 * n * n * 8,
+           "d2h_bytes_per_step": n * n * 8, "ms_per_step": e2e_ms}
+
+    # accuracy vs FP64 (device reference), for this form and the plain FP32 form
+    errors = {}
+    plain = None
+    out64 = torch.empty(n * n, dtype=torch.complex128, device=dev)
+    with torch.cuda.stream(stream):
+        h.zgemm_reference("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, out64)
+        for form in sorted({args.form, "fp32"}):
+            call(form)
+            errors[form] = h.error_report(n, n, C, n, out64)
+    if args.form != "fp32":
+        pms, _ = timed("fp32", max(3, args.steps // 2), 2)
+        plain = {"value": world * flops8 / (pms * 1e-3) / 1e12, "ms_per_step": pms}
+    del out64
+    status = h.device_status()
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.form == "fp32" else args.form, "data": "synthetic",
+        "config": {"workload": WORKLOAD, "form": args.form, "m": n, "n": n, "k": n, "transa": "N", "transb": "N",
+                   "alpha": [1, 0], "beta": [0, 0], "parallelism": f"replica x{world} (independent problems)",
+                   "l2": "inputs exceed L2: A, B, C 384 MiB plus packed planes; no flush needed",
+                   "plan": {k_: info[k_] for k_ in ("tile_m", "tile_n", "k_partitions", "k_span", "rounding",
+                                                    "kernels", "workspace_bytes")}},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": args.steps * info["kernels"],
+        "clocks": clocks,
+        "errors_vs_fp64": errors,
+        "plain_fp32": plain,
+        "tc_over_plain": (value / plain["value"]) if plain else None,
+        "device_status": status,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,231 @@
+/*
+ * cg3m.h -- C ABI of the B200-native cgemm3m (complex64 GEMM with three real
+ * matrix products), a drop-in for the reference's aclblasCgemm3m surface.
+ *
+ * All entry points are extern "C", take plain pointers and sizes, and return a
+ * cg3mStatus_t.  Citations name the reference interface each entry replaces
+ * (paths inside the reference's ops-blas/ tree).
+ *
+ * Conventions shared with the reference:
+ *   - A, B, C are column-major complex64 arrays in device memory owned by the
+ *     caller; alpha and beta are host pointers read during the call.
+ *   - Work is enqueued asynchronously on the handle's stream; no entry point
+ *     synchronizes except cg3mDestroy and cg3mGetDeviceStatus.
+ *   - One handle must not be used by several host threads at once (its
+ *     workspace is shared by every call made through it).
+ *   - C must not alias A or B.  Padding rows [m, ldc) of C are never written.
+ */
+#ifndef CG3M_H_
+#define CG3M_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference names are kept (cann_ops_blas.h:40-57 uses
+ * ACLBLAS_STATUS_*); their numeric values are not shipped with the reference,
+ * so these values are this library's own. */
+typedef enum {
+    CG3M_STATUS_SUCCESS = 0,
+    CG3M_STATUS_HANDLE_IS_NULLPTR = 1,
+    CG3M_STATUS_INVALID_VALUE = 2,
+    CG3M_STATUS_INVALID_ENUM = 3,
+    CG3M_STATUS_ALLOC_FAILED = 4,
+    CG3M_STATUS_INTERNAL_ERROR = 5,
+    CG3M_STATUS_EXECUTION_FAILED = 6,
+    CG3M_STATUS_NOT_SUPPORTED = 7
+} cg3mStatus_t;
+
+/* op() codes: N, T, C as in the reference (numeric values follow cuBLAS).
+ * CG3M_OP_R (conjugate without transpose) is accepted only by the extended
+ * entry points; the drop-in cg3mCgemm3m rejects it like any other bad enum. */
+typedef enum { CG3M_OP_N = 0, CG3M_OP_T = 1, CG3M_OP_C = 2, CG3M_OP_R = 3 } cg3mOperation_t;
+
+/* Arithmetic form of the three real products.
+ *   FP32     -- strict FP32 FFMA on the CUDA cores; the drop-in form;
+ *               bitwise deterministic run to run.
+ *   TF32X3   -- tensor-core 3xTF32: each operand split x = hi + lo (both TF32),
+ *               products hi*hi + hi*lo + lo*hi accumulated in FP32 (TMEM).
+ *   BF16X6   -- tensor-core split-BF16: x = b0 + b1 + b2, the six products
+ *               with b_i*b_j, i+j <= 2, accumulated in FP32 (TMEM).
+ *   BF16X9   -- as BF16X6 with all nine products.
+ * In every form the sums Ar+Ai, Br+Bi are formed in FP32 before splitting and
+ * the epilogue (Re = P0-P1, Im = P2-P0-P1, alpha, beta) runs in FP32. */
+typedef enum { CG3M_FORM_FP32 = 0, CG3M_FORM_TF32X3 = 1, CG3M_FORM_BF16X6 = 2, CG3M_FORM_BF16X9 = 3 } cg3mForm_t;
+
+/* Rounding-correction pass (reference: gemm_cgemm3m_rounding_do,
+ * blas/gemm/arch35/cgemm3m_rounding_kernel.cpp:474-497, gated at
+ * cgemm_host.cpp:234-238).
+ *   AUTO -- as the reference: only for m==n==k in [2048,4096], lda==ldb==ldc==m,
+ *           alpha==1, beta==0.  Flagged outputs are recomputed in FP32 fixed
+ *           order (FP32 form) or in FP64 (tensor-core forms).
+ *   OFF  -- never. */
+typedef enum { CG3M_ROUNDING_AUTO = 0, CG3M_ROUNDING_OFF = 1 } cg3mRounding_t;
+
+typedef struct {
+    float real;
+    float imag;
+} cg3mComplex; /* layout of aclblasComplex {float real; float imag;} (cgemm_host.cpp:719) */
+
+typedef struct cg3mContext* cg3mHandle_t;
+
+/* Options of the extended entry points (zero-initialised = drop-in behaviour). */
+typedef struct {
+    cg3mForm_t form;
+    cg3mRounding_t rounding;
+    int k_partitions; /* 0 = planner's choice; else force this many K partitions (1..64) */
+    int reserved[5];
+} cg3mOptions;
+
+/* What one call did (filled when a non-null pointer is passed). */
+typedef struct {
+    int path;            /* 0 quick return, 1 beta-scale only, 2 fused GEMM, 3 split-K GEMM + merge */
+    int form;            /* cg3mForm_t actually used */
+    int tile_m, tile_n;  /* output tile of the GEMM kernel */
+    int k_partitions;    /* K partitions (1 = none) */
+    int k_span;          /* K terms per partition */
+    int rounding;        /* 1 if the rounding-correction pass was enqueued */
+    int kernels;         /* kernels launched by this call */
+    size_t workspace_bytes;
+} cg3mCallInfo;
+
+/* ---- handle / stream / workspace (cann_ops_blas.h:31-98) ------------------ */
+
+/* aclblasCreate (cann_ops_blas.h:46).  *handle must be NULL on entry
+ * (non-null -> INVALID_VALUE).  Device resources (the 32 MiB default workspace
+ * and a status word) are bound to the current device on the first call that
+ * launches work, so a handle can be created and validated without a GPU. */
+cg3mStatus_t cg3mCreate(cg3mHandle_t* handle);
+
+/* aclblasDestroy (cann_ops_blas.h:59): synchronizes the handle's stream, frees
+ * the default workspace; a user workspace is forgotten, never freed. */
+cg3mStatus_t cg3mDestroy(cg3mHandle_t handle);
+
+/* aclblasSetStream (cann_ops_blas.h:71): NULL selects the legacy default
+ * stream; switching streams returns the handle to its default workspace. */
+cg3mStatus_t cg3mSetStream(cg3mHandle_t handle, void* stream);
+
+/* aclblasGetStream (cann_ops_blas.h:81). */
+cg3mStatus_t cg3mGetStream(cg3mHandle_t handle, void** stream);
+
+/* aclblasSetWorkspace (cann_ops_blas.h:98): borrows device memory (grow-only:
+ * kept only when larger than the current user workspace). */
+cg3mStatus_t cg3mSetWorkspace(cg3mHandle_t handle, void* workspace, size_t workspace_bytes);
+
+/* aclblasGetVersion (cann_ops_blas.h:108): MAJOR*10000 + MINOR*100 + PATCH. */
+cg3mStatus_t cg3mGetVersion(cg3mHandle_t handle, int* version);
+
+/* ---- the drop-in (cann_ops_blas.h:497-500; cgemm3m_host.cpp:17-23) ------- */
+
+/* C <- alpha*op(A)*op(B) + beta*C with three real products, strict FP32.
+ * Validation order and statuses follow LaunchComplexGemm/ValidateCgemmParams
+ * (cgemm_host.cpp:589-634,687-730): null handle -> HANDLE_IS_NULLPTR; bad
+ * transa/transb, negative m/n/k, lda/ldb/ldc too small, null alpha/beta ->
+ * INVALID_VALUE; then m==0||n==0 -> SUCCESS with nothing touched; then C must
+ * be non-null and, unless alpha==0, A and B must be non-null when k>0.
+ * k==0 or alpha==0 scales C by beta only (beta==1: nothing; beta==0: C=0
+ * without reading C).  beta==0 never reads C. */
+cg3mStatus_t cg3mCgemm3m(cg3mHandle_t handle, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                         const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B, int ldb,
+                         const cg3mComplex* beta, cg3mComplex* C, int ldc);
+
+/* ---- extensions (no single reference counterpart) ------------------------ */
+
+/* The drop-in with a form / rounding / K-split choice and an optional report of
+ * what ran.  Also accepts CG3M_OP_R.  opts == NULL means the drop-in. */
+cg3mStatus_t cg3mCgemm3mEx(cg3mHandle_t handle, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                           const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B, int ldb,
+                           const cg3mComplex* beta, cg3mComplex* C, int ldc, const cg3mOptions* opts,
+                           cg3mCallInfo* info);
+
+/* aclblasCgemm3mStridedBatched (cann_ops_blas.h:652; semantics
+ * blas/gemm/README.md:809-907): C_i = alpha*op(A_i)*op(B_i) + beta*C_i with
+ * X_i = X + i*strideX (complex elements, zero or negative allowed); when
+ * output batches overlap (strideC==0 included) they are updated in batch
+ * order.  Statuses as the reference's strided API: bad enum -> INVALID_ENUM. */
+cg3mStatus_t cg3mCgemm3mStridedBatched(cg3mHandle_t handle, cg3mOperation_t transa, cg3mOperation_t transb, int m,
+                                       int n, int k, const cg3mComplex* alpha, const cg3mComplex* A, int lda,
+                                       int64_t strideA, const cg3mComplex* B, int ldb, int64_t strideB,
+                                       const cg3mComplex* beta, cg3mComplex* C, int ldc, int64_t strideC,
+                                       int batch_count);
+
+/* One problem of a heterogeneous batch (device pointers, host scalars). */
+typedef struct {
+    int transa, transb;
+    int m, n, k;
+    cg3mComplex alpha, beta;
+    const cg3mComplex* A;
+    int lda;
+    const cg3mComplex* B;
+    int ldb;
+    cg3mComplex* C;
+    int ldc;
+} cg3mProblem;
+
+/* Opaque plan of a heterogeneous batch: tile/K-split tables chosen by the
+ * autotuner, a device-side task list, and (optionally) a captured CUDA graph
+ * holding the one persistent launch. */
+typedef struct cg3mBatchPlan* cg3mBatchPlan_t;
+
+/* Plans `count` problems (validated individually like cg3mCgemm3m; the first
+ * invalid one returns its status and its index in *bad_index).  `tune` != 0
+ * times the candidate tile/split tables on the device before choosing. */
+cg3mStatus_t cg3mBatchPlanCreate(cg3mHandle_t handle, const cg3mProblem* problems, int count, int tune,
+                                 cg3mBatchPlan_t* plan, int* bad_index);
+/* Enqueues the whole batch on the handle's stream as one persistent launch
+ * (replaying the captured graph when use_graph != 0). */
+cg3mStatus_t cg3mBatchPlanExecute(cg3mHandle_t handle, cg3mBatchPlan_t plan, int use_graph);
+cg3mStatus_t cg3mBatchPlanDestroy(cg3mBatchPlan_t plan);
+/* Tile shape / K split the plan chose per problem (arrays of `count`). */
+cg3mStatus_t cg3mBatchPlanDescribe(cg3mBatchPlan_t plan, int* tile_m, int* tile_n, int* k_partitions);
+
+/* Instrumentation: when count > 0, every later call made through the handle
+ * records events[0] on its stream before its first kernel and events[i] after
+ * its i-th kernel (i < count); no work is skipped or reordered.  The events are
+ * cudaEvent_t values owned by the caller.  count == 0 turns it off. */
+cg3mStatus_t cg3mSetStageEvents(cg3mHandle_t handle, void* const* events, int count);
+
+/* Device status word of the handle: synchronizes the stream, returns and
+ * clears the error bits kernels set when a bounded wait gave up
+ * (1: pipeline wait timed out).  0 means no device-side error. */
+cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t handle, int* flags);
+
+/* ---- host-only helpers (no device access; usable without a GPU) ---------- */
+
+/* Runs exactly the validation of cg3mCgemm3m (including the quick-return
+ * classification) without touching the device: returns the status the call
+ * would return, and in *action 0 = nothing to do, 1 = beta scale only,
+ * 2 = product path. */
+cg3mStatus_t cg3mValidate(cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                          const cg3mComplex* alpha, const void* A, int lda, const void* B, int ldb,
+                          const cg3mComplex* beta, const void* C, int ldc, int allow_conj_only, int* action);
+
+/* The planner's decision for a problem on a device with `sm_count` SMs
+ * (fills info; no device access). */
+cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k, const cg3mComplex* alpha,
+                      int lda, int ldb, const cg3mComplex* beta, int ldc, const cg3mOptions* opts, int sm_count,
+                      cg3mCallInfo* info);
+
+/* ---- diagnostics (not a compute path of cgemm3m) ------------------------- */
+
+/* FP64 reference product on the device, for error reports only:
+ * out64[j*m+i] = alpha*op(A)*op(B) (+ beta*C) in complex128, m x n packed. */
+cg3mStatus_t cg3mZgemmReference(cg3mHandle_t handle, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n,
+                                int k, const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B,
+                                int ldb, const cg3mComplex* beta, const cg3mComplex* C, int ldc, void* out64);
+
+/* Normwise and componentwise errors of C (ldc) against out64 (m x n packed),
+ * computed on the device.  report[0] = ||C-C64||_F/||C64||_F,
+ * report[1] = max |dRe|/|Re64|, report[2] = max |dIm|/|Im64|,
+ * report[3] = max |dRe|, report[4] = max |dIm| (host array of 5 doubles). */
+cg3mStatus_t cg3mErrorReport(cg3mHandle_t handle, int m, int n, const cg3mComplex* C, int ldc, const void* out64,
+                             double* report);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CG3M_H_ */

@@ -1,0 +1,195 @@
+"""CPU tests of the C-ABI library: it loads, exports every declared symbol, and
+its host logic (validation order, statuses, quick returns, handle semantics,
+planner) behaves as the reference's -- all without touching a GPU.
+
+Reference: ValidateCgemmParams / LaunchComplexGemm (ops-blas/blas/gemm/arch35/
+cgemm_host.cpp:589-634,687-730), handle API (ops-blas/include/cann_ops_blas.h
+:31-110), ED contract rows of cgemm3m_test.csv (TC_ED_306-337).
+"""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for h in ("cg3m.h", "cg3m_aclblas.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b((?:cg3m|aclblas)[A-Za-z0-9_]+)\s*\(", text)
+    return sorted(set(n for n in names if not n.endswith("_t")))
+
+
+def test_library_exports_every_declared_symbol(cg3m):
+    names = declared_functions()
+    assert "cg3mCgemm3m" in names and "aclblasCgemm3m" in names
+    for n in names:
+        assert hasattr(cg3m.lib, n), n
+    out = subprocess.run(["nm", "-D", "--defined-only", cg3m.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(line.split()[-1] for line in out.splitlines() if line.strip())
+    for n in names:
+        assert n in exported, n
+    # nothing but the C ABI is exported
+    assert all(s.startswith(("cg3m", "aclblas")) for s in exported if not s.startswith("_"))
+
+
+def test_no_cpu_fallback_symbols(cg3m):
+    """The library links no BLAS and carries no host GEMM: only CUDA kernels compute."""
+    out = subprocess.run(["nm", "-D", "--undefined-only", cg3m.LIB_PATH], capture_output=True, text=True).stdout
+    assert "gemm_" not in out and "cblas" not in out
+
+
+# ---------------------------------------------------------------- handle API
+
+def test_handle_lifecycle(cg3m):
+    L = cg3m.lib
+    h = ctypes.c_void_p()
+    assert L.cg3mCreate(None) == cg3m.HANDLE_IS_NULLPTR
+    assert L.cg3mCreate(ctypes.byref(h)) == cg3m.SUCCESS and h.value
+    again = ctypes.c_void_p(h.value)
+    assert L.cg3mCreate(ctypes.byref(again)) == cg3m.INVALID_VALUE  # *handle must be null
+    s = ctypes.c_void_p()
+    assert L.cg3mGetStream(h, ctypes.byref(s)) == cg3m.SUCCESS and not s.value
+    assert L.cg3mGetStream(h, None) == cg3m.INVALID_VALUE
+    assert L.cg3mSetStream(None, None) == cg3m.HANDLE_IS_NULLPTR
+    assert L.cg3mSetWorkspace(h, None, 16) == cg3m.INVALID_VALUE
+    assert L.cg3mSetWorkspace(h, ctypes.c_void_p(0x1000), 0) == cg3m.INVALID_VALUE
+    v = ctypes.c_int()
+    assert L.cg3mGetVersion(None, ctypes.byref(v)) == cg3m.SUCCESS and v.value == 10000
+    assert L.cg3mGetVersion(h, None) == cg3m.INVALID_VALUE
+    flags = ctypes.c_int(7)
+    assert L.cg3mGetDeviceStatus(h, ctypes.byref(flags)) == cg3m.SUCCESS and flags.value == 0
+    assert L.cg3mDestroy(h) == cg3m.SUCCESS
+    assert L.cg3mDestroy(None) == cg3m.HANDLE_IS_NULLPTR
+
+
+def test_aclblas_names_bind_the_same_handles(cg3m):
+    L = cg3m.lib
+    h = ctypes.c_void_p()
+    assert L.aclblasCreate(ctypes.byref(h)) == cg3m.SUCCESS
+    one, zero = cg3m.cx(1), cg3m.cx(0)
+    assert L.aclblasCgemm3m(None, 0, 0, 0, 0, 0, ctypes.byref(one), None, 1, None, 1, ctypes.byref(zero), None,
+                            1) == cg3m.HANDLE_IS_NULLPTR
+    assert L.aclblasCgemm3m(h, 0, 0, 0, 3, 2, ctypes.byref(one), None, 1, None, 2, ctypes.byref(zero), None,
+                            1) == cg3m.SUCCESS
+    assert L.aclblasDestroy(h) == cg3m.SUCCESS
+
+
+# ---------------------------------------------------------------- validation
+
+def _case_args(c, cg3m):
+    ta = 999 if c["transa"] == 999 else cg3m.OP[c["transa"]]
+    tb = 999 if c["transb"] == 999 else cg3m.OP[c["transb"]]
+    alpha = None if c["alpha"][0] is None else complex(c["alpha"][0], c["alpha"][1])
+    beta = None if c["beta"][0] is None else complex(c["beta"][0], c["beta"][1])
+    dummy = ctypes.c_void_p(0x1000)  # never dereferenced on these paths
+    A = None if c["a_fill"] == "NULLPTR" else dummy
+    B = None if c["b_fill"] == "NULLPTR" else dummy
+    C = None if c["c_fill"] == "NULLPTR" else dummy
+    return ta, tb, alpha, beta, A, B, C
+
+
+def test_contract_rows_statuses(cg3m, cases):
+    """Every row of the reference's case table gets the expected status from the
+    host-only validator, and the ED rows also from the drop-in entry itself
+    when the call needs no device."""
+    h = cg3m.Handle()
+    checked = 0
+    for c in cases["cases"]:
+        ta, tb, alpha, beta, A, B, C = _case_args(c, cg3m)
+        st, action = cg3m.validate(ta, tb, c["m"], c["n"], c["k"], alpha, A, c["lda"], B, c["ldb"], beta, C, c["ldc"])
+        expect = getattr(cg3m, c["expect"])
+        assert st == expect, c["name"]
+        if st != cg3m.SUCCESS or action == 0:
+            al = ctypes.byref(cg3m.cx(alpha)) if alpha is not None else None
+            be = ctypes.byref(cg3m.cx(beta)) if beta is not None else None
+            got = cg3m.lib.cg3mCgemm3m(h.h, ta, tb, c["m"], c["n"], c["k"], al, A, c["lda"], B, c["ldb"], be, C,
+                                       c["ldc"])
+            assert got == expect, c["name"]
+            checked += 1
+    assert checked >= 16
+
+
+@pytest.mark.parametrize("m,n,k,beta,action", [
+    (0, 16, 16, 0, 0), (16, 0, 16, 0, 0), (16, 16, 0, 1, 0), (16, 16, 0, 0, 1), (16, 16, 0, 0.5, 1),
+    (16, 16, 16, 0, 2),
+])
+def test_quick_return_classification(cg3m, m, n, k, beta, action):
+    dummy = ctypes.c_void_p(0x1000)
+    st, act = cg3m.validate("N", "N", m, n, k, 1.0, dummy, max(1, m), dummy, max(1, k), beta, dummy, max(1, m))
+    assert st == cg3m.SUCCESS and act == action
+
+
+def test_alpha_zero_allows_null_inputs(cg3m):
+    dummy = ctypes.c_void_p(0x1000)
+    st, act = cg3m.validate("N", "N", 3, 2, 7, 0.0, None, 3, None, 7, complex(0.5, -0.25), dummy, 5)
+    assert st == cg3m.SUCCESS and act == 1
+    st, _ = cg3m.validate("N", "N", 3, 2, 7, 1.0, None, 3, None, 7, 0.0, dummy, 5)
+    assert st == cg3m.INVALID_VALUE
+
+
+def test_conj_only_op_is_extension_only(cg3m):
+    dummy = ctypes.c_void_p(0x1000)
+    st, _ = cg3m.validate("R", "N", 4, 4, 4, 1.0, dummy, 4, dummy, 4, 0.0, dummy, 4)
+    assert st == cg3m.INVALID_VALUE
+    st, act = cg3m.validate("R", "R", 4, 4, 4, 1.0, dummy, 4, dummy, 4, 0.0, dummy, 4, allow_conj_only=True)
+    assert st == cg3m.SUCCESS and act == 2
+
+
+def test_validation_order(cg3m):
+    """Enum before dims before ld before scalars before pointers (cgemm_host.cpp:589-634)."""
+    dummy = ctypes.c_void_p(0x1000)
+    assert cg3m.validate(999, "N", -1, 4, 4, None, None, 0, None, 0, None, None, 0)[0] == cg3m.INVALID_VALUE
+    # bad ld is an error even for an empty output
+    assert cg3m.validate("N", "N", 0, 4, 4, 1.0, None, 0, None, 4, 0.0, None, 1)[0] == cg3m.INVALID_VALUE
+    # null scalars are errors even for an empty output
+    assert cg3m.validate("N", "N", 0, 4, 4, None, None, 1, None, 4, 0.0, None, 1)[0] == cg3m.INVALID_VALUE
+    # an empty output needs no matrices at all
+    assert cg3m.validate("N", "N", 0, 4, 4, 1.0, None, 1, None, 4, 0.0, None, 1) == (cg3m.SUCCESS, 0)
+    assert cg3m.validate("T", "N", 4, 4, 8, 1.0, dummy, 7, dummy, 8, 0.0, dummy, 4)[0] == cg3m.INVALID_VALUE
+
+
+def test_strided_batched_statuses_without_device(cg3m):
+    L = cg3m.lib
+    h = cg3m.Handle()
+    one, zero = ctypes.byref(cg3m.cx(1)), ctypes.byref(cg3m.cx(0))
+    assert L.cg3mCgemm3mStridedBatched(None, 0, 0, 2, 2, 2, one, None, 2, 4, None, 2, 4, zero, None, 2, 4,
+                                       1) == cg3m.HANDLE_IS_NULLPTR
+    assert L.cg3mCgemm3mStridedBatched(h.h, 999, 0, 2, 2, 2, one, None, 2, 4, None, 2, 4, zero, None, 2, 4,
+                                       1) == cg3m.INVALID_ENUM
+    assert L.cg3mCgemm3mStridedBatched(h.h, 0, 0, 2, 2, 2, one, None, 2, 4, None, 2, 4, zero, None, 2, 4,
+                                       -1) == cg3m.INVALID_VALUE
+    assert L.cg3mCgemm3mStridedBatched(h.h, 0, 0, 2, 2, 2, one, None, 2, 4, None, 2, 4, zero, None, 2, 4,
+                                       0) == cg3m.SUCCESS
+    assert L.cg3mCgemm3mStridedBatched(h.h, 0, 0, 2, 2, 2, None, None, 2, 4, None, 2, 4, zero, None, 2, 4,
+                                       0) == cg3m.INVALID_VALUE
+
+
+# ---------------------------------------------------------------- planner
+
+def test_planner_large_square_is_single_partition(cg3m):
+    p = cg3m.plan("N", "N", 4096, 4096, 4096)
+    assert p["k_partitions"] == 1 and (p["tile_m"], p["tile_n"]) == (128, 64)
+    assert p["k_span"] == 4096
+
+
+def test_planner_long_k_few_tiles_splits_k(cg3m):
+    p = cg3m.plan("N", "N", 128, 128, 65536, alpha=complex(0.7, 0.3), beta=complex(-1, 0.5))
+    assert p["k_partitions"] > 1
+    assert p["k_span"] % 16 == 0
+    assert (p["k_partitions"] - 1) * p["k_span"] < 65536 <= p["k_partitions"] * p["k_span"]
+
+
+def test_planner_narrow_long_k_forces_eight_parts(cg3m):
+    p = cg3m.plan("N", "N", 8, 16, 4096)
+    assert p["k_partitions"] >= 8
+
+
+def test_planner_forced_partitions(cg3m):
+    p = cg3m.plan("N", "N", 300, 200, 1000, k_partitions=3)
+    assert p["k_partitions"] == 3 and p["k_span"] == 336

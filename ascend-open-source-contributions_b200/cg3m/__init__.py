@@ -160,6 +160,9 @@ class Handle:
 
     def set_stage_events(self, events):
         """Record the given torch.cuda.Event objects around each kernel of later calls."""
+        for e in events:
+            if not e.cuda_event:  # torch creates the CUDA event lazily on first record
+                e.record()
         arr = (ctypes.c_void_p * max(1, len(events)))(*[ctypes.c_void_p(e.cuda_event) for e in events])
         _check(_lib.cg3mSetStageEvents(self.h, arr, len(events)), "cg3mSetStageEvents")
 

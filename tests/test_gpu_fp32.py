@@ -217,10 +217,10 @@ def test_runs_on_caller_stream(cg3m, oracle, cuda):
     a, lda, b, ldb, c, ldc = _operands(oracle, "N", "T", m, n, k, 1, "UNIFORM_1", 5)
     with torch.cuda.stream(s):
         A, B, C = to_dev(a, torch, cuda), to_dev(b, torch, cuda), to_dev(c, torch, cuda)
-        h.cgemm3m("N", "T", m, n, k, 1.0, A, lda, B, ldb, 0.5, C, ldc)
+        info = h.cgemm3m("N", "T", m, n, k, 1.0, A, lda, B, ldb, 0.5, C, ldc)
     s.synchronize()
     model = c.copy()
-    oracle.cgemm3m_fp32_model("N", "T", m, n, k, 1.0, a, lda, b, ldb, 0.5, model, ldc, span=k)
+    oracle.cgemm3m_fp32_model("N", "T", m, n, k, 1.0, a, lda, b, ldb, 0.5, model, ldc, span=info["k_span"])
     assert same_bits(to_host(C), model)
     assert h.device_status() == 0
 

@@ -82,6 +82,7 @@ SIGNATURES = {
     "cg3mBatchPlanDestroy": [_P],
     "cg3mBatchPlanDescribe": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "cg3mGetDeviceStatus": [_P, ctypes.POINTER(_I)],
+    "cg3mCgemm3mNoAlloc": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I],
     "cg3mSetStageEvents": [_P, ctypes.POINTER(_P), _I],
     "cg3mValidate": [_I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I, _I, ctypes.POINTER(_I)],
     "cg3mPlan": [_I, _I, _I, _I, _I, _CP, _I, _I, _CP, _I, ctypes.POINTER(cg3mOptions), _I,

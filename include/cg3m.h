@@ -193,6 +193,24 @@ cg3mStatus_t cg3mSetStageEvents(cg3mHandle_t handle, void* const* events, int co
  * (1: pipeline wait timed out).  0 means no device-side error. */
 cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t handle, int* flags);
 
+/* ---- allocation-free variant (no counterpart in the reference) ----------- */
+
+/* The drop-in FP32 product (same arguments, validation, statuses and result
+ * bits as cg3mCgemm3m) for callers that must not call cudaMalloc/cudaFree at
+ * this point -- e.g. under a caching allocator that owns the device heap, or
+ * in a loop where an allocation would synchronize the device.  It allocates
+ * nothing: its scratch is one fixed 32 MiB device array inside the library
+ * (held by every GPU that loads it, until exit).  It takes a CUDA stream
+ * instead of a handle.  The first call on each device resolves the array's
+ * device address (cudaGetSymbolAddress), so make that first call before any
+ * stream capture.  Problems whose scratch would exceed the array return
+ * CG3M_STATUS_INVALID_VALUE with C untouched.  Every call shares the one
+ * array, so calls whose work overlaps on the GPU (other streams, other host
+ * threads) race on it; serialise them. */
+cg3mStatus_t cg3mCgemm3mNoAlloc(void* stream, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                                const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B,
+                                int ldb, const cg3mComplex* beta, cg3mComplex* C, int ldc);
+
 /* ---- host-only helpers (no device access; usable without a GPU) ---------- */
 
 /* Runs exactly the validation of cg3mCgemm3m (including the quick-return

@@ -42,7 +42,7 @@ class cg3mComplex(ctypes.Structure):
 
 class cg3mOptions(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int), ("rounding", ctypes.c_int), ("k_partitions", ctypes.c_int),
-                ("reserved", ctypes.c_int * 5)]
+                ("tc_segment", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
 class cg3mCallInfo(ctypes.Structure):
@@ -173,7 +173,7 @@ class Handle:
         return f.value
 
     def cgemm3m(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, form="fp32", rounding="auto",
-                k_partitions=0, raw=False):
+                k_partitions=0, raw=False, tc_segment=0):
         """C <- alpha*op(A)*op(B) + beta*C on device buffers; returns the call info.
 
         ``raw=True`` calls the drop-in cg3mCgemm3m (FP32 form only) and returns
@@ -183,7 +183,7 @@ class Handle:
             return _lib.cg3mCgemm3m(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda, ptr(B),
                                     ldb, ctypes.byref(be), ptr(C), ldc)
         opts = cg3mOptions(FORM[form] if isinstance(form, str) else form,
-                           ROUNDING[rounding] if isinstance(rounding, str) else rounding, k_partitions)
+                           ROUNDING[rounding] if isinstance(rounding, str) else rounding, k_partitions, tc_segment)
         info = cg3mCallInfo()
         st = _lib.cg3mCgemm3mEx(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda, ptr(B), ldb,
                                 ctypes.byref(be), ptr(C), ldc, ctypes.byref(opts), ctypes.byref(info))

@@ -103,6 +103,10 @@ cg3mStatus_t to_status(cudaError_t e)
     if (e == cudaSuccess) {
         return CG3M_STATUS_SUCCESS;
     }
+    if (log_enabled()) {
+        std::fprintf(stderr, "{\"cg3m\":\"cuda error\",\"code\":%d,\"what\":\"%s\"}\n", (int)e,
+                     cudaGetErrorString(e));
+    }
     if (e == cudaErrorMemoryAllocation) {
         return CG3M_STATUS_ALLOC_FAILED;
     }

@@ -41,6 +41,7 @@ struct Plan {
     bool unit = false;       // alpha == 1, beta == 0
     bool beta_zero = false;
     bool rounding = false;
+    int tc_segment = 0;      // K terms per TMEM accumulation segment (tensor-core forms)
     // workspace layout (byte offsets from the workspace base)
     size_t planes_a_off = 0, planes_b_off = 0, partial_off = 0, round_off = 0, total = 0;
     int pitch_a = 0, pitch_b = 0;  // elements per plane row

@@ -21,30 +21,10 @@
 // split into partitions (grid.y); each writes (Re_p, Im_p) planes and a merge
 // kernel sums them in partition order before alpha/beta.
 #include "cg3m_internal.h"
+#include "epilogue.cuh"
 #include "ptx.cuh"
 
 namespace cg3m {
-
-struct EpiParams {
-    float ar, ai, br, bi;
-    int unit, beta_zero;
-};
-
-// alpha*(re,im) [+ beta*c]; one rounding per operation (no contraction).
-__device__ __forceinline__ float2 epilogue_value(float re, float im, const EpiParams& e, const float2* cptr)
-{
-    if (e.unit) {
-        return make_float2(re, im);
-    }
-    float xr = __fsub_rn(__fmul_rn(e.ar, re), __fmul_rn(e.ai, im));
-    float xi = __fadd_rn(__fmul_rn(e.ar, im), __fmul_rn(e.ai, re));
-    if (!e.beta_zero) {
-        const float2 c = *cptr;
-        xr = __fadd_rn(xr, __fsub_rn(__fmul_rn(e.br, c.x), __fmul_rn(e.bi, c.y)));
-        xi = __fadd_rn(xi, __fadd_rn(__fmul_rn(e.br, c.y), __fmul_rn(e.bi, c.x)));
-    }
-    return make_float2(xr, xi);
-}
 
 namespace {
 

@@ -1,11 +1,450 @@
-// gemm_tc.cu -- tensor-core (tcgen05) forms of the three real products.
+// gemm_tc.cu -- the three real products on the 5th-generation tensor cores
+// (tcgen05) with FP32 accumulators in TMEM: the precision forms 3xTF32 and
+// split-BF16 (x6 / x9 products).
+//
+// Reference counterpart: gemm_cgemm_fused_kernel (blas/gemm/arch35/
+// cgemm_compute_kernel.cpp:879-896), whose Cube unit keeps the three products
+// of one output tile in three L0C accumulators (:602) and whose vector cores
+// merge them and write C (:748-760).  The reference computes them in FP32 with
+// HF32 disabled (:356); here the products run on tensor cores with each FP32
+// operand split into TF32 or BF16 terms, which restores FP32-level products
+// while the accumulation stays FP32.
+//
+// B200 design.  One CTA per 128 x 128 output tile (cta_group::1, M = N = 128),
+// 320 threads:
+//   warp 0       TMA producer: per K-block and component c in {re, im, sum}
+//                one 3-D box for A (all split planes of c) and one for B,
+//                128 B rows with the 128-byte swizzle, into a STAGES ring;
+//   warp 1       allocates 512 TMEM columns; one lane issues every
+//                tcgen05.mma: accumulator c (columns [128c, 128c+128)) +=
+//                sum over split pairs (i, j) of A_c,i * B_c,j, smallest terms
+//                first; tcgen05.commit releases each ring slot;
+//   warps 2-9    epilogue: after every 128-term K segment, tcgen05.ld of
+//                P0, P1, P2 (one TMEM lane = one output row, 64 columns per
+//                warp), Re_s = P0-P1, Im_s = (P2-P0)-P1 added to running Re,
+//                Im in registers with round-to-nearest FP32; at the end
+//                alpha/beta and a column-major C store in which each warp
+//                instruction writes 32 consecutive rows of one column.
+// Why segments: the tensor core aligns the products of one MMA and the
+// accumulator to the largest exponent and truncates, a bias that grows
+// linearly with the number of MMAs chained into one accumulator.  Over a
+// 4096-term K (1536 chained MMAs for 3xTF32) that costs ~15x the error of a
+// round-to-nearest FP32 chain; restarting the accumulators every 128 terms
+// (the reference's own segment length for this shape, cgemm_host.cpp:257-260)
+// and merging segments on the CUDA cores brings the error below plain FP32.
+// Operand planes are K-major ([row][k]) and split by the pack kernel, so the
+// sums Ar+Ai and Br+Bi are formed in FP32 before any rounding to TF32/BF16.
+// Every wait on an mbarrier is bounded; a timeout sets the status word, the
+// CTA stops issuing work, waits for what is in flight, frees TMEM and exits.
+#include <cuda_bf16.h>
+
 #include "cg3m_internal.h"
+#include "epilogue.cuh"
+#include "ptx.cuh"
 
 namespace cg3m {
+namespace {
 
-cudaError_t launch_gemm_tc(cudaStream_t, const Problem&, const Plan&, void*, int*)
+constexpr int TILE = 128;                     // M and N of the MMA and the output tile
+constexpr int ROW_BYTES = 128;                // one K-block row of one plane
+constexpr int PLANE_TILE = TILE * ROW_BYTES;  // 16 KB: one plane, 128 rows
+constexpr int TMEM_COLS = 512;                // 3 x 128 accumulator columns, rounded to a power of two
+constexpr int kSegment = 64;                  // default K terms accumulated in TMEM before an FP32 merge
+constexpr int kEpilogueWarps = 8;
+constexpr int kThreads = (2 + kEpilogueWarps) * 32;
+// 10 warps land 3/3/2/2 on the SM's four sub-partitions, whose register files
+// hold 16K registers each: 3 warps x 32 threads x 168 registers is the most
+// that still launches, so the epilogue keeps 2 x 64 running sums per thread
+// and streams TMEM through 8-column pieces.
+
+template <int FORM>
+struct TcCfg;
+
+template <>
+struct TcCfg<CG3M_FORM_TF32X3> {
+    static constexpr int S = 2;        // split planes per component (hi, lo)
+    static constexpr int BK = 32;      // K elements per 128-byte row
+    static constexpr int NPAIRS = 3;   // lo*hi, hi*lo, hi*hi
+    static constexpr int STAGES = 3;
+    static constexpr uint32_t FMT = 2; // TF32
+    __device__ static int2 pair(int q) { return q == 0 ? make_int2(1, 0) : q == 1 ? make_int2(0, 1) : make_int2(0, 0); }
+};
+
+template <>
+struct TcCfg<CG3M_FORM_BF16X6> {
+    static constexpr int S = 3;        // b0, b1, b2
+    static constexpr int BK = 64;
+    static constexpr int NPAIRS = 6;   // b_i*b_j with i+j <= 2, smallest first
+    static constexpr int STAGES = 2;
+    static constexpr uint32_t FMT = 1; // BF16
+    __device__ static int2 pair(int q)
+    {
+        switch (q) {
+            case 0: return make_int2(2, 0);
+            case 1: return make_int2(1, 1);
+            case 2: return make_int2(0, 2);
+            case 3: return make_int2(1, 0);
+            case 4: return make_int2(0, 1);
+            default: return make_int2(0, 0);
+        }
+    }
+};
+
+template <>
+struct TcCfg<CG3M_FORM_BF16X9> {
+    static constexpr int S = 3;
+    static constexpr int BK = 64;
+    static constexpr int NPAIRS = 9;   // all b_i*b_j, smallest first
+    static constexpr int STAGES = 2;
+    static constexpr uint32_t FMT = 1;
+    __device__ static int2 pair(int q)
+    {
+        switch (q) {
+            case 0: return make_int2(2, 2);
+            case 1: return make_int2(2, 1);
+            case 2: return make_int2(1, 2);
+            case 3: return make_int2(2, 0);
+            case 4: return make_int2(1, 1);
+            case 5: return make_int2(0, 2);
+            case 6: return make_int2(1, 0);
+            case 7: return make_int2(0, 1);
+            default: return make_int2(0, 0);
+        }
+    }
+};
+
+struct TcParams {
+    int m, n, k;
+    int span, parts;
+    int tiles_m, tiles_n;
+    EpiParams epi;
+    float2* C;
+    int ldc;
+    float* partial;
+    int ppitch;
+    size_t pplane;
+    int* status;
+    int seg_blocks;  // K-blocks per accumulation segment
+};
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), leading offset unused (1), descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
 {
-    return cudaErrorNotSupported;
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(1024 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// Instruction descriptor: FP32 accumulate, A/B format, both K-major, N = M = 128.
+template <uint32_t FMT>
+__device__ __forceinline__ uint32_t instr_desc()
+{
+    return (1u << 4) | (FMT << 7) | (FMT << 10) | ((uint32_t)(TILE >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
+}
+
+template <int FORM>
+__global__ void __launch_bounds__(kThreads, 1)
+    gemm3m_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     const TcParams p)
+{
+    using Cfg = TcCfg<FORM>;
+    constexpr int STAGES = Cfg::STAGES;
+    constexpr int STAGE_BYTES = 2 * Cfg::S * PLANE_TILE;
+    constexpr int KSTEPS = ROW_BYTES / 32;  // 32 bytes of K per MMA: 8 tf32 or 16 bf16
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(ring + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* acc_full = empty + STAGES;  // [3] MMA -> epilogue: product c of the segment is in TMEM
+    uint64_t* acc_free = acc_full + 3;    // [3] epilogue -> MMA: accumulator c may be overwritten
+    uint64_t* mma_done = acc_free + 3;    // every MMA of the CTA has completed
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+
+    constexpr int GM = 8;
+    const int pid = blockIdx.x;
+    const int in_group = GM * p.tiles_n;
+    const int first_m = (pid / in_group) * GM;
+    const int gsz = min(p.tiles_m - first_m, GM);
+    const int tm = first_m + (pid % in_group) % gsz;
+    const int tn = (pid % in_group) / gsz;
+    const int m0 = tm * TILE, n0 = tn * TILE;
+    const int part = blockIdx.y;
+    const int kbeg = part * p.span;
+    const int kend = min(p.k, kbeg + p.span);
+    const int kblocks = (kend - kbeg + Cfg::BK - 1) / Cfg::BK;
+    const int seg_blocks = p.seg_blocks;
+    const int segments = (kblocks + seg_blocks - 1) / seg_blocks;
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int c = 0; c < 3; ++c) {
+            mbar_init(&acc_full[c], 1);
+            mbar_init(&acc_free[c], kEpilogueWarps);
+        }
+        mbar_init(mma_done, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    // Work order (producer and MMA issuer walk it identically): for each K
+    // segment, for each component c in {re, im, sum}, for each K-block of the
+    // segment, one ring stage holding component c's split planes of A and B.
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            tma_prefetch_desc(&tmA);
+            tma_prefetch_desc(&tmB);
+            int it = 0;
+            bool stop = false;
+            for (int seg = 0; seg < segments && !stop; ++seg) {
+                const int kb0 = seg * seg_blocks, kb1 = min(kblocks, kb0 + seg_blocks);
+                for (int c = 0; c < 3 && !stop; ++c) {
+                    for (int kb = kb0; kb < kb1; ++kb, ++it) {
+                        const int s = it % STAGES;
+                        if ((it >= STAGES && !mbar_wait(&empty[s], ((it / STAGES) - 1) & 1, p.status)) ||
+                            *abort_flag) {
+                            *abort_flag = 1;
+                            stop = true;
+                            break;
+                        }
+                        uint8_t* st = ring + s * STAGE_BYTES;
+                        mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+                        tma_load_3d(st, &tmA, &full[s], kbeg + kb * Cfg::BK, m0, c * Cfg::S);
+                        tma_load_3d(st + Cfg::S * PLANE_TILE, &tmB, &full[s], kbeg + kb * Cfg::BK, n0, c * Cfg::S);
+                    }
+                }
+            }
+            for (int j = it > STAGES ? it - STAGES : 0; j < it; ++j) {
+                mbar_wait(&full[j % STAGES], (j / STAGES) & 1, p.status);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc<Cfg::FMT>();
+            int it = 0;
+            bool stop = false;
+            for (int seg = 0; seg < segments && !stop; ++seg) {
+                const int kb0 = seg * seg_blocks, kb1 = min(kblocks, kb0 + seg_blocks);
+                for (int c = 0; c < 3 && !stop; ++c) {
+                    if (seg > 0) {
+                        if (!mbar_wait(&acc_free[c], (seg - 1) & 1, p.status)) {
+                            *abort_flag = 1;
+                            stop = true;
+                            break;
+                        }
+                        tc_fence_after();
+                    }
+                    const uint32_t d = tmem + (uint32_t)(c * TILE);
+                    for (int kb = kb0; kb < kb1; ++kb, ++it) {
+                        const int s = it % STAGES;
+                        if (!mbar_wait(&full[s], (it / STAGES) & 1, p.status)) {
+                            *abort_flag = 1;
+                            stop = true;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t a_base = smem_u32(ring + s * STAGE_BYTES);
+                        const uint32_t b_base = a_base + Cfg::S * PLANE_TILE;
+#pragma unroll
+                        for (int kk = 0; kk < KSTEPS; ++kk) {
+#pragma unroll
+                            for (int q = 0; q < Cfg::NPAIRS; ++q) {
+                                const int2 ij = Cfg::pair(q);
+                                const uint64_t ad = sw128_desc(a_base + ij.x * PLANE_TILE + kk * 32);
+                                const uint64_t bd = sw128_desc(b_base + ij.y * PLANE_TILE + kk * 32);
+                                const uint32_t acc = (kb > kb0 || kk > 0 || q > 0) ? 1u : 0u;
+                                if constexpr (Cfg::FMT == 2) {
+                                    umma_tf32(d, ad, bd, idesc, acc);
+                                } else {
+                                    umma_f16(d, ad, bd, idesc, acc);
+                                }
+                            }
+                        }
+                        umma_commit(&empty[s]);
+                    }
+                    if (!stop && c > 0) {
+                        // Fires when every MMA issued so far has completed: after c == 1
+                        // both P0 and P1 of the segment are final, after c == 2 all three.
+                        umma_commit(&acc_full[c]);
+                    }
+                }
+            }
+            umma_commit(mma_done);
+            mbar_wait(mma_done, 0, p.status);  // nothing may still write TMEM when it is freed
+        }
+    } else {
+        // ---------------- epilogue warps 2..9 ----------------
+        // TMEM lane quadrant = warp % 4; warps 2-5 take columns 0-63, warps 6-9
+        // columns 64-127 of every accumulator and of the spare block (cols 384+).
+        const int quad = warp & 3;
+        const int half = (warp - 2) >> 2;
+        const int row = m0 + quad * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * 64);
+        const uint32_t spare = lane_addr + (uint32_t)(3 * TILE);
+        float re[64], im[64];
+        bool go = true;
+        for (int seg = 0; seg < segments && go; ++seg) {
+            // P0 and P1 complete: Re_s = P0 - P1 joins the running sum; P0 + P1
+            // parks in the spare columns so both accumulators can be reused.
+            bool ready = mbar_wait(&acc_full[1], seg & 1, p.status);
+            tc_fence_after();
+            go = __all_sync(0xffffffffu, ready && !*abort_flag);
+            if (!go) {
+                break;
+            }
+#pragma unroll
+            for (int cb = 0; cb < 64; cb += 8) {
+                float v0[8], v1[8];
+                tmem_ld8x2(lane_addr + (uint32_t)cb, lane_addr + (uint32_t)(TILE + cb), v0, v1);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const float rs = __fsub_rn(v0[j], v1[j]);
+                    v1[j] = __fadd_rn(v0[j], v1[j]);
+                    re[cb + j] = seg == 0 ? rs : __fadd_rn(re[cb + j], rs);
+                }
+                tmem_st8(spare + (uint32_t)cb, v1);
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&acc_free[0]);
+                mbar_arrive(&acc_free[1]);
+            }
+            // P2 complete: Im_s = P2 - (P0 + P1).
+            ready = mbar_wait(&acc_full[2], seg & 1, p.status);
+            tc_fence_after();
+            go = __all_sync(0xffffffffu, ready && !*abort_flag);
+            if (!go) {
+                break;
+            }
+#pragma unroll
+            for (int cb = 0; cb < 64; cb += 8) {
+                float v2[8], u[8];
+                tmem_ld8x2(lane_addr + (uint32_t)(2 * TILE + cb), spare + (uint32_t)cb, v2, u);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const float is = __fsub_rn(v2[j], u[j]);
+                    im[cb + j] = seg == 0 ? is : __fadd_rn(im[cb + j], is);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&acc_free[2]);
+            }
+        }
+        if (go && row < p.m) {
+#pragma unroll
+            for (int j = 0; j < 64; ++j) {
+                const int col = n0 + half * 64 + j;
+                if (col < p.n) {
+                    if (p.parts == 1) {
+                        float2* cp = p.C + (size_t)col * p.ldc + row;
+                        *cp = epilogue_value(re[j], im[j], p.epi, cp);
+                    } else {
+                        const size_t o = (size_t)col * p.ppitch + row;
+                        p.partial[(size_t)(2 * part) * p.pplane + o] = re[j];
+                        p.partial[(size_t)(2 * part + 1) * p.pplane + o] = im[j];
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+template <int FORM>
+cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
+{
+    using Cfg = TcCfg<FORM>;
+    const bool bf16 = Cfg::FMT == 1;
+    const size_t elem = bf16 ? 2 : 4;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    CUtensorMap ta, tb;
+    const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.m, (uint64_t)(3 * Cfg::S)};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_a * elem, (uint64_t)plan.plane_a_elems * elem};
+        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)TILE, (uint32_t)Cfg::S};
+        if (!encode_tensor_map(&ta, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_a_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.n, (uint64_t)(3 * Cfg::S)};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_b * elem, (uint64_t)plan.plane_b_elems * elem};
+        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)TILE, (uint32_t)Cfg::S};
+        if (!encode_tensor_map(&tb, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_b_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    TcParams p{};
+    p.m = pr.m;
+    p.n = pr.n;
+    p.k = pr.k;
+    p.span = plan.span;
+    p.parts = plan.parts;
+    p.tiles_m = ceil_div(pr.m, TILE);
+    p.tiles_n = ceil_div(pr.n, TILE);
+    p.epi = EpiParams{pr.ar, pr.ai, pr.br, pr.bi, plan.unit ? 1 : 0, plan.beta_zero ? 1 : 0};
+    p.C = static_cast<float2*>(pr.C);
+    p.ldc = pr.ldc;
+    p.partial = reinterpret_cast<float*>(w + plan.partial_off);
+    p.ppitch = plan.partial_pitch;
+    p.pplane = plan.partial_plane_elems;
+    p.status = status;
+    p.seg_blocks = plan.tc_segment > 0 ? (plan.tc_segment + Cfg::BK - 1) / Cfg::BK : kSegment / Cfg::BK;
+    if (p.seg_blocks < 1) {
+        p.seg_blocks = 1;
+    }
+    const size_t smem = (size_t)Cfg::STAGES * 2 * Cfg::S * PLANE_TILE + 1024 + 256;
+    auto kernel = gemm3m_tc_kernel<FORM>;
+    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    const dim3 grid((unsigned)(p.tiles_m * p.tiles_n), (unsigned)plan.parts);
+    kernel<<<grid, kThreads, smem, stream>>>(ta, tb, p);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_gemm_tc(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
+{
+    switch (plan.form) {
+        case CG3M_FORM_TF32X3: return launch_form<CG3M_FORM_TF32X3>(stream, pr, plan, ws, status);
+        case CG3M_FORM_BF16X6: return launch_form<CG3M_FORM_BF16X6>(stream, pr, plan, ws, status);
+        case CG3M_FORM_BF16X9: return launch_form<CG3M_FORM_BF16X9>(stream, pr, plan, ws, status);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace cg3m

@@ -101,10 +101,13 @@ uint64_t core_work(const TileChoice& t, int m, int n, int parts, int sm_count)
     return waves * rows * cols * (uint64_t)t.slots_per_sm;
 }
 
-int k_span(int k, int parts)
+// kSpan = ceil(ceil(k/g)/parts)*g (cgemm_host.cpp:274-275 with g = 16).  The
+// granule g is the GEMM kernel's K-tile so that only the last partition has a
+// ragged tail: 16 for the FP32 kernel, 64 elements (one 128-byte row of the
+// widest split plane) for the tensor-core kernel.
+int k_span(int k, int parts, int g = 16)
 {
-    // kSpan = ceil(ceil(k/16)/parts)*16 (cgemm_host.cpp:274-275).
-    return ceil_div(ceil_div(k, 16), parts) * 16;
+    return ceil_div(ceil_div(k, g), parts) * g;
 }
 
 }  // namespace
@@ -115,6 +118,7 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     out.action = 2;
     out.form = opts.form;
     out.unit = p.ar == 1.0f && p.ai == 0.0f && p.br == 0.0f && p.bi == 0.0f;
+    out.tc_segment = opts.tc_segment;
     out.beta_zero = p.br == 0.0f && p.bi == 0.0f;
     if (sm_count <= 0) {
         sm_count = 148;
@@ -127,6 +131,7 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
 
     // ---- tile x K-partition search -------------------------------------------
     const TileChoice* tiles = tc ? kTcTiles : kFp32Tiles;
+    const int granule = tc ? 64 : 16;
     const int ntiles = tc ? 1 : 4;
     const uint64_t default_tiles = (uint64_t)ceil_div(p.m, tiles[0].bm) * ceil_div(p.n, tiles[0].bn);
     TileChoice best_tile = tiles[0];
@@ -146,7 +151,7 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
             int max_parts = (int)std::max<uint64_t>(4, (2 * slots) / std::max<uint64_t>(nt, 1));
             max_parts = std::min(max_parts, 64);
             for (int parts = 1; parts <= max_parts; ++parts) {
-                const int span = k_span(p.k, parts);
+                const int span = k_span(p.k, parts, granule);
                 if ((parts - 1) * span >= p.k) {
                     continue;
                 }
@@ -171,10 +176,10 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     out.tile_m = best_tile.bm;
     out.tile_n = best_tile.bn;
     out.parts = best_parts;
-    out.span = k_span(p.k, best_parts);
+    out.span = k_span(p.k, best_parts, granule);
     while (out.parts > 1 && (out.parts - 1) * out.span >= p.k) {
         --out.parts;
-        out.span = k_span(p.k, out.parts);
+        out.span = k_span(p.k, out.parts, granule);
     }
     if (out.parts == 1) {
         out.span = p.k;

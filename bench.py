@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="fp32", choices=["fp32", "tf32x3", "bf16x6", "bf16x9"])
     ap.add_argument("--size", type=int, default=SIZE)
+    ap.add_argument("--tc-segment", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -237,7 +238,7 @@ def main():
     sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
 
     def call(form):
-        return h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form)
+        return h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, tc_segment=args.tc_segment)
 
     def timed(form, steps, warmup):
         with torch.cuda.stream(stream):

@@ -77,7 +77,9 @@ typedef struct {
     cg3mForm_t form;
     cg3mRounding_t rounding;
     int k_partitions; /* 0 = planner's choice; else force this many K partitions (1..64) */
-    int reserved[5];
+    int tc_segment;   /* tensor-core forms: K terms accumulated in TMEM before each round-to-nearest
+                         FP32 merge (0 = default 64; rounded up to the kernel's K-block of 32 or 64) */
+    int reserved[4];
 } cg3mOptions;
 
 /* What one call did (filled when a non-null pointer is passed). */

@@ -1,0 +1,138 @@
+"""GPU parity of the tensor-core precision forms (3xTF32, split-BF16 x6/x9).
+
+The tensor-core accumulation order inside an MMA is the hardware's, so these
+forms are checked against FP64 rather than bit for bit: the reference accuracy
+criterion (cgemm3m_verify.h:22-84) against the FP64 result rounded to FP32, a
+normwise-error bound, run-to-run bitwise determinism, and the north-star bar --
+normwise error vs FP64 no worse than the plain FP32 3M form on the same inputs.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import run, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+FORMS = ["tf32x3", "bf16x6", "bf16x9"]
+OPS = ["N", "T", "C"]
+
+
+@pytest.fixture(scope="module")
+def h(cg3m, cuda):
+    return cg3m.Handle()
+
+
+def _operands(oracle, ta, tb, m, n, k, pad, fill, seed):
+    ar, ac = oracle.stored_shape(ta, m, k)
+    br, bc = oracle.stored_shape(tb, k, n)
+    lda, ldb, ldc = ar + pad, br + pad, m + pad
+    a = oracle.make_matrix(ar, ac, lda, fill, seed)
+    b = oracle.make_matrix(br, bc, ldb, fill, seed + 1)
+    c = oracle.make_matrix(m, n, ldc, fill, seed + 2)
+    return a, lda, b, ldb, c, ldc
+
+
+def _check(oracle, out, c, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, ldc, bound):
+    z = oracle.zgemm_numpy(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
+    golden = c.copy()
+    golden.reshape(n, ldc)[:, :m] = z.T.astype(np.complex64)
+    ok, re, im, pad = oracle.verify_cgemm3m(out, golden, c, m, n, ldc)
+    assert ok, (re.__dict__, im.__dict__, pad)
+    err = oracle.error_report(oracle.unpack(out, ldc, m, n), z)
+    assert err["normwise"] < bound, err
+    return err
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_tc_single_tile(cg3m, oracle, cuda, h, form):
+    import torch
+
+    m = n = 128
+    k = 64
+    a, lda, b, ldb, c, ldc = _operands(oracle, "N", "N", m, n, k, 0, "UNIFORM_1", 1)
+    out, info = run(cg3m, h, torch, cuda, "N", "N", m, n, k, 1.0, a, lda, b, ldb, 0.0, c, ldc, form=form)
+    assert info["form"] == cg3m.FORM[form]
+    _check(oracle, out, c, "N", "N", m, n, k, 1.0, a, lda, b, ldb, 0.0, ldc, 1e-6)
+    assert h.device_status() == 0
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("shape", [(1, 1, 1), (7, 5, 3), (130, 129, 70), (257, 300, 1000), (64, 200, 65)])
+@pytest.mark.parametrize("ops", [("N", "N"), ("T", "C"), ("C", "T")])
+def test_tc_edges(cg3m, oracle, cuda, h, form, shape, ops):
+    import torch
+
+    m, n, k = shape
+    ta, tb = ops
+    alpha, beta = complex(0.7, 0.3), complex(-1.0, 0.5)
+    a, lda, b, ldb, c, ldc = _operands(oracle, ta, tb, m, n, k, 3, "UNIFORM_1", m + n + k)
+    out, _ = run(cg3m, h, torch, cuda, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form)
+    again, _ = run(cg3m, h, torch, cuda, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form)
+    assert out.tobytes() == again.tobytes()
+    _check(oracle, out, c, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("ta", OPS)
+@pytest.mark.parametrize("tb", OPS)
+def test_tc_nine_ops_padded(cg3m, oracle, cuda, h, form, ta, tb):
+    import torch
+
+    m, n, k = 1000, 777, 3001
+    alpha, beta = complex(0.7, 0.3), complex(-1.0, 0.5)
+    a, lda, b, ldb, c, ldc = _operands(oracle, ta, tb, m, n, k, 13, "UNIFORM_1", 9000 + 3 * OPS.index(ta) +
+                                       OPS.index(tb))
+    out, _ = run(cg3m, h, torch, cuda, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form)
+    _check(oracle, out, c, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("parts", [2, 3])
+def test_tc_forced_partitions(cg3m, oracle, cuda, h, form, parts):
+    import torch
+
+    m, n, k = 200, 150, 1000
+    alpha, beta = complex(0.3, -1.25), complex(0.5, 0.5)
+    a, lda, b, ldb, c, ldc = _operands(oracle, "T", "N", m, n, k, 2, "RANDOM_NORM_5_5", 77)
+    out, info = run(cg3m, h, torch, cuda, "T", "N", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form,
+                    k_partitions=parts)
+    assert info["k_partitions"] == parts and info["k_span"] % 64 == 0
+    _check(oracle, out, c, "T", "N", m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_tc_long_k(cg3m, oracle, cuda, h, form):
+    import torch
+
+    m = n = 128
+    k = 65536
+    alpha, beta = complex(0.7, 0.3), complex(-1.0, 0.5)
+    a, lda, b, ldb, c, ldc = _operands(oracle, "N", "N", m, n, k, 0, "UNIFORM_1", 4243)
+    out, info = run(cg3m, h, torch, cuda, "N", "N", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form)
+    assert info["k_partitions"] > 1
+    _check(oracle, out, c, "N", "N", m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("size", [1024, 2048])
+def test_tc_error_no_worse_than_plain(cg3m, oracle, cuda, h, form, size):
+    """Precision-form data (Im scaled by 2^e, e in [-8, 8] per column, which
+    stresses the cancellation in Im = P2-P0-P1), alpha=1, beta=0, NN: the
+    tensor-core form's normwise error vs FP64 must not exceed the plain FP32
+    3M form's (rounding pass off in both, so only the products differ)."""
+    import torch
+
+    n = size
+    A = to_dev(oracle.precision_matrix(n, n, 11), torch, cuda)
+    B = to_dev(oracle.precision_matrix(n, n, 12), torch, cuda)
+    C = torch.zeros(n * n, dtype=torch.complex64, device=cuda)
+    ref = torch.empty(n * n, dtype=torch.complex128, device=cuda)
+    h.zgemm_reference("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, ref)
+    h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form="fp32", rounding="off")
+    plain = h.error_report(n, n, C, n, ref)
+    h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, rounding="off")
+    tc = h.error_report(n, n, C, n, ref)
+    torch.cuda.synchronize()
+    print(form, n, "plain", plain, "tc", tc)
+    assert tc["normwise"] <= plain["normwise"], (plain, tc)
+    assert tc["normwise"] < 1e-5

@@ -14,7 +14,9 @@
 // 320 threads:
 //   warp 0       TMA producer: per K-block and component c in {re, im, sum}
 //                one 3-D box for A (all split planes of c) and one for B,
-//                128 B rows with the 128-byte swizzle, into a STAGES ring;
+//                128-byte rows with the 128-byte swizzle, into a 192 KB
+//                ring (3 stages for 3xTF32, 2 for split-BF16; 64-byte rows
+//                give deeper rings but measured slower);
 //   warp 1       allocates 512 TMEM columns; one lane issues every
 //                tcgen05.mma: accumulator c (columns [128c, 128c+128)) +=
 //                sum over split pairs (i, j) of A_c,i * B_c,j, smallest terms
@@ -46,10 +48,10 @@ namespace cg3m {
 namespace {
 
 constexpr int TILE = 128;                     // M and N of the MMA and the output tile
-constexpr int ROW_BYTES = 128;                // one K-block row of one plane
+constexpr int ROW_BYTES = 128;                // one K-block row of one plane (128-byte swizzle)
 constexpr int PLANE_TILE = TILE * ROW_BYTES;  // 16 KB: one plane, 128 rows
+constexpr int RING_BYTES = 192 * 1024;        // operand ring; stages = RING_BYTES / stage size
 constexpr int TMEM_COLS = 512;                // 3 x 128 accumulator columns, rounded to a power of two
-constexpr int kSegment = 64;                  // default K terms accumulated in TMEM before an FP32 merge
 constexpr int kEpilogueWarps = 8;
 constexpr int kThreads = (2 + kEpilogueWarps) * 32;
 // 10 warps land 3/3/2/2 on the SM's four sub-partitions, whose register files
@@ -65,7 +67,7 @@ struct TcCfg<CG3M_FORM_TF32X3> {
     static constexpr int S = 2;        // split planes per component (hi, lo)
     static constexpr int BK = 32;      // K elements per 128-byte row
     static constexpr int NPAIRS = 3;   // lo*hi, hi*lo, hi*hi
-    static constexpr int STAGES = 3;
+    static constexpr int STAGES = RING_BYTES / (2 * S * PLANE_TILE);
     static constexpr uint32_t FMT = 2; // TF32
     __device__ static int2 pair(int q) { return q == 0 ? make_int2(1, 0) : q == 1 ? make_int2(0, 1) : make_int2(0, 0); }
 };
@@ -75,7 +77,7 @@ struct TcCfg<CG3M_FORM_BF16X6> {
     static constexpr int S = 3;        // b0, b1, b2
     static constexpr int BK = 64;
     static constexpr int NPAIRS = 6;   // b_i*b_j with i+j <= 2, smallest first
-    static constexpr int STAGES = 2;
+    static constexpr int STAGES = RING_BYTES / (2 * S * PLANE_TILE);
     static constexpr uint32_t FMT = 1; // BF16
     __device__ static int2 pair(int q)
     {
@@ -95,7 +97,7 @@ struct TcCfg<CG3M_FORM_BF16X9> {
     static constexpr int S = 3;
     static constexpr int BK = 64;
     static constexpr int NPAIRS = 9;   // all b_i*b_j, smallest first
-    static constexpr int STAGES = 2;
+    static constexpr int STAGES = RING_BYTES / (2 * S * PLANE_TILE);
     static constexpr uint32_t FMT = 1;
     __device__ static int2 pair(int q)
     {
@@ -127,14 +129,17 @@ struct TcParams {
     int seg_blocks;  // K-blocks per accumulation segment
 };
 
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart (SBO), leading offset unused (1), descriptor version 1.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle (layout type 2),
+// 8-row groups 8 x 128 = 1024 bytes apart (SBO), leading offset unused (1),
+// descriptor version 1.  Consecutive MMAs along K advance the start address by
+// 32 bytes inside the swizzled row, as the hardware swizzles on absolute
+// address bits and every plane tile starts on a 1024-byte boundary.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr)
 {
     uint64_t d = 0;
     d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
     d |= (uint64_t)1 << 16;
-    d |= (uint64_t)(1024 >> 4) << 32;
+    d |= (uint64_t)((8 * ROW_BYTES) >> 4) << 32;
     d |= (uint64_t)1 << 46;
     d |= (uint64_t)2 << 61;
     return d;
@@ -272,8 +277,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                             for (int q = 0; q < Cfg::NPAIRS; ++q) {
                                 const int2 ij = Cfg::pair(q);
-                                const uint64_t ad = sw128_desc(a_base + ij.x * PLANE_TILE + kk * 32);
-                                const uint64_t bd = sw128_desc(b_base + ij.y * PLANE_TILE + kk * 32);
+                                const uint64_t ad = smem_desc(a_base + ij.x * PLANE_TILE + kk * 32);
+                                const uint64_t bd = smem_desc(b_base + ij.y * PLANE_TILE + kk * 32);
                                 const uint32_t acc = (kb > kb0 || kk > 0 || q > 0) ? 1u : 0u;
                                 if constexpr (Cfg::FMT == 2) {
                                     umma_tf32(d, ad, bd, idesc, acc);
@@ -420,7 +425,7 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
     p.ppitch = plan.partial_pitch;
     p.pplane = plan.partial_plane_elems;
     p.status = status;
-    p.seg_blocks = plan.tc_segment > 0 ? (plan.tc_segment + Cfg::BK - 1) / Cfg::BK : kSegment / Cfg::BK;
+    p.seg_blocks = plan.tc_segment > 0 ? (plan.tc_segment + Cfg::BK - 1) / Cfg::BK : 64 / Cfg::BK;
     if (p.seg_blocks < 1) {
         p.seg_blocks = 1;
     }

@@ -118,7 +118,13 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     out.action = 2;
     out.form = opts.form;
     out.unit = p.ar == 1.0f && p.ai == 0.0f && p.br == 0.0f && p.bi == 0.0f;
-    out.tc_segment = opts.tc_segment;
+    // Tensor-core forms restart their TMEM accumulators every `tc_segment` K
+    // terms and merge segments with round-to-nearest FP32 adds.  The truncation
+    // error of one segment grows with its length, while the plain FP32 form's
+    // error grows with sqrt(K); these lengths keep the tensor-core error at or
+    // below the plain form's (measured on data with a 2^16 dynamic range in the
+    // imaginary parts), at the cost of more merges for short K.
+    out.tc_segment = opts.tc_segment > 0 ? opts.tc_segment : (p.k >= 2048 ? 128 : p.k > 1024 ? 64 : 32);
     out.beta_zero = p.br == 0.0f && p.bi == 0.0f;
     if (sm_count <= 0) {
         sm_count = 148;

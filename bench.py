@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp32", choices=["fp32", "tf32x3", "bf16x6", "bf16x9"])
+    ap.add_argument("--form", default="bf16x6", choices=["fp32", "tf32x3", "bf16x6", "bf16x9"])
     ap.add_argument("--size", type=int, default=SIZE)
     ap.add_argument("--tc-segment", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -78,7 +78,8 @@ typedef struct {
     cg3mRounding_t rounding;
     int k_partitions; /* 0 = planner's choice; else force this many K partitions (1..64) */
     int tc_segment;   /* tensor-core forms: K terms accumulated in TMEM before each round-to-nearest
-                         FP32 merge (0 = default 64; rounded up to the kernel's K-block of 32 or 64) */
+                         FP32 merge (0 = planner: 128 for k >= 2048, 64 for k > 1024, else 32;
+                         rounded up to the kernel's K-block of 32 or 64) */
     int reserved[4];
 } cg3mOptions;
 

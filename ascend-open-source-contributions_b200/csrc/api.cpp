@@ -186,8 +186,12 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
     cudaError_t err = launch_pack(s, p, plan, ws);
     mark(++count);
     if (err == cudaSuccess) {
-        err = plan.form == CG3M_FORM_FP32 ? launch_gemm_fp32(s, p, plan, ws, status)
-                                          : launch_gemm_tc(s, p, plan, ws, status);
+        if (plan.rounding) {
+            err = launch_gemm_with_path(s, p, plan, ws, status);
+        } else {
+            err = plan.form == CG3M_FORM_FP32 ? launch_gemm_fp32(s, p, plan, ws, status)
+                                              : launch_gemm_tc(s, p, plan, ws, status);
+        }
         mark(++count);
     }
     if (err == cudaSuccess && plan.parts > 1) {
@@ -196,9 +200,9 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
     }
     if (err == cudaSuccess && plan.rounding) {
         int launched = 0;
-        err = launch_rounding(s, p, plan, ws, status, &launched);
+        const int before = count;
+        err = launch_rounding(s, p, plan, ws, status, &launched, [&](int i) { mark(before + i); });
         count += launched;
-        mark(count);
     }
     if (kernels != nullptr) {
         *kernels = count;

@@ -7,6 +7,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 
 #include "../../include/cg3m.h"
 
@@ -79,7 +80,14 @@ cudaError_t launch_pack(cudaStream_t s, const Problem& p, const Plan& plan, void
 cudaError_t launch_gemm_fp32(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
 cudaError_t launch_gemm_tc(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
 cudaError_t launch_merge(cudaStream_t s, const Problem& p, const Plan& plan, void* ws);
-cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status, int* launched);
+// The rounding-correction kernels after the path GEMM; mark(i) is called after
+// the i-th of them (1-based) is enqueued.
+cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status, int* launched,
+                            const std::function<void(int)>& mark);
+// GEMM that also writes the risk plane used by the rounding-correction pass.
+cudaError_t launch_gemm_with_path(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
+// Bytes of the rounding-correction region for a square problem of order n.
+size_t rounding_bytes(int n);
 cudaError_t launch_zgemm_ref(cudaStream_t s, const Problem& p, const void* Cin, void* out64);
 cudaError_t launch_error_report(cudaStream_t s, int m, int n, const void* C, int ldc, const void* out64,
                                 double* dev_report);

@@ -205,6 +205,157 @@ __global__ void __launch_bounds__(Fp32Cfg<BM, BN>::THREADS, 1)
     __syncthreads();  // no CTA retires while its copies may still land
 }
 
+// ---------------------------------------------------------------------------
+// Path-tracking variant for the rounding-correction gate (square n in
+// [2048, 4096], contiguous, alpha = 1, beta = 0).  Reference: cgemm3m_path_kernel
+// and MergeProductsWithPath, blas/gemm/arch35/cgemm_compute_kernel.cpp:432-474,
+// 897-927: K is cut into 128-term parts accumulated from zero, merged in order
+// into the running sum s, and each part of depth d adds
+// d/9 * (s_old^2 + s_old*s_new + s_new^2) to the real and imaginary integrals;
+// path = max(I_re, I_im).  Each thread keeps a 4 x 4 complex micro-tile (three
+// product accumulators, the running sums and both integrals), CTA tile 64 x 64.
+// ---------------------------------------------------------------------------
+constexpr int kRiskSegment = 128;
+
+struct PathParams {
+    int n;
+    int tiles;
+    float2* C;    // ldc = n
+    float* path;  // ld = n
+    int* status;
+};
+
+__global__ void __launch_bounds__(288, 1)
+    gemm3m_fp32_path_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                            const PathParams p)
+{
+    constexpr int BM = 64, BN = 64, BK = 16, STAGES = 4, CONSUMER_WARPS = 8;
+    constexpr int A_STAGE = 3 * BK * BM, B_STAGE = 3 * BK * BN;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    float* sA = reinterpret_cast<float*>(base);
+    float* sB = sA + STAGES * A_STAGE;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * B_STAGE);
+    uint64_t* empty = full + STAGES;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tm = blockIdx.x % p.tiles, tn = blockIdx.x / p.tiles;
+    const int m0 = tm * BM, n0 = tn * BN;
+    const int ktiles = (p.n + BK - 1) / BK;
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], CONSUMER_WARPS);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (warp == CONSUMER_WARPS) {
+        if (lane == 0) {
+            int issued = 0;
+            for (int kt = 0; kt < ktiles; ++kt) {
+                const int s = kt % STAGES;
+                if (kt >= STAGES && !mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1, p.status)) {
+                    break;
+                }
+                mbar_arrive_expect_tx(&full[s], (A_STAGE + B_STAGE) * 4);
+                tma_load_3d(sA + s * A_STAGE, &tmA, &full[s], m0, kt * BK, 0);
+                tma_load_3d(sB + s * B_STAGE, &tmB, &full[s], n0, kt * BK, 0);
+                ++issued;
+            }
+            for (int kt = issued > STAGES ? issued - STAGES : 0; kt < issued; ++kt) {
+                mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1, p.status);
+            }
+        }
+    } else {
+        // warp -> 32 x 16 sub-tile (lanes 8 x 4), thread -> 4 x 4 outputs
+        const int wm = warp & 1, wn = warp >> 1;
+        const int tm0 = wm * 32 + (lane & 7) * 4;
+        const int tn0 = wn * 16 + (lane >> 3) * 4;
+        float p0[4][4], p1[4][4], p2[4][4], sr[4][4], si[4][4], ir[4][4], ii[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                p0[i][j] = p1[i][j] = p2[i][j] = 0.0f;
+                sr[i][j] = si[i][j] = ir[i][j] = ii[i][j] = 0.0f;
+            }
+        bool ok = true;
+        int seg_terms = 0;
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const int s = kt % STAGES;
+            if (!mbar_wait(&full[s], (kt / STAGES) & 1, p.status)) {
+                ok = false;
+                break;
+            }
+            const float* a = sA + s * A_STAGE + tm0;
+            const float* b = sB + s * B_STAGE + tn0;
+            const int kvalid = min(BK, p.n - kt * BK);
+#pragma unroll
+            for (int kk = 0; kk < BK; ++kk) {
+                float x0[4], x1[4], x2[4], y0[4], y1[4], y2[4];
+                *reinterpret_cast<float4*>(x0) = *reinterpret_cast<const float4*>(a + kk * BM);
+                *reinterpret_cast<float4*>(x1) = *reinterpret_cast<const float4*>(a + (BK + kk) * BM);
+                *reinterpret_cast<float4*>(x2) = *reinterpret_cast<const float4*>(a + (2 * BK + kk) * BM);
+                *reinterpret_cast<float4*>(y0) = *reinterpret_cast<const float4*>(b + kk * BN);
+                *reinterpret_cast<float4*>(y1) = *reinterpret_cast<const float4*>(b + (BK + kk) * BN);
+                *reinterpret_cast<float4*>(y2) = *reinterpret_cast<const float4*>(b + (2 * BK + kk) * BN);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        p0[i][j] = __fmaf_rn(x0[i], y0[j], p0[i][j]);
+                        p1[i][j] = __fmaf_rn(x1[i], y1[j], p1[i][j]);
+                        p2[i][j] = __fmaf_rn(x2[i], y2[j], p2[i][j]);
+                    }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&empty[s]);
+            }
+            seg_terms += kvalid;
+            // A segment closes every 128 terms (8 K-tiles) and at the end of K.
+            if (seg_terms == kRiskSegment || kt == ktiles - 1) {
+                const float w = __fdiv_rn((float)seg_terms, 9.0f);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float nr = __fadd_rn(sr[i][j], __fsub_rn(p0[i][j], p1[i][j]));
+                        const float ni = __fadd_rn(si[i][j], __fsub_rn(__fsub_rn(p2[i][j], p0[i][j]), p1[i][j]));
+                        float t = __fmul_rn(sr[i][j], sr[i][j]);
+                        t = __fmaf_rn(sr[i][j], nr, t);
+                        t = __fmaf_rn(nr, nr, t);
+                        ir[i][j] = __fadd_rn(ir[i][j], __fmul_rn(t, w));
+                        t = __fmul_rn(si[i][j], si[i][j]);
+                        t = __fmaf_rn(si[i][j], ni, t);
+                        t = __fmaf_rn(ni, ni, t);
+                        ii[i][j] = __fadd_rn(ii[i][j], __fmul_rn(t, w));
+                        sr[i][j] = nr;
+                        si[i][j] = ni;
+                        p0[i][j] = p1[i][j] = p2[i][j] = 0.0f;
+                    }
+                seg_terms = 0;
+            }
+        }
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int col = n0 + tn0 + j;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int row = m0 + tm0 + i;
+                    if (row < p.n && col < p.n) {
+                        const size_t o = (size_t)col * p.n + row;
+                        p.C[o] = make_float2(sr[i][j], si[i][j]);
+                        p.path[o] = ir[i][j] > ii[i][j] ? ir[i][j] : ii[i][j];
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
 // Sum of the partition partials in increasing partition order, then alpha/beta.
 __global__ void merge_kernel(int m, int n, int parts, const float* __restrict__ partial, int ppitch, size_t pplane,
                              EpiParams e, float2* C, int ldc)
@@ -312,6 +463,41 @@ cudaError_t launch_gemm_fp32(cudaStream_t stream, const Problem& pr, const Plan&
         return launch_fp32_tile<64, 32>(stream, pr, plan, ws, status);
     }
     return launch_fp32_tile<32, 32>(stream, pr, plan, ws, status);
+}
+
+cudaError_t launch_gemm_fp32_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, float* path,
+                                  int* status)
+{
+    constexpr int BM = 64, BN = 64, BK = 16, STAGES = 4;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    CUtensorMap ta, tb;
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.m, (uint64_t)pr.k, 3};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_a * 4, (uint64_t)plan.plane_a_elems * 4};
+        const uint32_t box[3] = {BM, BK, 3};
+        if (!encode_tensor_map(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, dims, strides, box,
+                               CU_TENSOR_MAP_SWIZZLE_NONE, w + plan.planes_a_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.n, (uint64_t)pr.k, 3};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_b * 4, (uint64_t)plan.plane_b_elems * 4};
+        const uint32_t box[3] = {BN, BK, 3};
+        if (!encode_tensor_map(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, dims, strides, box,
+                               CU_TENSOR_MAP_SWIZZLE_NONE, w + plan.planes_b_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    PathParams p{pr.n, ceil_div(pr.n, BM), static_cast<float2*>(pr.C), path, status};
+    const size_t smem = (size_t)STAGES * 3 * BK * (BM + BN) * 4 + 2 * STAGES * 8 + 1024;
+    cudaError_t err =
+        cudaFuncSetAttribute(gemm3m_fp32_path_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    gemm3m_fp32_path_kernel<<<p.tiles * p.tiles, 288, smem, stream>>>(ta, tb, p);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_merge(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws)

@@ -10,20 +10,21 @@
 // operand split into TF32 or BF16 terms, which restores FP32-level products
 // while the accumulation stays FP32.
 //
-// B200 design.  One CTA per 128 x 128 output tile (cta_group::1, M = N = 128),
-// 320 threads:
+// B200 design.  One CTA per 128 x BN output tile (cta_group::1, M = 128,
+// N = BN = 128; BN = 64 for the path-tracking variant), 320 threads:
 //   warp 0       TMA producer: per K-block and component c in {re, im, sum}
 //                one 3-D box for A (all split planes of c) and one for B,
 //                128-byte rows with the 128-byte swizzle, into a 192 KB
 //                ring (3 stages for 3xTF32, 2 for split-BF16; 64-byte rows
 //                give deeper rings but measured slower);
-//   warp 1       allocates 512 TMEM columns; one lane issues every
-//                tcgen05.mma: accumulator c (columns [128c, 128c+128)) +=
+//   warp 1       allocates TMEM (512 columns; 256 for BN = 64); one lane
+//                issues every tcgen05.mma: accumulator c (columns
+//                [BN*c, BN*c + BN)) +=
 //                sum over split pairs (i, j) of A_c,i * B_c,j, smallest terms
 //                first; tcgen05.commit releases each ring slot;
 //   warps 2-9    epilogue: after every 128-term K segment, tcgen05.ld of
-//                P0, P1, P2 (one TMEM lane = one output row, 64 columns per
-//                warp), Re_s = P0-P1, Im_s = (P2-P0)-P1 added to running Re,
+//                P0, P1, P2 (one TMEM lane = one output row, BN/2 columns per
+//                warp), Re_s = P0-P1, Im_s = P2-(P0+P1) added to running Re,
 //                Im in registers with round-to-nearest FP32; at the end
 //                alpha/beta and a column-major C store in which each warp
 //                instruction writes 32 consecutive rows of one column.
@@ -44,20 +45,25 @@
 #include "epilogue.cuh"
 #include "ptx.cuh"
 
+// Path-tracking variant (rounding-correction gate): with BN = 64 each epilogue
+// thread also keeps the two risk integrals of its 32 outputs and, after each
+// segment of depth d, adds d/9*(s_old^2 + s_old*s_new + s_new^2) as the
+// reference's MergeProductsWithPath does (cgemm_compute_kernel.cpp:432-474);
+// the risk plane max(I_re, I_im) is written beside C.
 namespace cg3m {
 namespace {
 
-constexpr int TILE = 128;                     // M and N of the MMA and the output tile
-constexpr int ROW_BYTES = 128;                // one K-block row of one plane (128-byte swizzle)
-constexpr int PLANE_TILE = TILE * ROW_BYTES;  // 16 KB: one plane, 128 rows
-constexpr int RING_BYTES = 192 * 1024;        // operand ring; stages = RING_BYTES / stage size
-constexpr int TMEM_COLS = 512;                // 3 x 128 accumulator columns, rounded to a power of two
+constexpr int TILE_M = 128;                     // M of the MMA and rows of the output tile
+constexpr int ROW_BYTES = 128;                  // one K-block row of one plane (128-byte swizzle)
+constexpr int A_PLANE = TILE_M * ROW_BYTES;     // 16 KB: one A plane, 128 rows
+constexpr int RING_BYTES = 192 * 1024;          // operand ring; stages = RING_BYTES / stage size
 constexpr int kEpilogueWarps = 8;
 constexpr int kThreads = (2 + kEpilogueWarps) * 32;
 // 10 warps land 3/3/2/2 on the SM's four sub-partitions, whose register files
 // hold 16K registers each: 3 warps x 32 threads x 168 registers is the most
-// that still launches, so the epilogue keeps 2 x 64 running sums per thread
-// and streams TMEM through 8-column pieces.
+// that still launches, so each epilogue thread keeps 2 x 64 running sums
+// (BN = 128) or 4 x 32 (BN = 64 with path tracking) and streams TMEM through
+// 8-column pieces.
 
 template <int FORM>
 struct TcCfg;
@@ -67,7 +73,6 @@ struct TcCfg<CG3M_FORM_TF32X3> {
     static constexpr int S = 2;        // split planes per component (hi, lo)
     static constexpr int BK = 32;      // K elements per 128-byte row
     static constexpr int NPAIRS = 3;   // lo*hi, hi*lo, hi*hi
-    static constexpr int STAGES = RING_BYTES / (2 * S * PLANE_TILE);
     static constexpr uint32_t FMT = 2; // TF32
     __device__ static int2 pair(int q) { return q == 0 ? make_int2(1, 0) : q == 1 ? make_int2(0, 1) : make_int2(0, 0); }
 };
@@ -77,7 +82,6 @@ struct TcCfg<CG3M_FORM_BF16X6> {
     static constexpr int S = 3;        // b0, b1, b2
     static constexpr int BK = 64;
     static constexpr int NPAIRS = 6;   // b_i*b_j with i+j <= 2, smallest first
-    static constexpr int STAGES = RING_BYTES / (2 * S * PLANE_TILE);
     static constexpr uint32_t FMT = 1; // BF16
     __device__ static int2 pair(int q)
     {
@@ -97,7 +101,6 @@ struct TcCfg<CG3M_FORM_BF16X9> {
     static constexpr int S = 3;
     static constexpr int BK = 64;
     static constexpr int NPAIRS = 9;   // all b_i*b_j, smallest first
-    static constexpr int STAGES = RING_BYTES / (2 * S * PLANE_TILE);
     static constexpr uint32_t FMT = 1;
     __device__ static int2 pair(int q)
     {
@@ -115,6 +118,19 @@ struct TcCfg<CG3M_FORM_BF16X9> {
     }
 };
 
+// Geometry of one instantiation: output tile 128 x BN.
+template <int FORM, int BN>
+struct TcGeom {
+    using Cfg = TcCfg<FORM>;
+    static constexpr int B_PLANE = BN * ROW_BYTES;
+    static constexpr int STAGE_BYTES = Cfg::S * (A_PLANE + B_PLANE);
+    static constexpr int STAGES = RING_BYTES / STAGE_BYTES;
+    static constexpr int COLS = BN / 2;                        // columns per epilogue thread
+    static constexpr int TMEM_COLS = 4 * BN;                   // 3 accumulators + the spare block
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 + 256;
+    static_assert(TMEM_COLS == 256 || TMEM_COLS == 512, "TMEM allocation must be a power of two");
+};
+
 struct TcParams {
     int m, n, k;
     int span, parts;
@@ -127,6 +143,7 @@ struct TcParams {
     size_t pplane;
     int* status;
     int seg_blocks;  // K-blocks per accumulation segment
+    float* path;     // risk plane (path-tracking variant), ld = ldc
 };
 
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle (layout type 2),
@@ -145,22 +162,33 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr)
     return d;
 }
 
-// Instruction descriptor: FP32 accumulate, A/B format, both K-major, N = M = 128.
-template <uint32_t FMT>
+// Instruction descriptor: FP32 accumulate, A/B format, both K-major, M = 128, N = BN.
+template <uint32_t FMT, int BN>
 __device__ __forceinline__ uint32_t instr_desc()
 {
-    return (1u << 4) | (FMT << 7) | (FMT << 10) | ((uint32_t)(TILE >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
+    return (1u << 4) | (FMT << 7) | (FMT << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TILE_M >> 4) << 24);
 }
 
-template <int FORM>
+// d/9 * (old^2 + old*new + new^2) added to the integral (MergeProductsWithPath).
+__device__ __forceinline__ float risk_step(float integral, float old, float nw, float w)
+{
+    float t = __fmul_rn(old, old);
+    t = __fmaf_rn(old, nw, t);
+    t = __fmaf_rn(nw, nw, t);
+    return __fadd_rn(integral, __fmul_rn(t, w));
+}
+
+template <int FORM, int BN, bool PATH>
 __global__ void __launch_bounds__(kThreads, 1)
     gemm3m_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const TcParams p)
 {
     using Cfg = TcCfg<FORM>;
-    constexpr int STAGES = Cfg::STAGES;
-    constexpr int STAGE_BYTES = 2 * Cfg::S * PLANE_TILE;
+    using G = TcGeom<FORM, BN>;
+    constexpr int STAGES = G::STAGES;
+    constexpr int STAGE_BYTES = G::STAGE_BYTES;
     constexpr int KSTEPS = ROW_BYTES / 32;  // 32 bytes of K per MMA: 8 tf32 or 16 bf16
+    constexpr int COLS = G::COLS;
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -182,7 +210,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int gsz = min(p.tiles_m - first_m, GM);
     const int tm = first_m + (pid % in_group) % gsz;
     const int tn = (pid % in_group) / gsz;
-    const int m0 = tm * TILE, n0 = tn * TILE;
+    const int m0 = tm * TILE_M, n0 = tn * BN;
     const int part = blockIdx.y;
     const int kbeg = part * p.span;
     const int kend = min(p.k, kbeg + p.span);
@@ -204,7 +232,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         fence_mbar_init();
     }
     if (warp == 1) {
-        tmem_alloc(tmem_slot, TMEM_COLS);
+        tmem_alloc(tmem_slot, G::TMEM_COLS);
         tmem_relinquish();
     }
     tc_fence_before();
@@ -236,7 +264,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         uint8_t* st = ring + s * STAGE_BYTES;
                         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
                         tma_load_3d(st, &tmA, &full[s], kbeg + kb * Cfg::BK, m0, c * Cfg::S);
-                        tma_load_3d(st + Cfg::S * PLANE_TILE, &tmB, &full[s], kbeg + kb * Cfg::BK, n0, c * Cfg::S);
+                        tma_load_3d(st + Cfg::S * A_PLANE, &tmB, &full[s], kbeg + kb * Cfg::BK, n0, c * Cfg::S);
                     }
                 }
             }
@@ -247,7 +275,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            const uint32_t idesc = instr_desc<Cfg::FMT>();
+            const uint32_t idesc = instr_desc<Cfg::FMT, BN>();
             int it = 0;
             bool stop = false;
             for (int seg = 0; seg < segments && !stop; ++seg) {
@@ -261,7 +289,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                         tc_fence_after();
                     }
-                    const uint32_t d = tmem + (uint32_t)(c * TILE);
+                    const uint32_t d = tmem + (uint32_t)(c * BN);
                     for (int kb = kb0; kb < kb1; ++kb, ++it) {
                         const int s = it % STAGES;
                         if (!mbar_wait(&full[s], (it / STAGES) & 1, p.status)) {
@@ -271,14 +299,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                         tc_fence_after();
                         const uint32_t a_base = smem_u32(ring + s * STAGE_BYTES);
-                        const uint32_t b_base = a_base + Cfg::S * PLANE_TILE;
+                        const uint32_t b_base = a_base + Cfg::S * A_PLANE;
 #pragma unroll
                         for (int kk = 0; kk < KSTEPS; ++kk) {
 #pragma unroll
                             for (int q = 0; q < Cfg::NPAIRS; ++q) {
                                 const int2 ij = Cfg::pair(q);
-                                const uint64_t ad = smem_desc(a_base + ij.x * PLANE_TILE + kk * 32);
-                                const uint64_t bd = smem_desc(b_base + ij.y * PLANE_TILE + kk * 32);
+                                const uint64_t ad = smem_desc(a_base + ij.x * A_PLANE + kk * 32);
+                                const uint64_t bd = smem_desc(b_base + ij.y * G::B_PLANE + kk * 32);
                                 const uint32_t acc = (kb > kb0 || kk > 0 || q > 0) ? 1u : 0u;
                                 if constexpr (Cfg::FMT == 2) {
                                     umma_tf32(d, ad, bd, idesc, acc);
@@ -301,16 +329,21 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else {
         // ---------------- epilogue warps 2..9 ----------------
-        // TMEM lane quadrant = warp % 4; warps 2-5 take columns 0-63, warps 6-9
-        // columns 64-127 of every accumulator and of the spare block (cols 384+).
+        // TMEM lane quadrant = warp % 4; warps 2-5 take the first BN/2 columns,
+        // warps 6-9 the second half, of every accumulator and of the spare block.
         const int quad = warp & 3;
         const int half = (warp - 2) >> 2;
         const int row = m0 + quad * 32 + lane;
-        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * 64);
-        const uint32_t spare = lane_addr + (uint32_t)(3 * TILE);
-        float re[64], im[64];
+        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * COLS);
+        const uint32_t spare = lane_addr + (uint32_t)(3 * BN);
+        float re[COLS], im[COLS];
+        float ir[PATH ? COLS : 1], ii[PATH ? COLS : 1];
         bool go = true;
         for (int seg = 0; seg < segments && go; ++seg) {
+            // Depth of this segment in K terms (the last one may be short).
+            const int t0 = kbeg + seg * seg_blocks * Cfg::BK;
+            const int depth = min(kend, t0 + seg_blocks * Cfg::BK) - t0;
+            const float w = __fdiv_rn((float)depth, 9.0f);
             // P0 and P1 complete: Re_s = P0 - P1 joins the running sum; P0 + P1
             // parks in the spare columns so both accumulators can be reused.
             bool ready = mbar_wait(&acc_full[1], seg & 1, p.status);
@@ -320,14 +353,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                 break;
             }
 #pragma unroll
-            for (int cb = 0; cb < 64; cb += 8) {
+            for (int cb = 0; cb < COLS; cb += 8) {
                 float v0[8], v1[8];
-                tmem_ld8x2(lane_addr + (uint32_t)cb, lane_addr + (uint32_t)(TILE + cb), v0, v1);
+                tmem_ld8x2(lane_addr + (uint32_t)cb, lane_addr + (uint32_t)(BN + cb), v0, v1);
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const float rs = __fsub_rn(v0[j], v1[j]);
                     v1[j] = __fadd_rn(v0[j], v1[j]);
-                    re[cb + j] = seg == 0 ? rs : __fadd_rn(re[cb + j], rs);
+                    const float nr = seg == 0 ? rs : __fadd_rn(re[cb + j], rs);
+                    if constexpr (PATH) {
+                        ir[cb + j] = risk_step(seg == 0 ? 0.0f : ir[cb + j], seg == 0 ? 0.0f : re[cb + j], nr, w);
+                    }
+                    re[cb + j] = nr;
                 }
                 tmem_st8(spare + (uint32_t)cb, v1);
             }
@@ -346,13 +383,17 @@ __global__ void __launch_bounds__(kThreads, 1)
                 break;
             }
 #pragma unroll
-            for (int cb = 0; cb < 64; cb += 8) {
+            for (int cb = 0; cb < COLS; cb += 8) {
                 float v2[8], u[8];
-                tmem_ld8x2(lane_addr + (uint32_t)(2 * TILE + cb), spare + (uint32_t)cb, v2, u);
+                tmem_ld8x2(lane_addr + (uint32_t)(2 * BN + cb), spare + (uint32_t)cb, v2, u);
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const float is = __fsub_rn(v2[j], u[j]);
-                    im[cb + j] = seg == 0 ? is : __fadd_rn(im[cb + j], is);
+                    const float ni = seg == 0 ? is : __fadd_rn(im[cb + j], is);
+                    if constexpr (PATH) {
+                        ii[cb + j] = risk_step(seg == 0 ? 0.0f : ii[cb + j], seg == 0 ? 0.0f : im[cb + j], ni, w);
+                    }
+                    im[cb + j] = ni;
                 }
             }
             tc_fence_before();
@@ -363,12 +404,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         if (go && row < p.m) {
 #pragma unroll
-            for (int j = 0; j < 64; ++j) {
-                const int col = n0 + half * 64 + j;
+            for (int j = 0; j < COLS; ++j) {
+                const int col = n0 + half * COLS + j;
                 if (col < p.n) {
                     if (p.parts == 1) {
                         float2* cp = p.C + (size_t)col * p.ldc + row;
                         *cp = epilogue_value(re[j], im[j], p.epi, cp);
+                        if constexpr (PATH) {
+                            p.path[(size_t)col * p.ldc + row] = ir[j] > ii[j] ? ir[j] : ii[j];
+                        }
                     } else {
                         const size_t o = (size_t)col * p.ppitch + row;
                         p.partial[(size_t)(2 * part) * p.pplane + o] = re[j];
@@ -381,14 +425,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tmem, TMEM_COLS);
+        tmem_dealloc(tmem, G::TMEM_COLS);
     }
 }
 
-template <int FORM>
-cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
+template <int FORM, int BN, bool PATH>
+cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status, float* path)
 {
     using Cfg = TcCfg<FORM>;
+    using G = TcGeom<FORM, BN>;
     const bool bf16 = Cfg::FMT == 1;
     const size_t elem = bf16 ? 2 : 4;
     uint8_t* w = static_cast<uint8_t*>(ws);
@@ -397,7 +442,7 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
     {
         const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.m, (uint64_t)(3 * Cfg::S)};
         const uint64_t strides[2] = {(uint64_t)plan.pitch_a * elem, (uint64_t)plan.plane_a_elems * elem};
-        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)TILE, (uint32_t)Cfg::S};
+        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)TILE_M, (uint32_t)Cfg::S};
         if (!encode_tensor_map(&ta, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_a_off)) {
             return cudaErrorInvalidValue;
         }
@@ -405,7 +450,7 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
     {
         const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.n, (uint64_t)(3 * Cfg::S)};
         const uint64_t strides[2] = {(uint64_t)plan.pitch_b * elem, (uint64_t)plan.plane_b_elems * elem};
-        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)TILE, (uint32_t)Cfg::S};
+        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)BN, (uint32_t)Cfg::S};
         if (!encode_tensor_map(&tb, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_b_off)) {
             return cudaErrorInvalidValue;
         }
@@ -416,8 +461,8 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
     p.k = pr.k;
     p.span = plan.span;
     p.parts = plan.parts;
-    p.tiles_m = ceil_div(pr.m, TILE);
-    p.tiles_n = ceil_div(pr.n, TILE);
+    p.tiles_m = ceil_div(pr.m, TILE_M);
+    p.tiles_n = ceil_div(pr.n, BN);
     p.epi = EpiParams{pr.ar, pr.ai, pr.br, pr.bi, plan.unit ? 1 : 0, plan.beta_zero ? 1 : 0};
     p.C = static_cast<float2*>(pr.C);
     p.ldc = pr.ldc;
@@ -429,14 +474,14 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
     if (p.seg_blocks < 1) {
         p.seg_blocks = 1;
     }
-    const size_t smem = (size_t)Cfg::STAGES * 2 * Cfg::S * PLANE_TILE + 1024 + 256;
-    auto kernel = gemm3m_tc_kernel<FORM>;
-    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    p.path = path;
+    auto kernel = gemm3m_tc_kernel<FORM, BN, PATH>;
+    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
     if (err != cudaSuccess) {
         return err;
     }
     const dim3 grid((unsigned)(p.tiles_m * p.tiles_n), (unsigned)plan.parts);
-    kernel<<<grid, kThreads, smem, stream>>>(ta, tb, p);
+    kernel<<<grid, kThreads, G::SMEM, stream>>>(ta, tb, p);
     return cudaGetLastError();
 }
 
@@ -445,9 +490,20 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
 cudaError_t launch_gemm_tc(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
 {
     switch (plan.form) {
-        case CG3M_FORM_TF32X3: return launch_form<CG3M_FORM_TF32X3>(stream, pr, plan, ws, status);
-        case CG3M_FORM_BF16X6: return launch_form<CG3M_FORM_BF16X6>(stream, pr, plan, ws, status);
-        case CG3M_FORM_BF16X9: return launch_form<CG3M_FORM_BF16X9>(stream, pr, plan, ws, status);
+        case CG3M_FORM_TF32X3: return launch_form<CG3M_FORM_TF32X3, 128, false>(stream, pr, plan, ws, status, nullptr);
+        case CG3M_FORM_BF16X6: return launch_form<CG3M_FORM_BF16X6, 128, false>(stream, pr, plan, ws, status, nullptr);
+        case CG3M_FORM_BF16X9: return launch_form<CG3M_FORM_BF16X9, 128, false>(stream, pr, plan, ws, status, nullptr);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, float* path,
+                                int* status)
+{
+    switch (plan.form) {
+        case CG3M_FORM_TF32X3: return launch_form<CG3M_FORM_TF32X3, 64, true>(stream, pr, plan, ws, status, path);
+        case CG3M_FORM_BF16X6: return launch_form<CG3M_FORM_BF16X6, 64, true>(stream, pr, plan, ws, status, path);
+        case CG3M_FORM_BF16X9: return launch_form<CG3M_FORM_BF16X9, 64, true>(stream, pr, plan, ws, status, path);
         default: return cudaErrorInvalidValue;
     }
 }

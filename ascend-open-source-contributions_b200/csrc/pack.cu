@@ -67,9 +67,19 @@ __device__ __forceinline__ void put(const PackSide& s, int c, size_t idx, float 
     }
 }
 
+// Interleaved complex rows of op(X) (conjugation applied) for the rounding-
+// correction pass: the reference's cgemm3m_pack_kernel transpose
+// (cgemm3m_rounding_kernel.cpp:148-190), so that every output's K vectors are
+// contiguous.
+constexpr int kFormRows = 100;
+
 template <int FORM>
 __device__ __forceinline__ void put_all(const PackSide& s, size_t idx, float2 v)
 {
+    if constexpr (FORM == kFormRows) {
+        static_cast<float2*>(s.out)[idx] = make_float2(v.x, v.y * s.conj);
+        return;
+    }
     const float re = v.x;
     const float im = v.y * s.conj;
     put<FORM>(s, 0, idx, re);
@@ -131,6 +141,36 @@ __global__ void __launch_bounds__(TILE* ROWS) pack_kernel(PackSide a, PackSide b
 }
 
 }  // namespace
+
+cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a, void* rows_b)
+{
+    auto side = [&](bool isA) {
+        PackSide s{};
+        const int op = isA ? p.transa : p.transb;
+        const bool normal = op == CG3M_OP_N || op == CG3M_OP_R;
+        const int opr = isA ? p.m : p.k;
+        const int opc = isA ? p.k : p.n;
+        s.src = static_cast<const float2*>(isA ? p.A : p.B);
+        s.rows = normal ? opr : opc;
+        s.cols = normal ? opc : opr;
+        s.ld = isA ? p.lda : p.ldb;
+        s.conj = (op == CG3M_OP_C || op == CG3M_OP_R) ? -1.0f : 1.0f;
+        // K-major rows: A row i holds op(A)(i, :), B row j holds op(B)(:, j).
+        s.trans = isA ? (normal ? 1 : 0) : (normal ? 0 : 1);
+        s.out = isA ? rows_a : rows_b;
+        s.pitch = p.k;
+        s.plane_elems = 0;
+        return s;
+    };
+    const PackSide a = side(true), b = side(false);
+    const int gx = ceil_div(a.rows > b.rows ? a.rows : b.rows, TILE);
+    const int gy = ceil_div(a.cols > b.cols ? a.cols : b.cols, TILE);
+    if (gy > 65535) {
+        return cudaErrorInvalidConfiguration;
+    }
+    pack_kernel<kFormRows><<<dim3(gx, gy, 2), dim3(TILE, ROWS), 0, stream>>>(a, b);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_pack(cudaStream_t stream, const Problem& p, const Plan& plan, void* ws)
 {

@@ -75,9 +75,6 @@ cg3mStatus_t validate(int transa, int transb, int m, int n, int k, const cg3mCom
 
 namespace {
 
-// The rounding-correction kernels (rounding.cu) are wired into the gate below.
-constexpr bool kRoundingImplemented = false;
-
 struct TileChoice {
     int bm, bn;
     int slots_per_sm;  // resident CTAs per SM of this tile's kernel
@@ -132,7 +129,7 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     const bool tc = opts.form != CG3M_FORM_FP32;
 
     // Rounding-correction gate (cgemm_host.cpp:234-238).
-    out.rounding = kRoundingImplemented && opts.rounding == CG3M_ROUNDING_AUTO && out.unit && p.m == p.n && p.n == p.k && p.k >= 2048 &&
+    out.rounding = opts.rounding == CG3M_ROUNDING_AUTO && out.unit && p.m == p.n && p.n == p.k && p.k >= 2048 &&
                    p.k <= 4096 && p.lda == p.m && p.ldb == p.m && p.ldc == p.m;
 
     // ---- tile x K-partition search -------------------------------------------
@@ -228,13 +225,7 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     }
     out.round_off = off;
     if (out.rounding) {
-        // risk plane n^2 floats, energies 2n floats, selected list n^2 u32,
-        // counters: see rounding.cu for the layout.
-        const size_t n = (size_t)p.n;
-        off = align_up(off + n * n * 4, kRegionAlign);
-        off = align_up(off + 2 * n * 4, kRegionAlign);
-        off = align_up(off + n * n * 4, kRegionAlign);
-        off = align_up(off + 4096, kRegionAlign);
+        off = align_up(off + rounding_bytes(p.n), kRegionAlign);  // layout in rounding.cu
     }
     out.total = off;
     *plan = out;

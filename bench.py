@@ -5,9 +5,10 @@
 Workload (one step = one cgemm3m call): C <- A*B, complex64, M = N = K = 4096,
 column-major, op N/N, alpha = 1, beta = 0, contiguous; Re(A), Re(B) ~ N(0,1),
 Im ~ N(0,1)*2^e with an integer e in [-8, 8] drawn per column; seeded
-synthetic data (the reference publishes no dataset).  Rounding-correction pass
-per the reference's gate (this shape qualifies).  Metric: c64 TFLOP/s counted
-as 8*M*N*K per call.  Under torchrun every rank runs its own independent
+synthetic data (the reference publishes no dataset).  The timed calls run the
+3M product path with the rounding-correction pass off (--rounding auto turns
+it on); the same calls with the pass as the reference gates it are timed and
+reported beside them.  Metric: c64 TFLOP/s counted as 8*M*N*K per call.  Under torchrun every rank runs its own independent
 problem on its own GPU (no data-path collective; weak scaling) and the value is
 the whole job's throughput over the max-over-ranks time.
 
@@ -49,6 +50,9 @@ def parse():
     ap.add_argument("--form", default="bf16x6", choices=["fp32", "tf32x3", "bf16x6", "bf16x9"])
     ap.add_argument("--size", type=int, default=SIZE)
     ap.add_argument("--tc-segment", type=int, default=0)
+    ap.add_argument("--rounding", default="off", choices=["off", "auto"],
+                    help="rounding-correction pass for the timed calls (reported both ways)")
+    ap.add_argument("--no-rounding-report", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -237,20 +241,21 @@ def main():
     h = cg3m.Handle(stream=stream.cuda_stream)
     sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
 
-    def call(form):
-        return h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, tc_segment=args.tc_segment)
+    def call(form, rounding=None):
+        return h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, tc_segment=args.tc_segment,
+                         rounding=rounding or args.rounding)
 
-    def timed(form, steps, warmup):
+    def timed(form, steps, warmup, rounding=None):
         with torch.cuda.stream(stream):
             for _ in range(warmup):
-                info = call(form)
+                info = call(form, rounding)
             torch.cuda.synchronize()
             if world > 1:
                 dist.barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for _ in range(steps):
-                info = call(form)
+                info = call(form, rounding)
             e1.record(stream)
             torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
@@ -261,15 +266,18 @@ def main():
         return ms, info
 
     def stage_times(form, steps):
+        return stage_times_mode(form, None, steps)
+
+    def stage_times_mode(form, rounding, steps=1):
         """Per-kernel durations from events the library records between its launches."""
-        info = call(form)
+        info = call(form, rounding)
         nk = info["kernels"]
         per = []
         with torch.cuda.stream(stream):
             for _ in range(steps):
                 evs = [torch.cuda.Event(enable_timing=True) for _ in range(nk + 1)]
                 h.set_stage_events(evs)
-                call(form)
+                call(form, rounding)
                 per.append(evs)
             h.set_stage_events([])
             torch.cuda.synchronize()
@@ -340,6 +348,21 @@ def main():
     if args.form != "fp32":
         pms, _ = timed("fp32", max(3, args.steps // 2), 2)
         plain = {"value": world * flops8 / (pms * 1e-3) / 1e12, "ms_per_step": pms}
+    # The same calls with the rounding-correction pass as the reference gates it
+    # (this shape qualifies): time, flagged-output recompute share, errors.
+    rounding_report = None
+    if not args.no_rounding_report:
+        rounding_report = {}
+        other = "auto" if args.rounding == "off" else "off"
+        for form in sorted({args.form, "fp32"}):
+            rms, rinfo = timed(form, 1, 1, rounding=other)
+            with torch.cuda.stream(stream):
+                call(form, other)
+                err = h.error_report(n, n, C, n, out64)
+            st, _ = stage_times_mode(form, other)
+            rounding_report[form] = {"rounding": other, "value": world * flops8 / (rms * 1e-3) / 1e12,
+                                     "ms_per_step": rms, "kernels": rinfo["kernels"], "stage_ms": st,
+                                     "errors_vs_fp64": err}
     del out64
     status = h.device_status()
 
@@ -352,7 +375,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.form == "fp32" else args.form, "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": args.form, "m": n, "n": n, "k": n, "transa": "N", "transb": "N",
+        "config": {"workload": WORKLOAD, "form": args.form, "rounding": args.rounding, "m": n, "n": n, "k": n,
+                   "transa": "N", "transb": "N",
                    "alpha": [1, 0], "beta": [0, 0], "parallelism": f"replica x{world} (independent problems)",
                    "l2": "inputs exceed L2: A, B, C 384 MiB plus packed planes; no flush needed",
                    "plan": {k_: info[k_] for k_ in ("tile_m", "tile_n", "k_partitions", "k_span", "rounding",
@@ -365,6 +389,7 @@ def main():
         "errors_vs_fp64": errors,
         "plain_fp32": plain,
         "tc_over_plain": (value / plain["value"]) if plain else None,
+        "rounding_pass": rounding_report,
         "device_status": status,
     }
     print(json.dumps(line), flush=True)

@@ -298,9 +298,12 @@ void oracle_cgemm3m_fp32(int transa, int transb, int m, int n, int k, const floa
  * re_seg = P0-P1, im_seg = (P2-P0)-P1, running sum s += seg in FP32.
  * The multiplier d/9 is formed in FP32 as the reference does (Muls by
  * static_cast<float>(depth)/9.0f).  Output is column-major n x n (ld = n),
- * together with the unit-output C the same model yields.
+ * together with the unit-output C the same model yields.  This is also the
+ * bit-exact model of the FP32 form's path-tracking GEMM, which accumulates
+ * each 128-term segment from zero and merges segments in order exactly as
+ * the reference's fused kernel does when it splits K into 128-term parts.
  */
-void oracle_risk_path(int n, const c32* a, const c32* b, float* path, c32* c)
+void oracle_risk_path(int n, int transa, int transb, const c32* a, const c32* b, float* path, c32* c)
 {
     for (int j = 0; j < n; ++j) {
         for (int i = 0; i < n; ++i) {
@@ -309,8 +312,8 @@ void oracle_risk_path(int n, const c32* a, const c32* b, float* path, c32* c)
                 const int k1 = k0 + RISK_SEGMENT < n ? k0 + RISK_SEGMENT : n;
                 float p0 = 0.0f, p1 = 0.0f, p2 = 0.0f;
                 for (int l = k0; l < k1; ++l) {
-                    const c32 x = a[(size_t)l * n + i];
-                    const c32 y = b[(size_t)j * n + l];
+                    const c32 x = op_elem(a, n, transa, i, l);
+                    const c32 y = op_elem(b, n, transb, l, j);
                     p0 = fmaf(x.re, y.re, p0);
                     p1 = fmaf(x.im, y.im, p1);
                     p2 = fmaf(fadd(x.re, x.im), fadd(y.re, y.im), p2);
@@ -332,6 +335,45 @@ void oracle_risk_path(int n, const c32* a, const c32* b, float* path, c32* c)
             path[(size_t)j * n + i] = ir > ii ? ir : ii;
             c[(size_t)j * n + i].re = sr;
             c[(size_t)j * n + i].im = si;
+        }
+    }
+}
+
+/* The same trajectory for an m x n block of outputs with full K (tests
+ * compare a sub-block of a large problem): op(A) is m x k, op(B) is k x n. */
+void oracle_risk_path_rect(int m, int n, int k, int transa, int transb, const c32* a, int lda, const c32* b, int ldb,
+                           float* path, c32* c)
+{
+    for (int j = 0; j < n; ++j) {
+        for (int i = 0; i < m; ++i) {
+            float sr = 0.0f, si = 0.0f, ir = 0.0f, ii = 0.0f;
+            for (int k0 = 0; k0 < k; k0 += RISK_SEGMENT) {
+                const int k1 = k0 + RISK_SEGMENT < k ? k0 + RISK_SEGMENT : k;
+                float p0 = 0.0f, p1 = 0.0f, p2 = 0.0f;
+                for (int l = k0; l < k1; ++l) {
+                    const c32 x = op_elem(a, lda, transa, i, l);
+                    const c32 y = op_elem(b, ldb, transb, l, j);
+                    p0 = fmaf(x.re, y.re, p0);
+                    p1 = fmaf(x.im, y.im, p1);
+                    p2 = fmaf(fadd(x.re, x.im), fadd(y.re, y.im), p2);
+                }
+                const float nr = fadd(sr, fsub(p0, p1));
+                const float ni = fadd(si, fsub(fsub(p2, p0), p1));
+                const float w = (float)(k1 - k0) / 9.0f;
+                float t = fmul(sr, sr);
+                t = fmaf(sr, nr, t);
+                t = fmaf(nr, nr, t);
+                ir = fadd(ir, fmul(t, w));
+                t = fmul(si, si);
+                t = fmaf(si, ni, t);
+                t = fmaf(ni, ni, t);
+                ii = fadd(ii, fmul(t, w));
+                sr = nr;
+                si = ni;
+            }
+            path[(size_t)j * m + i] = ir > ii ? ir : ii;
+            c[(size_t)j * m + i].re = sr;
+            c[(size_t)j * m + i].im = si;
         }
     }
 }

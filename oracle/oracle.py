@@ -41,7 +41,8 @@ def lib():
         L.oracle_cgemm.argtypes = [i, i, i, i, i, P, P, i, P, i, P, P, i]
         L.oracle_zgemm.argtypes = [i, i, i, i, i, P, P, i, P, i, P, P, i, P]
         L.oracle_cgemm3m_fp32.argtypes = [i, i, i, i, i, P, P, i, P, i, P, P, i, i]
-        L.oracle_risk_path.argtypes = [i, P, P, P, P]
+        L.oracle_risk_path.argtypes = [i, i, i, P, P, P, P]
+        L.oracle_risk_path_rect.argtypes = [i, i, i, i, i, P, i, P, i, P, P]
         L.oracle_energy.argtypes = [i, i, i, P, i, P, i, P]
         L.oracle_select.argtypes = [i, P, P, P, ctypes.c_float, P]
         L.oracle_select.restype = ctypes.c_long
@@ -117,12 +118,33 @@ def cgemm3m_fp32_model(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, 
     return c
 
 
-def risk_path(n, a, b):
-    """(path, C) of the unit-output square NN problem, both column-major n x n."""
+def risk_path(n, a, b, transa="N", transb="N"):
+    """(path, C) of the unit-output square problem (lda = ldb = n), both column-major n x n."""
     path = np.zeros(n * n, dtype=np.float32)
     c = np.zeros(n * n, dtype=np.complex64)
-    lib().oracle_risk_path(n, _ptr(_c64(a)), _ptr(_c64(b)), _ptr(path), _ptr(c))
+    lib().oracle_risk_path(n, _op(transa), _op(transb), _ptr(_c64(a)), _ptr(_c64(b)), _ptr(path), _ptr(c))
     return path, c
+
+
+def risk_path_rect(m, n, k, transa, a, lda, transb, b, ldb):
+    """(path, C) of an m x n output block with full K, column-major (ld = m)."""
+    path = np.zeros(m * n, dtype=np.float32)
+    c = np.zeros(m * n, dtype=np.complex64)
+    lib().oracle_risk_path_rect(m, n, k, _op(transa), _op(transb), _ptr(_c64(a)), lda, _ptr(_c64(b)), ldb,
+                                _ptr(path), _ptr(c))
+    return path, c
+
+
+def select_flags(path, c, e_rows, e_cols, bridge_value, confidence=3.75):
+    """Selection predicate elementwise in FP32 (same operations as oracle_select)."""
+    f32 = np.float32
+    c = np.asarray(c, np.complex64)
+    mag = np.maximum(np.abs(c.real), np.abs(c.imag)).astype(f32)
+    with np.errstate(over="ignore", invalid="ignore"):
+        ee = (np.asarray(e_rows, f32)[:, None] * np.asarray(e_cols, f32)[None, :]).astype(f32)
+        var = (f32(2.0 ** -48) * (np.asarray(path, f32) + (ee * f32(bridge_value)).astype(f32))).astype(f32)
+        conf2 = f32(confidence) * f32(confidence)
+        return (~np.isfinite(mag)) | (~np.isfinite(var)) | ((conf2 * var).astype(f32) >= f32(0.0001))
 
 
 def energy(n, transa, transb, a, lda, b, ldb):

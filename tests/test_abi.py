@@ -193,3 +193,15 @@ def test_planner_narrow_long_k_forces_eight_parts(cg3m):
 def test_planner_forced_partitions(cg3m):
     p = cg3m.plan("N", "N", 300, 200, 1000, k_partitions=3)
     assert p["k_partitions"] == 3 and p["k_span"] == 336
+
+
+def test_rounding_gate(cg3m):
+    """The pass runs exactly for square contiguous unit-output orders 2048..4096."""
+    assert cg3m.plan("N", "N", 2048, 2048, 2048)["rounding"] == 1
+    assert cg3m.plan("C", "T", 4096, 4096, 4096)["rounding"] == 1
+    assert cg3m.plan("N", "N", 2047, 2047, 2047)["rounding"] == 0
+    assert cg3m.plan("N", "N", 4097, 4097, 4097)["rounding"] == 0
+    assert cg3m.plan("N", "N", 2048, 2048, 2048, alpha=complex(1, 0.5))["rounding"] == 0
+    assert cg3m.plan("N", "N", 2048, 2048, 2048, beta=0.5)["rounding"] == 0
+    assert cg3m.plan("N", "N", 2048, 2048, 2048, lda=2050)["rounding"] == 0
+    assert cg3m.plan("N", "N", 2048, 2048, 2048, rounding="off")["rounding"] == 0

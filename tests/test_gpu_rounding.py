@@ -1,0 +1,129 @@
+"""GPU parity of the rounding-correction pass (north-star item (d)).
+
+Reference: gemm_cgemm3m_rounding_do and its kernels (ops-blas/blas/gemm/arch35/
+cgemm3m_rounding_kernel.cpp:43-497), gated at cgemm_host.cpp:234-238, and the
+path-tracking fused kernel (cgemm_compute_kernel.cpp:432-474, 897-927).
+
+FP32 form: every stage is bit-exact against the oracle -- the segmented path
+GEMM (C and risk plane), the energies, the selection predicate and the
+segmented prefix replay of flagged outputs -- checked on scattered output
+blocks of a 2048^3 call.  The reference's SegmentCancellation known answer
+(cgemm3m_test.cpp:212-240) must come back within 0.01 for every form.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import run, sub_problem, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+N = 2048
+
+
+@pytest.fixture(scope="module")
+def h(cg3m, cuda):
+    return cg3m.Handle()
+
+
+def _square(oracle, fill, seed, scale=1.0, n=N):
+    a = oracle.make_matrix(n, n, n, fill, seed)
+    b = oracle.make_matrix(n, n, n, fill, seed + 1)
+    if scale != 1.0:
+        a = (a * np.float32(scale)).astype(np.complex64)
+        b = (b * np.float32(scale)).astype(np.complex64)
+    return a, b
+
+
+@pytest.mark.parametrize("ops", [("N", "N"), ("C", "T")])
+def test_fp32_rounding_pass_bit_exact_blocks(cg3m, oracle, cuda, h, ops):
+    import torch
+
+    ta, tb = ops
+    # Precision-form data (Im scaled by 2^e per column): about 70% of the
+    # outputs are flagged, the rest keep the path GEMM's value.
+    a = oracle.precision_matrix(N, N, 11)
+    b = oracle.precision_matrix(N, N, 12)
+    c0 = np.zeros(N * N, np.complex64)
+    out, info = run(cg3m, h, torch, cuda, ta, tb, N, N, N, 1.0, a, N, b, N, 0.0, c0, N)
+    assert info["rounding"] == 1 and info["kernels"] == 6
+    again, _ = run(cg3m, h, torch, cuda, ta, tb, N, N, N, 1.0, a, N, b, N, 0.0, c0, N)
+    assert out.tobytes() == again.tobytes()
+    e = oracle.energy(N, ta, tb, a, N, b, N)
+    rows = np.r_[0:8, 1000:1008, N - 8:N]
+    cols = np.r_[0:6, 1500:1506, N - 6:N]
+    sa, slda = sub_problem(oracle, ta, a, N, N, N, rows, 0)
+    sb, sldb = sub_problem(oracle, tb, b, N, N, N, cols, 1)
+    path, cpath = oracle.risk_path_rect(len(rows), len(cols), N, ta, sa, slda, tb, sb, sldb)
+    P = path.reshape(len(cols), len(rows)).T
+    Cm = cpath.reshape(len(cols), len(rows)).T
+    flags = oracle.select_flags(P, Cm, e[rows], e[N + cols], oracle.bridge(N))
+    assert flags.any() and not flags.all()
+    opa = oracle.op_matrix(a, N, ta, N, N)
+    opb = oracle.op_matrix(b, N, tb, N, N)
+    expect = Cm.copy()
+    for (r, q) in zip(*np.nonzero(flags)):
+        expect[r, q] = oracle.recompute_dot(np.ascontiguousarray(opa[rows[r], :]), np.ascontiguousarray(opb[:, cols[q]]))
+    got = oracle.unpack(out, N, N, N)[np.ix_(rows, cols)]
+    assert got.tobytes() == expect.astype(np.complex64).tobytes()
+
+
+def _kat_inputs(residual):
+    size, tps = 2048, 33
+    a = np.zeros(size * size, np.complex64)
+    b = np.zeros(size * size, np.complex64)
+    for inner in range(40 * tps):
+        a[inner * size] = 1.0  # A(0, inner)
+        b[inner] = 4096.1 if inner < 20 * tps else -4096.1  # B(inner, 0)
+    a[(size - 1) * size] = 1.0
+    b[size - 1] = residual
+    return a, b
+
+
+@pytest.mark.parametrize("form", ["fp32", "tf32x3", "bf16x6", "bf16x9"])
+def test_segment_cancellation_kat(cg3m, oracle, cuda, h, form):
+    """cgemm3m_test.cpp:212-240: C(0,0) = residual within 0.01 (sequential FP32
+    accumulation alone drifts by ~0.015); everything else is exactly zero."""
+    import torch
+
+    size = 2048
+    for residual in (0.0, 1.0):
+        a, b = _kat_inputs(residual)
+        c0 = np.zeros(size * size, np.complex64)
+        out, info = run(cg3m, h, torch, cuda, "N", "N", size, size, size, 1.0, a, size, b, size, 0.0, c0, size,
+                        form=form)
+        assert info["rounding"] == 1
+        assert abs(out[0].real - residual) <= 0.01 and abs(out[0].imag) <= 0.01, out[0]
+        expect = c0.copy()
+        expect[0] = residual
+        assert oracle.verify_cgemm3m(out, expect, c0, size, size, size)[0]
+
+
+@pytest.mark.parametrize("form", ["tf32x3", "bf16x6", "bf16x9"])
+def test_tc_rounding_pass_recomputes_in_fp64(cg3m, oracle, cuda, h, form):
+    """Tensor-core forms recompute flagged outputs in FP64: those outputs are
+    within one FP32 rounding of the FP64 product, and the whole result's
+    normwise error is no worse than with the pass off."""
+    import torch
+
+    a = oracle.precision_matrix(N, N, 21)
+    b = oracle.precision_matrix(N, N, 22)
+    A, B = to_dev(a, torch, cuda), to_dev(b, torch, cuda)
+    C = torch.zeros(N * N, dtype=torch.complex64, device=cuda)
+    ref = torch.empty(N * N, dtype=torch.complex128, device=cuda)
+    h.zgemm_reference("N", "N", N, N, N, 1.0, A, N, B, N, 0.0, C, N, ref)
+    info = h.cgemm3m("N", "N", N, N, N, 1.0, A, N, B, N, 0.0, C, N, form=form)
+    assert info["rounding"] == 1
+    on = h.error_report(N, N, C, N, ref)
+    got_on = C.clone()
+    h.cgemm3m("N", "N", N, N, N, 1.0, A, N, B, N, 0.0, C, N, form=form, rounding="off")
+    off = h.error_report(N, N, C, N, ref)
+    torch.cuda.synchronize()
+    assert on["normwise"] <= off["normwise"]
+    changed = (got_on != C).cpu().numpy()
+    assert changed.any()
+    x = got_on.cpu().numpy()[changed].astype(np.complex128)
+    z = ref.cpu().numpy()[changed]
+    assert np.all(np.abs(x.real - z.real) <= np.spacing(np.abs(z.real).astype(np.float32)))
+    assert np.all(np.abs(x.imag - z.imag) <= np.spacing(np.abs(z.imag).astype(np.float32)))
+
+

@@ -11,19 +11,21 @@
 //                           reduced across lanes;
 //   3. select (:43-130)     flag output (i,j) when max(|Re|,|Im|) or
 //                           var = 2^-48 (path + E_i E_j bridge) is not finite,
-//                           or 3.75^2 var >= 1e-4; flagged indices are
-//                           compacted into a list;
+//                           or 3.75^2 var >= 1e-4; the reference compacts
+//                           flagged indices into per-core lists;
 //   4. recompute (:192-404) each flagged output again, in a fixed order.
 // B200 design: one CTA of 64 threads per row for the energies (the row is
 // staged in shared memory; span is odd so the strided lane reads are
-// conflict-free); a grid-stride select with an atomic append (the list order
-// does not matter: each flagged output is recomputed independently, so the
-// result bits do not depend on it); one warp per flagged output for the
-// recompute.  FP32 form: the reference's segmented replay -- the 64 lanes are
-// held two per thread, the lane reductions and the inclusive lane scan follow
-// a fixed pairwise order.  Tensor-core forms: the flagged outputs are
-// recomputed as an FP64 dot product (32 contiguous K chunks, one per thread,
-// summed in a fixed tree) and rounded once to FP32.
+// conflict-free); a grid-stride select that sets one bit per flagged output
+// and one word per 16 x 16 output tile (each flagged output is recomputed
+// independently, so no ordering is needed to keep the result bits fixed); the
+// recompute works on
+// output tiles so operand rows are staged once per tile instead of once per
+// output, and skips tiles with no flagged output.  FP32 form: the reference's
+// segmented replay, one output per thread over 16 x 16 tiles, with the 64
+// lane sums in shared memory and the lane reductions and the inclusive lane
+// scan in fixed orders.  Tensor-core forms: flagged outputs are recomputed
+// in FP64 over 64 x 64 tiles (K in order) and rounded once to FP32.
 #include <cstring>
 #include <functional>
 
@@ -40,6 +42,8 @@ cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Pl
 namespace {
 
 constexpr int kLanes = 64;
+constexpr int kTile = 16;             // flag granule: 16 x 16 outputs
+constexpr int kMaxSpan = 65;          // ceil(4096/64) | 1
 constexpr float kConfidence = 3.75f;  // CGEMM_ROUNDING_CONFIDENCE, cgemm_host.cpp:37
 
 // ---- 2. energies ----------------------------------------------------------------
@@ -83,11 +87,13 @@ __global__ void __launch_bounds__(kLanes) energy_kernel(const float2* __restrict
 // ---- 3. selection -----------------------------------------------------------------
 
 __global__ void select_kernel(int n, const float2* __restrict__ C, const float* __restrict__ energy,
-                              const float* __restrict__ path, float bridge, uint32_t* __restrict__ list,
-                              uint32_t* __restrict__ count)
+                              const float* __restrict__ path, float bridge, uint32_t* __restrict__ flag_bits,
+                              uint32_t* __restrict__ tile_flags, uint32_t* __restrict__ count)
 {
     const size_t total = (size_t)n * n;
+    const int tiles = (n + kTile - 1) / kTile;
     const float conf2 = __fmul_rn(kConfidence, kConfidence);
+    uint32_t local = 0;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
         const int j = (int)(idx / n), i = (int)(idx - (size_t)j * n);
@@ -98,10 +104,17 @@ __global__ void select_kernel(int n, const float2* __restrict__ C, const float* 
             __fmul_rn(0x1p-48f, __fadd_rn(path[idx], __fmul_rn(__fmul_rn(energy[i], energy[n + j]), bridge)));
         const bool sel = !isfinite(magnitude) || !isfinite(variance) || __fmul_rn(conf2, variance) >= 0.0001f;
         if (sel) {
-            const uint32_t pos = atomicAdd(count, 1u);
-            list[pos] = (uint32_t)idx;
+            atomicOr(&flag_bits[idx >> 5], 1u << (idx & 31));
+            atomicOr(&tile_flags[(j / kTile) * tiles + i / kTile], 1u);
+            ++local;
         }
     }
+    atomicAdd(count, local);
+}
+
+__device__ __forceinline__ bool flagged(const uint32_t* bits, size_t idx)
+{
+    return (bits[idx >> 5] >> (idx & 31)) & 1u;
 }
 
 // ---- 4a. FP32 segmented replay (FastSegmentDot) ---------------------------------------
@@ -119,118 +132,133 @@ __device__ __forceinline__ Cf term(float2 x, float2 y)
     return Cf{__fsub_rn(p, rr), __fadd_rn(p, q)};
 }
 
-// Sum over 64 lanes held as (a = lane t, b = lane t+32) in a warp, in the
-// pairwise order v[l] += v[l+stride] for stride 32, 16, ..., 1.
-__device__ __forceinline__ float lane_reduce(float a, float b)
+// FP32 segmented replay of one 16 x 16 output tile, one output per thread.
+// For each of the 64 K lanes (lane l holds k in [l*span, (l+1)*span)) the
+// tile's op(A) rows and op(B) columns are staged in shared memory and every
+// thread accumulates its output's lane sum; the 64 lane sums of each output sit
+// in shared memory (S[l][thread]) for the reduction, the inclusive scan and
+// the seeded replay, all in the oracle's fixed orders.  Only flagged outputs
+// are written.
+__global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, const float2* __restrict__ rows_a,
+                                                            const float2* __restrict__ rows_b,
+                                                            const uint32_t* __restrict__ flag_bits,
+                                                            const uint32_t* __restrict__ tile_flags,
+                                                            float2* __restrict__ C)
 {
-    float v = __fadd_rn(a, b);  // stride 32
-#pragma unroll
-    for (int stride = 16; stride >= 1; stride /= 2) {
-        const float o = __shfl_down_sync(0xffffffffu, v, stride);
-        if ((int)(threadIdx.x & 31) < stride) {
-            v = __fadd_rn(v, o);
-        }
+    __shared__ float2 xs[kMaxSpan][kTile];
+    __shared__ float2 ys[kMaxSpan][kTile];
+    extern __shared__ float lane_sums[];  // [2][64][256]: real then imaginary
+    float* sr = lane_sums;
+    float* si = lane_sums + kLanes * 256;
+    const int tiles = (n + kTile - 1) / kTile;
+    if (tile_flags[blockIdx.x] == 0) {
+        return;
     }
-    return __shfl_sync(0xffffffffu, v, 0);
-}
-
-__device__ __forceinline__ float lane_max(float a, float b)
-{
-    float v = fmaxf(a, b);
-#pragma unroll
-    for (int stride = 16; stride >= 1; stride /= 2) {
-        v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, stride));
-    }
-    return v;
-}
-
-// Inclusive Hillis-Steele scan over 64 lanes (a = lane t, b = lane t+32):
-// new[l] = l >= d ? s[l] + s[l-d] : s[l], d = 1, 2, ..., 32.
-__device__ __forceinline__ void lane_scan(float& a, float& b)
-{
-    const int t = threadIdx.x & 31;
-#pragma unroll
-    for (int d = 1; d < 32; d *= 2) {
-        const float a_up = __shfl_up_sync(0xffffffffu, a, d);        // lane t-d (t >= d)
-        const float b_up = __shfl_up_sync(0xffffffffu, b, d);        // lane t+32-d (t >= d)
-        const float a_wrap = __shfl_sync(0xffffffffu, a, (t + 32 - d) & 31);  // lane t+32-d (t < d)
-        const float na = t >= d ? __fadd_rn(a, a_up) : a;
-        const float nb = __fadd_rn(b, t >= d ? b_up : a_wrap);
-        a = na;
-        b = nb;
-    }
-    b = __fadd_rn(b, a);  // d = 32: lane t+32 adds lane t
-}
-
-__global__ void recompute_fp32_kernel(int n, int span, const float2* __restrict__ rows_a,
-                                      const float2* __restrict__ rows_b, const uint32_t* __restrict__ list,
-                                      const uint32_t* __restrict__ count, float2* __restrict__ C)
-{
-    const uint32_t total = *count;
-    const int t = threadIdx.x & 31;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total; w += warps) {
-        const uint32_t idx = list[w];
-        const int j = (int)(idx / (uint32_t)n), i = (int)(idx - (uint32_t)j * n);
-        const float2* x = rows_a + (size_t)i * n;
-        const float2* y = rows_b + (size_t)j * n;
-        Cf s[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int l = t + 32 * h;
-            Cf acc{0.0f, 0.0f};
-            for (int q = 0; q < span; ++q) {
-                const int k = l * span + q;
-                if (k >= n) {
-                    break;
+    const int i0 = (blockIdx.x % tiles) * kTile, j0 = (blockIdx.x / tiles) * kTile;
+    const int tid = threadIdx.x;
+    const int ti = tid & (kTile - 1), tj = tid >> 4;
+    const int i = i0 + ti, j = j0 + tj;
+    auto stage = [&](int l) {
+        const int k0 = l * span;
+        const int cnt = max(0, min(span, n - k0));
+        __syncthreads();
+        for (int e = tid; e < kTile * span; e += 256) {
+            const int r = e / span, q = e - r * span;
+            float2 xv = make_float2(0.0f, 0.0f), yv = make_float2(0.0f, 0.0f);
+            if (q < cnt) {
+                if (i0 + r < n) {
+                    xv = rows_a[(size_t)(i0 + r) * n + k0 + q];
                 }
-                const Cf tv = term(x[k], y[k]);
-                acc.r = __fadd_rn(acc.r, tv.r);
-                acc.i = __fadd_rn(acc.i, tv.i);
-            }
-            s[h] = acc;
-        }
-        const float direct_r = lane_reduce(s[0].r, s[1].r);
-        const float direct_i = lane_reduce(s[0].i, s[1].i);
-        float pr0 = s[0].r, pr1 = s[1].r, pi0 = s[0].i, pi1 = s[1].i;
-        lane_scan(pr0, pr1);
-        lane_scan(pi0, pi1);
-        // exclusive prefix: lane l gets the inclusive value of lane l-1
-        const float prev_r0 = __shfl_up_sync(0xffffffffu, pr0, 1), prev_i0 = __shfl_up_sync(0xffffffffu, pi0, 1);
-        const float prev_r1 = __shfl_up_sync(0xffffffffu, pr1, 1), prev_i1 = __shfl_up_sync(0xffffffffu, pi1, 1);
-        const float last_r0 = __shfl_sync(0xffffffffu, pr0, 31), last_i0 = __shfl_sync(0xffffffffu, pi0, 31);
-        Cf init[2];
-        init[0] = t >= 1 ? Cf{prev_r0, prev_i0} : Cf{0.0f, 0.0f};
-        init[1] = t >= 1 ? Cf{prev_r1, prev_i1} : Cf{last_r0, last_i0};
-        Cf fin[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int l = t + 32 * h;
-            float r = __fadd_rn(init[h].r, 0.0f), im = __fadd_rn(init[h].i, 0.0f);
-            for (int q = 0; q < span; ++q) {
-                const int k = l * span + q;
-                if (k >= n) {
-                    break;
+                if (j0 + r < n) {
+                    yv = rows_b[(size_t)(j0 + r) * n + k0 + q];
                 }
-                const Cf tv = term(x[k], y[k]);
-                r = __fadd_rn(r, tv.r);
-                im = __fadd_rn(im, tv.i);
             }
-            fin[h] = Cf{__fsub_rn(r, init[h].r), __fsub_rn(im, init[h].i)};
+            xs[q][r] = xv;
+            ys[q][r] = yv;
         }
-        float bridged_r = lane_reduce(fin[0].r, fin[1].r);
-        float bridged_i = lane_reduce(fin[0].i, fin[1].i);
-        const float max_r = lane_max(fabsf(pr0), fabsf(pr1));
-        const float max_i = lane_max(fabsf(pi0), fabsf(pi1));
-        // SelectStableSegmentSum (:243-262): keep the direct sum when the
-        // prefixes are at least 32x the result.
-        if (max_r >= __fmul_rn(fabsf(direct_r), 32.0f)) {
-            bridged_r = direct_r;
+        __syncthreads();
+        return cnt;
+    };
+    // pass 1: lane sums
+    for (int l = 0; l < kLanes; ++l) {
+        const int cnt = stage(l);
+        Cf acc{0.0f, 0.0f};
+        for (int q = 0; q < cnt; ++q) {
+            const Cf t = term(xs[q][ti], ys[q][tj]);
+            acc.r = __fadd_rn(acc.r, t.r);
+            acc.i = __fadd_rn(acc.i, t.i);
         }
-        if (max_i >= __fmul_rn(fabsf(direct_i), 32.0f)) {
-            bridged_i = direct_i;
+        sr[l * 256 + tid] = acc.r;
+        si[l * 256 + tid] = acc.i;
+    }
+    // direct reduction (pairwise, stride 32 .. 1) in registers
+    float vr[kLanes], vi[kLanes];
+#pragma unroll
+    for (int l = 0; l < kLanes; ++l) {
+        vr[l] = sr[l * 256 + tid];
+        vi[l] = si[l * 256 + tid];
+    }
+#pragma unroll
+    for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
+#pragma unroll
+        for (int l = 0; l < stride; ++l) {
+            vr[l] = __fadd_rn(vr[l], vr[l + stride]);
+            vi[l] = __fadd_rn(vi[l], vi[l + stride]);
         }
-        if (t == 0) {
+    }
+    const float direct_r = vr[0], direct_i = vi[0];
+    // inclusive Hillis-Steele scan in place: new[l] = s[l] + s[l-d] for l >= d
+    for (int d = 1; d < kLanes; d *= 2) {
+        for (int l = kLanes - 1; l >= d; --l) {
+            sr[l * 256 + tid] = __fadd_rn(sr[l * 256 + tid], sr[(l - d) * 256 + tid]);
+            si[l * 256 + tid] = __fadd_rn(si[l * 256 + tid], si[(l - d) * 256 + tid]);
+        }
+    }
+    float max_r = 0.0f, max_i = 0.0f;
+    for (int l = 0; l < kLanes; ++l) {
+        const float ar = fabsf(sr[l * 256 + tid]), ai = fabsf(si[l * 256 + tid]);
+        max_r = ar > max_r ? ar : max_r;
+        max_i = ai > max_i ? ai : max_i;
+    }
+    // pass 2: replay each lane seeded with the previous lanes' prefix
+    float prev_r = 0.0f, prev_i = 0.0f;
+    for (int l = 0; l < kLanes; ++l) {
+        const int cnt = stage(l);
+        const float init_r = prev_r, init_i = prev_i;
+        prev_r = sr[l * 256 + tid];
+        prev_i = si[l * 256 + tid];
+        float r = __fadd_rn(init_r, 0.0f), im = __fadd_rn(init_i, 0.0f);
+        for (int q = 0; q < cnt; ++q) {
+            const Cf t = term(xs[q][ti], ys[q][tj]);
+            r = __fadd_rn(r, t.r);
+            im = __fadd_rn(im, t.i);
+        }
+        sr[l * 256 + tid] = __fsub_rn(r, init_r);
+        si[l * 256 + tid] = __fsub_rn(im, init_i);
+    }
+#pragma unroll
+    for (int l = 0; l < kLanes; ++l) {
+        vr[l] = sr[l * 256 + tid];
+        vi[l] = si[l * 256 + tid];
+    }
+#pragma unroll
+    for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
+#pragma unroll
+        for (int l = 0; l < stride; ++l) {
+            vr[l] = __fadd_rn(vr[l], vr[l + stride]);
+            vi[l] = __fadd_rn(vi[l], vi[l + stride]);
+        }
+    }
+    float bridged_r = vr[0], bridged_i = vi[0];
+    if (max_r >= __fmul_rn(fabsf(direct_r), 32.0f)) {
+        bridged_r = direct_r;
+    }
+    if (max_i >= __fmul_rn(fabsf(direct_i), 32.0f)) {
+        bridged_i = direct_i;
+    }
+    if (i < n && j < n) {
+        const size_t idx = (size_t)j * n + i;
+        if (flagged(flag_bits, idx)) {
             C[idx] = make_float2(bridged_r, bridged_i);
         }
     }
@@ -238,37 +266,83 @@ __global__ void recompute_fp32_kernel(int n, int span, const float2* __restrict_
 
 // ---- 4b. FP64 recompute (tensor-core forms) -----------------------------------------
 
-__global__ void recompute_fp64_kernel(int n, const float2* __restrict__ rows_a, const float2* __restrict__ rows_b,
-                                      const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
-                                      float2* __restrict__ C)
+// FP64 product of one 64 x 64 output tile (each thread 4 x 4 outputs, K in
+// order), computed only when one of its 16 x 16 flag granules is set; flagged
+// outputs are rounded once to FP32 and written.
+constexpr int kT64 = 64;
+
+__global__ void __launch_bounds__(256) recompute_fp64_tiled(int n, const float2* __restrict__ rows_a,
+                                                            const float2* __restrict__ rows_b,
+                                                            const uint32_t* __restrict__ flag_bits,
+                                                            const uint32_t* __restrict__ tile_flags,
+                                                            float2* __restrict__ C)
 {
-    const uint32_t total = *count;
-    const int t = threadIdx.x & 31;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const int chunk = (n + 31) / 32;
-    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total; w += warps) {
-        const uint32_t idx = list[w];
-        const int j = (int)(idx / (uint32_t)n), i = (int)(idx - (uint32_t)j * n);
-        const float2* x = rows_a + (size_t)i * n;
-        const float2* y = rows_b + (size_t)j * n;
-        double sr = 0.0, si = 0.0;
-        const int k1 = min(n, (t + 1) * chunk);
-        for (int k = t * chunk; k < k1; ++k) {
-            const float2 a = x[k], b = y[k];
-            sr = fma((double)a.x, (double)b.x, fma(-(double)a.y, (double)b.y, sr));
-            si = fma((double)a.x, (double)b.y, fma((double)a.y, (double)b.x, si));
+    __shared__ __align__(16) float2 xs[16][kT64];
+    __shared__ __align__(16) float2 ys[16][kT64];
+    const int tiles16 = (n + kTile - 1) / kTile;
+    const int tiles64 = (n + kT64 - 1) / kT64;
+    const int i0 = (blockIdx.x % tiles64) * kT64, j0 = (blockIdx.x / tiles64) * kT64;
+    uint32_t any = 0;
+    for (int q = 0; q < 16; ++q) {
+        const int gi = i0 / kTile + (q & 3), gj = j0 / kTile + (q >> 2);
+        if (gi < tiles16 && gj < tiles16) {
+            any |= tile_flags[gj * tiles16 + gi];
         }
+    }
+    if (any == 0) {
+        return;
+    }
+    const int tid = threadIdx.x;
+    const int ti = (tid & 15) * 4, tj = (tid >> 4) * 4;
+    double ar[4][4], ai[4][4];
 #pragma unroll
-        for (int stride = 16; stride >= 1; stride /= 2) {
-            const double or_ = __shfl_down_sync(0xffffffffu, sr, stride);
-            const double oi = __shfl_down_sync(0xffffffffu, si, stride);
-            if (t < stride) {
-                sr += or_;
-                si += oi;
-            }
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            ar[a][b] = 0.0;
+            ai[a][b] = 0.0;
         }
-        if (t == 0) {
-            C[idx] = make_float2((float)sr, (float)si);
+    for (int k0 = 0; k0 < n; k0 += 16) {
+        __syncthreads();
+        for (int e = tid; e < 16 * kT64; e += 256) {
+            const int r = e >> 4, q = e & 15;
+            const int k = k0 + q;
+            xs[q][r] = (k < n && i0 + r < n) ? rows_a[(size_t)(i0 + r) * n + k] : make_float2(0.0f, 0.0f);
+            ys[q][r] = (k < n && j0 + r < n) ? rows_b[(size_t)(j0 + r) * n + k] : make_float2(0.0f, 0.0f);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int q = 0; q < 16; ++q) {
+            double xr[4], xi[4], yr[4], yi[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const float2 x = xs[q][ti + a], y = ys[q][tj + a];
+                xr[a] = x.x;
+                xi[a] = x.y;
+                yr[a] = y.x;
+                yi[a] = y.y;
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    ar[a][b] = fma(xr[a], yr[b], fma(-xi[a], yi[b], ar[a][b]));
+                    ai[a][b] = fma(xr[a], yi[b], fma(xi[a], yr[b], ai[a][b]));
+                }
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int j = j0 + tj + b;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = i0 + ti + a;
+            if (i < n && j < n) {
+                const size_t idx = (size_t)j * n + i;
+                if (flagged(flag_bits, idx)) {
+                    C[idx] = make_float2((float)ar[a][b], (float)ai[a][b]);
+                }
+            }
         }
     }
 }
@@ -289,15 +363,25 @@ static float bridge_term(int n)
 
 // Layout of the rounding region (Plan::round_off): path n^2 floats | rows of
 // op(A) n^2 complex | columns of op(B) n^2 complex | energies 2n floats |
-// flagged list n^2 u32 | counter.
+// flags (one bit per output, then one word per 16 x 16 tile, then the flagged
+// count), zeroed before every selection.
 struct RoundLayout {
     float* path;
     float2* rows_a;
     float2* rows_b;
     float* energy;
-    uint32_t* list;
+    uint32_t* flag_bits;
+    uint32_t* tile_flags;
     uint32_t* count;
+    size_t flag_bytes;  // flag_bits + tile_flags + count, one memset
 };
+
+static size_t flag_words(int n) { return ((size_t)n * n + 31) / 32; }
+static size_t tile_words(int n)
+{
+    const size_t t = (size_t)(n + kTile - 1) / kTile;
+    return t * t;
+}
 
 static RoundLayout round_layout(const Plan& plan, void* ws, int n)
 {
@@ -313,9 +397,10 @@ static RoundLayout round_layout(const Plan& plan, void* ws, int n)
     off = align_up(off + nn * 8, kRegionAlign);
     L.energy = reinterpret_cast<float*>(b + off);
     off = align_up(off + (size_t)2 * n * 4, kRegionAlign);
-    L.list = reinterpret_cast<uint32_t*>(b + off);
-    off = align_up(off + nn * 4, kRegionAlign);
-    L.count = reinterpret_cast<uint32_t*>(b + off);
+    L.flag_bits = reinterpret_cast<uint32_t*>(b + off);
+    L.tile_flags = L.flag_bits + flag_words(n);
+    L.count = L.tile_flags + tile_words(n);
+    L.flag_bytes = (flag_words(n) + tile_words(n) + 1) * 4;
     return L;
 }
 
@@ -327,8 +412,7 @@ size_t rounding_bytes(int n)
     off = align_up(off + nn * 8, kRegionAlign);
     off = align_up(off + nn * 8, kRegionAlign);
     off = align_up(off + (size_t)2 * n * 4, kRegionAlign);
-    off = align_up(off + nn * 4, kRegionAlign);
-    off = align_up(off + 256, kRegionAlign);
+    off = align_up(off + (flag_words(n) + tile_words(n) + 1) * 4, kRegionAlign);
     return off;
 }
 
@@ -354,23 +438,31 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
         mark(++count);
     }
     if (err == cudaSuccess) {
-        err = cudaMemsetAsync(L.count, 0, sizeof(uint32_t), s);
+        err = cudaMemsetAsync(L.flag_bits, 0, L.flag_bytes, s);
     }
     if (err == cudaSuccess) {
         select_kernel<<<148 * 8, 256, 0, s>>>(n, static_cast<const float2*>(p.C), L.energy, L.path, bridge_term(n),
-                                              L.list, L.count);
+                                              L.flag_bits, L.tile_flags, L.count);
         err = cudaGetLastError();
         mark(++count);
     }
     if (err == cudaSuccess) {
         if (plan.form == CG3M_FORM_FP32) {
-            recompute_fp32_kernel<<<148 * 16, 128, 0, s>>>(n, span, L.rows_a, L.rows_b, L.list, L.count,
-                                                          static_cast<float2*>(p.C));
+            const int tiles = (n + kTile - 1) / kTile;
+            const size_t smem = (size_t)2 * kLanes * 256 * sizeof(float);
+            err = cudaFuncSetAttribute(recompute_fp32_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (err == cudaSuccess) {
+                recompute_fp32_tiled<<<tiles * tiles, 256, smem, s>>>(n, span, L.rows_a, L.rows_b, L.flag_bits,
+                                                                     L.tile_flags, static_cast<float2*>(p.C));
+            }
         } else {
-            recompute_fp64_kernel<<<148 * 16, 128, 0, s>>>(n, L.rows_a, L.rows_b, L.list, L.count,
-                                                          static_cast<float2*>(p.C));
+            const int tiles = (n + kT64 - 1) / kT64;
+            recompute_fp64_tiled<<<tiles * tiles, 256, 0, s>>>(n, L.rows_a, L.rows_b, L.flag_bits, L.tile_flags,
+                                                             static_cast<float2*>(p.C));
         }
-        err = cudaGetLastError();
+        if (err == cudaSuccess) {
+            err = cudaGetLastError();
+        }
         mark(++count);
     }
     if (launched != nullptr) {

@@ -190,6 +190,14 @@ class Handle:
         _check(st, "cg3mCgemm3mEx")
         return info.as_dict()
 
+    def batch_plan(self, problems, tune=True):
+        """Plan a heterogeneous batch (one persistent launch per execute).
+
+        ``problems``: sequence of (transa, transb, m, n, k, alpha, A, lda, B,
+        ldb, beta, C, ldc) with device buffers (torch tensors or addresses).
+        The buffers must stay alive while the plan is used."""
+        return BatchPlan(self, problems, tune)
+
     def zgemm_reference(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, out64):
         al, be = cx(alpha), cx(beta)
         _check(_lib.cg3mZgemmReference(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda,
@@ -199,6 +207,56 @@ class Handle:
         rep = (ctypes.c_double * 5)()
         _check(_lib.cg3mErrorReport(self.h, m, n, ptr(C), ldc, ptr(out64), rep), "cg3mErrorReport")
         return {"normwise": rep[0], "comp_re": rep[1], "comp_im": rep[2], "abs_re": rep[3], "abs_im": rep[4]}
+
+
+def _addr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return ctypes.c_void_p(x)
+    return ctypes.c_void_p(x.data_ptr())
+
+
+class BatchPlan:
+    """cg3mBatchPlan: the batch's tile/K-split tables and device task list."""
+
+    def __init__(self, handle, problems, tune=True):
+        self.handle = handle
+        self._keep = list(problems)  # buffers referenced by the plan
+        arr = (cg3mProblem * max(1, len(problems)))()
+        for i, (ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc) in enumerate(problems):
+            arr[i] = cg3mProblem(_op(ta), _op(tb), m, n, k, cx(alpha), cx(beta), _addr(A), lda, _addr(B), ldb,
+                                 _addr(C), ldc)
+        self.count = len(problems)
+        self.p = ctypes.c_void_p()
+        bad = ctypes.c_int(-1)
+        st = _lib.cg3mBatchPlanCreate(handle.h, arr, self.count, int(bool(tune)), ctypes.byref(self.p),
+                                      ctypes.byref(bad))
+        if st != SUCCESS:
+            err = Cg3mError(st, f"cg3mBatchPlanCreate (problem {bad.value})")
+            err.bad_index = bad.value
+            raise err
+
+    def execute(self, use_graph=True):
+        _check(_lib.cg3mBatchPlanExecute(self.handle.h, self.p, int(bool(use_graph))), "cg3mBatchPlanExecute")
+
+    def describe(self):
+        """Per problem: (tile_m, tile_n, k_partitions); zeros for quick returns."""
+        n = max(1, self.count)
+        tm, tn, kp = (ctypes.c_int * n)(), (ctypes.c_int * n)(), (ctypes.c_int * n)()
+        _check(_lib.cg3mBatchPlanDescribe(self.p, tm, tn, kp), "cg3mBatchPlanDescribe")
+        return [(tm[i], tn[i], kp[i]) for i in range(self.count)]
+
+    def close(self):
+        if self.p:
+            _lib.cg3mBatchPlanDestroy(self.p)
+            self.p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def validate(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, allow_conj_only=False):

@@ -1,12 +1,747 @@
-// batched.cu -- heterogeneous batched form.
+// batched.cu -- many cgemm3m problems of uneven shape and mixed op() in one
+// persistent launch (the batching form).
+//
+// Reference hooks for batched 3M: LaunchCgemm3mOnchipBatches /
+// LaunchCgemm3mUnitBatches (blas/gemm/arch35/cgemm_host.cpp:749-782,
+// gemm_host_common.h:84-97), used by aclblasCgemm3mStridedBatched
+// (cann_ops_blas.h:652).  The reference batches equal shapes only; this form
+// takes a heterogeneous list, and like the reference's on-chip batch kernel
+// (cgemm_onchip_kernel.h:84 ProducePanel) it deinterleaves inside the GEMM
+// instead of through a workspace.
+//
+// Design.  One persistent kernel (grid = SM count x resident blocks) pulls
+// tasks from a device list through an atomic counter; a task is (problem,
+// output tile, K partition), and the list is sorted by decreasing work so the
+// schedule ends on small tasks.  A task stages op(A) and op(B) straight from
+// the caller's interleaved complex matrices into shared-memory planes re, im,
+// fl(re+im) (op() and conjugation applied while staging, the next K-block
+// prefetched into registers during the current one's FFMAs), runs the 3M FFMA
+// micro-kernel of the drop-in (one thread per output, K in increasing order,
+// fmaf into P0, P1, P2 from +0), and either applies alpha/beta and stores, or
+// writes its partition's (Re, Im) partials and counts in on a per-tile counter;
+// the last partition to arrive merges all partitions in partition order with
+// the merge arithmetic of the drop-in and stores.  No block ever waits on
+// another.  Each output is thus a fixed function of the inputs and its K
+// split, bit-identical to the drop-in called with the same k_partitions.
+//
+// Tile (128x64, 64x64, 64x32, 32x32) and K split are chosen per problem from a
+// policy table; the autotuner times every candidate policy on the device with
+// the caller's A and B and a scratch C, keeps the fastest and caches it per
+// batch signature (device, ops, shapes).  Execute may replay a captured CUDA
+// graph holding the counter reset and the one kernel.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
 #include "cg3m_internal.h"
+#include "epilogue.cuh"
+
+namespace cg3m {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int BK = 16;
+
+struct BProblem {
+    int ta, tb, m, n, k;  // k = 0: beta-scale only (k == 0 or alpha == 0)
+    EpiParams epi;
+    const float2* A;
+    const float2* B;
+    float2* C;
+    int lda, ldb, ldc;
+    int tile;  // 0: 128x64, 1: 64x64, 2: 64x32, 3: 32x32
+    int parts, span, tiles_m, tiles_n, ppitch;
+    size_t partial_off;  // floats into the partial arena
+    size_t counter_off;  // words into the tile counters
+};
+
+struct BTask {
+    int problem, tile, part, pad;
+};
+
+__host__ __device__ constexpr int tile_bm(int t) { return t == 0 ? 128 : t == 3 ? 32 : 64; }
+__host__ __device__ constexpr int tile_bn(int t) { return t <= 1 ? 64 : 32; }
+
+template <int BM, int BN>
+struct Cfg {
+    static constexpr int MT = BM / 16, NT = BN / 16;  // outputs per thread along m, n
+    static constexpr int VA = MT >= 4 ? 4 : MT, HA = MT / VA;
+    static constexpr int VB = NT >= 4 ? 4 : NT, HB = NT / VB;
+    static constexpr int SA = BM + 4, SB = BN + 4;  // padded plane strides (floats)
+    static constexpr int EA = BM * BK / kThreads, EB = BN * BK / kThreads;
+    static constexpr int A_FLOATS = 3 * BK * SA, B_FLOATS = 3 * BK * SB;
+};
+
+constexpr size_t kSmemBytes = 2 * (3 * BK * (128 + 4) + 3 * BK * (64 + 4)) * sizeof(float);
+
+// Element e of a R x BK block of op(X): (r, kk).  The contiguous source
+// dimension maps to consecutive threads: rows for op(A) in {N, R} and op(B) in
+// {T, C}; K otherwise.
+__device__ __forceinline__ void block_coord(int e, int R, bool rows_contig, int& r, int& kk)
+{
+    if (rows_contig) {
+        r = e % R;
+        kk = e / R;
+    } else {
+        kk = e % BK;
+        r = e / BK;
+    }
+}
+
+template <int R, int E>
+__device__ __forceinline__ void load_block(float2 (&v)[E], const float2* X, int ld, bool normal, bool isA, float conj,
+                                           int r0, int rows, int k0, int kend)
+{
+    const bool rows_contig = isA ? normal : !normal;
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+        int r, kk;
+        block_coord(threadIdx.x + q * kThreads, R, rows_contig, r, kk);
+        v[q] = make_float2(0.0f, 0.0f);
+        if (r < rows && k0 + kk < kend) {
+            const size_t row = (size_t)(r0 + r), kidx = (size_t)(k0 + kk);
+            // op(A)(row, k) = A[row + k*lda] (N/R) or A[k + row*lda] (T/C);
+            // op(B)(k, col) = B[k + col*ldb] (N/R) or B[col + k*ldb] (T/C).
+            const size_t off = isA ? (normal ? row + kidx * ld : kidx + row * ld)
+                                   : (normal ? kidx + row * ld : row + kidx * ld);
+            const float2 x = __ldg(X + off);
+            v[q] = make_float2(x.x, x.y * conj);
+        }
+    }
+}
+
+template <int R, int S, int E>
+__device__ __forceinline__ void store_block(float* dst, const float2 (&v)[E], bool rows_contig)
+{
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+        int r, kk;
+        block_coord(threadIdx.x + q * kThreads, R, rows_contig, r, kk);
+        dst[(0 * BK + kk) * S + r] = v[q].x;
+        dst[(1 * BK + kk) * S + r] = v[q].y;
+        dst[(2 * BK + kk) * S + r] = __fadd_rn(v[q].x, v[q].y);
+    }
+}
+
+template <int V>
+__device__ __forceinline__ void ld_vec(const float* p, float* out)
+{
+    if constexpr (V == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        out[0] = t.x;
+        out[1] = t.y;
+        out[2] = t.z;
+        out[3] = t.w;
+    } else if constexpr (V == 2) {
+        const float2 t = *reinterpret_cast<const float2*>(p);
+        out[0] = t.x;
+        out[1] = t.y;
+    } else {
+        out[0] = *p;
+    }
+}
+
+// C = beta*C for k == 0 or alpha == 0 (beta == 0: zeros, C not read).
+__device__ __forceinline__ float2 beta_scaled(const EpiParams& e, const float2* cp)
+{
+    if (e.beta_zero) {
+        return make_float2(0.0f, 0.0f);
+    }
+    const float2 c = *cp;
+    return make_float2(__fsub_rn(__fmul_rn(e.br, c.x), __fmul_rn(e.bi, c.y)),
+                       __fadd_rn(__fmul_rn(e.br, c.y), __fmul_rn(e.bi, c.x)));
+}
+
+template <int BM, int BN>
+__device__ void run_task(const BProblem& p, int tile, int part, float* smem, float* partials, uint32_t* counters,
+                         int* last_flag)
+{
+    using G = Cfg<BM, BN>;
+    const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+    const int m0 = tm * BM, n0 = tn * BN;
+    const int rows = min(BM, p.m - m0), cols = min(BN, p.n - n0);
+    const int kbeg = part * p.span;
+    const int kend = min(p.k, kbeg + p.span);
+    const int nk = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const bool na = p.ta == CG3M_OP_N || p.ta == CG3M_OP_R;
+    const bool nb = p.tb == CG3M_OP_N || p.tb == CG3M_OP_R;
+    const float ca = (p.ta == CG3M_OP_C || p.ta == CG3M_OP_R) ? -1.0f : 1.0f;
+    const float cb = (p.tb == CG3M_OP_C || p.tb == CG3M_OP_R) ? -1.0f : 1.0f;
+
+    float p0[G::MT][G::NT], p1[G::MT][G::NT], p2[G::MT][G::NT];
+#pragma unroll
+    for (int i = 0; i < G::MT; ++i)
+#pragma unroll
+        for (int j = 0; j < G::NT; ++j) {
+            p0[i][j] = 0.0f;
+            p1[i][j] = 0.0f;
+            p2[i][j] = 0.0f;
+        }
+
+    float2 va[G::EA], vb[G::EB];
+    if (nk > 0) {
+        load_block<BM, G::EA>(va, p.A, p.lda, na, true, ca, m0, rows, kbeg, kend);
+        load_block<BN, G::EB>(vb, p.B, p.ldb, nb, false, cb, n0, cols, kbeg, kend);
+    }
+    for (int kb = 0; kb < nk; ++kb) {
+        // Two buffers: the block written here was last read two iterations
+        // ago, and the barrier of the previous iteration separates the two.
+        float* sA = smem + (kb & 1) * (G::A_FLOATS + G::B_FLOATS);
+        float* sB = sA + G::A_FLOATS;
+        store_block<BM, G::SA, G::EA>(sA, va, na);
+        store_block<BN, G::SB, G::EB>(sB, vb, !nb);
+        __syncthreads();
+        if (kb + 1 < nk) {
+            const int k0 = kbeg + (kb + 1) * BK;
+            load_block<BM, G::EA>(va, p.A, p.lda, na, true, ca, m0, rows, k0, kend);
+            load_block<BN, G::EB>(vb, p.B, p.ldb, nb, false, cb, n0, cols, k0, kend);
+        }
+        const float* a = sA + tx * G::VA;
+        const float* b = sB + ty * G::VB;
+#pragma unroll 2
+        for (int kk = 0; kk < BK; ++kk) {
+            float x0[G::MT], x1[G::MT], x2[G::MT], y0[G::NT], y1[G::NT], y2[G::NT];
+#pragma unroll
+            for (int h = 0; h < G::HA; ++h) {
+                ld_vec<G::VA>(a + (0 * BK + kk) * G::SA + h * 16 * G::VA, x0 + h * G::VA);
+                ld_vec<G::VA>(a + (1 * BK + kk) * G::SA + h * 16 * G::VA, x1 + h * G::VA);
+                ld_vec<G::VA>(a + (2 * BK + kk) * G::SA + h * 16 * G::VA, x2 + h * G::VA);
+            }
+#pragma unroll
+            for (int h = 0; h < G::HB; ++h) {
+                ld_vec<G::VB>(b + (0 * BK + kk) * G::SB + h * 16 * G::VB, y0 + h * G::VB);
+                ld_vec<G::VB>(b + (1 * BK + kk) * G::SB + h * 16 * G::VB, y1 + h * G::VB);
+                ld_vec<G::VB>(b + (2 * BK + kk) * G::SB + h * 16 * G::VB, y2 + h * G::VB);
+            }
+#pragma unroll
+            for (int i = 0; i < G::MT; ++i)
+#pragma unroll
+                for (int j = 0; j < G::NT; ++j) {
+                    p0[i][j] = __fmaf_rn(x0[i], y0[j], p0[i][j]);
+                    p1[i][j] = __fmaf_rn(x1[i], y1[j], p1[i][j]);
+                    p2[i][j] = __fmaf_rn(x2[i], y2[j], p2[i][j]);
+                }
+        }
+    }
+
+    // Output (i, j) of this thread: row m0 + (i / VA)*16*VA + tx*VA + i % VA,
+    // column n0 + (j / VB)*16*VB + ty*VB + j % VB.
+    if (p.parts == 1) {
+#pragma unroll
+        for (int j = 0; j < G::NT; ++j) {
+            const int col = n0 + (j / G::VB) * 16 * G::VB + ty * G::VB + j % G::VB;
+#pragma unroll
+            for (int i = 0; i < G::MT; ++i) {
+                const int row = m0 + (i / G::VA) * 16 * G::VA + tx * G::VA + i % G::VA;
+                if (row < p.m && col < p.n) {
+                    float2* cp = p.C + (size_t)col * p.ldc + row;
+                    if (p.k == 0) {
+                        *cp = beta_scaled(p.epi, cp);
+                    } else {
+                        const float re = __fsub_rn(p0[i][j], p1[i][j]);
+                        const float im = __fsub_rn(__fsub_rn(p2[i][j], p0[i][j]), p1[i][j]);
+                        *cp = epilogue_value(re, im, p.epi, cp);
+                    }
+                }
+            }
+        }
+        return;
+    }
+
+    // K split: store this partition's (Re, Im), count in; the last to arrive merges.
+    float* base = partials + p.partial_off;
+    const size_t plane = (size_t)p.ppitch * p.n;
+#pragma unroll
+    for (int j = 0; j < G::NT; ++j) {
+        const int col = n0 + (j / G::VB) * 16 * G::VB + ty * G::VB + j % G::VB;
+#pragma unroll
+        for (int i = 0; i < G::MT; ++i) {
+            const int row = m0 + (i / G::VA) * 16 * G::VA + tx * G::VA + i % G::VA;
+            if (row < p.m && col < p.n) {
+                const size_t o = (size_t)col * p.ppitch + row;
+                __stcg(base + (size_t)(2 * part) * plane + o, __fsub_rn(p0[i][j], p1[i][j]));
+                __stcg(base + (size_t)(2 * part + 1) * plane + o, __fsub_rn(__fsub_rn(p2[i][j], p0[i][j]), p1[i][j]));
+            }
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t* ctr = counters + p.counter_off + tile;
+        const uint32_t prev = atomicAdd(ctr, 1u);
+        const int last = prev == (uint32_t)(p.parts - 1);
+        if (last) {
+            *ctr = 0;  // ready for the next execution of the plan
+        }
+        *last_flag = last;
+    }
+    __syncthreads();
+    if (!*last_flag) {
+        return;
+    }
+    __threadfence();
+    for (int e = threadIdx.x; e < BM * BN; e += kThreads) {
+        const int r = e % BM, c = e / BM;
+        const int row = m0 + r, col = n0 + c;
+        if (row < p.m && col < p.n) {
+            const size_t o = (size_t)col * p.ppitch + row;
+            float re = __ldcg(base + o), im = __ldcg(base + plane + o);
+            for (int q = 1; q < p.parts; ++q) {
+                re = __fadd_rn(re, __ldcg(base + (size_t)(2 * q) * plane + o));
+                im = __fadd_rn(im, __ldcg(base + (size_t)(2 * q + 1) * plane + o));
+            }
+            float2* cp = p.C + (size_t)col * p.ldc + row;
+            *cp = epilogue_value(re, im, p.epi, cp);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) batched_kernel(const BProblem* __restrict__ problems,
+                                                           const BTask* __restrict__ tasks, int ntasks,
+                                                           int* __restrict__ next, float* partials,
+                                                           uint32_t* counters)
+{
+    extern __shared__ __align__(16) float smem[];
+    __shared__ int task_id;
+    __shared__ int last_flag;
+    for (;;) {
+        __syncthreads();  // the previous task's shared-memory reads are done
+        if (threadIdx.x == 0) {
+            task_id = atomicAdd(next, 1);
+        }
+        __syncthreads();
+        const int t = task_id;
+        if (t >= ntasks) {
+            return;
+        }
+        const BTask tk = tasks[t];
+        const BProblem& p = problems[tk.problem];
+        switch (p.tile) {
+            case 0: run_task<128, 64>(p, tk.tile, tk.part, smem, partials, counters, &last_flag); break;
+            case 1: run_task<64, 64>(p, tk.tile, tk.part, smem, partials, counters, &last_flag); break;
+            case 2: run_task<64, 32>(p, tk.tile, tk.part, smem, partials, counters, &last_flag); break;
+            default: run_task<32, 32>(p, tk.tile, tk.part, smem, partials, counters, &last_flag); break;
+        }
+    }
+}
+
+}  // namespace
+}  // namespace cg3m
+
+using namespace cg3m;
+
+struct cg3mBatchPlan {
+    int device = -1;
+    int count = 0;
+    int sm_count = 148;
+    int blocks_per_sm = 1;
+    std::vector<int> index;  // caller's problem i -> host[] position, -1 for quick returns
+    std::vector<BProblem> host;
+    std::vector<BTask> tasks;
+    BProblem* d_problems = nullptr;
+    BTask* d_tasks = nullptr;
+    float* d_partials = nullptr;
+    uint32_t* d_counters = nullptr;
+    int* d_next = nullptr;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~cg3mBatchPlan()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+        cudaFree(d_problems);
+        cudaFree(d_tasks);
+        cudaFree(d_partials);
+        cudaFree(d_counters);
+        cudaFree(d_next);
+    }
+};
+
+namespace {
+
+// One candidate table: the largest tile tried first and the cap on K
+// partitions.  A problem steps down to smaller tiles while half a tile would
+// cover it; it is split along K only when one of its tile tasks would exceed
+// a quarter of the batch's average work per SM (the longest task bounds the
+// persistent schedule), keeping >= 128 K terms per partition.
+struct Policy {
+    int level;
+    int split_cap;
+};
+
+constexpr Policy kPolicies[] = {{0, 1}, {0, 2}, {0, 4}, {0, 8}, {1, 1}, {1, 2},
+                                {1, 4}, {1, 8}, {2, 1}, {2, 4}, {2, 8}};
+constexpr Policy kDefaultPolicy = {1, 4};
+
+int span_for(int k, int parts) { return ceil_div(ceil_div(k, 16), parts) * 16; }
+
+void apply_policy(std::vector<BProblem>& ps, const Policy& pol, int sm_count)
+{
+    double total = 0.0;
+    for (auto& p : ps) {
+        int t = pol.level;
+        while (t < 3 && (p.m <= tile_bm(t) / 2 || p.n <= tile_bn(t) / 2)) {
+            ++t;
+        }
+        p.tile = t;
+        p.tiles_m = ceil_div(p.m, tile_bm(t));
+        p.tiles_n = ceil_div(p.n, tile_bn(t));
+        total += (double)p.tiles_m * p.tiles_n * tile_bm(t) * tile_bn(t) * (p.k + 16);
+    }
+    const double per_sm = total / std::max(sm_count, 1);
+    for (auto& p : ps) {
+        int parts = 1;
+        if (pol.split_cap > 1 && p.k >= 256) {
+            const double task = (double)tile_bm(p.tile) * tile_bn(p.tile) * (p.k + 16);
+            const int want = (int)std::ceil(task / (0.25 * per_sm));
+            parts = std::max(1, std::min({want, pol.split_cap, p.k / 128}));
+        }
+        p.parts = parts;
+        p.span = span_for(p.k, parts);
+        while (p.parts > 1 && (p.parts - 1) * p.span >= p.k) {
+            --p.parts;
+            p.span = span_for(p.k, p.parts);
+        }
+        if (p.parts == 1) {
+            p.span = p.k;
+        }
+    }
+}
+
+// Lays out partials and counters, and lists the tasks by decreasing work.
+void build_tasks(std::vector<BProblem>& ps, std::vector<BTask>& tasks, size_t* partial_floats,
+                 size_t* counter_words)
+{
+    std::vector<std::pair<double, BTask>> v;
+    size_t pf = 0, cw = 0;
+    for (size_t i = 0; i < ps.size(); ++i) {
+        BProblem& p = ps[i];
+        p.ppitch = (int)align_up((size_t)p.m, 32);
+        p.partial_off = pf;
+        p.counter_off = cw;
+        if (p.parts > 1) {
+            pf += (size_t)p.ppitch * p.n * 2 * p.parts;
+            cw += (size_t)p.tiles_m * p.tiles_n;
+        }
+        const double cost = (double)tile_bm(p.tile) * tile_bn(p.tile) * ((p.parts > 1 ? p.span : p.k) + 16);
+        for (int t = 0; t < p.tiles_m * p.tiles_n; ++t) {
+            for (int q = 0; q < p.parts; ++q) {
+                v.push_back({cost, BTask{(int)i, t, q, 0}});
+            }
+        }
+    }
+    std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    tasks.clear();
+    tasks.reserve(v.size());
+    for (auto& x : v) {
+        tasks.push_back(x.second);
+    }
+    *partial_floats = pf;
+    *counter_words = cw;
+}
+
+void release_device(cg3mBatchPlan* plan)
+{
+    if (plan->exec) {
+        cudaGraphExecDestroy(plan->exec);
+        plan->exec = nullptr;
+    }
+    if (plan->graph) {
+        cudaGraphDestroy(plan->graph);
+        plan->graph = nullptr;
+    }
+    cudaFree(plan->d_problems);
+    cudaFree(plan->d_tasks);
+    cudaFree(plan->d_partials);
+    cudaFree(plan->d_counters);
+    plan->d_problems = nullptr;
+    plan->d_tasks = nullptr;
+    plan->d_partials = nullptr;
+    plan->d_counters = nullptr;
+}
+
+// (Re)builds the task list of `ps` under `pol` and uploads it with zeroed
+// tile counters.
+cudaError_t materialise(cg3mBatchPlan* plan, std::vector<BProblem>& ps, const Policy& pol)
+{
+    release_device(plan);
+    apply_policy(ps, pol, plan->sm_count);
+    size_t pf = 0, cw = 0;
+    build_tasks(ps, plan->tasks, &pf, &cw);
+    cudaError_t e = cudaMalloc(&plan->d_problems, sizeof(BProblem) * std::max<size_t>(1, ps.size()));
+    if (e == cudaSuccess) e = cudaMalloc(&plan->d_tasks, sizeof(BTask) * std::max<size_t>(1, plan->tasks.size()));
+    if (e == cudaSuccess) e = cudaMalloc(&plan->d_partials, sizeof(float) * std::max<size_t>(1, pf));
+    if (e == cudaSuccess) e = cudaMalloc(&plan->d_counters, sizeof(uint32_t) * std::max<size_t>(1, cw));
+    if (e == cudaSuccess && plan->d_next == nullptr) e = cudaMalloc(&plan->d_next, sizeof(int));
+    if (e == cudaSuccess && !ps.empty())
+        e = cudaMemcpy(plan->d_problems, ps.data(), sizeof(BProblem) * ps.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !plan->tasks.empty())
+        e = cudaMemcpy(plan->d_tasks, plan->tasks.data(), sizeof(BTask) * plan->tasks.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(plan->d_counters, 0, sizeof(uint32_t) * std::max<size_t>(1, cw));
+    // Pageable uploads may still be in flight on the legacy stream when
+    // cudaMemcpy returns; the plan's launches go to other streams.
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return e;
+}
+
+cudaError_t launch(cg3mBatchPlan* plan, cudaStream_t s)
+{
+    if (plan->tasks.empty()) {
+        return cudaSuccess;
+    }
+    cudaError_t e = cudaMemsetAsync(plan->d_next, 0, sizeof(int), s);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    const int grid = (int)std::min<size_t>(plan->tasks.size(), (size_t)plan->sm_count * plan->blocks_per_sm);
+    batched_kernel<<<grid, kThreads, kSmemBytes, s>>>(plan->d_problems, plan->d_tasks, (int)plan->tasks.size(),
+                                                      plan->d_next, plan->d_partials, plan->d_counters);
+    return cudaGetLastError();
+}
+
+std::mutex g_tune_mutex;
+std::map<std::string, Policy> g_tuned;  // batch signature -> chosen policy
+
+std::string signature(int device, const std::vector<BProblem>& ps)
+{
+    std::string s = std::to_string(device) + ":";
+    s.reserve(ps.size() * 24);
+    char b[80];
+    for (const auto& p : ps) {
+        std::snprintf(b, sizeof b, "%d%d,%d,%d,%d,%d;", p.ta, p.tb, p.m, p.n, p.k, p.epi.beta_zero);
+        s += b;
+    }
+    return s;
+}
+
+// Times every candidate policy (median of 3 launches after one warm-up) with
+// the caller's A and B and a scratch C, and returns the fastest.  The
+// caller's C is never written.
+Policy autotune(cg3mBatchPlan* plan, cudaStream_t s)
+{
+    size_t celems = 0;
+    for (const auto& p : plan->host) {
+        celems += (size_t)p.ldc * p.n;
+    }
+    float2* scratch = nullptr;
+    if (cudaMalloc(&scratch, sizeof(float2) * std::max<size_t>(1, celems)) != cudaSuccess) {
+        cudaGetLastError();
+        return kDefaultPolicy;
+    }
+    cudaMemsetAsync(scratch, 0, sizeof(float2) * std::max<size_t>(1, celems), s);
+    std::vector<BProblem> trial = plan->host;
+    size_t off = 0;
+    for (auto& p : trial) {
+        p.C = scratch + off;
+        off += (size_t)p.ldc * p.n;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    Policy best = kDefaultPolicy;
+    float best_ms = 1e30f;
+    for (const Policy& pol : kPolicies) {
+        if (materialise(plan, trial, pol) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        float times[3] = {0, 0, 0};
+        bool ok = true;
+        for (int r = 0; r < 4 && ok; ++r) {
+            ok = cudaEventRecord(e0, s) == cudaSuccess && launch(plan, s) == cudaSuccess &&
+                 cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+            if (ok && r > 0) {
+                cudaEventElapsedTime(&times[r - 1], e0, e1);
+            }
+        }
+        if (!ok) {
+            cudaGetLastError();
+            continue;
+        }
+        std::sort(times, times + 3);
+        if (times[1] < best_ms) {
+            best_ms = times[1];
+            best = pol;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamSynchronize(s);
+    cudaFree(scratch);
+    return best;
+}
+
+}  // namespace
 
 extern "C" {
-cg3mStatus_t cg3mBatchPlanCreate(cg3mHandle_t, const cg3mProblem*, int, int, cg3mBatchPlan_t*, int*)
+
+cg3mStatus_t cg3mBatchPlanCreate(cg3mHandle_t handle, const cg3mProblem* problems, int count, int tune,
+                                 cg3mBatchPlan_t* out, int* bad_index)
 {
-    return CG3M_STATUS_NOT_SUPPORTED;
+    if (handle == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (out == nullptr || count < 0 || (count > 0 && problems == nullptr)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    *out = nullptr;
+    std::vector<BProblem> ps;
+    std::vector<int> index((size_t)count, -1);
+    for (int i = 0; i < count; ++i) {
+        const cg3mProblem& q = problems[i];
+        int action = 0;
+        const cg3mStatus_t st = validate(q.transa, q.transb, q.m, q.n, q.k, &q.alpha, q.A, q.lda, q.B, q.ldb, &q.beta,
+                                         q.C, q.ldc, true, &action);
+        if (st != CG3M_STATUS_SUCCESS) {
+            if (bad_index != nullptr) {
+                *bad_index = i;
+            }
+            return st;
+        }
+        if (action == 0) {
+            continue;  // quick return: C unchanged
+        }
+        BProblem p{};
+        p.ta = q.transa;
+        p.tb = q.transb;
+        p.m = q.m;
+        p.n = q.n;
+        p.k = action == 1 ? 0 : q.k;
+        const bool beta_zero = q.beta.real == 0.0f && q.beta.imag == 0.0f;
+        const bool unit = q.alpha.real == 1.0f && q.alpha.imag == 0.0f && beta_zero;
+        p.epi = EpiParams{q.alpha.real, q.alpha.imag, q.beta.real, q.beta.imag, unit ? 1 : 0, beta_zero ? 1 : 0};
+        p.A = reinterpret_cast<const float2*>(q.A);
+        p.B = reinterpret_cast<const float2*>(q.B);
+        p.C = reinterpret_cast<float2*>(q.C);
+        p.lda = q.lda;
+        p.ldb = q.ldb;
+        p.ldc = q.ldc;
+        index[(size_t)i] = (int)ps.size();
+        ps.push_back(p);
+    }
+    cg3mBatchPlan* plan = new (std::nothrow) cg3mBatchPlan();
+    if (plan == nullptr) {
+        return CG3M_STATUS_ALLOC_FAILED;
+    }
+    plan->count = count;
+    plan->index = std::move(index);
+    plan->host = std::move(ps);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&plan->sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&plan->blocks_per_sm, batched_kernel, kThreads, kSmemBytes) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        delete plan;
+        return CG3M_STATUS_INTERNAL_ERROR;
+    }
+    plan->device = dev;
+    plan->blocks_per_sm = std::max(1, plan->blocks_per_sm);
+    Policy pol = kDefaultPolicy;
+    const std::string sig = signature(dev, plan->host);
+    bool cached = false;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tuned.find(sig);
+        if (it != g_tuned.end()) {
+            pol = it->second;
+            cached = true;
+        }
+    }
+    if (tune && !cached && !plan->host.empty()) {
+        pol = autotune(plan, handle->stream);
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned[sig] = pol;
+    }
+    if (materialise(plan, plan->host, pol) != cudaSuccess) {
+        cudaGetLastError();
+        delete plan;
+        return CG3M_STATUS_ALLOC_FAILED;
+    }
+    *out = plan;
+    return CG3M_STATUS_SUCCESS;
 }
-cg3mStatus_t cg3mBatchPlanExecute(cg3mHandle_t, cg3mBatchPlan_t, int) { return CG3M_STATUS_NOT_SUPPORTED; }
-cg3mStatus_t cg3mBatchPlanDestroy(cg3mBatchPlan_t) { return CG3M_STATUS_NOT_SUPPORTED; }
-cg3mStatus_t cg3mBatchPlanDescribe(cg3mBatchPlan_t, int*, int*, int*) { return CG3M_STATUS_NOT_SUPPORTED; }
+
+cg3mStatus_t cg3mBatchPlanExecute(cg3mHandle_t handle, cg3mBatchPlan_t plan, int use_graph)
+{
+    if (handle == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (plan == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (!use_graph || plan->tasks.empty()) {
+        return launch(plan, handle->stream) == cudaSuccess ? CG3M_STATUS_SUCCESS : CG3M_STATUS_EXECUTION_FAILED;
+    }
+    if (plan->exec == nullptr) {
+        if (plan->capture_stream == nullptr &&
+            cudaStreamCreateWithFlags(&plan->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            return CG3M_STATUS_INTERNAL_ERROR;
+        }
+        if (cudaStreamBeginCapture(plan->capture_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return CG3M_STATUS_EXECUTION_FAILED;
+        }
+        const cudaError_t le = launch(plan, plan->capture_stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(plan->capture_stream, &g);
+        if (le != cudaSuccess || ce != cudaSuccess || g == nullptr) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return CG3M_STATUS_EXECUTION_FAILED;
+        }
+        plan->graph = g;
+        if (cudaGraphInstantiate(&plan->exec, g, 0) != cudaSuccess) {
+            cudaGetLastError();
+            plan->exec = nullptr;
+            return CG3M_STATUS_EXECUTION_FAILED;
+        }
+    }
+    return cudaGraphLaunch(plan->exec, handle->stream) == cudaSuccess ? CG3M_STATUS_SUCCESS
+                                                                      : CG3M_STATUS_EXECUTION_FAILED;
 }
+
+cg3mStatus_t cg3mBatchPlanDestroy(cg3mBatchPlan_t plan)
+{
+    if (plan == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    // Work enqueued with the plan may still read its task list.
+    if (plan->device >= 0) {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(plan->device);
+        cudaDeviceSynchronize();
+        cudaSetDevice(cur);
+    }
+    delete plan;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mBatchPlanDescribe(cg3mBatchPlan_t plan, int* tile_m, int* tile_n, int* k_partitions)
+{
+    if (plan == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    for (int i = 0; i < plan->count; ++i) {
+        const int h = plan->index[(size_t)i];
+        const BProblem* p = h >= 0 ? &plan->host[(size_t)h] : nullptr;
+        if (tile_m) tile_m[i] = p ? tile_bm(p->tile) : 0;
+        if (tile_n) tile_n[i] = p ? tile_bn(p->tile) : 0;
+        if (k_partitions) k_partitions[i] = p ? (p->k > 0 ? p->parts : 0) : 0;
+    }
+    return CG3M_STATUS_SUCCESS;
+}
+
+}  // extern "C"

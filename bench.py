@@ -44,7 +44,7 @@ PASSES = {"fp32": 1, "tf32x3": 3, "bf16x6": 6, "bf16x9": 9}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="bf16x6", choices=["fp32", "tf32x3", "bf16x6", "bf16x9"])
@@ -54,25 +54,48 @@ def parse():
                     help="rounding-correction pass for the timed calls (reported both ways)")
     ap.add_argument("--no-rounding-report", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batching-report", action="store_true")
     return ap.parse_args()
 
 
 # ----------------------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    """SM clock and clock-event reasons sampled every ~2 ms (NVML, read-only
+    queries) while the timed region runs; nvidia-smi at 200 ms if NVML is
+    unavailable."""
 
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("sw_power_cap", 0x4))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, pci_bus_id=None):
         self.gpu = gpu_index
+        self.pci = pci_bus_id
         self.proc = None
-        self.lines = []
         self.thread = None
+        self.stop_flag = threading.Event()
+        self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
+        self.lines = []
+        self.nvml = None
 
     def start(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            if self.pci:
+                dev = pynvml.nvmlDeviceGetHandleByPciBusId(self.pci)
+            else:
+                dev = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.nvml = (pynvml, dev)
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -83,21 +106,39 @@ class ClockSampler:
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
 
+    def _poll(self):
+        nv, dev = self.nvml
+        mx = nv.nvmlDeviceGetMaxClockInfo(dev, nv.NVML_CLOCK_SM)
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(dev, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(dev)
+                self.samples.append((float(sm), float(mx), int(rs)))
+            except Exception:
+                break
+            time.sleep(0.002)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        self.stop_flag.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
         sm, mx, reasons = [], [], set()
+        for s_, m_, r_ in self.samples:
+            sm.append(s_)
+            mx.append(m_)
+            for nm, bit in self.REASONS:
+                if r_ & bit:
+                    reasons.add(nm)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
@@ -111,10 +152,22 @@ class ClockSampler:
             for nm, flag in zip(names, parts[5:9]):
                 if flag.lower() in ("active", "1"):
                     reasons.add(nm)
+        if self.nvml is not None:
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
+
+
+def pci_bus_id(props):
+    try:
+        return f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+    except AttributeError:
+        return None
 
 
 # ----------------------------------------------------------------------------- peaks
@@ -200,6 +253,63 @@ def run_reference(args, rank):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- batching form
+
+def batching_report(h, stream, dev, world, args):
+    """512 heterogeneous problems (m, n, k log-uniform in [16, 1024], 9 op
+    pairs, random alpha/beta): one graph-replayed persistent launch of the
+    autotuned plan vs 512 separate cg3mCgemm3m calls; metric sum(8mnk)/t."""
+    import torch
+
+    from cg3m.workloads import batch_flops, batch_problems
+
+    probs = batch_problems(dev, count=512)
+    fl = batch_flops(probs)
+    steps = max(5, min(args.steps, 20))
+
+    def timeit(fn, n_steps, warm):
+        with torch.cuda.stream(stream):
+            for _ in range(warm):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(n_steps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n_steps
+
+    with torch.cuda.stream(stream):
+        t0 = time.perf_counter()
+        plan = h.batch_plan(probs, tune=True)
+        torch.cuda.synchronize()
+        plan_s = time.perf_counter() - t0
+    desc = plan.describe()
+    batch_ms = timeit(lambda: plan.execute(use_graph=True), steps, 3)
+    direct_ms = timeit(lambda: plan.execute(use_graph=False), steps, 1)
+
+    def separate():
+        for (ta, tb, m, n, k, al, A, lda, B, ldb, be, C, ldc) in probs:
+            st = h.cgemm3m(ta, tb, m, n, k, al, A, lda, B, ldb, be, C, ldc, raw=True)
+            if st != 0:
+                raise RuntimeError(f"cg3mCgemm3m status {st}")
+
+    sep_ms = timeit(separate, max(2, steps // 4), 1)
+    plan.close()
+    tiles = {}
+    for tm, tn, kp in desc:
+        key = f"{tm}x{tn}/k{kp}"
+        tiles[key] = tiles.get(key, 0) + 1
+    del probs
+    torch.cuda.empty_cache()
+    return {"workload": "512 cgemm3m, m,n,k log-uniform [16,1024], 9 op pairs, |alpha|,|beta|<=1, plain FP32 3M",
+            "flops8": fl, "value": world * fl / (batch_ms * 1e-3) / 1e12, "unit": UNIT, "ms": batch_ms,
+            "direct_launch_ms": direct_ms, "separate_calls": {"value": world * fl / (sep_ms * 1e-3) / 1e12,
+                                                              "ms": sep_ms, "calls": 512},
+            "speedup_vs_separate": sep_ms / batch_ms, "plan_create_s": plan_s, "plan_tiles": tiles}
 
 
 # ----------------------------------------------------------------------------- our arm
@@ -289,7 +399,7 @@ def main():
     flops8 = 8.0 * n ** 3
     flops6 = 6.0 * n ** 3
 
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(local, pci_bus_id(torch.cuda.get_device_properties(dev)))
     sampler.start()
     ms, info = timed(args.form, args.steps, args.warmup)
     clocks = sampler.stop()
@@ -364,6 +474,7 @@ def main():
                                      "ms_per_step": rms, "kernels": rinfo["kernels"], "stage_ms": st,
                                      "errors_vs_fp64": err}
     del out64
+    batching = None if args.no_batching_report else batching_report(h, stream, dev, world, args)
     status = h.device_status()
 
     if world > 1:
@@ -390,6 +501,7 @@ def main():
         "plain_fp32": plain,
         "tc_over_plain": (value / plain["value"]) if plain else None,
         "rounding_pass": rounding_report,
+        "batching_form": batching,
         "device_status": status,
     }
     print(json.dumps(line), flush=True)

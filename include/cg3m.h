@@ -173,9 +173,13 @@ typedef struct {
  * holding the one persistent launch. */
 typedef struct cg3mBatchPlan* cg3mBatchPlan_t;
 
-/* Plans `count` problems (validated individually like cg3mCgemm3m; the first
- * invalid one returns its status and its index in *bad_index).  `tune` != 0
- * times the candidate tile/split tables on the device before choosing. */
+/* Plans `count` problems (validated individually like cg3mCgemm3m, op code R
+ * also accepted; the first invalid one returns its status and its index in
+ * *bad_index).  `tune` != 0 times the candidate tile/split tables on the
+ * device before choosing (the problems' A and B are read, C is not written;
+ * the choice is cached per device and batch shape).  Each output is
+ * bit-identical to cg3mCgemm3mEx (FP32 form) with the K split the plan chose.
+ * A plan is executed on one stream at a time; its buffers must stay valid. */
 cg3mStatus_t cg3mBatchPlanCreate(cg3mHandle_t handle, const cg3mProblem* problems, int count, int tune,
                                  cg3mBatchPlan_t* plan, int* bad_index);
 /* Enqueues the whole batch on the handle's stream as one persistent launch

@@ -205,3 +205,37 @@ def test_rounding_gate(cg3m):
     assert cg3m.plan("N", "N", 2048, 2048, 2048, beta=0.5)["rounding"] == 0
     assert cg3m.plan("N", "N", 2048, 2048, 2048, lda=2050)["rounding"] == 0
     assert cg3m.plan("N", "N", 2048, 2048, 2048, rounding="off")["rounding"] == 0
+
+
+def test_batch_plan_validation_without_device(cg3m):
+    """Argument errors of cg3mBatchPlanCreate come from the host-side
+    validation, per problem in order, before any device work."""
+    L = cg3m.lib
+    h = cg3m.Handle()
+    plan = ctypes.c_void_p()
+    bad = ctypes.c_int(-1)
+    arr = (cg3m.cg3mProblem * 3)()
+    dummy = ctypes.c_void_p(0x1000)
+    for i in range(3):
+        arr[i] = cg3m.cg3mProblem(0, 0, 4, 4, 4, cg3m.cx(1), cg3m.cx(0), dummy, 4, dummy, 4, dummy, 4)
+    arr[1].lda = 2  # lda < m
+    assert L.cg3mBatchPlanCreate(None, arr, 3, 0, ctypes.byref(plan), ctypes.byref(bad)) == cg3m.HANDLE_IS_NULLPTR
+    assert L.cg3mBatchPlanCreate(h.h, arr, -1, 0, ctypes.byref(plan), ctypes.byref(bad)) == cg3m.INVALID_VALUE
+    assert L.cg3mBatchPlanCreate(h.h, None, 3, 0, ctypes.byref(plan), ctypes.byref(bad)) == cg3m.INVALID_VALUE
+    assert L.cg3mBatchPlanCreate(h.h, arr, 3, 0, None, ctypes.byref(bad)) == cg3m.INVALID_VALUE
+    assert L.cg3mBatchPlanCreate(h.h, arr, 3, 0, ctypes.byref(plan), ctypes.byref(bad)) == cg3m.INVALID_VALUE
+    assert bad.value == 1 and not plan.value
+    arr[1].lda = 4
+    arr[2].transb = 7  # an unknown op: the single call's status
+    assert L.cg3mBatchPlanCreate(h.h, arr, 3, 0, ctypes.byref(plan), ctypes.byref(bad)) == cg3m.validate(
+        "N", 7, 4, 4, 4, 1.0, 0x1000, 4, 0x1000, 4, 0.0, 0x1000, 4)[0] == cg3m.INVALID_VALUE
+    assert bad.value == 2
+    # op code R is accepted in a batch (the differentiable form's conj-only op)
+    arr[2].transb = 3
+    arr[0].C = None
+    assert L.cg3mBatchPlanCreate(h.h, arr, 3, 0, ctypes.byref(plan), ctypes.byref(bad)) == cg3m.INVALID_VALUE
+    assert bad.value == 0
+    assert L.cg3mBatchPlanExecute(None, None, 0) == cg3m.HANDLE_IS_NULLPTR
+    assert L.cg3mBatchPlanExecute(h.h, None, 0) == cg3m.INVALID_VALUE
+    assert L.cg3mBatchPlanDestroy(None) == cg3m.INVALID_VALUE
+    assert L.cg3mBatchPlanDescribe(None, None, None, None) == cg3m.INVALID_VALUE

@@ -55,7 +55,7 @@ struct BProblem {
     const float2* B;
     float2* C;
     int lda, ldb, ldc;
-    int tile;  // 0: 128x64, 1: 64x64, 2: 64x32, 3: 32x32
+    int tile;  // index into the tile shapes below
     int parts, span, tiles_m, tiles_n, ppitch;
     size_t partial_off;  // floats into the partial arena
     size_t counter_off;  // words into the tile counters
@@ -65,8 +65,16 @@ struct BTask {
     int problem, tile, part, pad;
 };
 
-__host__ __device__ constexpr int tile_bm(int t) { return t == 0 ? 128 : t == 3 ? 32 : 64; }
-__host__ __device__ constexpr int tile_bn(int t) { return t <= 1 ? 64 : 32; }
+// Tile shapes (BM x BN): 0: 128x64, 1: 64x64, 2: 128x32, 3: 32x128, 4: 64x32, 5: 32x32.
+constexpr int kTileCount = 6;
+__host__ __device__ constexpr int tile_bm(int t)
+{
+    return (t == 0 || t == 2) ? 128 : (t == 1 || t == 4) ? 64 : 32;
+}
+__host__ __device__ constexpr int tile_bn(int t)
+{
+    return t == 3 ? 128 : (t == 0 || t == 1) ? 64 : 32;
+}
 
 template <int BM, int BN>
 struct Cfg {
@@ -74,58 +82,107 @@ struct Cfg {
     static constexpr int VA = MT >= 4 ? 4 : MT, HA = MT / VA;
     static constexpr int VB = NT >= 4 ? 4 : NT, HB = NT / VB;
     static constexpr int SA = BM + 4, SB = BN + 4;  // padded plane strides (floats)
-    static constexpr int EA = BM * BK / kThreads, EB = BN * BK / kThreads;
+    static constexpr int EA = BM * BK / kThreads, EB = BN * BK / kThreads;  // elements per thread per K-block
     static constexpr int A_FLOATS = 3 * BK * SA, B_FLOATS = 3 * BK * SB;
 };
 
-constexpr size_t kSmemBytes = 2 * (3 * BK * (128 + 4) + 3 * BK * (64 + 4)) * sizeof(float);
+// Shared memory: kStages raw stages of interleaved complex elements (as
+// copied, one slot per (thread, element)), then two plane buffers.
+constexpr int kStages = 4;
+constexpr int kRawElems = (128 + 64) * BK;  // largest BM + BN of any tile, times BK
+constexpr int kPlaneFloats = 3 * BK * (128 + 4) + 3 * BK * (64 + 4);
+constexpr size_t kSmemBytes = (size_t)kStages * kRawElems * sizeof(float2) + 2 * (size_t)kPlaneFloats * sizeof(float);
 
-// Element e of a R x BK block of op(X): (r, kk).  The contiguous source
-// dimension maps to consecutive threads: rows for op(A) in {N, R} and op(B) in
-// {T, C}; K otherwise.
-__device__ __forceinline__ void block_coord(int e, int R, bool rows_contig, int& r, int& kk)
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// 8-byte asynchronous copy global -> shared; src_bytes = 0 writes zeros
+// (the source is then not read).
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int src_bytes)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// One operand's share of a K-block for this thread.  Element q of the thread
+// is e = tid + q*kThreads of the R x BK block.  The source's contiguous
+// dimension goes to consecutive threads: rows ("rows_contig": op(A) in {N, R},
+// op(B) in {T, C}; r = e % R, kk = e / R) or K (r = e / BK, kk = e % BK).
+//   rows_contig: X[(row0 + r) + k*ld]      else: X[k + (row0 + r)*ld]
+struct Feed {
+    const float2* origin;  // the matrix (source of the zero-byte copies)
+    const float2* base;    // element q = 0 at K-block 0
+    long long qstep;     // element offset between consecutive q
+    long long kbstep;    // element offset between consecutive K-blocks
+    int r, kk;           // block coordinates of element q = 0
+    int rq, kq;          // coordinate steps between consecutive q
+    int rows;            // valid rows of this tile
+    float conj;          // -1 for op C / R
+};
+
+template <int R>
+__device__ __forceinline__ Feed make_feed(const float2* X, int ld, bool rows_contig, int row0, int rows, int kbeg,
+                                          float conj)
+{
+    Feed f;
+    const int tid = threadIdx.x;
     if (rows_contig) {
-        r = e % R;
-        kk = e / R;
+        f.r = tid % R;
+        f.kk = tid / R;
+        f.rq = 0;
+        f.kq = kThreads / R;
+        f.base = X + (long long)(row0 + f.r) + (long long)(kbeg + f.kk) * ld;
+        f.qstep = (long long)f.kq * ld;
+        f.kbstep = (long long)BK * ld;
     } else {
-        kk = e % BK;
-        r = e / BK;
+        f.kk = tid % BK;
+        f.r = tid / BK;
+        f.rq = kThreads / BK;
+        f.kq = 0;
+        f.base = X + (long long)(kbeg + f.kk) + (long long)(row0 + f.r) * ld;
+        f.qstep = (long long)f.rq * ld;
+        f.kbstep = BK;
+    }
+    f.origin = X;
+    f.rows = rows;
+    f.conj = conj;
+    return f;
+}
+
+// Issue this thread's copies of K-block kb (global K index k0 = kbeg + kb*BK)
+// into raw slot `raw`; elements past the tile or past kend read as zero.
+template <int E>
+__device__ __forceinline__ void issue(const Feed& f, float2* raw, int kb, int krel_end)
+{
+    const float2* src = f.base + (long long)kb * f.kbstep;
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+        const int r = f.r + q * f.rq;
+        const int kk = kb * BK + f.kk + q * f.kq;
+        const bool ok = r < f.rows && kk < krel_end;
+        cp_async8(smem_u32(raw + threadIdx.x + q * kThreads), ok ? (const void*)(src + q * f.qstep) : (const void*)f.origin,
+                  ok ? 8 : 0);
     }
 }
 
-template <int R, int E>
-__device__ __forceinline__ void load_block(float2 (&v)[E], const float2* X, int ld, bool normal, bool isA, float conj,
-                                           int r0, int rows, int k0, int kend)
-{
-    const bool rows_contig = isA ? normal : !normal;
-#pragma unroll
-    for (int q = 0; q < E; ++q) {
-        int r, kk;
-        block_coord(threadIdx.x + q * kThreads, R, rows_contig, r, kk);
-        v[q] = make_float2(0.0f, 0.0f);
-        if (r < rows && k0 + kk < kend) {
-            const size_t row = (size_t)(r0 + r), kidx = (size_t)(k0 + kk);
-            // op(A)(row, k) = A[row + k*lda] (N/R) or A[k + row*lda] (T/C);
-            // op(B)(k, col) = B[k + col*ldb] (N/R) or B[col + k*ldb] (T/C).
-            const size_t off = isA ? (normal ? row + kidx * ld : kidx + row * ld)
-                                   : (normal ? kidx + row * ld : row + kidx * ld);
-            const float2 x = __ldg(X + off);
-            v[q] = make_float2(x.x, x.y * conj);
-        }
-    }
-}
-
-template <int R, int S, int E>
-__device__ __forceinline__ void store_block(float* dst, const float2 (&v)[E], bool rows_contig)
+// Convert this thread's own elements of a raw slot into the planes
+// re, im (conjugated), fl(re + im) at dst[(c*BK + kk)*S + r].
+template <int S, int E>
+__device__ __forceinline__ void convert(const Feed& f, const float2* raw, float* dst)
 {
 #pragma unroll
     for (int q = 0; q < E; ++q) {
-        int r, kk;
-        block_coord(threadIdx.x + q * kThreads, R, rows_contig, r, kk);
-        dst[(0 * BK + kk) * S + r] = v[q].x;
-        dst[(1 * BK + kk) * S + r] = v[q].y;
-        dst[(2 * BK + kk) * S + r] = __fadd_rn(v[q].x, v[q].y);
+        const float2 v = raw[threadIdx.x + q * kThreads];
+        const float re = v.x, im = v.y * f.conj;
+        const int r = f.r + q * f.rq;
+        const int kk = f.kk + q * f.kq;
+        dst[(0 * BK + kk) * S + r] = re;
+        dst[(1 * BK + kk) * S + r] = im;
+        dst[(2 * BK + kk) * S + r] = __fadd_rn(re, im);
     }
 }
 
@@ -159,21 +216,27 @@ __device__ __forceinline__ float2 beta_scaled(const EpiParams& e, const float2* 
 }
 
 template <int BM, int BN>
-__device__ void run_task(const BProblem& p, int tile, int part, float* smem, float* partials, uint32_t* counters,
-                         int* last_flag)
+__device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, float* planes, float* partials,
+                         uint32_t* counters, int* last_flag)
 {
     using G = Cfg<BM, BN>;
+    static_assert(G::A_FLOATS + G::B_FLOATS <= kPlaneFloats, "planes exceed their buffer");
+    static_assert((BM + BN) * BK <= kRawElems, "raw stage exceeds its slot");
+    static_assert((BM * BK) % kThreads == 0 && (BN * BK) % kThreads == 0, "whole elements per thread");
+    const BProblem p = prob;  // registers: no reloads after barriers
     const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
     const int m0 = tm * BM, n0 = tn * BN;
-    const int rows = min(BM, p.m - m0), cols = min(BN, p.n - n0);
     const int kbeg = part * p.span;
     const int kend = min(p.k, kbeg + p.span);
-    const int nk = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
+    const int klen = kend > kbeg ? kend - kbeg : 0;
+    const int nk = (klen + BK - 1) / BK;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const bool na = p.ta == CG3M_OP_N || p.ta == CG3M_OP_R;
     const bool nb = p.tb == CG3M_OP_N || p.tb == CG3M_OP_R;
-    const float ca = (p.ta == CG3M_OP_C || p.ta == CG3M_OP_R) ? -1.0f : 1.0f;
-    const float cb = (p.tb == CG3M_OP_C || p.tb == CG3M_OP_R) ? -1.0f : 1.0f;
+    const Feed fa = make_feed<BM>(p.A, p.lda, na, m0, min(BM, p.m - m0), kbeg,
+                                  (p.ta == CG3M_OP_C || p.ta == CG3M_OP_R) ? -1.0f : 1.0f);
+    const Feed fb = make_feed<BN>(p.B, p.ldb, !nb, n0, min(BN, p.n - n0), kbeg,
+                                  (p.tb == CG3M_OP_C || p.tb == CG3M_OP_R) ? -1.0f : 1.0f);
 
     float p0[G::MT][G::NT], p1[G::MT][G::NT], p2[G::MT][G::NT];
 #pragma unroll
@@ -185,24 +248,36 @@ __device__ void run_task(const BProblem& p, int tile, int part, float* smem, flo
             p2[i][j] = 0.0f;
         }
 
-    float2 va[G::EA], vb[G::EB];
-    if (nk > 0) {
-        load_block<BM, G::EA>(va, p.A, p.lda, na, true, ca, m0, rows, kbeg, kend);
-        load_block<BN, G::EB>(vb, p.B, p.ldb, nb, false, cb, n0, cols, kbeg, kend);
+    // Prologue: K-blocks 0 .. kStages-2 in flight (one commit group each,
+    // empty groups past the end keep the counting uniform).
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < nk) {
+            float2* slot = raw + s * kRawElems;
+            issue<G::EA>(fa, slot, s, klen);
+            issue<G::EB>(fb, slot + BM * BK, s, klen);
+        }
+        cp_async_commit();
     }
     for (int kb = 0; kb < nk; ++kb) {
-        // Two buffers: the block written here was last read two iterations
-        // ago, and the barrier of the previous iteration separates the two.
-        float* sA = smem + (kb & 1) * (G::A_FLOATS + G::B_FLOATS);
-        float* sB = sA + G::A_FLOATS;
-        store_block<BM, G::SA, G::EA>(sA, va, na);
-        store_block<BN, G::SB, G::EB>(sB, vb, !nb);
-        __syncthreads();
-        if (kb + 1 < nk) {
-            const int k0 = kbeg + (kb + 1) * BK;
-            load_block<BM, G::EA>(va, p.A, p.lda, na, true, ca, m0, rows, k0, kend);
-            load_block<BN, G::EB>(vb, p.B, p.ldb, nb, false, cb, n0, cols, k0, kend);
+        // Refill the slot converted in the previous iteration (by this same
+        // thread: each thread copies and converts only its own elements).
+        const int nxt = kb + kStages - 1;
+        if (nxt < nk) {
+            float2* slot = raw + (nxt % kStages) * kRawElems;
+            issue<G::EA>(fa, slot, nxt, klen);
+            issue<G::EB>(fb, slot + BM * BK, nxt, klen);
         }
+        cp_async_commit();
+        cp_async_wait<kStages - 1>();  // this thread's copies of K-block kb have landed
+        const float2* slot = raw + (kb % kStages) * kRawElems;
+        float* sA = planes + (kb & 1) * kPlaneFloats;
+        float* sB = sA + G::A_FLOATS;
+        convert<G::SA, G::EA>(fa, slot, sA);
+        convert<G::SB, G::EB>(fb, slot + BM * BK, sB);
+        // Plane buffer kb&1 was last read in iteration kb-2; this barrier also
+        // orders iteration kb-1's reads before the next iteration's writes.
+        __syncthreads();
         const float* a = sA + tx * G::VA;
         const float* b = sB + ty * G::VB;
 #pragma unroll 2
@@ -230,6 +305,7 @@ __device__ void run_task(const BProblem& p, int tile, int part, float* smem, flo
                 }
         }
     }
+    cp_async_wait<0>();  // only empty groups can remain; keep the count at zero between tasks
 
     // Output (i, j) of this thread: row m0 + (i / VA)*16*VA + tx*VA + i % VA,
     // column n0 + (j / VB)*16*VB + ty*VB + j % VB.
@@ -308,7 +384,9 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(const BProblem* __res
                                                            int* __restrict__ next, float* partials,
                                                            uint32_t* counters)
 {
-    extern __shared__ __align__(16) float smem[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* raw = reinterpret_cast<float2*>(smem_raw);
+    float* planes = reinterpret_cast<float*>(smem_raw + (size_t)kStages * kRawElems * sizeof(float2));
     __shared__ int task_id;
     __shared__ int last_flag;
     for (;;) {
@@ -324,10 +402,12 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(const BProblem* __res
         const BTask tk = tasks[t];
         const BProblem& p = problems[tk.problem];
         switch (p.tile) {
-            case 0: run_task<128, 64>(p, tk.tile, tk.part, smem, partials, counters, &last_flag); break;
-            case 1: run_task<64, 64>(p, tk.tile, tk.part, smem, partials, counters, &last_flag); break;
-            case 2: run_task<64, 32>(p, tk.tile, tk.part, smem, partials, counters, &last_flag); break;
-            default: run_task<32, 32>(p, tk.tile, tk.part, smem, partials, counters, &last_flag); break;
+            case 0: run_task<128, 64>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
+            case 1: run_task<64, 64>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
+            case 2: run_task<128, 32>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
+            case 3: run_task<32, 128>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
+            case 4: run_task<64, 32>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
+            default: run_task<32, 32>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
         }
     }
 }
@@ -368,19 +448,23 @@ struct cg3mBatchPlan {
 
 namespace {
 
-// One candidate table: the largest tile tried first and the cap on K
-// partitions.  A problem steps down to smaller tiles while half a tile would
-// cover it; it is split along K only when one of its tile tasks would exceed
-// a quarter of the batch's average work per SM (the longest task bounds the
-// persistent schedule), keeping >= 128 K terms per partition.
+// One candidate table: the largest tile area allowed and the cap on K
+// partitions.  Each problem takes the allowed tile with the least estimated
+// time -- padded work (tiles x BM x BN x (k + 16)) over the tile's relative
+// FFMA efficiency -- and is split along K only when one of its tile tasks
+// would exceed a quarter of the batch's average work per SM (the longest task
+// bounds the persistent schedule), keeping >= 128 K terms per partition.
 struct Policy {
-    int level;
+    int max_area;
     int split_cap;
 };
 
-constexpr Policy kPolicies[] = {{0, 1}, {0, 2}, {0, 4}, {0, 8}, {1, 1}, {1, 2},
-                                {1, 4}, {1, 8}, {2, 1}, {2, 4}, {2, 8}};
-constexpr Policy kDefaultPolicy = {1, 4};
+constexpr Policy kPolicies[] = {{8192, 1}, {8192, 2}, {8192, 4}, {8192, 8}, {4096, 1},
+                                {4096, 2}, {4096, 4}, {4096, 8}, {2048, 1}, {2048, 4}};
+constexpr Policy kDefaultPolicy = {8192, 4};
+
+// Relative FFMA efficiency of each tile shape (per output-element-term).
+constexpr double kTileEfficiency[kTileCount] = {1.0, 0.85, 0.8, 0.8, 0.65, 0.45};
 
 int span_for(int k, int parts) { return ceil_div(ceil_div(k, 16), parts) * 16; }
 
@@ -388,20 +472,30 @@ void apply_policy(std::vector<BProblem>& ps, const Policy& pol, int sm_count)
 {
     double total = 0.0;
     for (auto& p : ps) {
-        int t = pol.level;
-        while (t < 3 && (p.m <= tile_bm(t) / 2 || p.n <= tile_bn(t) / 2)) {
-            ++t;
+        int best = kTileCount - 1;
+        double best_cost = 1e300;
+        for (int t = 0; t < kTileCount; ++t) {
+            if (tile_bm(t) * tile_bn(t) > pol.max_area) {
+                continue;
+            }
+            const double work = (double)ceil_div(p.m, tile_bm(t)) * ceil_div(p.n, tile_bn(t)) * tile_bm(t) *
+                                tile_bn(t) * (p.k + 16);
+            const double cost = work / kTileEfficiency[t];
+            if (cost < best_cost) {
+                best_cost = cost;
+                best = t;
+            }
         }
-        p.tile = t;
-        p.tiles_m = ceil_div(p.m, tile_bm(t));
-        p.tiles_n = ceil_div(p.n, tile_bn(t));
-        total += (double)p.tiles_m * p.tiles_n * tile_bm(t) * tile_bn(t) * (p.k + 16);
+        p.tile = best;
+        p.tiles_m = ceil_div(p.m, tile_bm(best));
+        p.tiles_n = ceil_div(p.n, tile_bn(best));
+        total += best_cost;
     }
     const double per_sm = total / std::max(sm_count, 1);
     for (auto& p : ps) {
         int parts = 1;
         if (pol.split_cap > 1 && p.k >= 256) {
-            const double task = (double)tile_bm(p.tile) * tile_bn(p.tile) * (p.k + 16);
+            const double task = (double)tile_bm(p.tile) * tile_bn(p.tile) * (p.k + 16) / kTileEfficiency[p.tile];
             const int want = (int)std::ceil(task / (0.25 * per_sm));
             parts = std::max(1, std::min({want, pol.split_cap, p.k / 128}));
         }
@@ -432,7 +526,8 @@ void build_tasks(std::vector<BProblem>& ps, std::vector<BTask>& tasks, size_t* p
             pf += (size_t)p.ppitch * p.n * 2 * p.parts;
             cw += (size_t)p.tiles_m * p.tiles_n;
         }
-        const double cost = (double)tile_bm(p.tile) * tile_bn(p.tile) * ((p.parts > 1 ? p.span : p.k) + 16);
+        const double cost =
+            (double)tile_bm(p.tile) * tile_bn(p.tile) * ((p.parts > 1 ? p.span : p.k) + 16) / kTileEfficiency[p.tile];
         for (int t = 0; t < p.tiles_m * p.tiles_n; ++t) {
             for (int q = 0; q < p.parts; ++q) {
                 v.push_back({cost, BTask{(int)i, t, q, 0}});

@@ -77,6 +77,8 @@ SIGNATURES = {
                       ctypes.POINTER(cg3mCallInfo)],
     "cg3mCgemm3mStridedBatched": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, ctypes.c_int64, _P, _I, ctypes.c_int64, _CP,
                                   _P, _I, ctypes.c_int64, _I],
+    "cg3mCgemm3mHost": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I, ctypes.POINTER(cg3mOptions), _I,
+                        ctypes.POINTER(cg3mCallInfo)],
     "cg3mBatchPlanCreate": [_P, ctypes.POINTER(cg3mProblem), _I, _I, ctypes.POINTER(_P), ctypes.POINTER(_I)],
     "cg3mBatchPlanExecute": [_P, _P, _I],
     "cg3mBatchPlanDestroy": [_P],
@@ -188,6 +190,21 @@ class Handle:
         st = _lib.cg3mCgemm3mEx(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda, ptr(B), ldb,
                                 ctypes.byref(be), ptr(C), ldc, ctypes.byref(opts), ctypes.byref(info))
         _check(st, "cg3mCgemm3mEx")
+        return info.as_dict()
+
+    def cgemm3m_host(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, form="fp32",
+                     rounding="auto", k_partitions=0, tc_segment=0, panels=0):
+        """cg3mCgemm3mHost: A, B, C are HOST buffers (page-locked torch CPU
+        tensors overlap best); copies and panels are pipelined inside the
+        call, which returns with C on the host.  Returns the call info."""
+        al, be = cx(alpha), cx(beta)
+        opts = cg3mOptions(FORM[form] if isinstance(form, str) else form,
+                           ROUNDING[rounding] if isinstance(rounding, str) else rounding, k_partitions, tc_segment)
+        info = cg3mCallInfo()
+        st = _lib.cg3mCgemm3mHost(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), _addr(A), lda,
+                                  _addr(B), ldb, ctypes.byref(be), _addr(C), ldc, ctypes.byref(opts), int(panels),
+                                  ctypes.byref(info))
+        _check(st, "cg3mCgemm3mHost")
         return info.as_dict()
 
     def batch_plan(self, problems, tune=True):

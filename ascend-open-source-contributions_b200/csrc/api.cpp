@@ -4,11 +4,14 @@
 // LaunchComplexGemm (cgemm_host.cpp:701-730) -> LaunchCgemmKernel (:553-587)
 // -> HandleCgemmAlphaZero (:636-663) or LaunchGeneralCgemm (:503-551); handle
 // API cann_ops_blas.h:31-110.  Every launch goes to the handle's stream and
-// nothing here synchronizes except Destroy and GetDeviceStatus.
+// nothing here synchronizes except Destroy, GetDeviceStatus and the
+// host-buffer entry point (which returns with C on the host).
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "../../include/cg3m_aclblas.h"
 #include "cg3m_internal.h"
@@ -242,6 +245,13 @@ cg3mStatus_t cg3mDestroy(cg3mHandle_t h)
         }
         cudaFree(h->default_ws);
         cudaFree(h->status);
+        cudaFree(h->host_arena);
+        if (h->h2d != nullptr) {
+            cudaStreamDestroy(h->h2d);
+        }
+        if (h->d2h != nullptr) {
+            cudaStreamDestroy(h->d2h);
+        }
     }
     delete h;
     return st;
@@ -354,6 +364,167 @@ cg3mStatus_t cg3mCgemm3mStridedBatched(cg3mHandle_t h, cg3mOperation_t transa, c
         }
     }
     return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mCgemm3mHost(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                             const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B, int ldb,
+                             const cg3mComplex* beta, cg3mComplex* C, int ldc, const cg3mOptions* opts, int panels,
+                             cg3mCallInfo* info)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    int action = 0;
+    const cg3mStatus_t st = validate(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, true, &action);
+    if (info != nullptr) {
+        std::memset(info, 0, sizeof(*info));
+    }
+    if (st != CG3M_STATUS_SUCCESS || action == 0) {
+        return st;
+    }
+    cg3mOptions o = opts != nullptr ? *opts : cg3mOptions{};
+    const cg3mStatus_t bs = bind_device(h);
+    if (bs != CG3M_STATUS_SUCCESS) {
+        return bs;
+    }
+    const bool a_normal = transa == CG3M_OP_N || transa == CG3M_OP_R;
+    const bool b_normal = transb == CG3M_OP_N || transb == CG3M_OP_R;
+    const bool beta_zero = beta->real == 0.0f && beta->imag == 0.0f;
+    const bool product = action == 2;
+    // Stored shapes: A is (a_rows x a_cols, lda), B (b_rows x b_cols, ldb).
+    const int a_rows = a_normal ? m : k, a_cols = a_normal ? k : m;
+    const int b_rows = b_normal ? k : n, b_cols = b_normal ? n : k;
+
+    // Panel width: whole output tiles of the whole problem's plan, with the
+    // whole problem's K split for every panel (same bits as one call).
+    int tile_n = 64;
+    if (product) {
+        Problem whole{transa, transb, m, n, k, alpha->real, alpha->imag, beta->real, beta->imag, A, lda, B, ldb, C,
+                      ldc};
+        Plan plan;
+        if (!make_plan(whole, o, h->sm_count, &plan)) {
+            return CG3M_STATUS_INVALID_VALUE;
+        }
+        if (o.k_partitions <= 0) {
+            o.k_partitions = plan.parts;
+        }
+        tile_n = plan.tile_n;
+        if (plan.rounding) {
+            panels = 1;
+        }
+    }
+    if (panels <= 0) {
+        const int per = std::max(tile_n, ceil_div(ceil_div(n, 8), tile_n) * tile_n);
+        panels = ceil_div(n, per);
+    }
+    panels = std::max(1, std::min(panels, n));
+    const int nb = ceil_div(n, panels);
+    panels = ceil_div(n, nb);
+
+    // Device copies with the caller's leading dimensions.
+    const size_t a_elems = product ? (size_t)lda * a_cols : 0;
+    const size_t b_elems = product ? (size_t)ldb * b_cols : 0;
+    const size_t c_elems = (size_t)ldc * n;
+    const size_t a_off = 0, b_off = align_up(a_elems * 8, 256), c_off = b_off + align_up(b_elems * 8, 256);
+    const size_t bytes = c_off + c_elems * 8;
+    if (h->host_arena_bytes < bytes) {
+        cudaFree(h->host_arena);  // synchronizes with work that may still use it
+        h->host_arena = nullptr;
+        h->host_arena_bytes = 0;
+        if (cudaMalloc(&h->host_arena, bytes) != cudaSuccess) {
+            h->host_arena = nullptr;
+            return CG3M_STATUS_ALLOC_FAILED;
+        }
+        h->host_arena_bytes = bytes;
+    }
+    if ((h->h2d == nullptr && cudaStreamCreateWithFlags(&h->h2d, cudaStreamNonBlocking) != cudaSuccess) ||
+        (h->d2h == nullptr && cudaStreamCreateWithFlags(&h->d2h, cudaStreamNonBlocking) != cudaSuccess)) {
+        return CG3M_STATUS_INTERNAL_ERROR;
+    }
+    char* arena = static_cast<char*>(h->host_arena);
+    cg3mComplex* dA = reinterpret_cast<cg3mComplex*>(arena + a_off);
+    cg3mComplex* dB = reinterpret_cast<cg3mComplex*>(arena + b_off);
+    cg3mComplex* dC = reinterpret_cast<cg3mComplex*>(arena + c_off);
+
+    std::vector<cudaEvent_t> ev(2 * (size_t)panels + 2, nullptr);
+    cudaError_t err = cudaSuccess;
+    for (auto& e : ev) {
+        if (err == cudaSuccess) {
+            err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        }
+    }
+    cudaEvent_t ev_start = ev[0], ev_a = ev[1];
+    // Copies start after the handle stream's earlier work (which may read the arena).
+    if (err == cudaSuccess) err = cudaEventRecord(ev_start, h->stream);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(h->h2d, ev_start, 0);
+    if (err == cudaSuccess && product) {
+        err = cudaMemcpy2DAsync(dA, (size_t)lda * 8, A, (size_t)lda * 8, (size_t)a_rows * 8, a_cols,
+                                cudaMemcpyHostToDevice, h->h2d);
+    }
+    if (err == cudaSuccess) err = cudaEventRecord(ev_a, h->h2d);
+    // Uploads of op(B) and C panels, in panel order on the copy-in stream.
+    for (int j = 0; j < panels && err == cudaSuccess; ++j) {
+        const int j0 = j * nb, w = std::min(nb, n - j0);
+        if (product) {
+            if (b_normal) {  // columns j0.. of the stored k x n
+                err = cudaMemcpy2DAsync(dB + (size_t)j0 * ldb, (size_t)ldb * 8, B + (size_t)j0 * ldb, (size_t)ldb * 8,
+                                        (size_t)b_rows * 8, w, cudaMemcpyHostToDevice, h->h2d);
+            } else {  // rows j0.. of the stored n x k
+                err = cudaMemcpy2DAsync(dB + j0, (size_t)ldb * 8, B + j0, (size_t)ldb * 8, (size_t)w * 8, b_cols,
+                                        cudaMemcpyHostToDevice, h->h2d);
+            }
+        }
+        if (err == cudaSuccess && !beta_zero) {
+            err = cudaMemcpy2DAsync(dC + (size_t)j0 * ldc, (size_t)ldc * 8, C + (size_t)j0 * ldc, (size_t)ldc * 8,
+                                    (size_t)m * 8, w, cudaMemcpyHostToDevice, h->h2d);
+        }
+        if (err == cudaSuccess) err = cudaEventRecord(ev[2 + 2 * j], h->h2d);
+    }
+    cg3mStatus_t result = to_status(err);
+    int kernels = 0;
+    for (int j = 0; j < panels && result == CG3M_STATUS_SUCCESS; ++j) {
+        const int j0 = j * nb, w = std::min(nb, n - j0);
+        err = cudaStreamWaitEvent(h->stream, ev_a, 0);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(h->stream, ev[2 + 2 * j], 0);
+        if (err != cudaSuccess) {
+            result = to_status(err);
+            break;
+        }
+        cg3mCallInfo pi{};
+        const cg3mComplex* bj = product ? (b_normal ? dB + (size_t)j0 * ldb : dB + j0) : nullptr;
+        result = run_one(h, transa, transb, m, w, k, alpha, product ? dA : nullptr, lda, bj, ldb, beta,
+                         dC + (size_t)j0 * ldc, ldc, o, true, &pi);
+        if (result != CG3M_STATUS_SUCCESS) {
+            break;
+        }
+        kernels += pi.kernels;
+        if (j == 0 && info != nullptr) {
+            *info = pi;
+        }
+        err = cudaEventRecord(ev[3 + 2 * j], h->stream);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(h->d2h, ev[3 + 2 * j], 0);
+        if (err == cudaSuccess) {
+            err = cudaMemcpy2DAsync(C + (size_t)j0 * ldc, (size_t)ldc * 8, dC + (size_t)j0 * ldc, (size_t)ldc * 8,
+                                    (size_t)m * 8, w, cudaMemcpyDeviceToHost, h->d2h);
+        }
+        result = to_status(err);
+    }
+    // Drain all three streams before returning (also on errors).
+    const cudaError_t s1 = cudaStreamSynchronize(h->h2d);
+    const cudaError_t s2 = cudaStreamSynchronize(h->stream);
+    const cudaError_t s3 = cudaStreamSynchronize(h->d2h);
+    for (auto& e : ev) {
+        if (e != nullptr) {
+            cudaEventDestroy(e);
+        }
+    }
+    if (result == CG3M_STATUS_SUCCESS) {
+        result = to_status(s1 != cudaSuccess ? s1 : s2 != cudaSuccess ? s2 : s3);
+    }
+    if (info != nullptr && result == CG3M_STATUS_SUCCESS) {
+        info->kernels = kernels;  // over all panels
+    }
+    return result;
 }
 
 cg3mStatus_t cg3mSetStageEvents(cg3mHandle_t h, void* const* events, int count)

@@ -22,6 +22,11 @@ struct cg3mContext {
     int* status = nullptr;       // device status word (bounded-wait failures)
     cudaEvent_t stage_events[16] = {};
     int stage_event_count = 0;
+    // host-buffer entry point: device copies of A, B, C and its copy streams
+    void* host_arena = nullptr;
+    size_t host_arena_bytes = 0;
+    cudaStream_t h2d = nullptr;
+    cudaStream_t d2h = nullptr;
 };
 
 namespace cg3m {

@@ -218,6 +218,22 @@ cg3mStatus_t cg3mCgemm3mNoAlloc(void* stream, cg3mOperation_t transa, cg3mOperat
                                 const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B,
                                 int ldb, const cg3mComplex* beta, cg3mComplex* C, int ldc);
 
+/* Host-buffer form (extension): A, B and C live in HOST memory (page-locked
+ * for the copies to overlap).  The call uploads A, streams op(B) and C in
+ * column panels -- panel j+1 uploads while panel j computes on the handle's
+ * stream and panel j-1 downloads -- and returns once all of C is back on the
+ * host.  Every panel is the cg3mCgemm3mEx call on device copies that keep the
+ * caller's leading dimensions, with the K split of the whole problem, so C
+ * holds the bits the device call on the whole problem would give.  When the
+ * rounding-correction pass applies to the whole problem it runs as one panel.
+ * `panels` <= 0 picks the count (about 8 panels of whole tiles); the device
+ * copies are kept in the handle for later calls.  op code R is accepted.
+ * C rows past m (padding) are neither read nor written. */
+cg3mStatus_t cg3mCgemm3mHost(cg3mHandle_t handle, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                             const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B, int ldb,
+                             const cg3mComplex* beta, cg3mComplex* C, int ldc, const cg3mOptions* opts, int panels,
+                             cg3mCallInfo* info);
+
 /* ---- host-only helpers (no device access; usable without a GPU) ---------- */
 
 /* Runs exactly the validation of cg3mCgemm3m (including the quick-return

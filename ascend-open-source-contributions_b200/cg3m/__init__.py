@@ -77,6 +77,8 @@ SIGNATURES = {
                       ctypes.POINTER(cg3mCallInfo)],
     "cg3mCgemm3mStridedBatched": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, ctypes.c_int64, _P, _I, ctypes.c_int64, _CP,
                                   _P, _I, ctypes.c_int64, _I],
+    "cg3mCgemm": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I],
+    "aclblasCgemm": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I],
     "cg3mCgemm3mHost": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I, ctypes.POINTER(cg3mOptions), _I,
                         ctypes.POINTER(cg3mCallInfo)],
     "cg3mBatchPlanCreate": [_P, ctypes.POINTER(cg3mProblem), _I, _I, ctypes.POINTER(_P), ctypes.POINTER(_I)],
@@ -89,6 +91,7 @@ SIGNATURES = {
     "cg3mValidate": [_I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I, _I, ctypes.POINTER(_I)],
     "cg3mPlan": [_I, _I, _I, _I, _I, _CP, _I, _I, _CP, _I, ctypes.POINTER(cg3mOptions), _I,
                  ctypes.POINTER(cg3mCallInfo)],
+    "cg3mPlanOnchip": [_I, _I, _I, _I, _I, _I, ctypes.POINTER(cg3mCallInfo)],
     "cg3mZgemmReference": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I, _P],
     "cg3mErrorReport": [_P, _I, _I, _P, _I, _P, ctypes.POINTER(ctypes.c_double)],
     "aclblasCreate": [ctypes.POINTER(_P)],
@@ -191,6 +194,19 @@ class Handle:
                                 ctypes.byref(be), ptr(C), ldc, ctypes.byref(opts), ctypes.byref(info))
         _check(st, "cg3mCgemm3mEx")
         return info.as_dict()
+
+    def cgemm(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+        """cg3mCgemm (the reference's aclblasCgemm); returns the status."""
+        al, be = cx(alpha), cx(beta)
+        return _lib.cg3mCgemm(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda, ptr(B), ldb,
+                              ctypes.byref(be), ptr(C), ldc)
+
+    def cgemm3m_strided_batched(self, transa, transb, m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC,
+                                batch):
+        """cg3mCgemm3mStridedBatched on device buffers; returns the status."""
+        al, be = cx(alpha), cx(beta)
+        return _lib.cg3mCgemm3mStridedBatched(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A),
+                                              lda, sA, ptr(B), ldb, sB, ctypes.byref(be), ptr(C), ldc, sC, batch)
 
     def cgemm3m_host(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, form="fp32",
                      rounding="auto", k_partitions=0, tc_segment=0, panels=0):
@@ -297,6 +313,13 @@ def plan(transa, transb, m, n, k, alpha=1, beta=0, lda=None, ldb=None, ldc=None,
     info = cg3mCallInfo()
     _check(_lib.cg3mPlan(ta, tb, m, n, k, ctypes.byref(cx(alpha)), lda, ldb, ctypes.byref(cx(beta)), ldc,
                          ctypes.byref(opts), sm_count, ctypes.byref(info)), "cg3mPlan")
+    return info.as_dict()
+
+
+def plan_onchip(m, n, k, mode=0, batch=1, sm_count=148):
+    """The on-chip family's plan (cg3mCgemm / strided batches), host only."""
+    info = cg3mCallInfo()
+    _check(_lib.cg3mPlanOnchip(m, n, k, int(mode), int(batch), int(sm_count), ctypes.byref(info)), "cg3mPlanOnchip")
     return info.as_dict()
 
 

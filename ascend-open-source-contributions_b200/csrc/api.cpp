@@ -354,16 +354,102 @@ cg3mStatus_t cg3mCgemm3mStridedBatched(cg3mHandle_t h, cg3mOperation_t transa, c
     if (st != CG3M_STATUS_SUCCESS || action == 0 || batch_count == 0) {
         return st;
     }
-    const cg3mOptions opts{};
-    for (int i = 0; i < batch_count; ++i) {
-        const cg3mStatus_t r = run_one(h, transa, transb, m, n, k, alpha, A == nullptr ? nullptr : A + i * strideA,
-                                       lda, B == nullptr ? nullptr : B + i * strideB, ldb, beta, C + i * strideC, ldc,
-                                       opts, false, nullptr);
-        if (r != CG3M_STATUS_SUCCESS) {
-            return r;
+    const cg3mStatus_t bs = bind_device(h);
+    if (bs != CG3M_STATUS_SUCCESS) {
+        return bs;
+    }
+    if (action == 1) {  // k == 0 or alpha == 0: beta scaling of every batch, in batch order
+        for (int i = 0; i < batch_count; ++i) {
+            const cudaError_t e = launch_beta_scale(h->stream, m, n, beta->real, beta->imag, C + i * strideC, ldc);
+            if (e != cudaSuccess) {
+                return to_status(e);
+            }
+        }
+        return CG3M_STATUS_SUCCESS;
+    }
+    // The reference runs strided 3M batches on its on-chip kernel with the
+    // non-finite repair (cgemm_host.cpp:749-782, cgemm_compute_kernel.cpp:672-706):
+    // here one persistent launch of the on-chip product family (3M, repair on).
+    // Output batches that overlap (strideC == 0 included) are updated in batch
+    // order, one launch each (blas/gemm/README.md:850-858).
+    const long long span_c = (long long)(n - 1) * ldc + m;
+    const bool overlap = batch_count > 1 && (strideC < 0 ? -strideC : strideC) < span_c;
+    const int per_launch = overlap ? 1 : batch_count;
+    Problem p{transa, transb, m, n, k, alpha->real, alpha->imag, beta->real, beta->imag, A, lda, B, ldb, C, ldc};
+    StridedPlan plan;
+    if (!make_strided_plan(p, 0, per_launch, h->sm_count, &plan)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    void* ws = nullptr;
+    const cg3mStatus_t wst = workspace(h, plan.bytes, &ws);
+    if (wst != CG3M_STATUS_SUCCESS) {
+        return wst;
+    }
+    for (int i = 0; i < batch_count; i += per_launch) {
+        Problem pi = p;
+        pi.A = A + i * strideA;
+        pi.B = B + i * strideB;
+        pi.C = C + i * strideC;
+        const cudaError_t e = launch_strided(h->stream, pi, 0, 1, strideA, strideB, strideC, per_launch, plan, ws,
+                                             h->sm_count);
+        if (e != cudaSuccess) {
+            return to_status(e);
         }
     }
     return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mCgemm(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                       const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B, int ldb,
+                       const cg3mComplex* beta, cg3mComplex* C, int ldc)
+{
+    // aclblasCgemm (cgemm_host.cpp:701-738 with forceThreeProducts = false):
+    // enum errors stay INVALID_ENUM, and A, B must be non-null whenever k > 0
+    // for a non-empty output, alpha == 0 included.
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    auto op_ok = [](int op) { return op == CG3M_OP_N || op == CG3M_OP_T || op == CG3M_OP_C; };
+    if (!op_ok(transa) || !op_ok(transb)) {
+        return CG3M_STATUS_INVALID_ENUM;
+    }
+    int action = 0;
+    const cg3mStatus_t st = validate(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, false, &action);
+    if (st != CG3M_STATUS_SUCCESS) {
+        return st;
+    }
+    if (m == 0 || n == 0) {
+        return CG3M_STATUS_SUCCESS;
+    }
+    if (k > 0 && (A == nullptr || B == nullptr)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (action == 0) {
+        return CG3M_STATUS_SUCCESS;
+    }
+    const cg3mStatus_t bs = bind_device(h);
+    if (bs != CG3M_STATUS_SUCCESS) {
+        return bs;
+    }
+    if (action == 1) {
+        return to_status(launch_beta_scale(h->stream, m, n, beta->real, beta->imag, C, ldc));
+    }
+    // Unit outputs (alpha = 1, beta = 0) take three products with the
+    // non-finite repair, as the reference's cgemm does (cgemm_host.cpp:239-241,
+    // 444-453); general alpha/beta take four real products.
+    const bool unit = alpha->real == 1.0f && alpha->imag == 0.0f && beta->real == 0.0f && beta->imag == 0.0f;
+    const int mode = unit ? 0 : 1;
+    Problem p{transa, transb, m, n, k, alpha->real, alpha->imag, beta->real, beta->imag, A, lda, B, ldb, C, ldc};
+    StridedPlan plan;
+    if (!make_strided_plan(p, mode, 1, h->sm_count, &plan)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    void* ws = nullptr;
+    const cg3mStatus_t wst = workspace(h, plan.bytes, &ws);
+    if (wst != CG3M_STATUS_SUCCESS) {
+        return wst;
+    }
+    return to_status(launch_strided(h->stream, p, mode, unit ? 1 : 0, 0, 0, 0, 1, plan, ws, h->sm_count));
 }
 
 cg3mStatus_t cg3mCgemm3mHost(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
@@ -606,6 +692,27 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
     return CG3M_STATUS_SUCCESS;
 }
 
+cg3mStatus_t cg3mPlanOnchip(int m, int n, int k, int mode, int batch, int sm_count, cg3mCallInfo* info)
+{
+    if (info == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    Problem p{CG3M_OP_N, CG3M_OP_N, m, n, k, 1.0f, 0.0f, 0.0f, 0.0f, nullptr, m, nullptr, k, nullptr, m};
+    StridedPlan plan;
+    if (!make_strided_plan(p, mode, batch, sm_count > 0 ? sm_count : 148, &plan)) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    std::memset(info, 0, sizeof(*info));
+    info->path = plan.parts > 1 ? 3 : 2;
+    info->tile_m = plan.tile_m;
+    info->tile_n = plan.tile_n;
+    info->k_partitions = plan.parts;
+    info->k_span = plan.span;
+    info->kernels = 1;
+    info->workspace_bytes = plan.bytes;
+    return CG3M_STATUS_SUCCESS;
+}
+
 cg3mStatus_t cg3mZgemmReference(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
                                 const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B,
                                 int ldb, const cg3mComplex* beta, const cg3mComplex* C, int ldc, void* out64)
@@ -679,6 +786,13 @@ aclblasStatus_t aclblasSetWorkspace(aclblasHandle_t handle, void* workspace, siz
     return cg3mSetWorkspace(handle, workspace, bytes);
 }
 aclblasStatus_t aclblasGetVersion(aclblasHandle_t handle, int* version) { return cg3mGetVersion(handle, version); }
+
+aclblasStatus_t aclblasCgemm(aclblasHandle_t handle, aclblasOperation_t transa, aclblasOperation_t transb, int m,
+                             int n, int k, const aclblasComplex* alpha, const aclblasComplex* A, int lda,
+                             const aclblasComplex* B, int ldb, const aclblasComplex* beta, aclblasComplex* C, int ldc)
+{
+    return cg3mCgemm(handle, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
 
 aclblasStatus_t aclblasCgemm3m(aclblasHandle_t handle, aclblasOperation_t transa, aclblasOperation_t transb, int m,
                                int n, int k, const aclblasComplex* alpha, const aclblasComplex* A, int lda,

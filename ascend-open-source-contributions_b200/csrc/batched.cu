@@ -47,6 +47,16 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int BK = 16;
+#ifndef CG3M_BATCH_UNROLL
+#define CG3M_BATCH_UNROLL 4
+#endif
+constexpr int kUnroll = CG3M_BATCH_UNROLL;  // K terms unrolled in the FFMA loop
+
+// Product modes: the standard 3M identity (P0 = Ar.Br, P1 = Ai.Bi,
+// P2 = (Ar+Ai).(Br+Bi); Re = P0 - P1, Im = (P2 - P0) - P1) or four real
+// products (Re = Ar.Br - Ai.Bi, Im = Ar.Bi + Ai.Br).
+constexpr int kMode3M = 0;
+constexpr int kMode4M = 1;
 
 struct BProblem {
     int ta, tb, m, n, k;  // k = 0: beta-scale only (k == 0 or alpha == 0)
@@ -55,7 +65,8 @@ struct BProblem {
     const float2* B;
     float2* C;
     int lda, ldb, ldc;
-    int tile;  // index into the tile shapes below
+    int tile;    // index into the tile shapes below
+    int repair;  // recompute non-finite products with explicit FP32 four-product terms
     int parts, span, tiles_m, tiles_n, ppitch;
     size_t partial_off;  // floats into the partial arena
     size_t counter_off;  // words into the tile counters
@@ -66,6 +77,7 @@ struct BTask {
 };
 
 // Tile shapes (BM x BN): 0: 128x64, 1: 64x64, 2: 128x32, 3: 32x128, 4: 64x32, 5: 32x32.
+// The four-product mode does not use tile 0 (its accumulators would not fit).
 constexpr int kTileCount = 6;
 __host__ __device__ constexpr int tile_bm(int t)
 {
@@ -76,14 +88,16 @@ __host__ __device__ constexpr int tile_bn(int t)
     return t == 3 ? 128 : (t == 0 || t == 1) ? 64 : 32;
 }
 
-template <int BM, int BN>
+template <int BM, int BN, int MODE>
 struct Cfg {
     static constexpr int MT = BM / 16, NT = BN / 16;  // outputs per thread along m, n
     static constexpr int VA = MT >= 4 ? 4 : MT, HA = MT / VA;
     static constexpr int VB = NT >= 4 ? 4 : NT, HB = NT / VB;
     static constexpr int SA = BM + 4, SB = BN + 4;  // padded plane strides (floats)
     static constexpr int EA = BM * BK / kThreads, EB = BN * BK / kThreads;  // elements per thread per K-block
-    static constexpr int A_FLOATS = 3 * BK * SA, B_FLOATS = 3 * BK * SB;
+    static constexpr int COMPS = MODE == kMode3M ? 3 : 2;                      // planes per operand
+    static constexpr int A_FLOATS = COMPS * BK * SA, B_FLOATS = COMPS * BK * SB;
+    static constexpr int ACC = MODE == kMode3M ? 3 : 4;                        // accumulators per output
 };
 
 // Shared memory: kStages raw stages of interleaved complex elements (as
@@ -116,12 +130,12 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 struct Feed {
     const float2* origin;  // the matrix (source of the zero-byte copies)
     const float2* base;    // element q = 0 at K-block 0
-    long long qstep;     // element offset between consecutive q
-    long long kbstep;    // element offset between consecutive K-blocks
-    int r, kk;           // block coordinates of element q = 0
-    int rq, kq;          // coordinate steps between consecutive q
-    int rows;            // valid rows of this tile
-    float conj;          // -1 for op C / R
+    long long qstep;       // element offset between consecutive q
+    long long kbstep;      // element offset between consecutive K-blocks
+    int r, kk;             // block coordinates of element q = 0
+    int rq, kq;            // coordinate steps between consecutive q
+    int rows;              // valid rows of this tile
+    float conj;            // -1 for op C / R
 };
 
 template <int R>
@@ -153,8 +167,8 @@ __device__ __forceinline__ Feed make_feed(const float2* X, int ld, bool rows_con
     return f;
 }
 
-// Issue this thread's copies of K-block kb (global K index k0 = kbeg + kb*BK)
-// into raw slot `raw`; elements past the tile or past kend read as zero.
+// Issue this thread's copies of K-block kb into raw slot `raw`; elements past
+// the tile or past the partition's K range read as zero.
 template <int E>
 __device__ __forceinline__ void issue(const Feed& f, float2* raw, int kb, int krel_end)
 {
@@ -164,14 +178,14 @@ __device__ __forceinline__ void issue(const Feed& f, float2* raw, int kb, int kr
         const int r = f.r + q * f.rq;
         const int kk = kb * BK + f.kk + q * f.kq;
         const bool ok = r < f.rows && kk < krel_end;
-        cp_async8(smem_u32(raw + threadIdx.x + q * kThreads), ok ? (const void*)(src + q * f.qstep) : (const void*)f.origin,
-                  ok ? 8 : 0);
+        cp_async8(smem_u32(raw + threadIdx.x + q * kThreads),
+                  ok ? (const void*)(src + q * f.qstep) : (const void*)f.origin, ok ? 8 : 0);
     }
 }
 
 // Convert this thread's own elements of a raw slot into the planes
-// re, im (conjugated), fl(re + im) at dst[(c*BK + kk)*S + r].
-template <int S, int E>
+// re, im (conjugated) [, fl(re + im) for 3M] at dst[(c*BK + kk)*S + r].
+template <int S, int E, int COMPS>
 __device__ __forceinline__ void convert(const Feed& f, const float2* raw, float* dst)
 {
 #pragma unroll
@@ -182,7 +196,9 @@ __device__ __forceinline__ void convert(const Feed& f, const float2* raw, float*
         const int kk = f.kk + q * f.kq;
         dst[(0 * BK + kk) * S + r] = re;
         dst[(1 * BK + kk) * S + r] = im;
-        dst[(2 * BK + kk) * S + r] = __fadd_rn(re, im);
+        if constexpr (COMPS == 3) {
+            dst[(2 * BK + kk) * S + r] = __fadd_rn(re, im);
+        }
     }
 }
 
@@ -215,11 +231,48 @@ __device__ __forceinline__ float2 beta_scaled(const EpiParams& e, const float2* 
                        __fadd_rn(__fmul_rn(e.br, c.y), __fmul_rn(e.bi, c.x)));
 }
 
-template <int BM, int BN>
+// Non-finite repair (RepairNonFiniteOutput, cgemm_compute_kernel.cpp:672-706):
+// the product op(A)(row, :) . op(B)(:, col) recomputed over the whole K in
+// increasing order with each FP32 product materialised (rr, ii, ri, ir) and
+// re += rr - ii, im += ri + ir, one rounding per operation.  A 3M product that
+// overflowed before cancelling gets the four-product value scalar BLAS gives.
+__device__ float2 repair_product(const BProblem& p, int row, int col)
+{
+    const bool na = p.ta == CG3M_OP_N || p.ta == CG3M_OP_R;
+    const bool nb = p.tb == CG3M_OP_N || p.tb == CG3M_OP_R;
+    const float ca = (p.ta == CG3M_OP_C || p.ta == CG3M_OP_R) ? -1.0f : 1.0f;
+    const float cb = (p.tb == CG3M_OP_C || p.tb == CG3M_OP_R) ? -1.0f : 1.0f;
+    float re = 0.0f, im = 0.0f;
+    for (int k = 0; k < p.k; ++k) {
+        const float2 a = p.A[na ? (size_t)row + (size_t)k * p.lda : (size_t)k + (size_t)row * p.lda];
+        const float2 b = p.B[nb ? (size_t)k + (size_t)col * p.ldb : (size_t)col + (size_t)k * p.ldb];
+        const float av = a.y * ca, bv = b.y * cb;
+        const float rr = __fmul_rn(a.x, b.x), ii = __fmul_rn(av, bv);
+        const float ri = __fmul_rn(a.x, bv), ir = __fmul_rn(av, b.x);
+        re = __fadd_rn(re, __fsub_rn(rr, ii));
+        im = __fadd_rn(im, __fadd_rn(ri, ir));
+    }
+    return make_float2(re, im);
+}
+
+// Partition product (before alpha/beta) of the accumulators of one output.
+template <int MODE>
+__device__ __forceinline__ float2 part_product(float q0, float q1, float q2, float q3)
+{
+    if constexpr (MODE == kMode3M) {
+        return make_float2(__fsub_rn(q0, q1), __fsub_rn(__fsub_rn(q2, q0), q1));
+    } else {
+        return make_float2(__fsub_rn(q0, q1), __fadd_rn(q2, q3));
+    }
+}
+
+__device__ __forceinline__ bool finite2(float2 v) { return isfinite(v.x) && isfinite(v.y); }
+
+template <int BM, int BN, int MODE>
 __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, float* planes, float* partials,
                          uint32_t* counters, int* last_flag)
 {
-    using G = Cfg<BM, BN>;
+    using G = Cfg<BM, BN, MODE>;
     static_assert(G::A_FLOATS + G::B_FLOATS <= kPlaneFloats, "planes exceed their buffer");
     static_assert((BM + BN) * BK <= kRawElems, "raw stage exceeds its slot");
     static_assert((BM * BK) % kThreads == 0 && (BN * BK) % kThreads == 0, "whole elements per thread");
@@ -230,7 +283,11 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
     const int kend = min(p.k, kbeg + p.span);
     const int klen = kend > kbeg ? kend - kbeg : 0;
     const int nk = (klen + BK - 1) / BK;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    // 16 x 16 threads over the tile; each warp is 8 (along m) x 4 (along n)
+    // threads, so one vector load of A or B per warp spans at most 128 bytes
+    // (one shared-memory wavefront).
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tx = (warp & 1) * 8 + (lane & 7), ty = (warp >> 1) * 4 + (lane >> 3);
     const bool na = p.ta == CG3M_OP_N || p.ta == CG3M_OP_R;
     const bool nb = p.tb == CG3M_OP_N || p.tb == CG3M_OP_R;
     const Feed fa = make_feed<BM>(p.A, p.lda, na, m0, min(BM, p.m - m0), kbeg,
@@ -238,15 +295,15 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
     const Feed fb = make_feed<BN>(p.B, p.ldb, !nb, n0, min(BN, p.n - n0), kbeg,
                                   (p.tb == CG3M_OP_C || p.tb == CG3M_OP_R) ? -1.0f : 1.0f);
 
-    float p0[G::MT][G::NT], p1[G::MT][G::NT], p2[G::MT][G::NT];
+    float acc[G::ACC][G::MT][G::NT];
 #pragma unroll
-    for (int i = 0; i < G::MT; ++i)
+    for (int c = 0; c < G::ACC; ++c)
 #pragma unroll
-        for (int j = 0; j < G::NT; ++j) {
-            p0[i][j] = 0.0f;
-            p1[i][j] = 0.0f;
-            p2[i][j] = 0.0f;
-        }
+        for (int i = 0; i < G::MT; ++i)
+#pragma unroll
+            for (int j = 0; j < G::NT; ++j) {
+                acc[c][i][j] = 0.0f;
+            }
 
     // Prologue: K-blocks 0 .. kStages-2 in flight (one commit group each,
     // empty groups past the end keep the counting uniform).
@@ -273,35 +330,41 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
         const float2* slot = raw + (kb % kStages) * kRawElems;
         float* sA = planes + (kb & 1) * kPlaneFloats;
         float* sB = sA + G::A_FLOATS;
-        convert<G::SA, G::EA>(fa, slot, sA);
-        convert<G::SB, G::EB>(fb, slot + BM * BK, sB);
+        convert<G::SA, G::EA, G::COMPS>(fa, slot, sA);
+        convert<G::SB, G::EB, G::COMPS>(fb, slot + BM * BK, sB);
         // Plane buffer kb&1 was last read in iteration kb-2; this barrier also
         // orders iteration kb-1's reads before the next iteration's writes.
         __syncthreads();
         const float* a = sA + tx * G::VA;
         const float* b = sB + ty * G::VB;
-#pragma unroll 2
+#pragma unroll kUnroll
         for (int kk = 0; kk < BK; ++kk) {
-            float x0[G::MT], x1[G::MT], x2[G::MT], y0[G::NT], y1[G::NT], y2[G::NT];
+            float x[G::COMPS][G::MT], y[G::COMPS][G::NT];
 #pragma unroll
-            for (int h = 0; h < G::HA; ++h) {
-                ld_vec<G::VA>(a + (0 * BK + kk) * G::SA + h * 16 * G::VA, x0 + h * G::VA);
-                ld_vec<G::VA>(a + (1 * BK + kk) * G::SA + h * 16 * G::VA, x1 + h * G::VA);
-                ld_vec<G::VA>(a + (2 * BK + kk) * G::SA + h * 16 * G::VA, x2 + h * G::VA);
-            }
+            for (int c = 0; c < G::COMPS; ++c) {
 #pragma unroll
-            for (int h = 0; h < G::HB; ++h) {
-                ld_vec<G::VB>(b + (0 * BK + kk) * G::SB + h * 16 * G::VB, y0 + h * G::VB);
-                ld_vec<G::VB>(b + (1 * BK + kk) * G::SB + h * 16 * G::VB, y1 + h * G::VB);
-                ld_vec<G::VB>(b + (2 * BK + kk) * G::SB + h * 16 * G::VB, y2 + h * G::VB);
+                for (int h = 0; h < G::HA; ++h) {
+                    ld_vec<G::VA>(a + (c * BK + kk) * G::SA + h * 16 * G::VA, x[c] + h * G::VA);
+                }
+#pragma unroll
+                for (int h = 0; h < G::HB; ++h) {
+                    ld_vec<G::VB>(b + (c * BK + kk) * G::SB + h * 16 * G::VB, y[c] + h * G::VB);
+                }
             }
 #pragma unroll
             for (int i = 0; i < G::MT; ++i)
 #pragma unroll
                 for (int j = 0; j < G::NT; ++j) {
-                    p0[i][j] = __fmaf_rn(x0[i], y0[j], p0[i][j]);
-                    p1[i][j] = __fmaf_rn(x1[i], y1[j], p1[i][j]);
-                    p2[i][j] = __fmaf_rn(x2[i], y2[j], p2[i][j]);
+                    if constexpr (MODE == kMode3M) {
+                        acc[0][i][j] = __fmaf_rn(x[0][i], y[0][j], acc[0][i][j]);
+                        acc[1][i][j] = __fmaf_rn(x[1][i], y[1][j], acc[1][i][j]);
+                        acc[2][i][j] = __fmaf_rn(x[2][i], y[2][j], acc[2][i][j]);
+                    } else {
+                        acc[0][i][j] = __fmaf_rn(x[0][i], y[0][j], acc[0][i][j]);  // Ar.Br
+                        acc[1][i][j] = __fmaf_rn(x[1][i], y[1][j], acc[1][i][j]);  // Ai.Bi
+                        acc[2][i][j] = __fmaf_rn(x[0][i], y[1][j], acc[2][i][j]);  // Ar.Bi
+                        acc[3][i][j] = __fmaf_rn(x[1][i], y[0][j], acc[3][i][j]);  // Ai.Br
+                    }
                 }
         }
     }
@@ -321,9 +384,12 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
                     if (p.k == 0) {
                         *cp = beta_scaled(p.epi, cp);
                     } else {
-                        const float re = __fsub_rn(p0[i][j], p1[i][j]);
-                        const float im = __fsub_rn(__fsub_rn(p2[i][j], p0[i][j]), p1[i][j]);
-                        *cp = epilogue_value(re, im, p.epi, cp);
+                        float2 v = part_product<MODE>(acc[0][i][j], acc[1][i][j], acc[2][i][j],
+                                                      acc[G::ACC - 1][i][j]);
+                        if (p.repair && !finite2(v)) {
+                            v = repair_product(p, row, col);
+                        }
+                        *cp = epilogue_value(v.x, v.y, p.epi, cp);
                     }
                 }
             }
@@ -342,8 +408,9 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
             const int row = m0 + (i / G::VA) * 16 * G::VA + tx * G::VA + i % G::VA;
             if (row < p.m && col < p.n) {
                 const size_t o = (size_t)col * p.ppitch + row;
-                __stcg(base + (size_t)(2 * part) * plane + o, __fsub_rn(p0[i][j], p1[i][j]));
-                __stcg(base + (size_t)(2 * part + 1) * plane + o, __fsub_rn(__fsub_rn(p2[i][j], p0[i][j]), p1[i][j]));
+                const float2 v = part_product<MODE>(acc[0][i][j], acc[1][i][j], acc[2][i][j], acc[G::ACC - 1][i][j]);
+                __stcg(base + (size_t)(2 * part) * plane + o, v.x);
+                __stcg(base + (size_t)(2 * part + 1) * plane + o, v.y);
             }
         }
     }
@@ -373,12 +440,35 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
                 re = __fadd_rn(re, __ldcg(base + (size_t)(2 * q) * plane + o));
                 im = __fadd_rn(im, __ldcg(base + (size_t)(2 * q + 1) * plane + o));
             }
+            float2 v = make_float2(re, im);
+            if (p.repair && !finite2(v)) {
+                v = repair_product(p, row, col);
+            }
             float2* cp = p.C + (size_t)col * p.ldc + row;
-            *cp = epilogue_value(re, im, p.epi, cp);
+            *cp = epilogue_value(v.x, v.y, p.epi, cp);
         }
     }
 }
 
+template <int MODE>
+__device__ __forceinline__ void dispatch_task(const BProblem& p, int tile, int part, float2* raw, float* planes,
+                                              float* partials, uint32_t* counters, int* last_flag)
+{
+    switch (p.tile) {
+        case 0:
+            if constexpr (MODE == kMode3M) {
+                run_task<128, 64, MODE>(p, tile, part, raw, planes, partials, counters, last_flag);
+            }
+            break;
+        case 1: run_task<64, 64, MODE>(p, tile, part, raw, planes, partials, counters, last_flag); break;
+        case 2: run_task<128, 32, MODE>(p, tile, part, raw, planes, partials, counters, last_flag); break;
+        case 3: run_task<32, 128, MODE>(p, tile, part, raw, planes, partials, counters, last_flag); break;
+        case 4: run_task<64, 32, MODE>(p, tile, part, raw, planes, partials, counters, last_flag); break;
+        default: run_task<32, 32, MODE>(p, tile, part, raw, planes, partials, counters, last_flag); break;
+    }
+}
+
+// Heterogeneous batch: tasks from a device list (problem, tile, partition).
 __global__ void __launch_bounds__(kThreads) batched_kernel(const BProblem* __restrict__ problems,
                                                            const BTask* __restrict__ tasks, int ntasks,
                                                            int* __restrict__ next, float* partials,
@@ -400,15 +490,45 @@ __global__ void __launch_bounds__(kThreads) batched_kernel(const BProblem* __res
             return;
         }
         const BTask tk = tasks[t];
-        const BProblem& p = problems[tk.problem];
-        switch (p.tile) {
-            case 0: run_task<128, 64>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
-            case 1: run_task<64, 64>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
-            case 2: run_task<128, 32>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
-            case 3: run_task<32, 128>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
-            case 4: run_task<64, 32>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
-            default: run_task<32, 32>(p, tk.tile, tk.part, raw, planes, partials, counters, &last_flag); break;
+        dispatch_task<kMode3M>(problems[tk.problem], tk.tile, tk.part, raw, planes, partials, counters, &last_flag);
+    }
+}
+
+// Strided batch (and single problems): batch b's problem is `proto` with
+// A + b*sA, B + b*sB, C + b*sC and its own partial / counter ranges; task t
+// is (b, tile, part) = (t / per_batch, (t % per_batch) / parts, t % parts).
+// counters[0] is the task counter; tile counters follow.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) strided_kernel(BProblem proto, long long sA, long long sB, long long sC,
+                                                           int batch, size_t partial_stride, float* partials,
+                                                           uint32_t* counters)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* raw = reinterpret_cast<float2*>(smem_raw);
+    float* planes = reinterpret_cast<float*>(smem_raw + (size_t)kStages * kRawElems * sizeof(float2));
+    __shared__ int task_id;
+    __shared__ int last_flag;
+    const int tiles = proto.tiles_m * proto.tiles_n;
+    const int per_batch = tiles * proto.parts;
+    const long long ntasks = (long long)per_batch * batch;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            task_id = (int)atomicAdd(counters, 1u);
         }
+        __syncthreads();
+        const int t = task_id;
+        if (t >= ntasks) {
+            return;
+        }
+        const int b = t / per_batch, r = t - b * per_batch;
+        BProblem p = proto;
+        p.A = proto.A + (long long)b * sA;
+        p.B = proto.B + (long long)b * sB;
+        p.C = proto.C + (long long)b * sC;
+        p.partial_off = (size_t)b * partial_stride;
+        p.counter_off = 1 + (size_t)b * tiles;
+        dispatch_task<MODE>(p, r / proto.parts, r % proto.parts, raw, planes, partials, counters, &last_flag);
     }
 }
 
@@ -468,46 +588,59 @@ constexpr double kTileEfficiency[kTileCount] = {1.0, 0.85, 0.8, 0.8, 0.65, 0.45}
 
 int span_for(int k, int parts) { return ceil_div(ceil_div(k, 16), parts) * 16; }
 
+// The allowed tile with the least estimated time for p; returns that time
+// (padded work over efficiency) and sets tile, tiles_m, tiles_n.
+double choose_tile(BProblem& p, int max_area, int mode)
+{
+    int best = kTileCount - 1;
+    double best_cost = 1e300;
+    for (int t = 0; t < kTileCount; ++t) {
+        if (tile_bm(t) * tile_bn(t) > max_area || (mode == kMode4M && t == 0)) {
+            continue;
+        }
+        const double work =
+            (double)ceil_div(p.m, tile_bm(t)) * ceil_div(p.n, tile_bn(t)) * tile_bm(t) * tile_bn(t) * (p.k + 16);
+        const double cost = work / kTileEfficiency[t];
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = t;
+        }
+    }
+    p.tile = best;
+    p.tiles_m = ceil_div(p.m, tile_bm(best));
+    p.tiles_n = ceil_div(p.n, tile_bn(best));
+    return best_cost;
+}
+
+// K partitions of p given the schedule's average work per SM.
+void choose_parts(BProblem& p, int split_cap, double per_sm)
+{
+    int parts = 1;
+    if (split_cap > 1 && p.k >= 256) {
+        const double task = (double)tile_bm(p.tile) * tile_bn(p.tile) * (p.k + 16) / kTileEfficiency[p.tile];
+        const int want = (int)std::ceil(task / (0.25 * per_sm));
+        parts = std::max(1, std::min({want, split_cap, p.k / 128}));
+    }
+    p.parts = parts;
+    p.span = span_for(p.k, parts);
+    while (p.parts > 1 && (p.parts - 1) * p.span >= p.k) {
+        --p.parts;
+        p.span = span_for(p.k, p.parts);
+    }
+    if (p.parts == 1) {
+        p.span = p.k;
+    }
+}
+
 void apply_policy(std::vector<BProblem>& ps, const Policy& pol, int sm_count)
 {
     double total = 0.0;
     for (auto& p : ps) {
-        int best = kTileCount - 1;
-        double best_cost = 1e300;
-        for (int t = 0; t < kTileCount; ++t) {
-            if (tile_bm(t) * tile_bn(t) > pol.max_area) {
-                continue;
-            }
-            const double work = (double)ceil_div(p.m, tile_bm(t)) * ceil_div(p.n, tile_bn(t)) * tile_bm(t) *
-                                tile_bn(t) * (p.k + 16);
-            const double cost = work / kTileEfficiency[t];
-            if (cost < best_cost) {
-                best_cost = cost;
-                best = t;
-            }
-        }
-        p.tile = best;
-        p.tiles_m = ceil_div(p.m, tile_bm(best));
-        p.tiles_n = ceil_div(p.n, tile_bn(best));
-        total += best_cost;
+        total += choose_tile(p, pol.max_area, kMode3M);
     }
     const double per_sm = total / std::max(sm_count, 1);
     for (auto& p : ps) {
-        int parts = 1;
-        if (pol.split_cap > 1 && p.k >= 256) {
-            const double task = (double)tile_bm(p.tile) * tile_bn(p.tile) * (p.k + 16) / kTileEfficiency[p.tile];
-            const int want = (int)std::ceil(task / (0.25 * per_sm));
-            parts = std::max(1, std::min({want, pol.split_cap, p.k / 128}));
-        }
-        p.parts = parts;
-        p.span = span_for(p.k, parts);
-        while (p.parts > 1 && (p.parts - 1) * p.span >= p.k) {
-            --p.parts;
-            p.span = span_for(p.k, p.parts);
-        }
-        if (p.parts == 1) {
-            p.span = p.k;
-        }
+        choose_parts(p, pol.split_cap, per_sm);
     }
 }
 
@@ -676,6 +809,88 @@ Policy autotune(cg3mBatchPlan* plan, cudaStream_t s)
 }
 
 }  // namespace
+
+namespace cg3m {
+
+bool make_strided_plan(const Problem& p, int mode, int batch, int sm_count, StridedPlan* out)
+{
+    if (batch <= 0 || p.m <= 0 || p.n <= 0 || p.k <= 0 || (mode != kMode3M && mode != kMode4M)) {
+        return false;
+    }
+    BProblem bp{};
+    bp.m = p.m;
+    bp.n = p.n;
+    bp.k = p.k;
+    const double one = choose_tile(bp, 8192, mode);
+    choose_parts(bp, 4, one * batch / std::max(sm_count, 1));
+    StridedPlan pl{};
+    pl.tile = bp.tile;
+    pl.tile_m = tile_bm(bp.tile);
+    pl.tile_n = tile_bn(bp.tile);
+    pl.parts = bp.parts;
+    pl.span = bp.span;
+    pl.tiles = bp.tiles_m * bp.tiles_n;
+    pl.ppitch = (int)align_up((size_t)p.m, 32);
+    pl.partial_stride = bp.parts > 1 ? (size_t)pl.ppitch * p.n * 2 * bp.parts : 0;
+    pl.counters = 1 + (size_t)batch * pl.tiles;
+    pl.partial_off = align_up(pl.counters * sizeof(uint32_t), 256);
+    pl.bytes = pl.partial_off + (size_t)batch * pl.partial_stride * sizeof(float);
+    *out = pl;
+    return true;
+}
+
+cudaError_t launch_strided(cudaStream_t s, const Problem& p, int mode, int repair, long long sA, long long sB,
+                           long long sC, int batch, const StridedPlan& plan, void* ws, int sm_count)
+{
+    BProblem proto{};
+    proto.ta = p.transa;
+    proto.tb = p.transb;
+    proto.m = p.m;
+    proto.n = p.n;
+    proto.k = p.k;
+    const bool beta_zero = p.br == 0.0f && p.bi == 0.0f;
+    const bool unit = p.ar == 1.0f && p.ai == 0.0f && beta_zero;
+    proto.epi = EpiParams{p.ar, p.ai, p.br, p.bi, unit ? 1 : 0, beta_zero ? 1 : 0};
+    proto.A = static_cast<const float2*>(p.A);
+    proto.B = static_cast<const float2*>(p.B);
+    proto.C = static_cast<float2*>(p.C);
+    proto.lda = p.lda;
+    proto.ldb = p.ldb;
+    proto.ldc = p.ldc;
+    proto.tile = plan.tile;
+    proto.repair = repair;
+    proto.parts = plan.parts;
+    proto.span = plan.span;
+    proto.tiles_m = ceil_div(p.m, plan.tile_m);
+    proto.tiles_n = ceil_div(p.n, plan.tile_n);
+    proto.ppitch = plan.ppitch;
+    uint32_t* counters = static_cast<uint32_t*>(ws);
+    float* partials = reinterpret_cast<float*>(static_cast<char*>(ws) + plan.partial_off);
+    cudaError_t e = cudaMemsetAsync(counters, 0, plan.counters * sizeof(uint32_t), s);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    const long long ntasks = (long long)plan.tiles * plan.parts * batch;
+    const int grid = (int)std::min<long long>(ntasks, (long long)std::max(sm_count, 1));
+    if (mode == kMode3M) {
+        e = cudaFuncSetAttribute(strided_kernel<kMode3M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSmemBytes);
+        if (e == cudaSuccess) {
+            strided_kernel<kMode3M><<<grid, kThreads, kSmemBytes, s>>>(proto, sA, sB, sC, batch, plan.partial_stride,
+                                                                       partials, counters);
+        }
+    } else {
+        e = cudaFuncSetAttribute(strided_kernel<kMode4M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSmemBytes);
+        if (e == cudaSuccess) {
+            strided_kernel<kMode4M><<<grid, kThreads, kSmemBytes, s>>>(proto, sA, sB, sC, batch, plan.partial_stride,
+                                                                       partials, counters);
+        }
+    }
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+}  // namespace cg3m
 
 extern "C" {
 

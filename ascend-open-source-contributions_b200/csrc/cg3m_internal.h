@@ -97,6 +97,22 @@ cudaError_t launch_zgemm_ref(cudaStream_t s, const Problem& p, const void* Cin, 
 cudaError_t launch_error_report(cudaStream_t s, int m, int n, const void* C, int ldc, const void* out64,
                                 double* dev_report);
 
+// On-chip product family (batched.cu): op() applied while staging the
+// caller's interleaved matrices, no pack pass.  mode 0 = standard 3M, 1 = four
+// real products; `repair` recomputes non-finite products with explicit FP32
+// four-product terms.  One launch covers `batch` problems at element strides
+// sA, sB, sC (a single problem is batch 1).
+struct StridedPlan {
+    int tile = 0, tile_m = 0, tile_n = 0, parts = 1, span = 0, tiles = 0, ppitch = 0;
+    size_t partial_stride = 0;  // floats of partials per batch
+    size_t counters = 0;        // task counter + tile counters (uint32)
+    size_t partial_off = 0;     // byte offset of the partials in the workspace
+    size_t bytes = 0;           // workspace bytes
+};
+bool make_strided_plan(const Problem& p, int mode, int batch, int sm_count, StridedPlan* out);
+cudaError_t launch_strided(cudaStream_t s, const Problem& p, int mode, int repair, long long sA, long long sB,
+                           long long sC, int batch, const StridedPlan& plan, void* ws, int sm_count);
+
 // Enqueue a fully planned call (pack + GEMM [+ merge] [+ rounding]); when
 // `events` is non-null, events[0] is recorded before the first launch and
 // events[i] after the i-th (i < nevents).

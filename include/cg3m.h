@@ -10,7 +10,8 @@
  *   - A, B, C are column-major complex64 arrays in device memory owned by the
  *     caller; alpha and beta are host pointers read during the call.
  *   - Work is enqueued asynchronously on the handle's stream; no entry point
- *     synchronizes except cg3mDestroy and cg3mGetDeviceStatus.
+ *     synchronizes except cg3mDestroy, cg3mGetDeviceStatus, the batch-plan
+ *     calls and the host-buffer cg3mCgemm3mHost.
  *   - One handle must not be used by several host threads at once (its
  *     workspace is shared by every call made through it).
  *   - C must not alias A or B.  Padding rows [m, ldc) of C are never written.
@@ -148,7 +149,20 @@ cg3mStatus_t cg3mCgemm3mEx(cg3mHandle_t handle, cg3mOperation_t transa, cg3mOper
  * blas/gemm/README.md:809-907): C_i = alpha*op(A_i)*op(B_i) + beta*C_i with
  * X_i = X + i*strideX (complex elements, zero or negative allowed); when
  * output batches overlap (strideC==0 included) they are updated in batch
- * order.  Statuses as the reference's strided API: bad enum -> INVALID_ENUM. */
+ * order.  Statuses as the reference's strided API: bad enum -> INVALID_ENUM.
+ * Runs as one persistent launch of 3M products read straight from A and B,
+ * with products that came out non-finite recomputed by explicit FP32
+ * four-product terms (the reference's RepairNonFiniteOutput,
+ * cgemm_compute_kernel.cpp:672-706); bitwise repeatable. */
+/* aclblasCgemm (cann_ops_blas.h:492; cgemm_host.cpp:701-738): the same
+ * product with the reference cgemm's statuses (bad enum -> INVALID_ENUM; A and
+ * B required whenever k > 0, alpha == 0 included).  alpha = 1, beta = 0 runs
+ * three products with the non-finite repair; other scalars run four real
+ * products (Re = Ar.Br - Ai.Bi, Im = Ar.Bi + Ai.Br) with one FFMA per term. */
+cg3mStatus_t cg3mCgemm(cg3mHandle_t handle, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
+                       const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B, int ldb,
+                       const cg3mComplex* beta, cg3mComplex* C, int ldc);
+
 cg3mStatus_t cg3mCgemm3mStridedBatched(cg3mHandle_t handle, cg3mOperation_t transa, cg3mOperation_t transb, int m,
                                        int n, int k, const cg3mComplex* alpha, const cg3mComplex* A, int lda,
                                        int64_t strideA, const cg3mComplex* B, int ldb, int64_t strideB,
@@ -249,6 +263,11 @@ cg3mStatus_t cg3mValidate(cg3mOperation_t transa, cg3mOperation_t transb, int m,
 cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k, const cg3mComplex* alpha,
                       int lda, int ldb, const cg3mComplex* beta, int ldc, const cg3mOptions* opts, int sm_count,
                       cg3mCallInfo* info);
+
+/* The on-chip family's decision (cg3mCgemm, cg3mCgemm3mStridedBatched) for
+ * one problem shape: mode 0 = three products, 1 = four; `batch` problems per
+ * launch.  Fills tile_m, tile_n, k_partitions, k_span and workspace_bytes. */
+cg3mStatus_t cg3mPlanOnchip(int m, int n, int k, int mode, int batch, int sm_count, cg3mCallInfo* info);
 
 /* ---- diagnostics (not a compute path of cgemm3m) ------------------------- */
 

@@ -48,6 +48,10 @@ aclblasStatus_t aclblasGetStream(aclblasHandle_t handle, aclrtStream* stream);
 aclblasStatus_t aclblasSetWorkspace(aclblasHandle_t handle, void* workspace, size_t workspaceSize);
 /* aclblasGetVersion, cann_ops_blas.h:108 */
 aclblasStatus_t aclblasGetVersion(aclblasHandle_t handle, int* version);
+/* aclblasCgemm, cann_ops_blas.h:492 (definition cgemm_host.cpp:732-738) */
+aclblasStatus_t aclblasCgemm(aclblasHandle_t handle, aclblasOperation_t transa, aclblasOperation_t transb, int m,
+                             int n, int k, const aclblasComplex* alpha, const aclblasComplex* A, int lda,
+                             const aclblasComplex* B, int ldb, const aclblasComplex* beta, aclblasComplex* C, int ldc);
 /* aclblasCgemm3m, cann_ops_blas.h:497-500 (definition cgemm3m_host.cpp:17-23) */
 aclblasStatus_t aclblasCgemm3m(aclblasHandle_t handle, aclblasOperation_t transa, aclblasOperation_t transb, int m,
                                int n, int k, const aclblasComplex* alpha, const aclblasComplex* A, int lda,

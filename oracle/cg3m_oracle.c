@@ -21,6 +21,9 @@
  *                           :35-46), per-partition sequential FFMA products,
  *                           fixed-order partition merge and alpha/beta epilogue
  *                           (cgemm_epilogue_kernel.cpp:247-279).
+ *   3b. oracle_cgemm_modes_fp32 -- bit-exact model of the on-chip product
+ *                           family (3M or four products, optional non-finite
+ *                           repair, cgemm_compute_kernel.cpp:672-706).
  *   4. rounding-correction restatement: risk integral (cgemm_compute_kernel.cpp
  *      :432-474), row/column energies (cgemm3m_rounding_kernel.cpp:406-435),
  *      selection (:43-100) and segmented prefix recompute (:192-309).
@@ -276,6 +279,89 @@ void oracle_cgemm3m_fp32(int transa, int transb, int m, int n, int k, const floa
     free(p2);
     free(re);
     free(im);
+}
+
+/*
+ * 3b. Bit-exact model of the on-chip product family (strided batches,
+ * cgemm): mode 0 = the standard 3M identity as in 3., mode 1 = four real
+ * products P0 = Ar.Br, P1 = Ai.Bi, P2 = Ar.Bi, P3 = Ai.Br accumulated with one
+ * FFMA per term, re_p = P0-P1, im_p = P2+P3.  Partitions of `span` K terms
+ * are merged in increasing order.  With repair != 0 a merged product with a
+ * non-finite component is replaced by the explicit four-product sum of
+ * RepairNonFiniteOutput (blas/gemm/arch35/cgemm_compute_kernel.cpp:672-706):
+ * over the whole K, rr, ii, ri, ir rounded separately, re += rr - ii,
+ * im += ri + ir.  Then the alpha/beta epilogue of 3.  Caller handles
+ * k == 0 / alpha == 0 as oracle_cgemm.
+ */
+void oracle_cgemm_modes_fp32(int mode, int repair, int transa, int transb, int m, int n, int k, const float* alpha2,
+                             const c32* a, int lda, const c32* b, int ldb, const float* beta2, c32* c, int ldc,
+                             int span)
+{
+    const float ar_ = alpha2[0], ai_ = alpha2[1], br_ = beta2[0], bi_ = beta2[1];
+    const int unit = ar_ == 1.0f && ai_ == 0.0f && br_ == 0.0f && bi_ == 0.0f;
+    const int beta_zero = br_ == 0.0f && bi_ == 0.0f;
+    if (span <= 0 || span > k) {
+        span = k;
+    }
+    for (int j = 0; j < n; ++j) {
+        for (int i = 0; i < m; ++i) {
+            float re = 0.0f, im = 0.0f;
+            for (int k0 = 0, part = 0; k0 < k; k0 += span, ++part) {
+                const int k1 = k0 + span < k ? k0 + span : k;
+                float q0 = 0.0f, q1 = 0.0f, q2 = 0.0f, q3 = 0.0f;
+                for (int l = k0; l < k1; ++l) {
+                    const c32 x = op_elem(a, lda, transa, i, l);
+                    const c32 y = op_elem(b, ldb, transb, l, j);
+                    if (mode == 0) {
+                        q0 = fmaf(x.re, y.re, q0);
+                        q1 = fmaf(x.im, y.im, q1);
+                        q2 = fmaf(fadd(x.re, x.im), fadd(y.re, y.im), q2);
+                    } else {
+                        q0 = fmaf(x.re, y.re, q0);
+                        q1 = fmaf(x.im, y.im, q1);
+                        q2 = fmaf(x.re, y.im, q2);
+                        q3 = fmaf(x.im, y.re, q3);
+                    }
+                }
+                const float rp = fsub(q0, q1);
+                const float ip = mode == 0 ? fsub(fsub(q2, q0), q1) : fadd(q2, q3);
+                if (part == 0) {
+                    re = rp;
+                    im = ip;
+                } else {
+                    re = fadd(re, rp);
+                    im = fadd(im, ip);
+                }
+            }
+            if (repair && !(isfinite(re) && isfinite(im))) {
+                re = 0.0f;
+                im = 0.0f;
+                for (int l = 0; l < k; ++l) {
+                    const c32 x = op_elem(a, lda, transa, i, l);
+                    const c32 y = op_elem(b, ldb, transb, l, j);
+                    const float rr = fmul(x.re, y.re), ii = fmul(x.im, y.im);
+                    const float ri = fmul(x.re, y.im), ir = fmul(x.im, y.re);
+                    re = fadd(re, fsub(rr, ii));
+                    im = fadd(im, fadd(ri, ir));
+                }
+            }
+            c32* v = &c[(size_t)j * ldc + i];
+            if (unit) {
+                v->re = re;
+                v->im = im;
+                continue;
+            }
+            float zr = fsub(fmul(ar_, re), fmul(ai_, im));
+            float zi = fadd(fmul(ar_, im), fmul(ai_, re));
+            if (!beta_zero) {
+                const float cr = v->re, ci = v->im;
+                zr = fadd(zr, fsub(fmul(br_, cr), fmul(bi_, ci)));
+                zi = fadd(zi, fadd(fmul(br_, ci), fmul(bi_, cr)));
+            }
+            v->re = zr;
+            v->im = zi;
+        }
+    }
 }
 
 /* ------------------------------------------------------------------------- */

@@ -41,6 +41,7 @@ def lib():
         L.oracle_cgemm.argtypes = [i, i, i, i, i, P, P, i, P, i, P, P, i]
         L.oracle_zgemm.argtypes = [i, i, i, i, i, P, P, i, P, i, P, P, i, P]
         L.oracle_cgemm3m_fp32.argtypes = [i, i, i, i, i, P, P, i, P, i, P, P, i, i]
+        L.oracle_cgemm_modes_fp32.argtypes = [i, i, i, i, i, i, i, P, P, i, P, i, P, P, i, i]
         L.oracle_risk_path.argtypes = [i, i, i, P, P, P, P]
         L.oracle_risk_path_rect.argtypes = [i, i, i, i, i, P, i, P, i, P, P]
         L.oracle_energy.argtypes = [i, i, i, P, i, P, i, P]
@@ -115,6 +116,17 @@ def cgemm3m_fp32_model(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, 
     be = np.array([beta.real, beta.imag], dtype=np.float32)
     lib().oracle_cgemm3m_fp32(_op(transa), _op(transb), m, n, k, _ptr(al), _ptr(_c64(a)), lda, _ptr(_c64(b)), ldb,
                               _ptr(be), _ptr(c), ldc, int(span))
+    return c
+
+
+def cgemm_modes_model(mode, repair, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, span=0):
+    """Bit-exact model of the on-chip product family (in place on ``c``):
+    mode 0 = standard 3M, 1 = four products; ``repair`` recomputes non-finite
+    products with the explicit four-product sum."""
+    al = np.array([complex(alpha).real, complex(alpha).imag], dtype=np.float32)
+    be = np.array([complex(beta).real, complex(beta).imag], dtype=np.float32)
+    lib().oracle_cgemm_modes_fp32(int(mode), int(repair), _op(transa), _op(transb), m, n, k, _ptr(al), _ptr(_c64(a)),
+                                  lda, _ptr(_c64(b)), ldb, _ptr(be), _ptr(c), ldc, int(span))
     return c
 
 

@@ -239,3 +239,34 @@ def test_batch_plan_validation_without_device(cg3m):
     assert L.cg3mBatchPlanExecute(h.h, None, 0) == cg3m.INVALID_VALUE
     assert L.cg3mBatchPlanDestroy(None) == cg3m.INVALID_VALUE
     assert L.cg3mBatchPlanDescribe(None, None, None, None) == cg3m.INVALID_VALUE
+
+
+def test_cgemm_statuses_without_device(cg3m):
+    """aclblasCgemm keeps INVALID_ENUM and needs A, B whenever k > 0 (alpha == 0 included)."""
+    L = cg3m.lib
+    h = cg3m.Handle()
+    one, zero = ctypes.byref(cg3m.cx(1)), ctypes.byref(cg3m.cx(0))
+    d = ctypes.c_void_p(0x1000)
+    assert L.cg3mCgemm(None, 0, 0, 2, 2, 2, one, d, 2, d, 2, zero, d, 2) == cg3m.HANDLE_IS_NULLPTR
+    assert L.cg3mCgemm(h.h, 5, 0, 2, 2, 2, one, d, 2, d, 2, zero, d, 2) == cg3m.INVALID_ENUM
+    assert L.aclblasCgemm(h.h, 0, 3, 2, 2, 2, one, d, 2, d, 2, zero, d, 2) == cg3m.INVALID_ENUM  # no R here
+    assert L.cg3mCgemm(h.h, 0, 0, -1, 2, 2, one, d, 2, d, 2, zero, d, 2) == cg3m.INVALID_VALUE
+    assert L.cg3mCgemm(h.h, 0, 0, 2, 2, 2, one, d, 1, d, 2, zero, d, 2) == cg3m.INVALID_VALUE
+    assert L.cg3mCgemm(h.h, 0, 0, 2, 2, 2, None, d, 2, d, 2, zero, d, 2) == cg3m.INVALID_VALUE
+    assert L.cg3mCgemm(h.h, 0, 0, 0, 2, 2, one, None, 1, None, 2, zero, None, 1) == cg3m.SUCCESS
+    assert L.cg3mCgemm(h.h, 0, 0, 2, 2, 2, one, d, 2, d, 2, zero, None, 2) == cg3m.INVALID_VALUE
+    # alpha == 0 still needs A and B when k > 0 (the 3m entry does not)
+    assert L.cg3mCgemm(h.h, 0, 0, 2, 2, 2, zero, None, 2, d, 2, one, d, 2) == cg3m.INVALID_VALUE
+    assert L.cg3mCgemm3m(h.h, 0, 0, 2, 2, 2, zero, None, 2, None, 2, one, d, 2) == cg3m.SUCCESS
+    # alpha == 0, beta == 1 with valid pointers: nothing to do
+    assert L.cg3mCgemm(h.h, 0, 0, 2, 2, 2, zero, d, 2, d, 2, one, d, 2) == cg3m.SUCCESS
+
+
+def test_onchip_plan(cg3m):
+    """The on-chip family splits K only when few tile tasks would leave SMs idle."""
+    big = cg3m.plan_onchip(1024, 1024, 1024, mode=0, batch=64)
+    assert big["k_partitions"] == 1 and big["tile_m"] * big["tile_n"] == 8192
+    few = cg3m.plan_onchip(64, 64, 4096, mode=0, batch=1)
+    assert few["k_partitions"] > 1 and few["k_span"] * (few["k_partitions"] - 1) < 4096
+    four = cg3m.plan_onchip(1024, 1024, 1024, mode=1, batch=8)
+    assert four["tile_m"] * four["tile_n"] <= 4096  # no 128x64 tile with four accumulators

@@ -429,6 +429,349 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// CTA-pair variant (the main path): a cluster of two CTAs computes a 256 x 128
+// output tile with cta_group::2 MMAs (M = 256).  CTA r holds rows
+// [128r, 128r + 128) of the A tile and columns [64r, 64r + 64) of the B tile
+// in its own shared memory; the even CTA's single MMA thread multiplies the
+// pair's operands into both CTAs' TMEM (each CTA's accumulators hold its own
+// 128 rows x all 128 columns).  Per CTA and K-block this moves 3/4 of the
+// operand bytes of the single-CTA kernel for the same MMA work, which leaves
+// room for a 3-stage ring (split-BF16) in 216 KB.
+//   - both producers load into their own shared memory; the transaction bytes
+//     of both land on the even CTA's `full` barrier, whose producer alone
+//     arms it with the pair's byte count;
+//   - MMA completion is committed to `empty`, `acc_full` and `mma_done` in
+//     both CTAs (multicast commit); the odd CTA's epilogue warps arrive on the
+//     even CTA's `acc_free` (16 arrivals per phase);
+//   - TMEM (512 columns) is allocated and freed by warp 1 of both CTAs;
+//   - a cluster barrier after set-up and before tear-down keeps both CTAs'
+//     barriers and shared memory alive while the peer may use them.
+// All mbarrier waits are bounded as in the single-CTA kernel.
+constexpr int PAIR_BN = 128;       // N of the pair MMA (B columns per pair tile)
+constexpr int PAIR_BHALF = 64;     // B columns staged by each CTA
+constexpr int PAIR_RING = 216 * 1024;
+
+template <int FORM>
+struct PairGeom {
+    using Cfg = TcCfg<FORM>;
+    static constexpr int B_PLANE = PAIR_BHALF * ROW_BYTES;            // 8 KB
+    static constexpr int STAGE_BYTES = Cfg::S * (A_PLANE + B_PLANE);   // per CTA
+    static constexpr int STAGES = PAIR_RING / STAGE_BYTES;
+    static constexpr int COLS = PAIR_BN / 2;
+    static constexpr int TMEM_COLS = 4 * PAIR_BN;
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 + 256;
+};
+
+template <int FORM>
+__global__ void __launch_bounds__(kThreads, 1)
+    gemm3m_tc_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                          const TcParams p)
+{
+    using Cfg = TcCfg<FORM>;
+    using G = PairGeom<FORM>;
+    constexpr int STAGES = G::STAGES;
+    constexpr int STAGE_BYTES = G::STAGE_BYTES;
+    constexpr int KSTEPS = ROW_BYTES / 32;
+    constexpr int COLS = G::COLS;
+    constexpr int BN = PAIR_BN;
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(ring + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* acc_full = empty + STAGES;  // [3]
+    uint64_t* acc_free = acc_full + 3;    // [3] (used in the even CTA)
+    uint64_t* mma_done = acc_free + 3;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const uint32_t rank = cluster_ctarank();
+    const bool leader = rank == 0;
+
+    constexpr int GM = 4;  // pair tiles per L2 group along m
+    const int pid = blockIdx.x >> 1;
+    const int tiles_m2 = p.tiles_m;  // pair tiles (256 rows) along m
+    const int in_group = GM * p.tiles_n;
+    const int first_m = (pid / in_group) * GM;
+    const int gsz = min(tiles_m2 - first_m, GM);
+    const int tm = first_m + (pid % in_group) % gsz;
+    const int tn = (pid % in_group) / gsz;
+    const int m0 = tm * 2 * TILE_M + (int)rank * TILE_M;  // this CTA's rows
+    const int n0 = tn * BN;
+    const int part = blockIdx.y;
+    const int kbeg = part * p.span;
+    const int kend = min(p.k, kbeg + p.span);
+    const int kblocks = (kend - kbeg + Cfg::BK - 1) / Cfg::BK;
+    const int seg_blocks = p.seg_blocks;
+    const int segments = (kblocks + seg_blocks - 1) / seg_blocks;
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int c = 0; c < 3; ++c) {
+            mbar_init(&acc_full[c], 1);
+            mbar_init(&acc_free[c], 2 * kEpilogueWarps);
+        }
+        mbar_init(mma_done, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc_pair(tmem_slot, G::TMEM_COLS);
+        tmem_relinquish_pair();
+    }
+    tc_fence_before();
+    cluster_sync();  // both CTAs' barriers initialised, TMEM allocated in both
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ---------------- TMA producer (both CTAs) ----------------
+        if (lane == 0) {
+            tma_prefetch_desc(&tmA);
+            tma_prefetch_desc(&tmB);
+            int it = 0;
+            bool stop = false;
+            for (int seg = 0; seg < segments && !stop; ++seg) {
+                const int kb0 = seg * seg_blocks, kb1 = min(kblocks, kb0 + seg_blocks);
+                for (int c = 0; c < 3 && !stop; ++c) {
+                    for (int kb = kb0; kb < kb1; ++kb, ++it) {
+                        const int s = it % STAGES;
+                        if ((it >= STAGES && !mbar_wait(&empty[s], ((it / STAGES) - 1) & 1, p.status)) ||
+                            *abort_flag) {
+                            *abort_flag = 1;
+                            stop = true;
+                            break;
+                        }
+                        uint8_t* st = ring + s * STAGE_BYTES;
+                        const uint32_t bar = mapa_shared(smem_u32(&full[s]), 0);
+                        if (leader) {
+                            mbar_arrive_expect_tx(&full[s], 2 * STAGE_BYTES);
+                        }
+                        tma_load_3d_pair(st, &tmA, bar, kbeg + kb * Cfg::BK, m0, c * Cfg::S);
+                        tma_load_3d_pair(st + Cfg::S * A_PLANE, &tmB, bar, kbeg + kb * Cfg::BK,
+                                         n0 + (int)rank * PAIR_BHALF, c * Cfg::S);
+                    }
+                }
+            }
+            if (leader) {
+                for (int j = it > STAGES ? it - STAGES : 0; j < it; ++j) {
+                    mbar_wait(&full[j % STAGES], (j / STAGES) & 1, p.status);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer (even CTA) ----------------
+        if (leader && lane == 0) {
+            const uint32_t idesc = (1u << 4) | (Cfg::FMT << 7) | (Cfg::FMT << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                   ((uint32_t)((2 * TILE_M) >> 4) << 24);
+            int it = 0;
+            bool stop = false;
+            for (int seg = 0; seg < segments && !stop; ++seg) {
+                const int kb0 = seg * seg_blocks, kb1 = min(kblocks, kb0 + seg_blocks);
+                for (int c = 0; c < 3 && !stop; ++c) {
+                    if (seg > 0) {
+                        if (!mbar_wait_cluster(&acc_free[c], (seg - 1) & 1, p.status)) {
+                            *abort_flag = 1;
+                            stop = true;
+                            break;
+                        }
+                        tc_fence_after();
+                    }
+                    const uint32_t d = tmem + (uint32_t)(c * BN);
+                    for (int kb = kb0; kb < kb1; ++kb, ++it) {
+                        const int s = it % STAGES;
+                        if (!mbar_wait(&full[s], (it / STAGES) & 1, p.status)) {
+                            *abort_flag = 1;
+                            stop = true;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t a_base = smem_u32(ring + s * STAGE_BYTES);
+                        const uint32_t b_base = a_base + Cfg::S * A_PLANE;
+#pragma unroll
+                        for (int kk = 0; kk < KSTEPS; ++kk) {
+#pragma unroll
+                            for (int q = 0; q < Cfg::NPAIRS; ++q) {
+                                const int2 ij = Cfg::pair(q);
+                                const uint64_t ad = smem_desc(a_base + ij.x * A_PLANE + kk * 32);
+                                const uint64_t bd = smem_desc(b_base + ij.y * G::B_PLANE + kk * 32);
+                                const uint32_t acc = (kb > kb0 || kk > 0 || q > 0) ? 1u : 0u;
+                                if constexpr (Cfg::FMT == 2) {
+                                    umma_tf32_pair(d, ad, bd, idesc, acc);
+                                } else {
+                                    umma_f16_pair(d, ad, bd, idesc, acc);
+                                }
+                            }
+                        }
+                        umma_commit_pair(&empty[s], 0x3);
+                    }
+                    if (!stop && c > 0) {
+                        umma_commit_pair(&acc_full[c], 0x3);
+                    }
+                }
+            }
+            umma_commit_pair(mma_done, 0x3);
+            mbar_wait(mma_done, 0, p.status);  // nothing may still write TMEM when it is freed
+        }
+    } else {
+        // ---------------- epilogue warps 2..9 (both CTAs) ----------------
+        const int quad = warp & 3;
+        const int half = (warp - 2) >> 2;
+        const int row = m0 + quad * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * COLS);
+        const uint32_t spare = lane_addr + (uint32_t)(3 * BN);
+        const uint32_t free0 = mapa_shared(smem_u32(&acc_free[0]), 0);
+        const uint32_t free1 = mapa_shared(smem_u32(&acc_free[1]), 0);
+        const uint32_t free2 = mapa_shared(smem_u32(&acc_free[2]), 0);
+        float re[COLS], im[COLS];
+        bool go = true;
+        for (int seg = 0; seg < segments && go; ++seg) {
+            bool ready = mbar_wait(&acc_full[1], seg & 1, p.status);
+            tc_fence_after();
+            go = __all_sync(0xffffffffu, ready && !*abort_flag);
+            if (!go) {
+                break;
+            }
+#pragma unroll
+            for (int cb = 0; cb < COLS; cb += 8) {
+                float v0[8], v1[8];
+                tmem_ld8x2(lane_addr + (uint32_t)cb, lane_addr + (uint32_t)(BN + cb), v0, v1);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const float rs = __fsub_rn(v0[j], v1[j]);
+                    v1[j] = __fadd_rn(v0[j], v1[j]);
+                    re[cb + j] = seg == 0 ? rs : __fadd_rn(re[cb + j], rs);
+                }
+                tmem_st8(spare + (uint32_t)cb, v1);
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive_cluster(free0);
+                mbar_arrive_cluster(free1);
+            }
+            ready = mbar_wait(&acc_full[2], seg & 1, p.status);
+            tc_fence_after();
+            go = __all_sync(0xffffffffu, ready && !*abort_flag);
+            if (!go) {
+                break;
+            }
+#pragma unroll
+            for (int cb = 0; cb < COLS; cb += 8) {
+                float v2[8], u[8];
+                tmem_ld8x2(lane_addr + (uint32_t)(2 * BN + cb), spare + (uint32_t)cb, v2, u);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const float is = __fsub_rn(v2[j], u[j]);
+                    im[cb + j] = seg == 0 ? is : __fadd_rn(im[cb + j], is);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive_cluster(free2);
+            }
+        }
+        if (go && row < p.m) {
+#pragma unroll
+            for (int j = 0; j < COLS; ++j) {
+                const int col = n0 + half * COLS + j;
+                if (col < p.n) {
+                    if (p.parts == 1) {
+                        float2* cp = p.C + (size_t)col * p.ldc + row;
+                        *cp = epilogue_value(re[j], im[j], p.epi, cp);
+                    } else {
+                        const size_t o = (size_t)col * p.ppitch + row;
+                        p.partial[(size_t)(2 * part) * p.pplane + o] = re[j];
+                        p.partial[(size_t)(2 * part + 1) * p.pplane + o] = im[j];
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();  // the even CTA's MMAs are complete; neither CTA's memory is used any more
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc_pair(tmem, G::TMEM_COLS);
+    }
+}
+
+template <int FORM>
+cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
+{
+    using Cfg = TcCfg<FORM>;
+    using G = PairGeom<FORM>;
+    const bool bf16 = Cfg::FMT == 1;
+    const size_t elem = bf16 ? 2 : 4;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    CUtensorMap ta, tb;
+    const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.m, (uint64_t)(3 * Cfg::S)};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_a * elem, (uint64_t)plan.plane_a_elems * elem};
+        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)TILE_M, (uint32_t)Cfg::S};
+        if (!encode_tensor_map(&ta, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_a_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.n, (uint64_t)(3 * Cfg::S)};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_b * elem, (uint64_t)plan.plane_b_elems * elem};
+        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)PAIR_BHALF, (uint32_t)Cfg::S};
+        if (!encode_tensor_map(&tb, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_b_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    TcParams p{};
+    p.m = pr.m;
+    p.n = pr.n;
+    p.k = pr.k;
+    p.span = plan.span;
+    p.parts = plan.parts;
+    p.tiles_m = ceil_div(pr.m, 2 * TILE_M);  // pair tiles
+    p.tiles_n = ceil_div(pr.n, PAIR_BN);
+    p.epi = EpiParams{pr.ar, pr.ai, pr.br, pr.bi, plan.unit ? 1 : 0, plan.beta_zero ? 1 : 0};
+    p.C = static_cast<float2*>(pr.C);
+    p.ldc = pr.ldc;
+    p.partial = reinterpret_cast<float*>(w + plan.partial_off);
+    p.ppitch = plan.partial_pitch;
+    p.pplane = plan.partial_plane_elems;
+    p.status = status;
+    p.seg_blocks = plan.tc_segment > 0 ? (plan.tc_segment + Cfg::BK - 1) / Cfg::BK : 64 / Cfg::BK;
+    if (p.seg_blocks < 1) {
+        p.seg_blocks = 1;
+    }
+    p.path = nullptr;
+    auto kernel = gemm3m_tc_pair_kernel<FORM>;
+    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(2 * p.tiles_m * p.tiles_n), (unsigned)plan.parts);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = G::SMEM;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    err = cudaLaunchKernelEx(&cfg, kernel, ta, tb, p);
+    return err != cudaSuccess ? err : cudaGetLastError();
+}
+
 template <int FORM, int BN, bool PATH>
 cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status, float* path)
 {
@@ -487,8 +830,22 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
 
 }  // namespace
 
+#ifndef CG3M_TC_PAIR
+#define CG3M_TC_PAIR 1
+#endif
+
 cudaError_t launch_gemm_tc(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
 {
+    // CTA pairs whenever the output has more than one 128-row tile; a single
+    // row tile would leave the odd CTA of every pair without rows.
+    if (CG3M_TC_PAIR && pr.m > TILE_M) {
+        switch (plan.form) {
+            case CG3M_FORM_TF32X3: return launch_pair<CG3M_FORM_TF32X3>(stream, pr, plan, ws, status);
+            case CG3M_FORM_BF16X6: return launch_pair<CG3M_FORM_BF16X6>(stream, pr, plan, ws, status);
+            case CG3M_FORM_BF16X9: return launch_pair<CG3M_FORM_BF16X9>(stream, pr, plan, ws, status);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (plan.form) {
         case CG3M_FORM_TF32X3: return launch_form<CG3M_FORM_TF32X3, 128, false>(stream, pr, plan, ws, status, nullptr);
         case CG3M_FORM_BF16X6: return launch_form<CG3M_FORM_BF16X6, 128, false>(stream, pr, plan, ws, status, nullptr);

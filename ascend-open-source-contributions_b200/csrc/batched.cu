@@ -122,10 +122,11 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// One operand's share of a K-block for this thread.  Element q of the thread
-// is e = tid + q*kThreads of the R x BK block.  The source's contiguous
-// dimension goes to consecutive threads: rows ("rows_contig": op(A) in {N, R},
-// op(B) in {T, C}; r = e % R, kk = e / R) or K (r = e / BK, kk = e % BK).
+// One operand's share of a K-block for this thread (q = 0 .. E-1).  The
+// source's contiguous dimension goes to consecutive threads: rows
+// ("rows_contig": op(A) in {N, R}, op(B) in {T, C}; r = e % R, kk = e / R with
+// e = tid + q*kThreads) or K (8 consecutive K of 4 rows per warp; row
+// 16q + r0(tid), K index kk0(tid)).
 //   rows_contig: X[(row0 + r) + k*ld]      else: X[k + (row0 + r)*ld]
 struct Feed {
     const float2* origin;  // the matrix (source of the zero-byte copies)
@@ -153,8 +154,10 @@ __device__ __forceinline__ Feed make_feed(const float2* X, int ld, bool rows_con
         f.qstep = (long long)f.kq * ld;
         f.kbstep = (long long)BK * ld;
     } else {
-        f.kk = tid % BK;
-        f.r = tid / BK;
+        // Each warp covers 4 rows x 8 consecutive K: 64-byte global segments,
+        // and conflict-free plane stores (row stride = 4 banks mod 32).
+        f.kk = (tid % 8) + 8 * ((tid / 32) % 2);
+        f.r = ((tid / 8) % 4) + 4 * (tid / 64);
         f.rq = kThreads / BK;
         f.kq = 0;
         f.base = X + (long long)(kbeg + f.kk) + (long long)(row0 + f.r) * ld;

@@ -139,17 +139,33 @@ __device__ __forceinline__ Cf term(float2 x, float2 y)
 // in shared memory (S[l][thread]) for the reduction, the inclusive scan and
 // the seeded replay, all in the oracle's fixed orders.  Only flagged outputs
 // are written.
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Shared memory of recompute_fp32_tiled: the 64 lane sums (real, imaginary)
+// of the tile's 256 outputs, then two staging buffers of one lane's operand
+// slices (16 rows of op(A) and 16 columns of op(B), span K terms each).
+constexpr size_t kLaneSumBytes = (size_t)2 * kLanes * 256 * sizeof(float);
+constexpr size_t kStageElems = (size_t)kMaxSpan * kTile;  // float2 per operand per buffer
+constexpr size_t kRecomputeSmem = kLaneSumBytes + 2 * 2 * kStageElems * sizeof(float2);
+
 __global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, const float2* __restrict__ rows_a,
                                                             const float2* __restrict__ rows_b,
                                                             const uint32_t* __restrict__ flag_bits,
                                                             const uint32_t* __restrict__ tile_flags,
                                                             float2* __restrict__ C)
 {
-    __shared__ float2 xs[kMaxSpan][kTile];
-    __shared__ float2 ys[kMaxSpan][kTile];
-    extern __shared__ float lane_sums[];  // [2][64][256]: real then imaginary
+    extern __shared__ __align__(16) float lane_sums[];  // [2][64][256]: real then imaginary
     float* sr = lane_sums;
     float* si = lane_sums + kLanes * 256;
+    float2* stage_base = reinterpret_cast<float2*>(reinterpret_cast<char*>(lane_sums) + kLaneSumBytes);
     const int tiles = (n + kTile - 1) / kTile;
     if (tile_flags[blockIdx.x] == 0) {
         return;
@@ -158,33 +174,42 @@ __global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, con
     const int tid = threadIdx.x;
     const int ti = tid & (kTile - 1), tj = tid >> 4;
     const int i = i0 + ti, j = j0 + tj;
-    auto stage = [&](int l) {
+    // Buffer b holds xs[q][r] at stage_base[b*2*kStageElems + q*kTile + r] and
+    // ys[q][r] kStageElems after it.
+    auto xs = [&](int b) { return stage_base + (size_t)b * 2 * kStageElems; };
+    auto ys = [&](int b) { return stage_base + (size_t)b * 2 * kStageElems + kStageElems; };
+    auto lane_count = [&](int l) { return max(0, min(span, n - l * span)); };
+    // Asynchronous copy of lane l's operand slices into buffer b; positions
+    // past the end of K or past the matrix read as zero.
+    auto issue = [&](int l, int b) {
         const int k0 = l * span;
-        const int cnt = max(0, min(span, n - k0));
-        __syncthreads();
+        const int cnt = lane_count(l);
+        float2* X = xs(b);
+        float2* Y = ys(b);
         for (int e = tid; e < kTile * span; e += 256) {
             const int r = e / span, q = e - r * span;
-            float2 xv = make_float2(0.0f, 0.0f), yv = make_float2(0.0f, 0.0f);
-            if (q < cnt) {
-                if (i0 + r < n) {
-                    xv = rows_a[(size_t)(i0 + r) * n + k0 + q];
-                }
-                if (j0 + r < n) {
-                    yv = rows_b[(size_t)(j0 + r) * n + k0 + q];
-                }
-            }
-            xs[q][r] = xv;
-            ys[q][r] = yv;
+            const bool okx = q < cnt && i0 + r < n, oky = q < cnt && j0 + r < n;
+            cp_async8(X + q * kTile + r, okx ? (const void*)(rows_a + (size_t)(i0 + r) * n + k0 + q) : rows_a,
+                      okx ? 8 : 0);
+            cp_async8(Y + q * kTile + r, oky ? (const void*)(rows_b + (size_t)(j0 + r) * n + k0 + q) : rows_b,
+                      oky ? 8 : 0);
         }
-        __syncthreads();
-        return cnt;
+        cp_async_commit();
     };
-    // pass 1: lane sums
+    // pass 1: lane sums (lane l+1 is copied while lane l is summed)
+    issue(0, 0);
     for (int l = 0; l < kLanes; ++l) {
-        const int cnt = stage(l);
+        cp_async_wait_all();
+        __syncthreads();  // lane l staged by every thread; lane l-1's buffer is free
+        if (l + 1 < kLanes) {
+            issue(l + 1, (l + 1) & 1);
+        }
+        const int cnt = lane_count(l);
+        const float2* X = xs(l & 1);
+        const float2* Y = ys(l & 1);
         Cf acc{0.0f, 0.0f};
         for (int q = 0; q < cnt; ++q) {
-            const Cf t = term(xs[q][ti], ys[q][tj]);
+            const Cf t = term(X[q * kTile + ti], Y[q * kTile + tj]);
             acc.r = __fadd_rn(acc.r, t.r);
             acc.i = __fadd_rn(acc.i, t.i);
         }
@@ -222,14 +247,23 @@ __global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, con
     }
     // pass 2: replay each lane seeded with the previous lanes' prefix
     float prev_r = 0.0f, prev_i = 0.0f;
+    __syncthreads();  // every thread is done with the last buffer of pass 1
+    issue(0, 0);
     for (int l = 0; l < kLanes; ++l) {
-        const int cnt = stage(l);
+        cp_async_wait_all();
+        __syncthreads();
+        if (l + 1 < kLanes) {
+            issue(l + 1, (l + 1) & 1);
+        }
+        const int cnt = lane_count(l);
+        const float2* X = xs(l & 1);
+        const float2* Y = ys(l & 1);
         const float init_r = prev_r, init_i = prev_i;
         prev_r = sr[l * 256 + tid];
         prev_i = si[l * 256 + tid];
         float r = __fadd_rn(init_r, 0.0f), im = __fadd_rn(init_i, 0.0f);
         for (int q = 0; q < cnt; ++q) {
-            const Cf t = term(xs[q][ti], ys[q][tj]);
+            const Cf t = term(X[q * kTile + ti], Y[q * kTile + tj]);
             r = __fadd_rn(r, t.r);
             im = __fadd_rn(im, t.i);
         }
@@ -271,14 +305,19 @@ __global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, con
 // outputs are rounded once to FP32 and written.
 constexpr int kT64 = 64;
 
-__global__ void __launch_bounds__(256) recompute_fp64_tiled(int n, const float2* __restrict__ rows_a,
+// Operand slabs of 16 K terms, converted to FP64 once while staging (each
+// value feeds 16 threads), double-buffered with the next slab held in
+// registers during the current slab's DFMAs.
+constexpr size_t kFp64Slab = (size_t)16 * kT64;  // double2 per operand per buffer
+constexpr size_t kFp64Smem = 2 * 2 * kFp64Slab * sizeof(double2);
+
+__global__ void __launch_bounds__(256, 2) recompute_fp64_tiled(int n, const float2* __restrict__ rows_a,
                                                             const float2* __restrict__ rows_b,
                                                             const uint32_t* __restrict__ flag_bits,
                                                             const uint32_t* __restrict__ tile_flags,
                                                             float2* __restrict__ C)
 {
-    __shared__ __align__(16) float2 xs[16][kT64];
-    __shared__ __align__(16) float2 ys[16][kT64];
+    extern __shared__ __align__(16) double2 slabs[];  // [buffer][x | y][16][64]
     const int tiles16 = (n + kTile - 1) / kTile;
     const int tiles64 = (n + kT64 - 1) / kT64;
     const int i0 = (blockIdx.x % tiles64) * kT64, j0 = (blockIdx.x / tiles64) * kT64;
@@ -293,7 +332,9 @@ __global__ void __launch_bounds__(256) recompute_fp64_tiled(int n, const float2*
         return;
     }
     const int tid = threadIdx.x;
-    const int ti = (tid & 15) * 4, tj = (tid >> 4) * 4;
+    // Thread (ti, tj) owns rows ti + 16a and columns tj + 16b (a, b < 4): for a
+    // fixed a the 16 row values a warp reads are 256 consecutive bytes.
+    const int ti = tid & 15, tj = tid >> 4;
     double ar[4][4], ai[4][4];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -302,41 +343,59 @@ __global__ void __launch_bounds__(256) recompute_fp64_tiled(int n, const float2*
             ar[a][b] = 0.0;
             ai[a][b] = 0.0;
         }
-    for (int k0 = 0; k0 < n; k0 += 16) {
-        __syncthreads();
-        for (int e = tid; e < 16 * kT64; e += 256) {
+    // Element e = tid + 256*u of a slab: row r = e >> 4, K offset q = e & 15.
+    float2 vx[4], vy[4];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = tid + 256 * u;
             const int r = e >> 4, q = e & 15;
             const int k = k0 + q;
-            xs[q][r] = (k < n && i0 + r < n) ? rows_a[(size_t)(i0 + r) * n + k] : make_float2(0.0f, 0.0f);
-            ys[q][r] = (k < n && j0 + r < n) ? rows_b[(size_t)(j0 + r) * n + k] : make_float2(0.0f, 0.0f);
+            vx[u] = (k < n && i0 + r < n) ? rows_a[(size_t)(i0 + r) * n + k] : make_float2(0.0f, 0.0f);
+            vy[u] = (k < n && j0 + r < n) ? rows_b[(size_t)(j0 + r) * n + k] : make_float2(0.0f, 0.0f);
         }
+    };
+    load(0);
+    const int slabs_n = (n + 15) / 16;
+    for (int t = 0; t < slabs_n; ++t) {
+        double2* xs = slabs + (size_t)(t & 1) * 2 * kFp64Slab;
+        double2* ys = xs + kFp64Slab;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = tid + 256 * u;
+            const int r = e >> 4, q = e & 15;
+            xs[q * kT64 + r] = make_double2((double)vx[u].x, (double)vx[u].y);
+            ys[q * kT64 + r] = make_double2((double)vy[u].x, (double)vy[u].y);
+        }
+        // Buffer t&1 was last read in slab t-2; this barrier also orders slab
+        // t-1's reads before slab t+1's writes.
         __syncthreads();
-#pragma unroll 4
+        if (t + 1 < slabs_n) {
+            load((t + 1) * 16);
+        }
+#pragma unroll 2
         for (int q = 0; q < 16; ++q) {
-            double xr[4], xi[4], yr[4], yi[4];
+            double2 x[4], y[4];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
-                const float2 x = xs[q][ti + a], y = ys[q][tj + a];
-                xr[a] = x.x;
-                xi[a] = x.y;
-                yr[a] = y.x;
-                yi[a] = y.y;
+                x[a] = xs[q * kT64 + ti + 16 * a];
+                y[a] = ys[q * kT64 + tj + 16 * a];
             }
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int b = 0; b < 4; ++b) {
-                    ar[a][b] = fma(xr[a], yr[b], fma(-xi[a], yi[b], ar[a][b]));
-                    ai[a][b] = fma(xr[a], yi[b], fma(xi[a], yr[b], ai[a][b]));
+                    ar[a][b] = fma(x[a].x, y[b].x, fma(-x[a].y, y[b].y, ar[a][b]));
+                    ai[a][b] = fma(x[a].x, y[b].y, fma(x[a].y, y[b].x, ai[a][b]));
                 }
         }
     }
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-        const int j = j0 + tj + b;
+        const int j = j0 + tj + 16 * b;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-            const int i = i0 + ti + a;
+            const int i = i0 + ti + 16 * a;
             if (i < n && j < n) {
                 const size_t idx = (size_t)j * n + i;
                 if (flagged(flag_bits, idx)) {
@@ -449,7 +508,7 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
     if (err == cudaSuccess) {
         if (plan.form == CG3M_FORM_FP32) {
             const int tiles = (n + kTile - 1) / kTile;
-            const size_t smem = (size_t)2 * kLanes * 256 * sizeof(float);
+            const size_t smem = kRecomputeSmem;
             err = cudaFuncSetAttribute(recompute_fp32_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (err == cudaSuccess) {
                 recompute_fp32_tiled<<<tiles * tiles, 256, smem, s>>>(n, span, L.rows_a, L.rows_b, L.flag_bits,
@@ -457,8 +516,12 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
             }
         } else {
             const int tiles = (n + kT64 - 1) / kT64;
-            recompute_fp64_tiled<<<tiles * tiles, 256, 0, s>>>(n, L.rows_a, L.rows_b, L.flag_bits, L.tile_flags,
-                                                             static_cast<float2*>(p.C));
+            err = cudaFuncSetAttribute(recompute_fp64_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kFp64Smem);
+            if (err == cudaSuccess) {
+                recompute_fp64_tiled<<<tiles * tiles, 256, kFp64Smem, s>>>(n, L.rows_a, L.rows_b, L.flag_bits,
+                                                                            L.tile_flags, static_cast<float2*>(p.C));
+            }
         }
         if (err == cudaSuccess) {
             err = cudaGetLastError();

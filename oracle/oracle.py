@@ -261,7 +261,11 @@ def make_matrix(rows, cols, ld, fill, seed):
         im = rng.choice([-1.0, 1.0], size) * np.exp2(rng.integers(-60, 61, size))
     else:
         raise ValueError(fill)
-    out = (re + 1j * im).astype(np.complex64)
+    # assign the parts separately: re + 1j*im would turn an infinite imaginary
+    # part into (nan, inf) through 0*inf
+    out = np.empty(size, dtype=np.complex64)
+    out.real = re
+    out.imag = im
     if ld > rows and cols > 0:
         view = out[: ld * cols].reshape(cols, ld)
         view[:, rows:] = np.complex64(complex(-7.25, 3.5))

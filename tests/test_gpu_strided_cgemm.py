@@ -229,3 +229,111 @@ def test_cgemm_bit_exact_and_reference_criterion(cg3m, oracle, cuda, h, case):
     oracle.cgemm(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, golden, ldc)
     ok, re, im, padok = oracle.verify_cgemm3m(out, golden, c, m, n, ldc)
     assert ok, (re.__dict__, im.__dict__, padok)
+
+
+def _table_rows(cases, limit=3_000_000):
+    out = []
+    for c in cases["cases"]:
+        if c["expect"] != "SUCCESS" or c["transa"] == 999 or c["transb"] == 999:
+            continue
+        if c["m"] * c["n"] * max(c["k"], 1) > limit:
+            continue
+        if any(f == "NULLPTR" for f in (c["a_fill"], c["b_fill"], c["c_fill"])):
+            continue
+        out.append(c)
+    return out
+
+
+def test_cgemm_case_table_rows(cg3m, oracle, cuda, h, cases):
+    """The reference's case table through cg3mCgemm (its legacy aclblasCgemm
+    regression): reference criterion vs reference-order cgemm, padding bytes,
+    determinism, and bit-exactness vs the family's model."""
+    import torch
+
+    rows = _table_rows(cases)
+    assert len(rows) > 500
+    sms = torch.cuda.get_device_properties(cuda).multi_processor_count
+    failures = []
+    for cs in rows:
+        ta, tb, m, n, k = cs["transa"], cs["transb"], cs["m"], cs["n"], cs["k"]
+        ar, ac = oracle.stored_shape(ta, m, k)
+        br, bc = oracle.stored_shape(tb, k, n)
+        a = oracle.make_matrix(ar, ac, cs["lda"], cs["a_fill"], cs["seed"])
+        b = oracle.make_matrix(br, bc, cs["ldb"], cs["b_fill"], cs["seed"] + 1)
+        c = oracle.make_matrix(m, n, cs["ldc"], cs["c_fill"], cs["seed"] + 2)
+        alpha, beta = complex(*cs["alpha"]), complex(*cs["beta"])
+        outs = []
+        for _ in range(2):
+            dC = to_dev(c, torch, cuda)
+            st = h.cgemm(ta, tb, m, n, k, alpha, to_dev(a, torch, cuda), cs["lda"],
+                         to_dev(b, torch, cuda), cs["ldb"], beta, dC, cs["ldc"])
+            torch.cuda.synchronize()
+            if st != cg3m.SUCCESS:
+                failures.append((cs["name"], "status", st))
+                break
+            outs.append(to_host(dC))
+        if len(outs) < 2:
+            continue
+        out = outs[0]
+        golden = c.copy()
+        oracle.cgemm(ta, tb, m, n, k, alpha, a, cs["lda"], b, cs["ldb"], beta, golden, cs["ldc"])
+        ok, re, im, pad = oracle.verify_cgemm3m(out, golden, c, m, n, cs["ldc"])
+        if not ok:
+            failures.append((cs["name"], "criterion", re.__dict__, im.__dict__, pad))
+        if not same_bits(out, outs[1]):
+            failures.append((cs["name"], "nondeterministic"))
+        if m and n and k and alpha != 0:
+            unit = alpha == 1 and beta == 0
+            mode = 0 if unit else 1
+            plan = cg3m.plan_onchip(m, n, k, mode, 1, sms)
+            model = c.copy()
+            oracle.cgemm_modes_model(mode, 1 if unit else 0, ta, tb, m, n, k, alpha, a, cs["lda"], b, cs["ldb"], beta,
+                                     model, cs["ldc"], span=plan["k_span"] if plan["k_partitions"] > 1 else 0)
+            if not same_bits(out, model):
+                failures.append((cs["name"], "model"))
+    assert not failures, failures[:10]
+
+
+def test_strided_case_table_rows(cg3m, oracle, cuda, h, cases):
+    """Every 4th successful case-table row as a strided batch of two (second
+    batch with its own data): reference criterion per batch and bits of the
+    family's model."""
+    import torch
+
+    rows = _table_rows(cases, limit=1_000_000)[::4]
+    sms = torch.cuda.get_device_properties(cuda).multi_processor_count
+    failures = []
+    for cs in rows:
+        ta, tb, m, n, k = cs["transa"], cs["transb"], cs["m"], cs["n"], cs["k"]
+        ar, ac = oracle.stored_shape(ta, m, k)
+        br, bc = oracle.stored_shape(tb, k, n)
+        lda, ldb, ldc = cs["lda"], cs["ldb"], cs["ldc"]
+        sA, sB, sC = lda * ac, ldb * bc, ldc * n
+        a = np.concatenate([oracle.make_matrix(ar, ac, lda, cs["a_fill"], cs["seed"] + 10 * t) for t in range(2)])
+        b = np.concatenate([oracle.make_matrix(br, bc, ldb, cs["b_fill"], cs["seed"] + 10 * t + 1) for t in range(2)])
+        c = np.concatenate([oracle.make_matrix(m, n, ldc, cs["c_fill"], cs["seed"] + 10 * t + 2) for t in range(2)])
+        alpha, beta = complex(*cs["alpha"]), complex(*cs["beta"])
+        dC = to_dev(c, torch, cuda)
+        st = h.cgemm3m_strided_batched(ta, tb, m, n, k, alpha, to_dev(a, torch, cuda), lda, sA,
+                                       to_dev(b, torch, cuda), ldb, sB, beta, dC, ldc, sC, 2)
+        torch.cuda.synchronize()
+        if st != cg3m.SUCCESS:
+            failures.append((cs["name"], "status", st))
+            continue
+        out = to_host(dC)
+        plan = cg3m.plan_onchip(m, n, k, 0, 2, sms) if m and n and k else None
+        for t in range(2):
+            ct = c[t * sC:(t + 1) * sC]
+            ot = out[t * sC:(t + 1) * sC]
+            golden = ct.copy()
+            oracle.cgemm(ta, tb, m, n, k, alpha, a[t * sA:], lda, b[t * sB:], ldb, beta, golden, ldc)
+            ok, re, im, pad = oracle.verify_cgemm3m(ot, golden, ct, m, n, ldc)
+            if not ok:
+                failures.append((cs["name"], t, "criterion", re.__dict__, im.__dict__, pad))
+            if m and n and k and alpha != 0:
+                model = ct.copy()
+                oracle.cgemm_modes_model(0, 1, ta, tb, m, n, k, alpha, a[t * sA:], lda, b[t * sB:], ldb, beta, model,
+                                         ldc, span=plan["k_span"] if plan["k_partitions"] > 1 else 0)
+                if not same_bits(ot, model):
+                    failures.append((cs["name"], t, "model"))
+    assert not failures, failures[:10]

@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-rounding-report", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batching-report", action="store_true")
+    ap.add_argument("--batching-only", action="store_true",
+                    help="run only the batching-form measurement (one JSON object; for profiling)")
     return ap.parse_args()
 
 
@@ -230,7 +232,7 @@ def run_reference(args, rank):
 
     n = args.size
     cores = os.cpu_count() or 1
-    cols_per_worker = 8
+    cols_per_worker = 4  # ~2 s of scalar work per step, so a 50-step run stays near two minutes
     ctx = mp.get_context("spawn")
     times = []
     with ctx.Pool(cores) as pool:
@@ -342,6 +344,16 @@ def main():
 
     import cg3m
 
+    if args.batching_only:
+        stream = torch.cuda.Stream(device=dev)
+        h = cg3m.Handle(stream=stream.cuda_stream)
+        rep = batching_report(h, stream, dev, world, args)
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"batching_form": rep}), flush=True)
+        return
+
     n = args.size
     a_host, b_host = host_operands(n)
     A = torch.from_numpy(a_host).to(dev)
@@ -411,8 +423,13 @@ def main():
     p = PASSES[args.form]
     peak, peak_src = pipe_peak(args.form, sm_count)
     achieved = flops6 * p / (gemm_ms * 1e-3) / 1e12
+    pk_all, _src = peaks()
+    sustained = pk_all.get("bf16_tflops_sustained")
+    if sustained and args.form != "fp32":
+        sustained = sustained / 2.0 if args.form == "tf32x3" else sustained
     roofline = {"bound": "tensor" if args.form != "fp32" else "fp32-pipe", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "kernel": "gemm",
+                "frac_vs_sustained_peak": (achieved / sustained) if sustained and args.form != "fp32" else None,
                 "peak_source": peak_src, "flops_per_launch": flops6 * p, "kernel_ms": gemm_ms,
                 "stage_ms": stages}
     traffic_file = os.path.join(ROOT, "profiles", "traffic.json")

@@ -57,6 +57,11 @@ def parse():
     ap.add_argument("--no-batching-report", action="store_true")
     ap.add_argument("--batching-only", action="store_true",
                     help="run only the batching-form measurement (one JSON object; for profiling)")
+    ap.add_argument("--pf-cases", action="store_true",
+                    help="run only the reference's 200 performance cases against its GPU baseline times")
+    ap.add_argument("--pf-forms", default="fp32,bf16x6",
+                    help="forms for --pf-cases: fp32 (the drop-in as called), fp32-norounding, cgemm, tf32x3, bf16x6")
+    ap.add_argument("--pf-per-case", action="store_true")
     return ap.parse_args()
 
 
@@ -314,6 +319,94 @@ def batching_report(h, stream, dev, world, args):
             "speedup_vs_separate": sep_ms / batch_ms, "plan_create_s": plan_s, "plan_tiles": tiles}
 
 
+# ----------------------------------------------------------------------------- reference performance cases
+
+def pf_cases_report(h, stream, dev, forms=("fp32", "bf16x6"), per_case=False):
+    """The reference's 200 performance cases (tests/golden/pf_gpu_baseline.json:
+    shapes, ops and leading dimensions of its TC_PF rows, alpha = 1, beta = 0,
+    entries uniform in [-5, 5] as RANDOM_NORM_5_5), 5 warm-up calls then 10
+    timed calls per case, two ways: back to back with CUDA events (host launch
+    costs included) and as a replayed CUDA graph of the 10 calls (device time,
+    closer to the reference's sum of kernel times).  Per form: the ratio of the
+    reference's GPU baseline time to this library's time per case (> 1:
+    faster), its minimum, median and mean, and the summed times.  `fp32` is the
+    drop-in exactly as called (rounding pass where the reference gates it)."""
+    import torch
+
+    with open(os.path.join(ROOT, "tests", "golden", "pf_gpu_baseline.json")) as f:
+        cases = json.load(f)["cases"]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(20262029)
+    out = {}
+    for form in forms:
+        rows = []
+        for cs in cases:
+            ta, tb, m, n, k = cs["transa"], cs["transb"], cs["m"], cs["n"], cs["k"]
+            a_cols = k if ta == "N" else m
+            b_cols = n if tb == "N" else k
+            with torch.cuda.stream(stream):
+                A = (torch.rand(2 * cs["lda"] * a_cols, generator=gen, device=dev) * 10 - 5).view(torch.complex64)
+                B = (torch.rand(2 * cs["ldb"] * b_cols, generator=gen, device=dev) * 10 - 5).view(torch.complex64)
+                C = torch.zeros(cs["ldc"] * n, dtype=torch.complex64, device=dev)
+
+                def call():
+                    if form == "fp32":
+                        st = h.cgemm3m(ta, tb, m, n, k, 1.0, A, cs["lda"], B, cs["ldb"], 0.0, C, cs["ldc"], raw=True)
+                        if st != 0:
+                            raise RuntimeError(f"cg3mCgemm3m status {st}")
+                    elif form == "fp32-norounding":
+                        h.cgemm3m(ta, tb, m, n, k, 1.0, A, cs["lda"], B, cs["ldb"], 0.0, C, cs["ldc"], form="fp32",
+                                  rounding="off")
+                    elif form == "cgemm":
+                        st = h.cgemm(ta, tb, m, n, k, 1.0, A, cs["lda"], B, cs["ldb"], 0.0, C, cs["ldc"])
+                        if st != 0:
+                            raise RuntimeError(f"cg3mCgemm status {st}")
+                    else:
+                        h.cgemm3m(ta, tb, m, n, k, 1.0, A, cs["lda"], B, cs["ldb"], 0.0, C, cs["ldc"], form=form,
+                                  rounding="off")
+
+                for _ in range(5):
+                    call()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(10):
+                    call()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / 10
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=stream):
+                    for _ in range(10):
+                        call()
+                g.replay()
+                torch.cuda.synchronize()
+                e0.record(stream)
+                g.replay()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                gms = e0.elapsed_time(e1) / 10
+                del g
+            rows.append((cs["gpu_ms"] / ms, cs["gpu_ms"] / gms, ms, gms, cs))
+            del A, B, C
+        def summary(idx, tidx):
+            r = sorted(x[idx] for x in rows)
+            worst = min(rows, key=lambda x: x[idx])
+            return {"ratio_min": r[0], "ratio_median": r[len(r) // 2], "ratio_mean": sum(r) / len(r),
+                    "ms_total": sum(x[tidx] for x in rows),
+                    "worst": {"ratio": worst[idx], "id": worst[4]["id"],
+                              "shape": f"{worst[4]['transa']}{worst[4]['transb']} "
+                                       f"{worst[4]['m']}x{worst[4]['n']}x{worst[4]['k']}",
+                              "ms": worst[tidx], "baseline_ms": worst[4]["gpu_ms"]}}
+        out[form] = {"cases": len(rows), "baseline_ms_total": sum(x[4]["gpu_ms"] for x in rows),
+                     "back_to_back": summary(0, 2), "graph_replay": summary(1, 3)}
+        if per_case:
+            out[form]["per_case"] = [[x[4]["id"], round(x[2], 4), round(x[3], 4)] for x in rows]
+    torch.cuda.empty_cache()
+    return {"what": "reference GPU baseline time / B200 time per case (its perf gate divides the same baseline by "
+                    "its NPU time: min 0.415, mean 0.635)", **out}
+
+
 # ----------------------------------------------------------------------------- our arm
 
 def main():
@@ -343,6 +436,16 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
     import cg3m
+
+    if args.pf_cases:
+        stream = torch.cuda.Stream(device=dev)
+        h = cg3m.Handle(stream=stream.cuda_stream)
+        rep = pf_cases_report(h, stream, dev, forms=tuple(args.pf_forms.split(",")), per_case=args.pf_per_case)
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"pf_cases": rep}), flush=True)
+        return
 
     if args.batching_only:
         stream = torch.cuda.Stream(device=dev)

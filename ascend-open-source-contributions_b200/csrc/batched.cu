@@ -433,22 +433,48 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
         return;
     }
     __threadfence();
-    for (int e = threadIdx.x; e < BM * BN; e += kThreads) {
-        const int r = e % BM, c = e / BM;
-        const int row = m0 + r, col = n0 + c;
-        if (row < p.m && col < p.n) {
-            const size_t o = (size_t)col * p.ppitch + row;
-            float re = __ldcg(base + o), im = __ldcg(base + plane + o);
-            for (int q = 1; q < p.parts; ++q) {
-                re = __fadd_rn(re, __ldcg(base + (size_t)(2 * q) * plane + o));
-                im = __fadd_rn(im, __ldcg(base + (size_t)(2 * q + 1) * plane + o));
+    // Three outputs per step (the most that fits the kernel's registers) so
+    // the loads of one partition for all three are in flight together; each
+    // output still adds its partitions in order.
+    constexpr int U = 3;
+    for (int e0 = threadIdx.x; e0 < BM * BN; e0 += U * kThreads) {
+        size_t o[U];
+        bool ok[U];
+        float re[U], im[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * kThreads;
+            const int row = m0 + e % BM, col = n0 + e / BM;
+            ok[u] = e < BM * BN && row < p.m && col < p.n;
+            o[u] = ok[u] ? (size_t)col * p.ppitch + row : 0;
+            re[u] = ok[u] ? __ldcg(base + o[u]) : 0.0f;
+            im[u] = ok[u] ? __ldcg(base + plane + o[u]) : 0.0f;
+        }
+        for (int q = 1; q < p.parts; ++q) {
+            float tr[U], ti[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                tr[u] = ok[u] ? __ldcg(base + (size_t)(2 * q) * plane + o[u]) : 0.0f;
+                ti[u] = ok[u] ? __ldcg(base + (size_t)(2 * q + 1) * plane + o[u]) : 0.0f;
             }
-            float2 v = make_float2(re, im);
-            if (p.repair && !finite2(v)) {
-                v = repair_product(p, row, col);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                re[u] = __fadd_rn(re[u], tr[u]);
+                im[u] = __fadd_rn(im[u], ti[u]);
             }
-            float2* cp = p.C + (size_t)col * p.ldc + row;
-            *cp = epilogue_value(v.x, v.y, p.epi, cp);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (ok[u]) {
+                const int e = e0 + u * kThreads;
+                const int row = m0 + e % BM, col = n0 + e / BM;
+                float2 v = make_float2(re[u], im[u]);
+                if (p.repair && !finite2(v)) {
+                    v = repair_product(p, row, col);
+                }
+                float2* cp = p.C + (size_t)col * p.ldc + row;
+                *cp = epilogue_value(v.x, v.y, p.epi, cp);
+            }
         }
     }
 }

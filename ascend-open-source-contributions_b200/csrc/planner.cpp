@@ -80,8 +80,19 @@ struct TileChoice {
     int slots_per_sm;  // resident CTAs per SM of this tile's kernel
 };
 
-// FP32 FFMA kernel tiles (gemm_fp32.cu) and how many fit on one SM.
-const TileChoice kFp32Tiles[] = {{128, 64, 1}, {64, 64, 2}, {64, 32, 3}, {32, 32, 6}};
+// FP32 FFMA kernel tile (gemm_fp32.cu).  The kernel also instantiates 64 x 64,
+// 64 x 32 and 32 x 32 tiles, but measured on B200 they run at about a third of
+// the 128 x 64 tile's per-SM FFMA rate (short pipelines, few warps), so the
+// planner splits K over 128 x 64 tiles instead (512^3: 64 x 32 x 3 parts
+// 62.9 us, 128 x 64 x 4 parts 38.8 us; 1024^3: 306 vs 174 us).
+const TileChoice kFp32Tiles[] = {{128, 64, 1}};
+// Cost of one wave of 128 x 64 FP32 tiles in K terms of that tile (0.133 us
+// per term): a fixed part of about 38 terms (pipeline fill, epilogue, wave
+// launch; fitted on 512^3 .. 2048^3) plus the span; the split-K merge costs
+// about 30 terms plus the partial planes it reads.
+constexpr uint64_t kFp32WaveFixed = 38;
+constexpr uint64_t kMergeFixed = 30;
+constexpr uint64_t kMergeFloatsPerTerm = 41500;
 // Tensor-core kernel tile (gemm_tc.cu): 128 x 128, one CTA per SM (TMEM).
 const TileChoice kTcTiles[] = {{128, 128, 1}};
 
@@ -135,12 +146,30 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     // ---- tile x K-partition search -------------------------------------------
     const TileChoice* tiles = tc ? kTcTiles : kFp32Tiles;
     const int granule = tc ? 64 : 16;
-    const int ntiles = tc ? 1 : 4;
+    const int ntiles = 1;
     const uint64_t default_tiles = (uint64_t)ceil_div(p.m, tiles[0].bm) * ceil_div(p.n, tiles[0].bn);
     TileChoice best_tile = tiles[0];
     int best_parts = 1;
     if (opts.k_partitions > 0) {
         best_parts = std::min(opts.k_partitions, 64);
+    } else if (!tc && !out.rounding) {
+        // FP32: waves of 128 x 64 tiles at (span + fixed) each, plus the merge
+        // (EstimateCgemmCoreWork's busiest-core work with measured B200 costs).
+        uint64_t best = std::numeric_limits<uint64_t>::max();
+        for (int parts = 1; parts <= 32; ++parts) {
+            const int span = k_span(p.k, parts, granule);
+            if ((parts - 1) * span >= p.k || (parts > 1 && span < 64)) {
+                continue;
+            }
+            const uint64_t waves = (default_tiles * parts + sm_count - 1) / sm_count;
+            const uint64_t gemm = waves * ((uint64_t)span + kFp32WaveFixed);
+            const uint64_t merge =
+                parts > 1 ? kMergeFixed + (uint64_t)(2 * parts + 2) * p.m * p.n / kMergeFloatsPerTerm : 0;
+            if (gemm + merge < best) {
+                best = gemm + merge;
+                best_parts = parts;
+            }
+        }
     } else if (default_tiles < (uint64_t)sm_count * tiles[0].slots_per_sm && !out.rounding) {
         // Few tiles: search jointly (SelectCgemm3mDecomposition, :174-200).
         // Partitions are bounded by what can still fill the machine: at most

@@ -208,6 +208,7 @@ __global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, con
         const float2* X = xs(l & 1);
         const float2* Y = ys(l & 1);
         Cf acc{0.0f, 0.0f};
+#pragma unroll 8
         for (int q = 0; q < cnt; ++q) {
             const Cf t = term(X[q * kTile + ti], Y[q * kTile + tj]);
             acc.r = __fadd_rn(acc.r, t.r);
@@ -262,6 +263,7 @@ __global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, con
         prev_r = sr[l * 256 + tid];
         prev_i = si[l * 256 + tid];
         float r = __fadd_rn(init_r, 0.0f), im = __fadd_rn(init_i, 0.0f);
+#pragma unroll 8
         for (int q = 0; q < cnt; ++q) {
             const Cf t = term(X[q * kTile + ti], Y[q * kTile + tj]);
             r = __fadd_rn(r, t.r);

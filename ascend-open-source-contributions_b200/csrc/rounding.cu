@@ -132,13 +132,15 @@ __device__ __forceinline__ Cf term(float2 x, float2 y)
     return Cf{__fsub_rn(p, rr), __fadd_rn(p, q)};
 }
 
-// FP32 segmented replay of one 16 x 16 output tile, one output per thread.
-// For each of the 64 K lanes (lane l holds k in [l*span, (l+1)*span)) the
-// tile's op(A) rows and op(B) columns are staged in shared memory and every
-// thread accumulates its output's lane sum; the 64 lane sums of each output sit
-// in shared memory (S[l][thread]) for the reduction, the inclusive scan and
-// the seeded replay, all in the oracle's fixed orders.  Only flagged outputs
-// are written.
+// FP32 segmented replay of one 16 x 16 output tile with 512 threads: two per
+// output, the lower half of the block summing K lanes 0..31 and the upper half
+// lanes 32..63 (lane l holds k in [l*span, (l+1)*span)), both halves on the
+// same lane step at a time while the next step's op(A) rows and op(B) columns
+// are copied into shared memory.  The 64 lane sums of each output sit in
+// shared memory (S[l][output]); the lower-half thread computes the reduction,
+// the inclusive scan and the final selection, and both halves replay their
+// lanes seeded with the scanned prefixes -- all in the oracle's fixed orders.
+// Only flagged outputs are written.
 __device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes)
 {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
@@ -150,13 +152,14 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Shared memory of recompute_fp32_tiled: the 64 lane sums (real, imaginary)
-// of the tile's 256 outputs, then two staging buffers of one lane's operand
-// slices (16 rows of op(A) and 16 columns of op(B), span K terms each).
+// of the tile's 256 outputs, then two staging buffers, each with the operand
+// slices (16 rows of op(A) and 16 columns of op(B), span K terms each) of two
+// lanes, one for each half of the block.
 constexpr size_t kLaneSumBytes = (size_t)2 * kLanes * 256 * sizeof(float);
 constexpr size_t kStageElems = (size_t)kMaxSpan * kTile;  // float2 per operand per buffer
-constexpr size_t kRecomputeSmem = kLaneSumBytes + 2 * 2 * kStageElems * sizeof(float2);
+constexpr size_t kRecomputeSmem = kLaneSumBytes + 2 * 2 * 2 * kStageElems * sizeof(float2);
 
-__global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, const float2* __restrict__ rows_a,
+__global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, const float2* __restrict__ rows_a,
                                                             const float2* __restrict__ rows_b,
                                                             const uint32_t* __restrict__ flag_bits,
                                                             const uint32_t* __restrict__ tile_flags,
@@ -172,41 +175,46 @@ __global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, con
     }
     const int i0 = (blockIdx.x % tiles) * kTile, j0 = (blockIdx.x / tiles) * kTile;
     const int tid = threadIdx.x;
-    const int ti = tid & (kTile - 1), tj = tid >> 4;
+    // Thread (o, half): output o of the 16 x 16 tile, K lanes [32*half, 32*half + 32).
+    const int o = tid & 255, half = tid >> 8;
+    const int ti = o & (kTile - 1), tj = o >> 4;
     const int i = i0 + ti, j = j0 + tj;
-    // Buffer b holds xs[q][r] at stage_base[b*2*kStageElems + q*kTile + r] and
-    // ys[q][r] kStageElems after it.
-    auto xs = [&](int b) { return stage_base + (size_t)b * 2 * kStageElems; };
-    auto ys = [&](int b) { return stage_base + (size_t)b * 2 * kStageElems + kStageElems; };
+    // Buffer b holds, for both halves h, xs[q][r] and ys[q][r] of lane
+    // 32h + step at slot(b, h, 0) and slot(b, h, 1).
+    auto slot = [&](int b, int h, int op) { return stage_base + (size_t)((b * 2 + h) * 2 + op) * kStageElems; };
     auto lane_count = [&](int l) { return max(0, min(span, n - l * span)); };
-    // Asynchronous copy of lane l's operand slices into buffer b; positions
+    // Asynchronous copy of lanes step and 32 + step into buffer b; positions
     // past the end of K or past the matrix read as zero.
-    auto issue = [&](int l, int b) {
-        const int k0 = l * span;
-        const int cnt = lane_count(l);
-        float2* X = xs(b);
-        float2* Y = ys(b);
-        for (int e = tid; e < kTile * span; e += 256) {
-            const int r = e / span, q = e - r * span;
-            const bool okx = q < cnt && i0 + r < n, oky = q < cnt && j0 + r < n;
-            cp_async8(X + q * kTile + r, okx ? (const void*)(rows_a + (size_t)(i0 + r) * n + k0 + q) : rows_a,
-                      okx ? 8 : 0);
-            cp_async8(Y + q * kTile + r, oky ? (const void*)(rows_b + (size_t)(j0 + r) * n + k0 + q) : rows_b,
-                      oky ? 8 : 0);
+    auto issue = [&](int step, int b) {
+        for (int h = 0; h < 2; ++h) {
+            const int l = step + 32 * h;
+            const int k0 = l * span;
+            const int cnt = lane_count(l);
+            float2* X = slot(b, h, 0);
+            float2* Y = slot(b, h, 1);
+            for (int e = tid; e < kTile * span; e += 512) {
+                const int r = e / span, q = e - r * span;
+                const bool okx = q < cnt && i0 + r < n, oky = q < cnt && j0 + r < n;
+                cp_async8(X + q * kTile + r, okx ? (const void*)(rows_a + (size_t)(i0 + r) * n + k0 + q) : rows_a,
+                          okx ? 8 : 0);
+                cp_async8(Y + q * kTile + r, oky ? (const void*)(rows_b + (size_t)(j0 + r) * n + k0 + q) : rows_b,
+                          oky ? 8 : 0);
+            }
         }
         cp_async_commit();
     };
-    // pass 1: lane sums (lane l+1 is copied while lane l is summed)
+    // pass 1: lane sums (the next lane pair is copied while this one is summed)
     issue(0, 0);
-    for (int l = 0; l < kLanes; ++l) {
+    for (int step = 0; step < kLanes / 2; ++step) {
         cp_async_wait_all();
-        __syncthreads();  // lane l staged by every thread; lane l-1's buffer is free
-        if (l + 1 < kLanes) {
-            issue(l + 1, (l + 1) & 1);
+        __syncthreads();  // this step staged by every thread; the previous step's buffer is free
+        if (step + 1 < kLanes / 2) {
+            issue(step + 1, (step + 1) & 1);
         }
+        const int l = step + 32 * half;
         const int cnt = lane_count(l);
-        const float2* X = xs(l & 1);
-        const float2* Y = ys(l & 1);
+        const float2* X = slot(step & 1, half, 0);
+        const float2* Y = slot(step & 1, half, 1);
         Cf acc{0.0f, 0.0f};
 #pragma unroll 8
         for (int q = 0; q < cnt; ++q) {
@@ -214,54 +222,62 @@ __global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, con
             acc.r = __fadd_rn(acc.r, t.r);
             acc.i = __fadd_rn(acc.i, t.i);
         }
-        sr[l * 256 + tid] = acc.r;
-        si[l * 256 + tid] = acc.i;
+        sr[l * 256 + o] = acc.r;
+        si[l * 256 + o] = acc.i;
     }
-    // direct reduction (pairwise, stride 32 .. 1) in registers
-    float vr[kLanes], vi[kLanes];
+    __syncthreads();  // all 64 lane sums of every output are in place
+    float direct_r = 0.0f, direct_i = 0.0f, max_r = 0.0f, max_i = 0.0f;
+    if (half == 0) {
+        // direct reduction (pairwise, stride 32 .. 1) in registers
+        float vr[kLanes], vi[kLanes];
 #pragma unroll
-    for (int l = 0; l < kLanes; ++l) {
-        vr[l] = sr[l * 256 + tid];
-        vi[l] = si[l * 256 + tid];
-    }
+        for (int l = 0; l < kLanes; ++l) {
+            vr[l] = sr[l * 256 + o];
+            vi[l] = si[l * 256 + o];
+        }
 #pragma unroll
-    for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
+        for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
 #pragma unroll
-        for (int l = 0; l < stride; ++l) {
-            vr[l] = __fadd_rn(vr[l], vr[l + stride]);
-            vi[l] = __fadd_rn(vi[l], vi[l + stride]);
+            for (int l = 0; l < stride; ++l) {
+                vr[l] = __fadd_rn(vr[l], vr[l + stride]);
+                vi[l] = __fadd_rn(vi[l], vi[l + stride]);
+            }
+        }
+        direct_r = vr[0];
+        direct_i = vi[0];
+        // inclusive Hillis-Steele scan in place: new[l] = s[l] + s[l-d] for l >= d
+        for (int d = 1; d < kLanes; d *= 2) {
+            for (int l = kLanes - 1; l >= d; --l) {
+                sr[l * 256 + o] = __fadd_rn(sr[l * 256 + o], sr[(l - d) * 256 + o]);
+                si[l * 256 + o] = __fadd_rn(si[l * 256 + o], si[(l - d) * 256 + o]);
+            }
+        }
+        for (int l = 0; l < kLanes; ++l) {
+            const float ar = fabsf(sr[l * 256 + o]), ai = fabsf(si[l * 256 + o]);
+            max_r = ar > max_r ? ar : max_r;
+            max_i = ai > max_i ? ai : max_i;
         }
     }
-    const float direct_r = vr[0], direct_i = vi[0];
-    // inclusive Hillis-Steele scan in place: new[l] = s[l] + s[l-d] for l >= d
-    for (int d = 1; d < kLanes; d *= 2) {
-        for (int l = kLanes - 1; l >= d; --l) {
-            sr[l * 256 + tid] = __fadd_rn(sr[l * 256 + tid], sr[(l - d) * 256 + tid]);
-            si[l * 256 + tid] = __fadd_rn(si[l * 256 + tid], si[(l - d) * 256 + tid]);
-        }
-    }
-    float max_r = 0.0f, max_i = 0.0f;
-    for (int l = 0; l < kLanes; ++l) {
-        const float ar = fabsf(sr[l * 256 + tid]), ai = fabsf(si[l * 256 + tid]);
-        max_r = ar > max_r ? ar : max_r;
-        max_i = ai > max_i ? ai : max_i;
-    }
-    // pass 2: replay each lane seeded with the previous lanes' prefix
-    float prev_r = 0.0f, prev_i = 0.0f;
-    __syncthreads();  // every thread is done with the last buffer of pass 1
+    __syncthreads();  // scanned prefixes in place; every thread is done with the last buffer
+    // pass 2: replay each lane seeded with the previous lanes' prefix.  The
+    // upper half starts from the prefix of lane 31, read before the lower half
+    // overwrites it (after at least 31 more barriers).
+    float prev_r = half == 0 ? 0.0f : sr[31 * 256 + o];
+    float prev_i = half == 0 ? 0.0f : si[31 * 256 + o];
     issue(0, 0);
-    for (int l = 0; l < kLanes; ++l) {
+    for (int step = 0; step < kLanes / 2; ++step) {
         cp_async_wait_all();
         __syncthreads();
-        if (l + 1 < kLanes) {
-            issue(l + 1, (l + 1) & 1);
+        if (step + 1 < kLanes / 2) {
+            issue(step + 1, (step + 1) & 1);
         }
+        const int l = step + 32 * half;
         const int cnt = lane_count(l);
-        const float2* X = xs(l & 1);
-        const float2* Y = ys(l & 1);
+        const float2* X = slot(step & 1, half, 0);
+        const float2* Y = slot(step & 1, half, 1);
         const float init_r = prev_r, init_i = prev_i;
-        prev_r = sr[l * 256 + tid];
-        prev_i = si[l * 256 + tid];
+        prev_r = sr[l * 256 + o];
+        prev_i = si[l * 256 + o];
         float r = __fadd_rn(init_r, 0.0f), im = __fadd_rn(init_i, 0.0f);
 #pragma unroll 8
         for (int q = 0; q < cnt; ++q) {
@@ -269,33 +285,37 @@ __global__ void __launch_bounds__(256) recompute_fp32_tiled(int n, int span, con
             r = __fadd_rn(r, t.r);
             im = __fadd_rn(im, t.i);
         }
-        sr[l * 256 + tid] = __fsub_rn(r, init_r);
-        si[l * 256 + tid] = __fsub_rn(im, init_i);
+        sr[l * 256 + o] = __fsub_rn(r, init_r);
+        si[l * 256 + o] = __fsub_rn(im, init_i);
     }
+    __syncthreads();  // every replayed lane is in place
+    if (half == 0) {
+        float vr[kLanes], vi[kLanes];
 #pragma unroll
-    for (int l = 0; l < kLanes; ++l) {
-        vr[l] = sr[l * 256 + tid];
-        vi[l] = si[l * 256 + tid];
-    }
-#pragma unroll
-    for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
-#pragma unroll
-        for (int l = 0; l < stride; ++l) {
-            vr[l] = __fadd_rn(vr[l], vr[l + stride]);
-            vi[l] = __fadd_rn(vi[l], vi[l + stride]);
+        for (int l = 0; l < kLanes; ++l) {
+            vr[l] = sr[l * 256 + o];
+            vi[l] = si[l * 256 + o];
         }
-    }
-    float bridged_r = vr[0], bridged_i = vi[0];
-    if (max_r >= __fmul_rn(fabsf(direct_r), 32.0f)) {
-        bridged_r = direct_r;
-    }
-    if (max_i >= __fmul_rn(fabsf(direct_i), 32.0f)) {
-        bridged_i = direct_i;
-    }
-    if (i < n && j < n) {
-        const size_t idx = (size_t)j * n + i;
-        if (flagged(flag_bits, idx)) {
-            C[idx] = make_float2(bridged_r, bridged_i);
+#pragma unroll
+        for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
+#pragma unroll
+            for (int l = 0; l < stride; ++l) {
+                vr[l] = __fadd_rn(vr[l], vr[l + stride]);
+                vi[l] = __fadd_rn(vi[l], vi[l + stride]);
+            }
+        }
+        float bridged_r = vr[0], bridged_i = vi[0];
+        if (max_r >= __fmul_rn(fabsf(direct_r), 32.0f)) {
+            bridged_r = direct_r;
+        }
+        if (max_i >= __fmul_rn(fabsf(direct_i), 32.0f)) {
+            bridged_i = direct_i;
+        }
+        if (i < n && j < n) {
+            const size_t idx = (size_t)j * n + i;
+            if (flagged(flag_bits, idx)) {
+                C[idx] = make_float2(bridged_r, bridged_i);
+            }
         }
     }
 }
@@ -513,7 +533,7 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
             const size_t smem = kRecomputeSmem;
             err = cudaFuncSetAttribute(recompute_fp32_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (err == cudaSuccess) {
-                recompute_fp32_tiled<<<tiles * tiles, 256, smem, s>>>(n, span, L.rows_a, L.rows_b, L.flag_bits,
+                recompute_fp32_tiled<<<tiles * tiles, 512, smem, s>>>(n, span, L.rows_a, L.rows_b, L.flag_bits,
                                                                      L.tile_flags, static_cast<float2*>(p.C));
             }
         } else {

@@ -179,8 +179,10 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
     const int o = tid & 255, half = tid >> 8;
     const int ti = o & (kTile - 1), tj = o >> 4;
     const int i = i0 + ti, j = j0 + tj;
-    // Buffer b holds, for both halves h, xs[q][r] and ys[q][r] of lane
-    // 32h + step at slot(b, h, 0) and slot(b, h, 1).
+    // Buffer b holds, for both halves h, xs[r][q] and ys[r][q] of lane
+    // 32h + step at slot(b, h, 0) and slot(b, h, 1), rows span apart: span is
+    // odd, so the 16 rows a warp reads at one q fall in distinct bank pairs,
+    // and consecutive threads stage consecutive q of one row.
     auto slot = [&](int b, int h, int op) { return stage_base + (size_t)((b * 2 + h) * 2 + op) * kStageElems; };
     auto lane_count = [&](int l) { return max(0, min(span, n - l * span)); };
     // Asynchronous copy of lanes step and 32 + step into buffer b; positions
@@ -195,9 +197,9 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
             for (int e = tid; e < kTile * span; e += 512) {
                 const int r = e / span, q = e - r * span;
                 const bool okx = q < cnt && i0 + r < n, oky = q < cnt && j0 + r < n;
-                cp_async8(X + q * kTile + r, okx ? (const void*)(rows_a + (size_t)(i0 + r) * n + k0 + q) : rows_a,
+                cp_async8(X + r * span + q, okx ? (const void*)(rows_a + (size_t)(i0 + r) * n + k0 + q) : rows_a,
                           okx ? 8 : 0);
-                cp_async8(Y + q * kTile + r, oky ? (const void*)(rows_b + (size_t)(j0 + r) * n + k0 + q) : rows_b,
+                cp_async8(Y + r * span + q, oky ? (const void*)(rows_b + (size_t)(j0 + r) * n + k0 + q) : rows_b,
                           oky ? 8 : 0);
             }
         }
@@ -218,7 +220,7 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
         Cf acc{0.0f, 0.0f};
 #pragma unroll 8
         for (int q = 0; q < cnt; ++q) {
-            const Cf t = term(X[q * kTile + ti], Y[q * kTile + tj]);
+            const Cf t = term(X[ti * span + q], Y[tj * span + q]);
             acc.r = __fadd_rn(acc.r, t.r);
             acc.i = __fadd_rn(acc.i, t.i);
         }
@@ -281,7 +283,7 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
         float r = __fadd_rn(init_r, 0.0f), im = __fadd_rn(init_i, 0.0f);
 #pragma unroll 8
         for (int q = 0; q < cnt; ++q) {
-            const Cf t = term(X[q * kTile + ti], Y[q * kTile + tj]);
+            const Cf t = term(X[ti * span + q], Y[tj * span + q]);
             r = __fadd_rn(r, t.r);
             im = __fadd_rn(im, t.i);
         }

@@ -157,6 +157,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // lanes, one for each half of the block.
 constexpr size_t kLaneSumBytes = (size_t)2 * kLanes * 256 * sizeof(float);
 constexpr size_t kStageElems = (size_t)kMaxSpan * kTile;  // float2 per operand per buffer
+constexpr int kStageIters = (kTile * kMaxSpan + 511) / 512;  // staging elements per thread
 constexpr size_t kRecomputeSmem = kLaneSumBytes + 2 * 2 * 2 * kStageElems * sizeof(float2);
 
 __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, const float2* __restrict__ rows_a,
@@ -176,31 +177,53 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
     const int i0 = (blockIdx.x % tiles) * kTile, j0 = (blockIdx.x / tiles) * kTile;
     const int tid = threadIdx.x;
     // Thread (o, half): output o of the 16 x 16 tile, K lanes [32*half, 32*half + 32).
+    // A warp covers 8 rows x 4 columns of the tile, so each of its operand
+    // reads touches at most 8 distinct shared addresses.
     const int o = tid & 255, half = tid >> 8;
-    const int ti = o & (kTile - 1), tj = o >> 4;
+    const int ti = (o & 7) | (((o >> 5) & 1) << 3), tj = ((o >> 3) & 3) | ((o >> 6) << 2);
     const int i = i0 + ti, j = j0 + tj;
     // Buffer b holds, for both halves h, xs[r][q] and ys[r][q] of lane
     // 32h + step at slot(b, h, 0) and slot(b, h, 1), rows span apart: span is
-    // odd, so the 16 rows a warp reads at one q fall in distinct bank pairs,
-    // and consecutive threads stage consecutive q of one row.
+    // odd, so the rows a warp reads at one q fall in distinct bank pairs, and
+    // consecutive threads stage consecutive q of one row.
     auto slot = [&](int b, int h, int op) { return stage_base + (size_t)((b * 2 + h) * 2 + op) * kStageElems; };
     auto lane_count = [&](int l) { return max(0, min(span, n - l * span)); };
+    // Staging element e = tid + 512u of a lane slice (u < staged): row
+    // r = e / span, K offset q = e % span, shared offset e.  These are fixed for
+    // the launch; a step only moves the source by the lane's K start.  A row
+    // outside the matrix gets q = span, which fails every q < count test.
+    const int slice = kTile * span;
+    const int staged = tid < slice ? (slice - tid + 511) / 512 : 0;
+    const float2* src_a[kStageIters];
+    const float2* src_b[kStageIters];
+    int qa[kStageIters], qb[kStageIters];
+#pragma unroll
+    for (int u = 0; u < kStageIters; ++u) {
+        const int e = tid + 512 * u;
+        const int r = e / span, q = e - r * span;
+        const bool in_a = u < staged && i0 + r < n, in_b = u < staged && j0 + r < n;
+        src_a[u] = in_a ? rows_a + (size_t)(i0 + r) * n + q : rows_a;
+        src_b[u] = in_b ? rows_b + (size_t)(j0 + r) * n + q : rows_b;
+        qa[u] = in_a ? q : span;
+        qb[u] = in_b ? q : span;
+    }
     // Asynchronous copy of lanes step and 32 + step into buffer b; positions
     // past the end of K or past the matrix read as zero.
     auto issue = [&](int step, int b) {
+#pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int l = step + 32 * h;
             const int k0 = l * span;
             const int cnt = lane_count(l);
-            float2* X = slot(b, h, 0);
-            float2* Y = slot(b, h, 1);
-            for (int e = tid; e < kTile * span; e += 512) {
-                const int r = e / span, q = e - r * span;
-                const bool okx = q < cnt && i0 + r < n, oky = q < cnt && j0 + r < n;
-                cp_async8(X + r * span + q, okx ? (const void*)(rows_a + (size_t)(i0 + r) * n + k0 + q) : rows_a,
-                          okx ? 8 : 0);
-                cp_async8(Y + r * span + q, oky ? (const void*)(rows_b + (size_t)(j0 + r) * n + k0 + q) : rows_b,
-                          oky ? 8 : 0);
+            float2* X = slot(b, h, 0) + tid;
+            float2* Y = slot(b, h, 1) + tid;
+#pragma unroll
+            for (int u = 0; u < kStageIters; ++u) {
+                if (u < staged) {
+                    const bool okx = qa[u] < cnt, oky = qb[u] < cnt;
+                    cp_async8(X + 512 * u, okx ? (const void*)(src_a[u] + k0) : rows_a, okx ? 8 : 0);
+                    cp_async8(Y + 512 * u, oky ? (const void*)(src_b[u] + k0) : rows_b, oky ? 8 : 0);
+                }
             }
         }
         cp_async_commit();

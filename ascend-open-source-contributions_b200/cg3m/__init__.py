@@ -34,6 +34,11 @@ STATUS_NAMES = {0: "SUCCESS", 1: "HANDLE_IS_NULLPTR", 2: "INVALID_VALUE", 3: "IN
 OP = {"N": 0, "T": 1, "C": 2, "R": 3}
 FORM = {"fp32": 0, "tf32x3": 1, "bf16x6": 2, "bf16x9": 3}
 ROUNDING = {"auto": 0, "off": 1}
+# FP32 engines: planner's choice, packed planes (pack + GEMM [+ merge]), one
+# launch with the K partitions merged in a thread-block cluster.
+ENGINE = {"auto": 0, "packed": 1, "onchip": 2}
+# Tiles of the one-launch engine (onchip_tile - 1 indexes this list).
+ONCHIP_TILES = [(128, 64), (64, 64), (128, 32), (32, 128), (64, 32), (32, 32)]
 
 
 class cg3mComplex(ctypes.Structure):
@@ -42,7 +47,8 @@ class cg3mComplex(ctypes.Structure):
 
 class cg3mOptions(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int), ("rounding", ctypes.c_int), ("k_partitions", ctypes.c_int),
-                ("tc_segment", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+                ("tc_segment", ctypes.c_int), ("engine", ctypes.c_int), ("onchip_tile", ctypes.c_int),
+                ("reserved", ctypes.c_int * 2)]
 
 
 class cg3mCallInfo(ctypes.Structure):
@@ -178,17 +184,19 @@ class Handle:
         return f.value
 
     def cgemm3m(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, form="fp32", rounding="auto",
-                k_partitions=0, raw=False, tc_segment=0):
+                k_partitions=0, raw=False, tc_segment=0, engine="auto", onchip_tile=0):
         """C <- alpha*op(A)*op(B) + beta*C on device buffers; returns the call info.
 
         ``raw=True`` calls the drop-in cg3mCgemm3m (FP32 form only) and returns
-        the status instead of raising."""
+        the status instead of raising.  ``engine`` ("auto", "packed", "onchip")
+        and ``onchip_tile`` (0 or 1..6, see ONCHIP_TILES) pick the FP32 engine."""
         al, be = cx(alpha), cx(beta)
         if raw:
             return _lib.cg3mCgemm3m(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda, ptr(B),
                                     ldb, ctypes.byref(be), ptr(C), ldc)
         opts = cg3mOptions(FORM[form] if isinstance(form, str) else form,
-                           ROUNDING[rounding] if isinstance(rounding, str) else rounding, k_partitions, tc_segment)
+                           ROUNDING[rounding] if isinstance(rounding, str) else rounding, k_partitions, tc_segment,
+                           ENGINE[engine] if isinstance(engine, str) else engine, onchip_tile)
         info = cg3mCallInfo()
         st = _lib.cg3mCgemm3mEx(self.h, _op(transa), _op(transb), m, n, k, ctypes.byref(al), ptr(A), lda, ptr(B), ldb,
                                 ctypes.byref(be), ptr(C), ldc, ctypes.byref(opts), ctypes.byref(info))
@@ -303,13 +311,14 @@ def validate(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, allow
 
 
 def plan(transa, transb, m, n, k, alpha=1, beta=0, lda=None, ldb=None, ldc=None, form="fp32", rounding="auto",
-         k_partitions=0, sm_count=148):
+         k_partitions=0, sm_count=148, engine="auto", onchip_tile=0):
     """The planner's decision (host only)."""
     ta, tb = _op(transa), _op(transb)
     lda = lda or (m if ta in (0, 3) else k)
     ldb = ldb or (k if tb in (0, 3) else n)
     ldc = ldc or m
-    opts = cg3mOptions(FORM[form], ROUNDING[rounding], k_partitions)
+    opts = cg3mOptions(FORM[form], ROUNDING[rounding], k_partitions, 0,
+                       ENGINE[engine] if isinstance(engine, str) else engine, onchip_tile)
     info = cg3mCallInfo()
     _check(_lib.cg3mPlan(ta, tb, m, n, k, ctypes.byref(cx(alpha)), lda, ldb, ctypes.byref(cx(beta)), ldc,
                          ctypes.byref(opts), sm_count, ctypes.byref(info)), "cg3mPlan")

@@ -160,7 +160,7 @@ cg3mStatus_t run_one(cg3mContext* h, int transa, int transb, int m, int n, int k
     const cudaError_t err = enqueue(h->stream, p, plan, ws, h->status, &kernels, h->stage_events,
                                     h->stage_event_count);
     if (info != nullptr) {
-        info->path = plan.parts > 1 ? 3 : 2;
+        info->path = plan.engine == 2 ? 4 : plan.parts > 1 ? 3 : 2;
         info->tile_m = plan.tile_m;
         info->tile_n = plan.tile_n;
         info->k_partitions = plan.parts;
@@ -186,6 +186,14 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
         }
     };
     mark(0);
+    if (plan.engine == 2) {
+        const cudaError_t e = launch_single(s, p, 0, 0, plan.onchip_tile, plan.parts);
+        mark(1);
+        if (kernels != nullptr) {
+            *kernels = 1;
+        }
+        return e;
+    }
     cudaError_t err = launch_pack(s, p, plan, ws);
     mark(++count);
     if (err == cudaSuccess) {
@@ -680,14 +688,14 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
         return CG3M_STATUS_INVALID_VALUE;
     }
     std::memset(info, 0, sizeof(*info));
-    info->path = plan.parts > 1 ? 3 : 2;
+    info->path = plan.engine == 2 ? 4 : plan.parts > 1 ? 3 : 2;
     info->form = plan.form;
     info->tile_m = plan.tile_m;
     info->tile_n = plan.tile_n;
     info->k_partitions = plan.parts;
     info->k_span = plan.span;
     info->rounding = plan.rounding ? 1 : 0;
-    info->kernels = 2 + (plan.parts > 1 ? 1 : 0) + (plan.rounding ? 4 : 0);
+    info->kernels = plan.engine == 2 ? 1 : 2 + (plan.parts > 1 ? 1 : 0) + (plan.rounding ? 4 : 0);
     info->workspace_bytes = plan.total;
     return CG3M_STATUS_SUCCESS;
 }

@@ -41,6 +41,7 @@
 
 #include "cg3m_internal.h"
 #include "epilogue.cuh"
+#include "ptx.cuh"
 
 namespace cg3m {
 namespace {
@@ -271,34 +272,34 @@ __device__ __forceinline__ float2 part_product(float q0, float q1, float q2, flo
 
 __device__ __forceinline__ bool finite2(float2 v) { return isfinite(v.x) && isfinite(v.y); }
 
+// 16 x 16 threads over the tile; each warp is 8 (along m) x 4 (along n)
+// threads, so one vector load of A or B per warp spans at most 128 bytes
+// (one shared-memory wavefront).
+__device__ __forceinline__ int thread_tx() { return ((threadIdx.x >> 5) & 1) * 8 + (threadIdx.x & 7); }
+__device__ __forceinline__ int thread_ty() { return (threadIdx.x >> 6) * 4 + ((threadIdx.x & 31) >> 3); }
+
 template <int BM, int BN, int MODE>
-__device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, float* planes, float* partials,
-                         uint32_t* counters, int* last_flag)
+using AccTile = float[Cfg<BM, BN, MODE>::ACC][Cfg<BM, BN, MODE>::MT][Cfg<BM, BN, MODE>::NT];
+
+// The products of K terms [kbeg, kbeg + klen) of the BM x BN tile at (m0, n0),
+// accumulated from zero into acc: kStages raw slots of RAWS elements and two
+// plane buffers of PLS floats.
+template <int BM, int BN, int MODE, int RAWS, int PLS>
+__device__ __forceinline__ void accumulate(const BProblem& p, int m0, int n0, int kbeg, int klen, float2* raw,
+                                           float* planes, AccTile<BM, BN, MODE>& acc)
 {
     using G = Cfg<BM, BN, MODE>;
-    static_assert(G::A_FLOATS + G::B_FLOATS <= kPlaneFloats, "planes exceed their buffer");
-    static_assert((BM + BN) * BK <= kRawElems, "raw stage exceeds its slot");
+    static_assert(G::A_FLOATS + G::B_FLOATS <= PLS, "planes exceed their buffer");
+    static_assert((BM + BN) * BK <= RAWS, "raw stage exceeds its slot");
     static_assert((BM * BK) % kThreads == 0 && (BN * BK) % kThreads == 0, "whole elements per thread");
-    const BProblem p = prob;  // registers: no reloads after barriers
-    const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
-    const int m0 = tm * BM, n0 = tn * BN;
-    const int kbeg = part * p.span;
-    const int kend = min(p.k, kbeg + p.span);
-    const int klen = kend > kbeg ? kend - kbeg : 0;
     const int nk = (klen + BK - 1) / BK;
-    // 16 x 16 threads over the tile; each warp is 8 (along m) x 4 (along n)
-    // threads, so one vector load of A or B per warp spans at most 128 bytes
-    // (one shared-memory wavefront).
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int tx = (warp & 1) * 8 + (lane & 7), ty = (warp >> 1) * 4 + (lane >> 3);
+    const int tx = thread_tx(), ty = thread_ty();
     const bool na = p.ta == CG3M_OP_N || p.ta == CG3M_OP_R;
     const bool nb = p.tb == CG3M_OP_N || p.tb == CG3M_OP_R;
     const Feed fa = make_feed<BM>(p.A, p.lda, na, m0, min(BM, p.m - m0), kbeg,
                                   (p.ta == CG3M_OP_C || p.ta == CG3M_OP_R) ? -1.0f : 1.0f);
     const Feed fb = make_feed<BN>(p.B, p.ldb, !nb, n0, min(BN, p.n - n0), kbeg,
                                   (p.tb == CG3M_OP_C || p.tb == CG3M_OP_R) ? -1.0f : 1.0f);
-
-    float acc[G::ACC][G::MT][G::NT];
 #pragma unroll
     for (int c = 0; c < G::ACC; ++c)
 #pragma unroll
@@ -313,7 +314,7 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
 #pragma unroll
     for (int s = 0; s < kStages - 1; ++s) {
         if (s < nk) {
-            float2* slot = raw + s * kRawElems;
+            float2* slot = raw + s * RAWS;
             issue<G::EA>(fa, slot, s, klen);
             issue<G::EB>(fb, slot + BM * BK, s, klen);
         }
@@ -324,14 +325,14 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
         // thread: each thread copies and converts only its own elements).
         const int nxt = kb + kStages - 1;
         if (nxt < nk) {
-            float2* slot = raw + (nxt % kStages) * kRawElems;
+            float2* slot = raw + (nxt % kStages) * RAWS;
             issue<G::EA>(fa, slot, nxt, klen);
             issue<G::EB>(fb, slot + BM * BK, nxt, klen);
         }
         cp_async_commit();
         cp_async_wait<kStages - 1>();  // this thread's copies of K-block kb have landed
-        const float2* slot = raw + (kb % kStages) * kRawElems;
-        float* sA = planes + (kb & 1) * kPlaneFloats;
+        const float2* slot = raw + (kb % kStages) * RAWS;
+        float* sA = planes + (kb & 1) * PLS;
         float* sB = sA + G::A_FLOATS;
         convert<G::SA, G::EA, G::COMPS>(fa, slot, sA);
         convert<G::SB, G::EB, G::COMPS>(fb, slot + BM * BK, sB);
@@ -372,6 +373,22 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
         }
     }
     cp_async_wait<0>();  // only empty groups can remain; keep the count at zero between tasks
+}
+
+template <int BM, int BN, int MODE>
+__device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, float* planes, float* partials,
+                         uint32_t* counters, int* last_flag)
+{
+    using G = Cfg<BM, BN, MODE>;
+    const BProblem p = prob;  // registers: no reloads after barriers
+    const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+    const int m0 = tm * BM, n0 = tn * BN;
+    const int kbeg = part * p.span;
+    const int kend = min(p.k, kbeg + p.span);
+    const int klen = kend > kbeg ? kend - kbeg : 0;
+    const int tx = thread_tx(), ty = thread_ty();
+    float acc[G::ACC][G::MT][G::NT];
+    accumulate<BM, BN, MODE, kRawElems, kPlaneFloats>(p, m0, n0, kbeg, klen, raw, planes, acc);
 
     // Output (i, j) of this thread: row m0 + (i / VA)*16*VA + tx*VA + i % VA,
     // column n0 + (j / VB)*16*VB + ty*VB + j % VB.
@@ -558,6 +575,164 @@ __global__ void __launch_bounds__(kThreads) strided_kernel(BProblem proto, long 
         p.partial_off = (size_t)b * partial_stride;
         p.counter_off = 1 + (size_t)b * tiles;
         dispatch_task<MODE>(p, r / proto.parts, r % proto.parts, raw, planes, partials, counters, &last_flag);
+    }
+}
+
+// ---- one problem, one launch: K partitions merged through the cluster -------
+//
+// Block (tile, part) of grid (tiles, parts) computes partition `part` of output
+// tile `tile` with the same K loop as the persistent kernels; the partitions
+// of a tile form one thread-block cluster (cluster dims 1 x parts).  Each block
+// leaves its partition's (Re, Im) in its own shared memory; after a cluster
+// barrier, block q merges the q-th slice of the tile's outputs, reading every
+// partition's value through distributed shared memory and adding them in
+// partition order with the merge arithmetic of the drop-in, then applies
+// alpha/beta and stores.  A second cluster barrier keeps every block's shared
+// memory in place until all reads are done.  Nothing goes through global
+// memory but A, B and C: no workspace, no counters, no second launch.  Both
+// barriers are reached by every thread of every block (no early exits).
+template <int BM, int BN, int MODE>
+struct SingleCfg {
+    static constexpr int RAWS = (BM + BN) * BK;  // elements per raw slot
+    static constexpr int PLS = Cfg<BM, BN, MODE>::A_FLOATS + Cfg<BM, BN, MODE>::B_FLOATS;
+    static constexpr size_t SMEM = (size_t)kStages * RAWS * sizeof(float2) + 2 * (size_t)PLS * sizeof(float);
+    static_assert((size_t)2 * BM * BN * sizeof(float) <= (size_t)kStages * RAWS * sizeof(float2),
+                  "partials exceed the raw slots");
+};
+
+__device__ __forceinline__ float ld_cluster_f32(uint32_t addr)
+{
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+    return v;
+}
+
+constexpr int kMaxClusterParts = 8;  // portable cluster size
+
+template <int BM, int BN, int MODE>
+__global__ void __launch_bounds__(kThreads) single_kernel(const BProblem p)
+{
+    using G = Cfg<BM, BN, MODE>;
+    using S = SingleCfg<BM, BN, MODE>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* raw = reinterpret_cast<float2*>(smem_raw);
+    float* planes = reinterpret_cast<float*>(smem_raw + (size_t)kStages * S::RAWS * sizeof(float2));
+    const int tile = blockIdx.x, part = blockIdx.y;
+    const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+    const int m0 = tm * BM, n0 = tn * BN;
+    const int kbeg = part * p.span;
+    const int kend = min(p.k, kbeg + p.span);
+    const int klen = kend > kbeg ? kend - kbeg : 0;
+    const int tx = thread_tx(), ty = thread_ty();
+    float acc[G::ACC][G::MT][G::NT];
+    accumulate<BM, BN, MODE, S::RAWS, S::PLS>(p, m0, n0, kbeg, klen, raw, planes, acc);
+
+    if (p.parts == 1) {
+#pragma unroll
+        for (int j = 0; j < G::NT; ++j) {
+            const int col = n0 + (j / G::VB) * 16 * G::VB + ty * G::VB + j % G::VB;
+#pragma unroll
+            for (int i = 0; i < G::MT; ++i) {
+                const int row = m0 + (i / G::VA) * 16 * G::VA + tx * G::VA + i % G::VA;
+                if (row < p.m && col < p.n) {
+                    float2 v =
+                        part_product<MODE>(acc[0][i][j], acc[1][i][j], acc[2][i][j], acc[G::ACC - 1][i][j]);
+                    if (p.repair && !finite2(v)) {
+                        v = repair_product(p, row, col);
+                    }
+                    float2* cp = p.C + (size_t)col * p.ldc + row;
+                    *cp = epilogue_value(v.x, v.y, p.epi, cp);
+                }
+            }
+        }
+        return;
+    }
+
+    // This partition's (Re, Im) at part_re[e], part_im[e], e = c*BM + r (tile
+    // coordinates), over the raw slots: every thread's copies have landed and
+    // been converted before the K loop's last barrier.
+    float* part_re = reinterpret_cast<float*>(raw);
+    float* part_im = part_re + BM * BN;
+#pragma unroll
+    for (int j = 0; j < G::NT; ++j) {
+        const int c = (j / G::VB) * 16 * G::VB + ty * G::VB + j % G::VB;
+#pragma unroll
+        for (int i = 0; i < G::MT; ++i) {
+            const int r = (i / G::VA) * 16 * G::VA + tx * G::VA + i % G::VA;
+            const float2 v = part_product<MODE>(acc[0][i][j], acc[1][i][j], acc[2][i][j], acc[G::ACC - 1][i][j]);
+            part_re[c * BM + r] = v.x;
+            part_im[c * BM + r] = v.y;
+        }
+    }
+    cluster_sync();  // every partition's values are in place and visible to the cluster
+    const uint32_t re_local = static_cast<uint32_t>(__cvta_generic_to_shared(part_re));
+    const uint32_t im_local = static_cast<uint32_t>(__cvta_generic_to_shared(part_im));
+    const int per = (BM * BN + p.parts - 1) / p.parts;  // outputs merged by each block
+    const int e_end = min(BM * BN, (part + 1) * per);
+    for (int e = part * per + (int)threadIdx.x; e < e_end; e += kThreads) {
+        const int r = e % BM, c = e / BM;
+        const int row = m0 + r, col = n0 + c;
+        float tr[kMaxClusterParts], ti[kMaxClusterParts];
+#pragma unroll
+        for (int q = 0; q < kMaxClusterParts; ++q) {
+            if (q < p.parts) {
+                tr[q] = ld_cluster_f32(mapa_shared(re_local + 4u * e, q));
+                ti[q] = ld_cluster_f32(mapa_shared(im_local + 4u * e, q));
+            }
+        }
+        float re = tr[0], im = ti[0];
+#pragma unroll
+        for (int q = 1; q < kMaxClusterParts; ++q) {
+            if (q < p.parts) {
+                re = __fadd_rn(re, tr[q]);
+                im = __fadd_rn(im, ti[q]);
+            }
+        }
+        if (row < p.m && col < p.n) {
+            float2 v = make_float2(re, im);
+            if (p.repair && !finite2(v)) {
+                v = repair_product(p, row, col);
+            }
+            float2* cp = p.C + (size_t)col * p.ldc + row;
+            *cp = epilogue_value(v.x, v.y, p.epi, cp);
+        }
+    }
+    cluster_sync();  // no block leaves while others may still read its shared memory
+}
+
+template <int MODE>
+cudaError_t launch_single_tile(cudaStream_t s, const BProblem& bp, int tile)
+{
+    auto run = [&](auto kernel, size_t smem) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) {
+            return e;
+        }
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)(bp.tiles_m * bp.tiles_n), (unsigned)bp.parts, 1);
+        cfg.blockDim = dim3(kThreads, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 1;
+        attr[0].val.clusterDim.y = (unsigned)bp.parts;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, kernel, bp);
+    };
+    switch (tile) {
+        case 0:
+            if constexpr (MODE == kMode3M) {
+                return run(single_kernel<128, 64, MODE>, SingleCfg<128, 64, MODE>::SMEM);
+            }
+            return cudaErrorInvalidValue;
+        case 1: return run(single_kernel<64, 64, MODE>, SingleCfg<64, 64, MODE>::SMEM);
+        case 2: return run(single_kernel<128, 32, MODE>, SingleCfg<128, 32, MODE>::SMEM);
+        case 3: return run(single_kernel<32, 128, MODE>, SingleCfg<32, 128, MODE>::SMEM);
+        case 4: return run(single_kernel<64, 32, MODE>, SingleCfg<64, 32, MODE>::SMEM);
+        default: return run(single_kernel<32, 32, MODE>, SingleCfg<32, 32, MODE>::SMEM);
     }
 }
 
@@ -866,6 +1041,114 @@ bool make_strided_plan(const Problem& p, int mode, int batch, int sm_count, Stri
     pl.bytes = pl.partial_off + (size_t)batch * pl.partial_stride * sizeof(float);
     *out = pl;
     return true;
+}
+
+int single_tile_bm(int tile) { return tile_bm(tile); }
+int single_tile_bn(int tile) { return tile_bn(tile); }
+
+// Time model of the one-launch kernel (three-product mode), in microseconds,
+// fitted on B200 to 1100 timed (shape, tile, partitions) launches (median
+// error 1.6 %).  Clusters of `parts` blocks run in waves of as many clusters
+// as fit at once (cudaOccupancyMaxActiveClusters on a 148-SM B200, scaled for
+// other SM counts); each wave costs the tile's fixed part (first copies,
+// epilogue) plus span x its per-term time, and tiles that share an SM (64 x 32:
+// two blocks, 32 x 32: three) add a per-term cost for every block on the
+// busiest SM.  The cluster merge costs a little per partition.
+namespace {
+struct SingleCost {
+    double fixed_us, term_ns, shared_term_ns;
+};
+constexpr SingleCost kSingleCost[kTileCount] = {{4.92, 188.9, 0.0},  {3.54, 143.7, 0.0}, {3.36, 150.1, 0.0},
+                                                {3.34, 130.7, 0.0},  {2.91, 45.6, 62.1}, {2.14, 19.9, 43.1}};
+constexpr int kSingleOcc[kTileCount] = {1, 1, 1, 1, 2, 3};
+// Clusters resident at once on 148 SMs, by blocks per SM (1..3) and cluster size (1..8).
+constexpr int kClusterCap[3][kMaxClusterParts] = {{148, 74, 45, 33, 26, 22, 15, 15},
+                                                  {296, 148, 93, 71, 56, 45, 37, 33},
+                                                  {444, 222, 142, 104, 82, 71, 56, 48}};
+constexpr double kSingleMergePerPartUs = 0.152;
+}  // namespace
+
+double plan_single(int m, int n, int k, int mode, int sm_count, int forced_tile, int forced_parts, int* tile,
+                   int* parts)
+{
+    sm_count = std::max(sm_count, 1);
+    double best = 1e300;
+    int bt = kTileCount - 1, bp = 1;
+    for (int t = 0; t < kTileCount; ++t) {
+        if ((forced_tile >= 0 && t != forced_tile) || (mode == kMode4M && t == 0)) {
+            continue;
+        }
+        const long long tiles = (long long)ceil_div(m, tile_bm(t)) * ceil_div(n, tile_bn(t));
+        for (int q = 1; q <= kMaxClusterParts; ++q) {
+            if (forced_parts > 0 && q != forced_parts) {
+                continue;
+            }
+            const int span = q == 1 ? k : span_for(k, q);
+            if (q > 1 && (q - 1) * span >= k) {
+                continue;
+            }
+            const long long cap =
+                std::max<long long>(1, (long long)kClusterCap[kSingleOcc[t] - 1][q - 1] * sm_count / 148);
+            const long long waves = (tiles + cap - 1) / cap;
+            const long long load = (tiles * q + sm_count - 1) / sm_count;
+            const SingleCost& c = kSingleCost[t];
+            double us = (double)waves * c.fixed_us +
+                        span * 1e-3 * ((double)waves * c.term_ns + (double)load * c.shared_term_ns);
+            if (q > 1) {
+                us += kSingleMergePerPartUs * q;
+            }
+            if (us < best) {
+                best = us;
+                bt = t;
+                bp = q;
+            }
+        }
+    }
+    if (tile != nullptr) {
+        *tile = bt;
+    }
+    if (parts != nullptr) {
+        *parts = bp;
+    }
+    return best;
+}
+
+cudaError_t launch_single(cudaStream_t s, const Problem& p, int mode, int repair, int tile, int parts)
+{
+    if (p.m <= 0 || p.n <= 0 || p.k <= 0 || parts < 1 || parts > kMaxClusterParts || tile < 0 ||
+        tile >= kTileCount || (mode != kMode3M && mode != kMode4M) || (mode == kMode4M && tile == 0)) {
+        return cudaErrorInvalidValue;
+    }
+    BProblem bp{};
+    bp.ta = p.transa;
+    bp.tb = p.transb;
+    bp.m = p.m;
+    bp.n = p.n;
+    bp.k = p.k;
+    const bool beta_zero = p.br == 0.0f && p.bi == 0.0f;
+    const bool unit = p.ar == 1.0f && p.ai == 0.0f && beta_zero;
+    bp.epi = EpiParams{p.ar, p.ai, p.br, p.bi, unit ? 1 : 0, beta_zero ? 1 : 0};
+    bp.A = static_cast<const float2*>(p.A);
+    bp.B = static_cast<const float2*>(p.B);
+    bp.C = static_cast<float2*>(p.C);
+    bp.lda = p.lda;
+    bp.ldb = p.ldb;
+    bp.ldc = p.ldc;
+    bp.tile = tile;
+    bp.repair = repair;
+    bp.parts = parts;
+    bp.span = span_for(p.k, parts);
+    if ((parts - 1) * bp.span >= p.k) {
+        return cudaErrorInvalidValue;  // the caller passes a partition count whose last part is non-empty
+    }
+    if (parts == 1) {
+        bp.span = p.k;
+    }
+    bp.tiles_m = ceil_div(p.m, tile_bm(tile));
+    bp.tiles_n = ceil_div(p.n, tile_bn(tile));
+    const cudaError_t e =
+        mode == kMode3M ? launch_single_tile<kMode3M>(s, bp, tile) : launch_single_tile<kMode4M>(s, bp, tile);
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_strided(cudaStream_t s, const Problem& p, int mode, int repair, long long sA, long long sB,

@@ -48,6 +48,8 @@ struct Plan {
     bool beta_zero = false;
     bool rounding = false;
     int tc_segment = 0;      // K terms per TMEM accumulation segment (tensor-core forms)
+    int engine = 1;          // 1 packed planes (pack + GEMM [+ merge]), 2 one cluster-merged launch
+    int onchip_tile = 0;     // engine 2: tile index of the on-chip family (0 128x64 .. 5 32x32)
     // workspace layout (byte offsets from the workspace base)
     size_t planes_a_off = 0, planes_b_off = 0, partial_off = 0, round_off = 0, total = 0;
     int pitch_a = 0, pitch_b = 0;  // elements per plane row
@@ -110,6 +112,18 @@ struct StridedPlan {
     size_t bytes = 0;           // workspace bytes
 };
 bool make_strided_plan(const Problem& p, int mode, int batch, int sm_count, StridedPlan* out);
+// One problem in one launch of the on-chip family: grid (tiles, parts), the
+// `parts` K partitions of a tile merged through its thread-block cluster
+// (parts <= 8, and (parts - 1) * span < k).  tile: 0 128x64, 1 64x64,
+// 2 128x32, 3 32x128, 4 64x32, 5 32x32.  No workspace.
+cudaError_t launch_single(cudaStream_t s, const Problem& p, int mode, int repair, int tile, int parts);
+// The one-launch plan for an m x n x k problem in `mode`: tile and K
+// partitions (each forced when >= 0), chosen to minimise the estimated time,
+// which is returned in microseconds.
+double plan_single(int m, int n, int k, int mode, int sm_count, int forced_tile, int forced_parts, int* tile,
+                   int* parts);
+int single_tile_bm(int tile);
+int single_tile_bn(int tile);
 cudaError_t launch_strided(cudaStream_t s, const Problem& p, int mode, int repair, long long sA, long long sB,
                            long long sC, int batch, const StridedPlan& plan, void* ws, int sm_count);
 

@@ -93,6 +93,14 @@ const TileChoice kFp32Tiles[] = {{128, 64, 1}};
 constexpr uint64_t kFp32WaveFixed = 38;
 constexpr uint64_t kMergeFixed = 30;
 constexpr uint64_t kMergeFloatsPerTerm = 41500;
+// The same costs in microseconds for the whole packed call (pack kernel over
+// op(A) and op(B) -- 8 bytes read, 12 written per element -- GEMM waves, merge
+// kernel), fitted on B200 to 28 timed shapes (median error 3.4 %).
+constexpr double kPackedFixedUs = 0.47;
+constexpr double kPackedUsPerMB = 0.127;
+constexpr double kPackedUsPerTerm = 0.1619;
+constexpr double kMergeLaunchUs = 3.0;
+constexpr double kMergeUsPerTerm = 0.0765;
 // Tensor-core kernel tile (gemm_tc.cu): 128 x 128, one CTA per SM (TMEM).
 const TileChoice kTcTiles[] = {{128, 128, 1}};
 
@@ -118,6 +126,17 @@ int k_span(int k, int parts, int g = 16)
     return ceil_div(ceil_div(k, g), parts) * g;
 }
 
+double packed_time_us(const Problem& p, int parts, int span, uint64_t tiles, int sm_count)
+{
+    const uint64_t waves = (tiles * parts + sm_count - 1) / sm_count;
+    const double bytes = ((double)p.m * p.k + (double)p.k * p.n) * 20.0;
+    double us = kPackedFixedUs + kPackedUsPerMB * bytes * 1e-6 + kPackedUsPerTerm * (double)waves * (span + kFp32WaveFixed);
+    if (parts > 1) {
+        us += kMergeLaunchUs + kMergeUsPerTerm * (kMergeFixed + (double)(2 * parts + 2) * p.m * p.n / kMergeFloatsPerTerm);
+    }
+    return us;
+}
+
 }  // namespace
 
 bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* plan)
@@ -138,10 +157,35 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
         sm_count = 148;
     }
     const bool tc = opts.form != CG3M_FORM_FP32;
+    if (opts.engine < 0 || opts.engine > 2 || opts.onchip_tile < 0 || opts.onchip_tile > 6) {
+        return false;
+    }
 
     // Rounding-correction gate (cgemm_host.cpp:234-238).
     out.rounding = opts.rounding == CG3M_ROUNDING_AUTO && out.unit && p.m == p.n && p.n == p.k && p.k >= 2048 &&
                    p.k <= 4096 && p.lda == p.m && p.ldb == p.m && p.ldc == p.m;
+
+    // ---- engine 2: one launch, K partitions merged in a cluster -----------------
+    if (opts.engine == 2) {
+        if (tc || out.rounding || opts.k_partitions > 8) {
+            return false;
+        }
+        int parts = opts.k_partitions;
+        while (parts > 1 && (parts - 1) * k_span(p.k, parts) >= p.k) {
+            --parts;
+        }
+        int tile = 0;
+        plan_single(p.m, p.n, p.k, 0, sm_count, opts.onchip_tile - 1, parts, &tile, &parts);
+        out.engine = 2;
+        out.onchip_tile = tile;
+        out.tile_m = single_tile_bm(tile);
+        out.tile_n = single_tile_bn(tile);
+        out.parts = parts;
+        out.span = parts > 1 ? k_span(p.k, parts) : p.k;
+        out.total = 0;
+        *plan = out;
+        return true;
+    }
 
     // ---- tile x K-partition search -------------------------------------------
     const TileChoice* tiles = tc ? kTcTiles : kFp32Tiles;
@@ -215,6 +259,28 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     }
     if (out.parts == 1) {
         out.span = p.k;
+    }
+
+    // ---- engine (FP32 form without the rounding pass) ---------------------------
+    // The one-launch engine skips the pack kernel and the merge kernel; it
+    // wins on small and latency-bound shapes, the packed engine's faster FFMA
+    // tile on large ones.  Both time models are fitted on B200.
+    if (!tc && !out.rounding && opts.engine == 0 && (opts.k_partitions <= 0 || out.parts <= 8)) {
+        const bool narrow = p.k >= 1024 && std::min(p.m, p.n) <= 16 && std::max(p.m, p.n) <= 32;
+        const int forced = opts.k_partitions > 0 ? out.parts : narrow ? 8 : 0;
+        int tile = 0, parts = 0;
+        const double single = plan_single(p.m, p.n, p.k, 0, sm_count, -1, forced, &tile, &parts);
+        if (single < packed_time_us(p, out.parts, out.span, default_tiles, sm_count)) {
+            out.engine = 2;
+            out.onchip_tile = tile;
+            out.tile_m = single_tile_bm(tile);
+            out.tile_n = single_tile_bn(tile);
+            out.parts = parts;
+            out.span = parts > 1 ? k_span(p.k, parts) : p.k;
+            out.total = 0;
+            *plan = out;
+            return true;
+        }
     }
 
     // ---- workspace layout -----------------------------------------------------

@@ -81,12 +81,19 @@ typedef struct {
     int tc_segment;   /* tensor-core forms: K terms accumulated in TMEM before each round-to-nearest
                          FP32 merge (0 = planner: 128 for k >= 2048, 64 for k > 1024, else 32;
                          rounded up to the kernel's K-block of 32 or 64) */
-    int reserved[4];
+    int engine;       /* FP32 form: 0 = planner's choice; 1 = packed planes (pack kernel, TMA-fed FFMA
+                         GEMM, split-K merge kernel); 2 = one launch that reads the caller's matrices and
+                         merges its K partitions (<= 8) inside a thread-block cluster.  For a given K
+                         split both give the same bits.  2 is refused (INVALID_VALUE) for the
+                         tensor-core forms, with the rounding pass, or with k_partitions > 8. */
+    int onchip_tile;  /* engine 2: 0 = planner, 1..6 = 128x64, 64x64, 128x32, 32x128, 64x32, 32x32 */
+    int reserved[2];
 } cg3mOptions;
 
 /* What one call did (filled when a non-null pointer is passed). */
 typedef struct {
-    int path;            /* 0 quick return, 1 beta-scale only, 2 fused GEMM, 3 split-K GEMM + merge */
+    int path;            /* 0 quick return, 1 beta-scale only, 2 fused GEMM, 3 split-K GEMM + merge,
+                            4 one launch with the K partitions merged in a cluster (engine 2) */
     int form;            /* cg3mForm_t actually used */
     int tile_m, tile_n;  /* output tile of the GEMM kernel */
     int k_partitions;    /* K partitions (1 = none) */

@@ -195,6 +195,25 @@ def test_planner_forced_partitions(cg3m):
     assert p["k_partitions"] == 3 and p["k_span"] == 336
 
 
+def test_planner_onchip_engine(cg3m):
+    """Engine 2 (one launch, cluster-merged K partitions): no workspace, one
+    kernel, at most 8 partitions; refused for the tensor-core forms, with the
+    rounding pass, beyond 8 partitions, and for unknown engines or tiles."""
+    p = cg3m.plan("N", "N", 300, 200, 1000, engine="onchip", onchip_tile=2, k_partitions=5)
+    assert p["path"] == 4 and p["kernels"] == 1 and p["workspace_bytes"] == 0
+    assert (p["tile_m"], p["tile_n"]) == (64, 64) and p["k_partitions"] == 5 and p["k_span"] == 208
+    p = cg3m.plan("N", "N", 300, 200, 40, engine="onchip", k_partitions=8)
+    assert p["k_partitions"] == 3 and p["k_span"] == 16  # the last partition must be non-empty
+    for kw in ({"form": "bf16x6"}, {"k_partitions": 9}, {"onchip_tile": 7}):
+        with pytest.raises(cg3m.Cg3mError):
+            cg3m.plan("N", "N", 300, 200, 1000, engine="onchip", **kw)
+    with pytest.raises(cg3m.Cg3mError):
+        cg3m.plan("N", "N", 2048, 2048, 2048, engine="onchip")  # the rounding pass needs the packed engine
+    with pytest.raises(cg3m.Cg3mError):
+        cg3m.plan("N", "N", 300, 200, 1000, engine=3)
+    assert cg3m.plan("N", "N", 300, 200, 1000, engine="packed", k_partitions=5)["path"] == 3
+
+
 def test_rounding_gate(cg3m):
     """The pass runs exactly for square contiguous unit-output orders 2048..4096."""
     assert cg3m.plan("N", "N", 2048, 2048, 2048)["rounding"] == 1

@@ -388,18 +388,26 @@ cg3mStatus_t cg3mCgemm3mStridedBatched(cg3mHandle_t h, cg3mOperation_t transa, c
     if (!make_strided_plan(p, 0, per_launch, h->sm_count, &plan)) {
         return CG3M_STATUS_INVALID_VALUE;
     }
+    // One problem per launch (a batch of one, or overlapping outputs): the
+    // one-launch kernel, no workspace.
+    int tile = 0, parts = 1;
     void* ws = nullptr;
-    const cg3mStatus_t wst = workspace(h, plan.bytes, &ws);
-    if (wst != CG3M_STATUS_SUCCESS) {
-        return wst;
+    if (per_launch == 1) {
+        plan_single(m, n, k, 0, h->sm_count, -1, 0, &tile, &parts);
+    } else {
+        const cg3mStatus_t wst = workspace(h, plan.bytes, &ws);
+        if (wst != CG3M_STATUS_SUCCESS) {
+            return wst;
+        }
     }
     for (int i = 0; i < batch_count; i += per_launch) {
         Problem pi = p;
         pi.A = A + i * strideA;
         pi.B = B + i * strideB;
         pi.C = C + i * strideC;
-        const cudaError_t e = launch_strided(h->stream, pi, 0, 1, strideA, strideB, strideC, per_launch, plan, ws,
-                                             h->sm_count);
+        const cudaError_t e = per_launch == 1 ? launch_single(h->stream, pi, 0, 1, tile, parts)
+                                              : launch_strided(h->stream, pi, 0, 1, strideA, strideB, strideC,
+                                                               per_launch, plan, ws, h->sm_count);
         if (e != cudaSuccess) {
             return to_status(e);
         }
@@ -448,16 +456,11 @@ cg3mStatus_t cg3mCgemm(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t t
     const bool unit = alpha->real == 1.0f && alpha->imag == 0.0f && beta->real == 0.0f && beta->imag == 0.0f;
     const int mode = unit ? 0 : 1;
     Problem p{transa, transb, m, n, k, alpha->real, alpha->imag, beta->real, beta->imag, A, lda, B, ldb, C, ldc};
-    StridedPlan plan;
-    if (!make_strided_plan(p, mode, 1, h->sm_count, &plan)) {
-        return CG3M_STATUS_INVALID_VALUE;
-    }
-    void* ws = nullptr;
-    const cg3mStatus_t wst = workspace(h, plan.bytes, &ws);
-    if (wst != CG3M_STATUS_SUCCESS) {
-        return wst;
-    }
-    return to_status(launch_strided(h->stream, p, mode, unit ? 1 : 0, 0, 0, 0, 1, plan, ws, h->sm_count));
+    // One problem: the one-launch kernel of the on-chip family (K partitions
+    // merged in a cluster; no workspace).
+    int tile = 0, parts = 1;
+    plan_single(m, n, k, mode, h->sm_count, -1, 0, &tile, &parts);
+    return to_status(launch_single(h->stream, p, mode, unit ? 1 : 0, tile, parts));
 }
 
 cg3mStatus_t cg3mCgemm3mHost(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
@@ -711,6 +714,17 @@ cg3mStatus_t cg3mPlanOnchip(int m, int n, int k, int mode, int batch, int sm_cou
         return CG3M_STATUS_INVALID_VALUE;
     }
     std::memset(info, 0, sizeof(*info));
+    if (batch == 1) {  // one problem: the one-launch kernel
+        int tile = 0, parts = 1;
+        plan_single(m, n, k, mode, sm_count > 0 ? sm_count : 148, -1, 0, &tile, &parts);
+        info->path = 4;
+        info->tile_m = single_tile_bm(tile);
+        info->tile_n = single_tile_bn(tile);
+        info->k_partitions = parts;
+        info->k_span = parts > 1 ? ceil_div(ceil_div(k, 16), parts) * 16 : k;
+        info->kernels = 1;
+        return CG3M_STATUS_SUCCESS;
+    }
     info->path = plan.parts > 1 ? 3 : 2;
     info->tile_m = plan.tile_m;
     info->tile_n = plan.tile_n;

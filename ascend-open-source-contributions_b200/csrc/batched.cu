@@ -1092,8 +1092,11 @@ double plan_single(int m, int n, int k, int mode, int sm_count, int forced_tile,
             const long long waves = (tiles + cap - 1) / cap;
             const long long load = (tiles * q + sm_count - 1) / sm_count;
             const SingleCost& c = kSingleCost[t];
+            // Four-product mode: four FFMA per output and K term instead of
+            // three (the per-term costs scaled by that ratio, not fitted).
+            const double fma = mode == kMode4M ? 4.0 / 3.0 : 1.0;
             double us = (double)waves * c.fixed_us +
-                        span * 1e-3 * ((double)waves * c.term_ns + (double)load * c.shared_term_ns);
+                        span * 1e-3 * fma * ((double)waves * c.term_ns + (double)load * c.shared_term_ns);
             if (q > 1) {
                 us += kSingleMergePerPartUs * q;
             }

@@ -273,7 +273,9 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
 
 /* The on-chip family's decision (cg3mCgemm, cg3mCgemm3mStridedBatched) for
  * one problem shape: mode 0 = three products, 1 = four; `batch` problems per
- * launch.  Fills tile_m, tile_n, k_partitions, k_span and workspace_bytes. */
+ * launch.  Fills tile_m, tile_n, k_partitions, k_span and workspace_bytes.
+ * batch == 1 (cg3mCgemm, a strided batch of one, or overlapping outputs run
+ * one per launch) reports the one-launch kernel: path 4, no workspace. */
 cg3mStatus_t cg3mPlanOnchip(int m, int n, int k, int mode, int batch, int sm_count, cg3mCallInfo* info);
 
 /* ---- diagnostics (not a compute path of cgemm3m) ------------------------- */

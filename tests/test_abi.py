@@ -287,5 +287,9 @@ def test_onchip_plan(cg3m):
     assert big["k_partitions"] == 1 and big["tile_m"] * big["tile_n"] == 8192
     few = cg3m.plan_onchip(64, 64, 4096, mode=0, batch=1)
     assert few["k_partitions"] > 1 and few["k_span"] * (few["k_partitions"] - 1) < 4096
+    # one problem: the one-launch kernel, K partitions merged in a cluster of <= 8
+    assert few["path"] == 4 and few["workspace_bytes"] == 0 and few["k_partitions"] <= 8
+    one4 = cg3m.plan_onchip(1024, 1024, 1024, mode=1, batch=1)
+    assert (one4["tile_m"], one4["tile_n"]) != (128, 64)  # four accumulators: no 128x64 tile
     four = cg3m.plan_onchip(1024, 1024, 1024, mode=1, batch=8)
     assert four["tile_m"] * four["tile_n"] <= 4096  # no 128x64 tile with four accumulators

@@ -120,9 +120,13 @@ def test_strided_overlap_in_batch_order(cg3m, oracle, cuda, h):
     assert h.cgemm3m_strided_batched("N", "N", m, n, k, alpha, to_dev(a, torch, cuda), m, m * k,
                                      to_dev(b, torch, cuda), k, k * n, beta, dC, m, 0, batch) == cg3m.SUCCESS
     torch.cuda.synchronize()
+    # overlapping outputs run one batch per launch: the one-problem plan
+    plan = cg3m.plan_onchip(m, n, k, 0, 1, torch.cuda.get_device_properties(cuda).multi_processor_count)
+    span = plan["k_span"] if plan["k_partitions"] > 1 else 0
     want = c.copy()
     for i in range(batch):
-        oracle.cgemm_modes_model(0, 1, "N", "N", m, n, k, alpha, a[i * m * k:], m, b[i * k * n:], k, beta, want, m)
+        oracle.cgemm_modes_model(0, 1, "N", "N", m, n, k, alpha, a[i * m * k:], m, b[i * k * n:], k, beta, want, m,
+                                 span=span)
     assert same_bits(to_host(dC), want)
 
 
@@ -166,11 +170,13 @@ def test_nonfinite_repair(cg3m, oracle, cuda, h):
                                      0, 0.0, dC, m, 0, 1) == cg3m.SUCCESS
     torch.cuda.synchronize()
     out = to_host(dC)
+    plan = cg3m.plan_onchip(m, n, k, 0, 1, torch.cuda.get_device_properties(cuda).multi_processor_count)
+    span = plan["k_span"] if plan["k_partitions"] > 1 else 0
     want = c.copy()
-    oracle.cgemm_modes_model(0, 1, "N", "N", m, n, k, 1.0, a, m, b, k, 0.0, want, m)
+    oracle.cgemm_modes_model(0, 1, "N", "N", m, n, k, 1.0, a, m, b, k, 0.0, want, m, span=span)
     assert same_bits(out, want)
     plain = c.copy()
-    oracle.cgemm_modes_model(0, 0, "N", "N", m, n, k, 1.0, a, m, b, k, 0.0, plain, m)
+    oracle.cgemm_modes_model(0, 0, "N", "N", m, n, k, 1.0, a, m, b, k, 0.0, plain, m, span=span)
     assert not np.all(np.isfinite(plain.view(np.float32)))  # 3M alone overflows ...
     assert np.all(np.isfinite(out.view(np.float32)))        # ... the repaired output does not
 

@@ -206,6 +206,197 @@ __global__ void __launch_bounds__(Fp32Cfg<BM, BN>::THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Warp-specialised 128 x 64 variant (the packed engine's tile).  A warp's
+// 128-bit shared-memory load costs four wavefronts whether or not its lanes
+// share addresses, so the 8 x 4 complex micro-tile above (nine loads per 96
+// FFMA) is bound by shared-memory wavefronts at about two thirds of the FFMA
+// rate.  Here each of the three real products P0 = Ar.Br, P1 = Ai.Bi,
+// P2 = (Ar+Ai).(Br+Bi) has its own four consumer warps, and every thread an
+// 8 x 8 real micro-tile of one product: four 128-bit loads per 64 FMAs, the
+// ratio at which the SM's FMA pipe and shared-memory wavefronts balance.  The
+// FMAs issue as 32 packed pairs (two independent FP32 FMAs per instruction,
+// each rounded to nearest), which halves the issue slots they take.
+// Each product's K terms are still one thread's FFMA chain in increasing k,
+// so the bits are those of the kernel above.  After the K loop the three
+// products meet in shared memory (over the drained stage ring) and all 384
+// consumer threads form Re = P0 - P1, Im = (P2 - P0) - P1, apply alpha/beta
+// and store with coalesced column-major writes.
+// ---------------------------------------------------------------------------
+#ifndef CG3M_FP32_WS_UNROLL
+#define CG3M_FP32_WS_UNROLL 16
+#endif
+namespace ws {
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 4;
+constexpr int KK_UNROLL = CG3M_FP32_WS_UNROLL;  // K terms per unrolled step (16 measured fastest)
+constexpr int WARPS = 12;  // 4 per product; thread 0 also issues the copies
+constexpr int THREADS = WARPS * 32;
+constexpr int A_STAGE = 3 * BK * BM, B_STAGE = 3 * BK * BN;  // floats
+constexpr size_t RING = size_t(STAGES) * (A_STAGE + B_STAGE) * 4;
+constexpr size_t SMEM = RING + 2 * STAGES * 8 + 1024;
+static_assert((size_t)3 * BM * BN * 4 <= RING, "product exchange exceeds the stage ring");
+}  // namespace ws
+
+// Twelve warps fall three to each of the SM's four sub-partitions (16K
+// registers each), so 168 registers per thread is the launch limit; a
+// thirteenth (producer) warp would cut it to 128.  Thread 0 therefore issues
+// the TMA copies itself: the first STAGES K-tiles up front, then the refill of
+// each stage once every warp has released it.
+__global__ void __launch_bounds__(ws::THREADS, 1)
+    gemm3m_fp32_ws_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                          const Fp32Params p)
+{
+    using namespace ws;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    float* sA = reinterpret_cast<float*>(base);
+    float* sB = sA + STAGES * A_STAGE;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * B_STAGE);
+    uint64_t* empty = full + STAGES;
+    __shared__ int failed;
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+
+    constexpr int GM = 8;  // grouped rasterisation, as the kernel above
+    const int pid = blockIdx.x;
+    const int in_group = GM * p.tiles_n;
+    const int first_m = (pid / in_group) * GM;
+    const int gsz = min(p.tiles_m - first_m, GM);
+    const int tm = first_m + (pid % in_group) % gsz;
+    const int tn = (pid % in_group) / gsz;
+    const int m0 = tm * BM, n0 = tn * BN;
+    const int part = blockIdx.y;
+    const int kbeg = part * p.span;
+    const int kend = min(p.k, kbeg + p.span);
+    const int ktiles = (kend - kbeg + BK - 1) / BK;
+
+    auto issue = [&](int kt) {
+        const int s = kt % STAGES;
+        mbar_arrive_expect_tx(&full[s], (A_STAGE + B_STAGE) * 4);
+        tma_load_3d(sA + s * A_STAGE, &tmA, &full[s], m0, kbeg + kt * BK, 0);
+        tma_load_3d(sB + s * B_STAGE, &tmB, &full[s], n0, kbeg + kt * BK, 0);
+    };
+    int issued = 0;  // thread 0 only
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], WARPS);
+        }
+        fence_mbar_init();
+        failed = 0;
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+        for (; issued < STAGES && issued < ktiles; ++issued) {
+            issue(issued);
+        }
+    }
+    __syncthreads();
+
+    // Warp w: product w / 4, warp tile 64 x 32 at (64 (w & 1), 32 ((w & 3) >> 1)); lane
+    // (mi, ni) = (lane & 7, lane >> 3): rows am + {0..3, 32..35}, columns bn + {0..3, 16..19}.
+    const int plane = warp >> 2, wq = warp & 3;
+    const int am = (wq & 1) * 64 + (lane & 7) * 4;
+    const int bn = (wq >> 1) * 32 + (lane >> 3) * 4;
+    // acc[i][jj] = (P(row i, col 2jj), P(row i, col 2jj + 1)): one packed FMA
+    // (__ffma2_rn: two independent round-to-nearest FMAs) updates both.
+    float2 acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            acc[i][jj] = make_float2(0.0f, 0.0f);
+        }
+    }
+    bool ok = true;
+    int consumed = 0;
+    for (int kt = 0; kt < ktiles; ++kt) {
+        const int s = kt % STAGES;
+        if (!mbar_wait(&full[s], (kt / STAGES) & 1, p.status)) {
+            ok = false;
+            break;
+        }
+        consumed = kt + 1;
+        const float* a = sA + s * A_STAGE + plane * BK * BM + am;
+        const float* b = sB + s * B_STAGE + plane * BK * BN + bn;
+#pragma unroll KK_UNROLL
+        for (int kk = 0; kk < BK; ++kk) {
+            float x[8];
+            float2 y[4];
+            *reinterpret_cast<float4*>(&x[0]) = *reinterpret_cast<const float4*>(a + kk * BM);
+            *reinterpret_cast<float4*>(&x[4]) = *reinterpret_cast<const float4*>(a + kk * BM + 32);
+            *reinterpret_cast<float4*>(&y[0]) = *reinterpret_cast<const float4*>(b + kk * BN);
+            *reinterpret_cast<float4*>(&y[2]) = *reinterpret_cast<const float4*>(b + kk * BN + 16);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float2 xi = make_float2(x[i], x[i]);
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) acc[i][jj] = __ffma2_rn(xi, y[jj], acc[i][jj]);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(&empty[s]);
+        }
+        // Refill stage s with K-tile kt + STAGES once all twelve warps have released it.
+        if (tid == 0 && issued < ktiles) {
+            if (!mbar_wait(&empty[s], (kt / STAGES) & 1, p.status)) {
+                ok = false;
+                break;
+            }
+            issue(issued);
+            ++issued;
+        }
+    }
+    if (tid == 0) {
+        // Copies this thread issued but no longer waits for (after a timeout) must land
+        // before the ring is reused or the CTA retires.
+        for (int kt = consumed; kt < issued; ++kt) {
+            mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1, p.status);
+        }
+    }
+    if (!ok) {
+        failed = 1;
+    }
+    // Every warp is past its last stage read and every copy has landed: the
+    // ring becomes the exchange P[plane][col][row].
+    __syncthreads();
+    float* P = sA;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int col = bn + (j < 4 ? j : 12 + j);
+        auto v = [&](int i) { return (j & 1) ? acc[i][j >> 1].y : acc[i][j >> 1].x; };
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            *reinterpret_cast<float4*>(P + (size_t)(plane * BN + col) * BM + am + 32 * h) =
+                make_float4(v(4 * h), v(4 * h + 1), v(4 * h + 2), v(4 * h + 3));
+        }
+    }
+    __syncthreads();
+    if (failed) {
+        return;
+    }
+    for (int e = tid; e < BM * BN; e += THREADS) {
+        const int r = e % BM, c = e / BM;
+        const int row = m0 + r, col = n0 + c;
+        if (row >= p.m || col >= p.n) {
+            continue;
+        }
+        const float q0 = P[(0 * BN + c) * BM + r], q1 = P[(1 * BN + c) * BM + r];
+        const float q2 = P[(2 * BN + c) * BM + r];
+        const float re = __fsub_rn(q0, q1);
+        const float im = __fsub_rn(__fsub_rn(q2, q0), q1);
+        if (p.parts == 1) {
+            float2* cp = p.C + (size_t)col * p.ldc + row;
+            *cp = epilogue_value(re, im, p.epi, cp);
+        } else {
+            const size_t o = (size_t)col * p.ppitch + row;
+            p.partial[(size_t)(2 * part) * p.pplane + o] = re;
+            p.partial[(size_t)(2 * part + 1) * p.pplane + o] = im;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Path-tracking variant for the rounding-correction gate (square n in
 // [2048, 4096], contiguous, alpha = 1, beta = 0).  Reference: cgemm3m_path_kernel
 // and MergeProductsWithPath, blas/gemm/arch35/cgemm_compute_kernel.cpp:432-474,
@@ -439,12 +630,21 @@ cudaError_t launch_fp32_tile(cudaStream_t stream, const Problem& pr, const Plan&
     p.ppitch = plan.partial_pitch;
     p.pplane = plan.partial_plane_elems;
     p.status = status;
+    const dim3 grid((unsigned)(p.tiles_m * p.tiles_n), (unsigned)plan.parts);
+    if constexpr (BM == ws::BM && BN == ws::BN) {
+        cudaError_t err = cudaFuncSetAttribute(gemm3m_fp32_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)ws::SMEM);
+        if (err != cudaSuccess) {
+            return err;
+        }
+        gemm3m_fp32_ws_kernel<<<grid, ws::THREADS, ws::SMEM, stream>>>(ta, tb, p);
+        return cudaGetLastError();
+    }
     auto kernel = gemm3m_fp32_kernel<BM, BN>;
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
     if (err != cudaSuccess) {
         return err;
     }
-    const dim3 grid((unsigned)(p.tiles_m * p.tiles_n), (unsigned)plan.parts);
     kernel<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(ta, tb, p);
     return cudaGetLastError();
 }

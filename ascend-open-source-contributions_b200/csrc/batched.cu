@@ -278,8 +278,27 @@ __device__ __forceinline__ bool finite2(float2 v) { return isfinite(v.x) && isfi
 __device__ __forceinline__ int thread_tx() { return ((threadIdx.x >> 5) & 1) * 8 + (threadIdx.x & 7); }
 __device__ __forceinline__ int thread_ty() { return (threadIdx.x >> 6) * 4 + ((threadIdx.x & 31) >> 3); }
 
+// Accumulators: acc[c][i][jj] holds outputs (i, 2jj) and (i, 2jj + 1) of
+// accumulator c, updated together by one packed FMA (__ffma2_rn: two
+// independent round-to-nearest FP32 FMAs), so each output is still the same
+// FMA chain in increasing K.
 template <int BM, int BN, int MODE>
-using AccTile = float[Cfg<BM, BN, MODE>::ACC][Cfg<BM, BN, MODE>::MT][Cfg<BM, BN, MODE>::NT];
+using AccTile = float2[Cfg<BM, BN, MODE>::ACC][Cfg<BM, BN, MODE>::MT][Cfg<BM, BN, MODE>::NT / 2];
+
+template <int BM, int BN, int MODE>
+__device__ __forceinline__ float acc_at(const AccTile<BM, BN, MODE>& acc, int c, int i, int j)
+{
+    return (j & 1) ? acc[c][i][j >> 1].y : acc[c][i][j >> 1].x;
+}
+
+// Partition product of output (i, j) of this thread.
+template <int BM, int BN, int MODE>
+__device__ __forceinline__ float2 acc_product(const AccTile<BM, BN, MODE>& acc, int i, int j)
+{
+    constexpr int L = Cfg<BM, BN, MODE>::ACC - 1;
+    return part_product<MODE>(acc_at<BM, BN, MODE>(acc, 0, i, j), acc_at<BM, BN, MODE>(acc, 1, i, j),
+                              acc_at<BM, BN, MODE>(acc, 2, i, j), acc_at<BM, BN, MODE>(acc, L, i, j));
+}
 
 // The products of K terms [kbeg, kbeg + klen) of the BM x BN tile at (m0, n0),
 // accumulated from zero into acc: kStages raw slots of RAWS elements and two
@@ -305,8 +324,8 @@ __device__ __forceinline__ void accumulate(const BProblem& p, int m0, int n0, in
 #pragma unroll
         for (int i = 0; i < G::MT; ++i)
 #pragma unroll
-            for (int j = 0; j < G::NT; ++j) {
-                acc[c][i][j] = 0.0f;
+            for (int j = 0; j < G::NT / 2; ++j) {
+                acc[c][i][j] = make_float2(0.0f, 0.0f);
             }
 
     // Prologue: K-blocks 0 .. kStages-2 in flight (one commit group each,
@@ -356,20 +375,31 @@ __device__ __forceinline__ void accumulate(const BProblem& p, int m0, int n0, in
                 }
             }
 #pragma unroll
-            for (int i = 0; i < G::MT; ++i)
+            for (int i = 0; i < G::MT; ++i) {
+                float2 xb[G::COMPS];
 #pragma unroll
-                for (int j = 0; j < G::NT; ++j) {
+                for (int c = 0; c < G::COMPS; ++c) {
+                    xb[c] = make_float2(x[c][i], x[c][i]);
+                }
+#pragma unroll
+                for (int jj = 0; jj < G::NT / 2; ++jj) {
+                    float2 yp[G::COMPS];
+#pragma unroll
+                    for (int c = 0; c < G::COMPS; ++c) {
+                        yp[c] = make_float2(y[c][2 * jj], y[c][2 * jj + 1]);
+                    }
                     if constexpr (MODE == kMode3M) {
-                        acc[0][i][j] = __fmaf_rn(x[0][i], y[0][j], acc[0][i][j]);
-                        acc[1][i][j] = __fmaf_rn(x[1][i], y[1][j], acc[1][i][j]);
-                        acc[2][i][j] = __fmaf_rn(x[2][i], y[2][j], acc[2][i][j]);
+                        acc[0][i][jj] = __ffma2_rn(xb[0], yp[0], acc[0][i][jj]);
+                        acc[1][i][jj] = __ffma2_rn(xb[1], yp[1], acc[1][i][jj]);
+                        acc[2][i][jj] = __ffma2_rn(xb[2], yp[2], acc[2][i][jj]);
                     } else {
-                        acc[0][i][j] = __fmaf_rn(x[0][i], y[0][j], acc[0][i][j]);  // Ar.Br
-                        acc[1][i][j] = __fmaf_rn(x[1][i], y[1][j], acc[1][i][j]);  // Ai.Bi
-                        acc[2][i][j] = __fmaf_rn(x[0][i], y[1][j], acc[2][i][j]);  // Ar.Bi
-                        acc[3][i][j] = __fmaf_rn(x[1][i], y[0][j], acc[3][i][j]);  // Ai.Br
+                        acc[0][i][jj] = __ffma2_rn(xb[0], yp[0], acc[0][i][jj]);  // Ar.Br
+                        acc[1][i][jj] = __ffma2_rn(xb[1], yp[1], acc[1][i][jj]);  // Ai.Bi
+                        acc[2][i][jj] = __ffma2_rn(xb[0], yp[1], acc[2][i][jj]);  // Ar.Bi
+                        acc[3][i][jj] = __ffma2_rn(xb[1], yp[0], acc[3][i][jj]);  // Ai.Br
                     }
                 }
+            }
         }
     }
     cp_async_wait<0>();  // only empty groups can remain; keep the count at zero between tasks
@@ -387,7 +417,7 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
     const int kend = min(p.k, kbeg + p.span);
     const int klen = kend > kbeg ? kend - kbeg : 0;
     const int tx = thread_tx(), ty = thread_ty();
-    float acc[G::ACC][G::MT][G::NT];
+    AccTile<BM, BN, MODE> acc;
     accumulate<BM, BN, MODE, kRawElems, kPlaneFloats>(p, m0, n0, kbeg, klen, raw, planes, acc);
 
     // Output (i, j) of this thread: row m0 + (i / VA)*16*VA + tx*VA + i % VA,
@@ -404,8 +434,7 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
                     if (p.k == 0) {
                         *cp = beta_scaled(p.epi, cp);
                     } else {
-                        float2 v = part_product<MODE>(acc[0][i][j], acc[1][i][j], acc[2][i][j],
-                                                      acc[G::ACC - 1][i][j]);
+                        float2 v = acc_product<BM, BN, MODE>(acc, i, j);
                         if (p.repair && !finite2(v)) {
                             v = repair_product(p, row, col);
                         }
@@ -428,7 +457,7 @@ __device__ void run_task(const BProblem& prob, int tile, int part, float2* raw, 
             const int row = m0 + (i / G::VA) * 16 * G::VA + tx * G::VA + i % G::VA;
             if (row < p.m && col < p.n) {
                 const size_t o = (size_t)col * p.ppitch + row;
-                const float2 v = part_product<MODE>(acc[0][i][j], acc[1][i][j], acc[2][i][j], acc[G::ACC - 1][i][j]);
+                const float2 v = acc_product<BM, BN, MODE>(acc, i, j);
                 __stcg(base + (size_t)(2 * part) * plane + o, v.x);
                 __stcg(base + (size_t)(2 * part + 1) * plane + o, v.y);
             }
@@ -624,7 +653,7 @@ __global__ void __launch_bounds__(kThreads) single_kernel(const BProblem p)
     const int kend = min(p.k, kbeg + p.span);
     const int klen = kend > kbeg ? kend - kbeg : 0;
     const int tx = thread_tx(), ty = thread_ty();
-    float acc[G::ACC][G::MT][G::NT];
+    AccTile<BM, BN, MODE> acc;
     accumulate<BM, BN, MODE, S::RAWS, S::PLS>(p, m0, n0, kbeg, klen, raw, planes, acc);
 
     if (p.parts == 1) {
@@ -636,7 +665,7 @@ __global__ void __launch_bounds__(kThreads) single_kernel(const BProblem p)
                 const int row = m0 + (i / G::VA) * 16 * G::VA + tx * G::VA + i % G::VA;
                 if (row < p.m && col < p.n) {
                     float2 v =
-                        part_product<MODE>(acc[0][i][j], acc[1][i][j], acc[2][i][j], acc[G::ACC - 1][i][j]);
+                        acc_product<BM, BN, MODE>(acc, i, j);
                     if (p.repair && !finite2(v)) {
                         v = repair_product(p, row, col);
                     }
@@ -659,7 +688,7 @@ __global__ void __launch_bounds__(kThreads) single_kernel(const BProblem p)
 #pragma unroll
         for (int i = 0; i < G::MT; ++i) {
             const int r = (i / G::VA) * 16 * G::VA + tx * G::VA + i % G::VA;
-            const float2 v = part_product<MODE>(acc[0][i][j], acc[1][i][j], acc[2][i][j], acc[G::ACC - 1][i][j]);
+            const float2 v = acc_product<BM, BN, MODE>(acc, i, j);
             part_re[c * BM + r] = v.x;
             part_im[c * BM + r] = v.y;
         }

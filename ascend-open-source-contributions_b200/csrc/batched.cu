@@ -1077,7 +1077,7 @@ int single_tile_bn(int tile) { return tile_bn(tile); }
 
 // Time model of the one-launch kernel (three-product mode), in microseconds,
 // fitted on B200 to 1100 timed (shape, tile, partitions) launches (median
-// error 1.6 %).  Clusters of `parts` blocks run in waves of as many clusters
+// error 1.5 %).  Clusters of `parts` blocks run in waves of as many clusters
 // as fit at once (cudaOccupancyMaxActiveClusters on a 148-SM B200, scaled for
 // other SM counts); each wave costs the tile's fixed part (first copies,
 // epilogue) plus span x its per-term time, and tiles that share an SM (64 x 32:
@@ -1087,14 +1087,14 @@ namespace {
 struct SingleCost {
     double fixed_us, term_ns, shared_term_ns;
 };
-constexpr SingleCost kSingleCost[kTileCount] = {{4.92, 188.9, 0.0},  {3.54, 143.7, 0.0}, {3.36, 150.1, 0.0},
-                                                {3.34, 130.7, 0.0},  {2.91, 45.6, 62.1}, {2.14, 19.9, 43.1}};
+constexpr SingleCost kSingleCost[kTileCount] = {{4.96, 183.8, 0.0},  {3.55, 129.2, 0.0}, {3.31, 176.6, 0.0},
+                                                {3.29, 118.7, 0.0},  {2.99, 51.4, 59.7}, {2.26, 15.3, 43.7}};
 constexpr int kSingleOcc[kTileCount] = {1, 1, 1, 1, 2, 3};
 // Clusters resident at once on 148 SMs, by blocks per SM (1..3) and cluster size (1..8).
 constexpr int kClusterCap[3][kMaxClusterParts] = {{148, 74, 45, 33, 26, 22, 15, 15},
                                                   {296, 148, 93, 71, 56, 45, 37, 33},
                                                   {444, 222, 142, 104, 82, 71, 56, 48}};
-constexpr double kSingleMergePerPartUs = 0.152;
+constexpr double kSingleMergePerPartUs = 0.146;
 }  // namespace
 
 double plan_single(int m, int n, int k, int mode, int sm_count, int forced_tile, int forced_parts, int* tile,

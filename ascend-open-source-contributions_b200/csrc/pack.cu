@@ -94,12 +94,17 @@ template <int FORM>
 __global__ void __launch_bounds__(TILE* ROWS) pack_kernel(PackSide a, PackSide b)
 {
     __shared__ float2 tile[TILE][TILE + 1];
+    // Block x of side z covers tile (x mod tiles_r, x / tiles_r) of that side's
+    // own tile grid, so a long-K shape launches no blocks over the other
+    // side's extent.
     const PackSide& s = blockIdx.z == 0 ? a : b;
-    const int r0 = blockIdx.x * TILE;
-    const int c0 = blockIdx.y * TILE;
-    if (r0 >= s.rows || c0 >= s.cols) {
+    const int tiles_r = (s.rows + TILE - 1) / TILE;
+    const long long tiles = (long long)tiles_r * ((s.cols + TILE - 1) / TILE);
+    if ((long long)blockIdx.x >= tiles) {
         return;
     }
+    const int r0 = (int)(blockIdx.x % tiles_r) * TILE;
+    const int c0 = (int)(blockIdx.x / tiles_r) * TILE;
     const int tx = threadIdx.x, ty = threadIdx.y;
     if (!s.trans) {
         // Plane row = source column, plane column = source row: both contiguous.
@@ -140,6 +145,14 @@ __global__ void __launch_bounds__(TILE* ROWS) pack_kernel(PackSide a, PackSide b
     }
 }
 
+// Blocks per side: the larger of the two sides' 32 x 32 tile counts.
+unsigned pack_blocks(const PackSide& a, const PackSide& b)
+{
+    const long long ta = (long long)ceil_div(a.rows, TILE) * ceil_div(a.cols, TILE);
+    const long long tb = (long long)ceil_div(b.rows, TILE) * ceil_div(b.cols, TILE);
+    return (unsigned)(ta > tb ? ta : tb);
+}
+
 }  // namespace
 
 cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a, void* rows_b)
@@ -163,12 +176,7 @@ cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a
         return s;
     };
     const PackSide a = side(true), b = side(false);
-    const int gx = ceil_div(a.rows > b.rows ? a.rows : b.rows, TILE);
-    const int gy = ceil_div(a.cols > b.cols ? a.cols : b.cols, TILE);
-    if (gy > 65535) {
-        return cudaErrorInvalidConfiguration;
-    }
-    pack_kernel<kFormRows><<<dim3(gx, gy, 2), dim3(TILE, ROWS), 0, stream>>>(a, b);
+    pack_kernel<kFormRows><<<dim3(pack_blocks(a, b), 1, 2), dim3(TILE, ROWS), 0, stream>>>(a, b);
     return cudaGetLastError();
 }
 
@@ -197,12 +205,7 @@ cudaError_t launch_pack(cudaStream_t stream, const Problem& p, const Plan& plan,
         return s;
     };
     const PackSide a = side(true), b = side(false);
-    const int gx = ceil_div(a.rows > b.rows ? a.rows : b.rows, TILE);
-    const int gy = ceil_div(a.cols > b.cols ? a.cols : b.cols, TILE);
-    if (gy > 65535) {
-        return cudaErrorInvalidConfiguration;
-    }
-    const dim3 grid(gx, gy, 2), block(TILE, ROWS);
+    const dim3 grid(pack_blocks(a, b), 1, 2), block(TILE, ROWS);
     switch (plan.form) {
         case CG3M_FORM_FP32: pack_kernel<CG3M_FORM_FP32><<<grid, block, 0, stream>>>(a, b); break;
         case CG3M_FORM_TF32X3: pack_kernel<CG3M_FORM_TF32X3><<<grid, block, 0, stream>>>(a, b); break;

@@ -95,12 +95,12 @@ constexpr uint64_t kMergeFixed = 30;
 constexpr uint64_t kMergeFloatsPerTerm = 41500;
 // The same costs in microseconds for the whole packed call (pack kernel over
 // op(A) and op(B) -- 8 bytes read, 12 written per element -- GEMM waves, merge
-// kernel), fitted on B200 to 28 timed shapes (median error 3.4 %).
-constexpr double kPackedFixedUs = 0.47;
-constexpr double kPackedUsPerMB = 0.127;
-constexpr double kPackedUsPerTerm = 0.1619;
-constexpr double kMergeLaunchUs = 3.0;
-constexpr double kMergeUsPerTerm = 0.0765;
+// kernel), fitted on B200 to 28 timed shapes (median error 3.3 %).
+constexpr double kPackedFixedUs = 1.64;
+constexpr double kPackedUsPerMB = 0.199;
+constexpr double kPackedUsPerTerm = 0.1205;
+constexpr double kMergeLaunchUs = 3.53;
+constexpr double kMergeUsPerTerm = 0.0;
 // Tensor-core kernel tile (gemm_tc.cu): 128 x 128, one CTA per SM (TMEM).
 const TileChoice kTcTiles[] = {{128, 128, 1}};
 

@@ -161,6 +161,7 @@ cg3mStatus_t run_one(cg3mContext* h, int transa, int transb, int m, int n, int k
                                     h->stage_event_count);
     if (info != nullptr) {
         info->path = plan.engine == 2 ? 4 : plan.parts > 1 ? 3 : 2;
+        info->form = plan.form;
         info->tile_m = plan.tile_m;
         info->tile_n = plan.tile_n;
         info->k_partitions = plan.parts;
@@ -505,6 +506,7 @@ cg3mStatus_t cg3mCgemm3mHost(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperati
         if (o.k_partitions <= 0) {
             o.k_partitions = plan.parts;
         }
+        o.form = static_cast<cg3mForm_t>(plan.form);  // a small tensor-core call may run as plain FP32
         tile_n = plan.tile_n;
         if (plan.rounding) {
             panels = 1;

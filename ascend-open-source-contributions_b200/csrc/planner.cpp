@@ -137,6 +137,22 @@ double packed_time_us(const Problem& p, int parts, int span, uint64_t tiles, int
     return us;
 }
 
+// Tensor-core call in microseconds (pack of the split planes, waves of CTA-pair
+// tiles, merge), fitted on B200 to the 200 performance shapes (graph replay;
+// median error 13-19 %, hence the margin where it is compared).
+double tc_time_us(const Problem& p, int form, int parts, int span, int sm_count)
+{
+    const uint64_t tiles = p.m > 128 ? (uint64_t)ceil_div(p.m, 256) * ceil_div(p.n, 128)
+                                     : (uint64_t)ceil_div(p.n, 128);
+    const double waves = (double)((tiles * parts + sm_count - 1) / sm_count);
+    const double elems = (double)p.m * p.k + (double)p.k * p.n;
+    if (form == CG3M_FORM_TF32X3) {
+        return 11.80 + 0.1374 * elems * 32e-6 + 0.11003 * waves * span + (parts > 1 ? 1.25 : 0.0);
+    }
+    const double terms = form == CG3M_FORM_BF16X9 ? 1.5 : 1.0;  // nine products instead of six
+    return 13.27 + 0.1055 * elems * 44e-6 + 0.08315 * terms * waves * span;
+}
+
 }  // namespace
 
 bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* plan)
@@ -271,6 +287,30 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
         int tile = 0, parts = 0;
         const double single = plan_single(p.m, p.n, p.k, 0, sm_count, -1, forced, &tile, &parts);
         if (single < packed_time_us(p, out.parts, out.span, default_tiles, sm_count)) {
+            out.engine = 2;
+            out.onchip_tile = tile;
+            out.tile_m = single_tile_bm(tile);
+            out.tile_n = single_tile_bn(tile);
+            out.parts = parts;
+            out.span = parts > 1 ? k_span(p.k, parts) : p.k;
+            out.total = 0;
+            *plan = out;
+            return true;
+        }
+    }
+
+    // ---- tensor-core forms on small shapes ---------------------------------------
+    // A tensor-core call carries a fixed cost of 12-13 us (pack, TMEM set-up,
+    // pipeline fill) that the one-launch FP32 kernel does not.  Where the FP32
+    // one-launch estimate is clearly lower (a 1.25x margin over the rougher
+    // tensor-core model), the call runs in plain FP32 -- its error is the
+    // plain form's, which every form promises not to exceed -- and reports
+    // form FP32.  engine 1 (or a forced K split) keeps the tensor-core path.
+    if (tc && !out.rounding && opts.engine == 0 && opts.k_partitions <= 0) {
+        int tile = 0, parts = 0;
+        const double single = plan_single(p.m, p.n, p.k, 0, sm_count, -1, 0, &tile, &parts);
+        if (single * 1.25 < tc_time_us(p, opts.form, out.parts, out.span, sm_count)) {
+            out.form = CG3M_FORM_FP32;
             out.engine = 2;
             out.onchip_tile = tile;
             out.tile_m = single_tile_bm(tile);

@@ -212,6 +212,13 @@ def test_planner_onchip_engine(cg3m):
     with pytest.raises(cg3m.Cg3mError):
         cg3m.plan("N", "N", 300, 200, 1000, engine=3)
     assert cg3m.plan("N", "N", 300, 200, 1000, engine="packed", k_partitions=5)["path"] == 3
+    # small tensor-core calls run as the plain FP32 one-launch product unless forced
+    small = cg3m.plan("N", "N", 128, 128, 128, form="bf16x6", rounding="off")
+    assert small["form"] == cg3m.FORM["fp32"] and small["path"] == 4
+    forced = cg3m.plan("N", "N", 128, 128, 128, form="bf16x6", rounding="off", engine="packed")
+    assert forced["form"] == cg3m.FORM["bf16x6"] and forced["path"] in (2, 3)
+    big = cg3m.plan("N", "N", 4096, 4096, 4096, form="bf16x6", rounding="off")
+    assert big["form"] == cg3m.FORM["bf16x6"]
 
 
 def test_rounding_gate(cg3m):

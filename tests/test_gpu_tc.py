@@ -1,7 +1,9 @@
 """GPU parity of the tensor-core precision forms (3xTF32, split-BF16 x6/x9).
 
 The tensor-core accumulation order inside an MMA is the hardware's, so these
-forms are checked against FP64 rather than bit for bit: the reference accuracy
+forms are checked against FP64 rather than bit for bit (engine="packed" keeps
+every call on the tensor cores; the planner may otherwise run a small problem
+as plain FP32): the reference accuracy
 criterion (cgemm3m_verify.h:22-84) against the FP64 result rounded to FP32, a
 normwise-error bound, run-to-run bitwise determinism, and the north-star bar --
 normwise error vs FP64 no worse than the plain FP32 3M form on the same inputs.
@@ -50,7 +52,8 @@ def test_tc_single_tile(cg3m, oracle, cuda, h, form):
     m = n = 128
     k = 64
     a, lda, b, ldb, c, ldc = _operands(oracle, "N", "N", m, n, k, 0, "UNIFORM_1", 1)
-    out, info = run(cg3m, h, torch, cuda, "N", "N", m, n, k, 1.0, a, lda, b, ldb, 0.0, c, ldc, form=form)
+    out, info = run(cg3m, h, torch, cuda, "N", "N", m, n, k, 1.0, a, lda, b, ldb, 0.0, c, ldc, form=form,
+                    engine="packed")
     assert info["form"] == cg3m.FORM[form]
     _check(oracle, out, c, "N", "N", m, n, k, 1.0, a, lda, b, ldb, 0.0, ldc, 1e-6)
     assert h.device_status() == 0
@@ -66,8 +69,10 @@ def test_tc_edges(cg3m, oracle, cuda, h, form, shape, ops):
     ta, tb = ops
     alpha, beta = complex(0.7, 0.3), complex(-1.0, 0.5)
     a, lda, b, ldb, c, ldc = _operands(oracle, ta, tb, m, n, k, 3, "UNIFORM_1", m + n + k)
-    out, _ = run(cg3m, h, torch, cuda, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form)
-    again, _ = run(cg3m, h, torch, cuda, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form)
+    out, _ = run(cg3m, h, torch, cuda, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form,
+                 engine="packed")
+    again, _ = run(cg3m, h, torch, cuda, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form,
+                   engine="packed")
     assert out.tobytes() == again.tobytes()
     _check(oracle, out, c, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)
 
@@ -82,7 +87,8 @@ def test_tc_nine_ops_padded(cg3m, oracle, cuda, h, form, ta, tb):
     alpha, beta = complex(0.7, 0.3), complex(-1.0, 0.5)
     a, lda, b, ldb, c, ldc = _operands(oracle, ta, tb, m, n, k, 13, "UNIFORM_1", 9000 + 3 * OPS.index(ta) +
                                        OPS.index(tb))
-    out, _ = run(cg3m, h, torch, cuda, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form)
+    out, _ = run(cg3m, h, torch, cuda, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form,
+                 engine="packed")
     _check(oracle, out, c, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)
 
 
@@ -95,7 +101,7 @@ def test_tc_forced_partitions(cg3m, oracle, cuda, h, form, parts):
     alpha, beta = complex(0.3, -1.25), complex(0.5, 0.5)
     a, lda, b, ldb, c, ldc = _operands(oracle, "T", "N", m, n, k, 2, "RANDOM_NORM_5_5", 77)
     out, info = run(cg3m, h, torch, cuda, "T", "N", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form,
-                    k_partitions=parts)
+                    k_partitions=parts, engine="packed")
     assert info["k_partitions"] == parts and info["k_span"] % 64 == 0
     _check(oracle, out, c, "T", "N", m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)
 
@@ -108,7 +114,8 @@ def test_tc_long_k(cg3m, oracle, cuda, h, form):
     k = 65536
     alpha, beta = complex(0.7, 0.3), complex(-1.0, 0.5)
     a, lda, b, ldb, c, ldc = _operands(oracle, "N", "N", m, n, k, 0, "UNIFORM_1", 4243)
-    out, info = run(cg3m, h, torch, cuda, "N", "N", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form)
+    out, info = run(cg3m, h, torch, cuda, "N", "N", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form,
+                    engine="packed")
     assert info["k_partitions"] > 1
     _check(oracle, out, c, "N", "N", m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)
 
@@ -130,9 +137,27 @@ def test_tc_error_no_worse_than_plain(cg3m, oracle, cuda, h, form, size):
     h.zgemm_reference("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, ref)
     h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form="fp32", rounding="off")
     plain = h.error_report(n, n, C, n, ref)
-    h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, rounding="off")
+    h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, rounding="off", engine="packed")
     tc = h.error_report(n, n, C, n, ref)
     torch.cuda.synchronize()
     print(form, n, "plain", plain, "tc", tc)
     assert tc["normwise"] <= plain["normwise"], (plain, tc)
     assert tc["normwise"] < 1e-5
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_tc_small_problem_runs_plain_fp32(cg3m, oracle, cuda, h, form):
+    """Planner's choice for a small tensor-core call: the one-launch FP32
+    product (info reports form FP32, path 4), bit-identical to the FP32 form
+    with the same K split, and within the reference criterion."""
+    import torch
+
+    m, n, k = 96, 80, 200
+    alpha, beta = complex(0.7, 0.3), complex(-1.0, 0.5)
+    a, lda, b, ldb, c, ldc = _operands(oracle, "T", "C", m, n, k, 2, "UNIFORM_1", 616)
+    out, info = run(cg3m, h, torch, cuda, "T", "C", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form)
+    assert info["form"] == cg3m.FORM["fp32"] and info["path"] == 4
+    model = c.copy()
+    oracle.cgemm3m_fp32_model("T", "C", m, n, k, alpha, a, lda, b, ldb, beta, model, ldc, span=info["k_span"])
+    assert out.tobytes() == model.tobytes()
+    _check(oracle, out, c, "T", "C", m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)

@@ -187,9 +187,34 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def pipe_peak(form, sm_count):
+def sgemm_tflops(torch, dev, n=4096, reps=5):
+    """cuBLAS FP32 SGEMM (TF32 off) at n^3 on this GPU, timed with CUDA events:
+    the measured FP32-pipe peak (2n^3 flop per call)."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        a = torch.randn(n, n, device=dev)
+        b = torch.randn(n, n, device=dev)
+        for _ in range(2):
+            c = a @ b
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            c = a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        del a, b, c
+        return 2.0 * n ** 3 / (e0.elapsed_time(e1) / reps * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+
+
+def pipe_peak(form, sm_count, sgemm=None):
     pk, src = peaks()
     if form == "fp32":
+        if sgemm:
+            return sgemm, "measured: cuBLAS FP32 SGEMM 4096^3 (TF32 off) on this GPU, timed in this run"
         mhz = pk.get("sm_max_mhz", 1965.0)
         return sm_count * 128 * 2 * mhz * 1e6 / 1e12, f"nominal: {sm_count} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz"
     if form == "tf32x3":
@@ -524,7 +549,8 @@ def main():
     stages, _ = stage_times(args.form, max(3, min(args.steps, 10)))
     gemm_ms = stages[1]
     p = PASSES[args.form]
-    peak, peak_src = pipe_peak(args.form, sm_count)
+    sgemm = sgemm_tflops(torch, dev)
+    peak, peak_src = pipe_peak(args.form, sm_count, sgemm)
     achieved = flops6 * p / (gemm_ms * 1e-3) / 1e12
     pk_all, _src = peaks()
     sustained = pk_all.get("bf16_tflops_sustained")
@@ -598,7 +624,12 @@ def main():
             errors[form] = h.error_report(n, n, C, n, out64)
     if args.form != "fp32":
         pms, _ = timed("fp32", max(3, args.steps // 2), 2)
-        plain = {"value": world * flops8 / (pms * 1e-3) / 1e12, "ms_per_step": pms}
+        pst, _ = stage_times("fp32", 3)
+        plain = {"value": world * flops8 / (pms * 1e-3) / 1e12, "ms_per_step": pms, "gemm_ms": pst[1],
+                 "gemm_fp32_tflops": flops6 / (pst[1] * 1e-3) / 1e12, "sgemm_tflops_measured": sgemm,
+                 "gemm_frac_of_sgemm": flops6 / (pst[1] * 1e-3) / 1e12 / sgemm,
+                 "what": "plain FP32 3M GEMM kernel: 6MNK FFMA flop over its time, against cuBLAS FP32 SGEMM "
+                         "(TF32 off) timed on the same GPU in this run"}
     # The same calls with the rounding-correction pass as the reference gates it
     # (this shape qualifies): time, flagged-output recompute share, errors.
     rounding_report = None

@@ -37,7 +37,8 @@ METRIC = "c64 TFLOP/s (8MNK) at 4096^3: tensor-core 3M vs FP32 3M, same err vs F
 UNIT = "TFLOP/s"
 SIZE = 4096
 SEED_A, SEED_B = 20261203, 20261204
-WORKLOAD = "cgemm3m 4096x4096x4096 complex64 NN alpha=1 beta=0, precision-form data"
+def workload(n):
+    return f"cgemm3m {n}x{n}x{n} complex64 NN alpha=1 beta=0, precision-form data"
 PASSES = {"fp32": 1, "tf32x3": 3, "bf16x6": 6, "bf16x9": 9}
 
 
@@ -280,7 +281,7 @@ def run_reference(args, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": "reference-BLAS order FP32 (oracle port)", "sample": sample},
+        "config": {"workload": workload(args.size), "form": "reference-BLAS order FP32 (oracle port)", "sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -660,7 +661,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.form == "fp32" else args.form, "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": args.form, "rounding": args.rounding, "m": n, "n": n, "k": n,
+        "config": {"workload": workload(n), "form": args.form, "rounding": args.rounding, "m": n, "n": n, "k": n,
                    "transa": "N", "transb": "N",
                    "alpha": [1, 0], "beta": [0, 0], "parallelism": f"replica x{world} (independent problems)",
                    "l2": "inputs exceed L2: A, B, C 384 MiB plus packed planes; no flush needed",

@@ -206,7 +206,7 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
         }
         mark(++count);
     }
-    if (err == cudaSuccess && plan.parts > 1) {
+    if (err == cudaSuccess && plan.parts > 1 && !plan.cluster_merge) {
         err = launch_merge(s, p, plan, ws);
         mark(++count);
     }
@@ -700,7 +700,8 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
     info->k_partitions = plan.parts;
     info->k_span = plan.span;
     info->rounding = plan.rounding ? 1 : 0;
-    info->kernels = plan.engine == 2 ? 1 : 2 + (plan.parts > 1 ? 1 : 0) + (plan.rounding ? 4 : 0);
+    info->kernels =
+        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? 4 : 0);
     info->workspace_bytes = plan.total;
     return CG3M_STATUS_SUCCESS;
 }

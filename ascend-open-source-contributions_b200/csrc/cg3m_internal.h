@@ -50,6 +50,7 @@ struct Plan {
     int tc_segment = 0;      // K terms per TMEM accumulation segment (tensor-core forms)
     int engine = 1;          // 1 packed planes (pack + GEMM [+ merge]), 2 one cluster-merged launch
     int onchip_tile = 0;     // engine 2: tile index of the on-chip family (0 128x64 .. 5 32x32)
+    bool cluster_merge = false;  // FP32 packed engine: the K partitions (2..8) merge inside their cluster
     // workspace layout (byte offsets from the workspace base)
     size_t planes_a_off = 0, planes_b_off = 0, partial_off = 0, round_off = 0, total = 0;
     int pitch_a = 0, pitch_b = 0;  // elements per plane row

@@ -39,6 +39,7 @@ struct Fp32Params {
     int ppitch;
     size_t pplane;
     int* status;
+    int cluster_merge;  // the `parts` partitions of a tile form one cluster and merge on chip
 };
 
 template <int BM, int BN>
@@ -222,6 +223,20 @@ __global__ void __launch_bounds__(Fp32Cfg<BM, BN>::THREADS, 1)
 // consumer threads form Re = P0 - P1, Im = (P2 - P0) - P1, apply alpha/beta
 // and store with coalesced column-major writes.
 // ---------------------------------------------------------------------------
+// Loads from a shared::cluster address (a peer block's shared memory).
+__device__ __forceinline__ float ld_dsmem_f32(uint32_t addr)
+{
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_dsmem_s32(uint32_t addr)
+{
+    int v;
+    asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
+
 #ifndef CG3M_FP32_WS_UNROLL
 #define CG3M_FP32_WS_UNROLL 16
 #endif
@@ -372,28 +387,68 @@ __global__ void __launch_bounds__(ws::THREADS, 1)
         }
     }
     __syncthreads();
-    if (failed) {
+    if (!p.cluster_merge) {
+        if (failed) {
+            return;
+        }
+        for (int e = tid; e < BM * BN; e += THREADS) {
+            const int r = e % BM, c = e / BM;
+            const int row = m0 + r, col = n0 + c;
+            if (row >= p.m || col >= p.n) {
+                continue;
+            }
+            const float q0 = P[(0 * BN + c) * BM + r], q1 = P[(1 * BN + c) * BM + r];
+            const float q2 = P[(2 * BN + c) * BM + r];
+            const float re = __fsub_rn(q0, q1);
+            const float im = __fsub_rn(__fsub_rn(q2, q0), q1);
+            if (p.parts == 1) {
+                float2* cp = p.C + (size_t)col * p.ldc + row;
+                *cp = epilogue_value(re, im, p.epi, cp);
+            } else {
+                const size_t o = (size_t)col * p.ppitch + row;
+                p.partial[(size_t)(2 * part) * p.pplane + o] = re;
+                p.partial[(size_t)(2 * part + 1) * p.pplane + o] = im;
+            }
+        }
         return;
     }
+    // K split merged through the cluster (grid.y = cluster.y = parts): this
+    // partition's (Re, Im) replace planes 0 and 1 in place (element e read and
+    // written by one thread), a cluster barrier publishes them, and block q
+    // sums the q-th slice of the tile over partitions 0, 1, ... in order -- the
+    // merge kernel's arithmetic -- reading its peers' shared memory, then
+    // applies alpha/beta.  Every thread of every block reaches both barriers.
     for (int e = tid; e < BM * BN; e += THREADS) {
-        const int r = e % BM, c = e / BM;
-        const int row = m0 + r, col = n0 + c;
-        if (row >= p.m || col >= p.n) {
-            continue;
-        }
-        const float q0 = P[(0 * BN + c) * BM + r], q1 = P[(1 * BN + c) * BM + r];
-        const float q2 = P[(2 * BN + c) * BM + r];
-        const float re = __fsub_rn(q0, q1);
-        const float im = __fsub_rn(__fsub_rn(q2, q0), q1);
-        if (p.parts == 1) {
+        const float q0 = P[e], q1 = P[BN * BM + e], q2 = P[2 * BN * BM + e];
+        P[e] = __fsub_rn(q0, q1);
+        P[BN * BM + e] = __fsub_rn(__fsub_rn(q2, q0), q1);
+    }
+    cluster_sync();
+    const uint32_t re_local = smem_u32(P), im_local = smem_u32(P + BN * BM);
+    int bad = 0;
+    for (int q = 0; q < p.parts; ++q) {
+        bad |= ld_dsmem_s32(mapa_shared(smem_u32(&failed), q));
+    }
+    if (!bad) {
+        const int per = (BM * BN + p.parts - 1) / p.parts;
+        const int e_end = min(BM * BN, (part + 1) * per);
+        for (int e = part * per + tid; e < e_end; e += THREADS) {
+            const int r = e % BM, c = e / BM;
+            const int row = m0 + r, col = n0 + c;
+            if (row >= p.m || col >= p.n) {
+                continue;
+            }
+            float re = ld_dsmem_f32(mapa_shared(re_local + 4u * e, 0));
+            float im = ld_dsmem_f32(mapa_shared(im_local + 4u * e, 0));
+            for (int q = 1; q < p.parts; ++q) {
+                re = __fadd_rn(re, ld_dsmem_f32(mapa_shared(re_local + 4u * e, q)));
+                im = __fadd_rn(im, ld_dsmem_f32(mapa_shared(im_local + 4u * e, q)));
+            }
             float2* cp = p.C + (size_t)col * p.ldc + row;
             *cp = epilogue_value(re, im, p.epi, cp);
-        } else {
-            const size_t o = (size_t)col * p.ppitch + row;
-            p.partial[(size_t)(2 * part) * p.pplane + o] = re;
-            p.partial[(size_t)(2 * part + 1) * p.pplane + o] = im;
         }
     }
+    cluster_sync();  // no block leaves while others may still read its shared memory
 }
 
 // ---------------------------------------------------------------------------
@@ -637,8 +692,25 @@ cudaError_t launch_fp32_tile(cudaStream_t stream, const Problem& pr, const Plan&
         if (err != cudaSuccess) {
             return err;
         }
-        gemm3m_fp32_ws_kernel<<<grid, ws::THREADS, ws::SMEM, stream>>>(ta, tb, p);
-        return cudaGetLastError();
+        p.cluster_merge = plan.cluster_merge ? 1 : 0;
+        if (!p.cluster_merge) {
+            gemm3m_fp32_ws_kernel<<<grid, ws::THREADS, ws::SMEM, stream>>>(ta, tb, p);
+            return cudaGetLastError();
+        }
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(ws::THREADS, 1, 1);
+        cfg.dynamicSmemBytes = ws::SMEM;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 1;
+        attr[0].val.clusterDim.y = (unsigned)plan.parts;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        err = cudaLaunchKernelEx(&cfg, gemm3m_fp32_ws_kernel, ta, tb, p);
+        return err != cudaSuccess ? err : cudaGetLastError();
     }
     auto kernel = gemm3m_fp32_kernel<BM, BN>;
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);

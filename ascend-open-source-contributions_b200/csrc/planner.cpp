@@ -93,6 +93,22 @@ const TileChoice kFp32Tiles[] = {{128, 64, 1}};
 constexpr uint64_t kFp32WaveFixed = 38;
 constexpr uint64_t kMergeFixed = 30;
 constexpr uint64_t kMergeFloatsPerTerm = 41500;
+// With 2..8 partitions the partitions of a tile form one thread-block cluster
+// and merge through distributed shared memory inside the GEMM (no merge
+// kernel, no partial planes): waves then hold as many clusters as fit at once
+// (cudaOccupancyMaxActiveClusters for one block per SM on 148 SMs), and the
+// merge costs about one K term per partition.
+constexpr int kClusterMergeMax = 8;
+constexpr uint64_t kClusterCapOneBlock[kClusterMergeMax] = {148, 74, 45, 33, 26, 22, 15, 15};
+
+uint64_t fp32_waves(uint64_t tiles, int parts, int sm_count)
+{
+    if (parts > 1 && parts <= kClusterMergeMax) {
+        const uint64_t cap = std::max<uint64_t>(1, kClusterCapOneBlock[parts - 1] * (uint64_t)sm_count / 148);
+        return (tiles + cap - 1) / cap;
+    }
+    return (tiles * parts + sm_count - 1) / sm_count;
+}
 // The same costs in microseconds for the whole packed call (pack kernel over
 // op(A) and op(B) -- 8 bytes read, 12 written per element -- GEMM waves, merge
 // kernel), fitted on B200 to 28 timed shapes (median error 3.3 %).
@@ -128,11 +144,13 @@ int k_span(int k, int parts, int g = 16)
 
 double packed_time_us(const Problem& p, int parts, int span, uint64_t tiles, int sm_count)
 {
-    const uint64_t waves = (tiles * parts + sm_count - 1) / sm_count;
+    const uint64_t waves = fp32_waves(tiles, parts, sm_count);
     const double bytes = ((double)p.m * p.k + (double)p.k * p.n) * 20.0;
     double us = kPackedFixedUs + kPackedUsPerMB * bytes * 1e-6 + kPackedUsPerTerm * (double)waves * (span + kFp32WaveFixed);
-    if (parts > 1) {
+    if (parts > kClusterMergeMax) {
         us += kMergeLaunchUs + kMergeUsPerTerm * (kMergeFixed + (double)(2 * parts + 2) * p.m * p.n / kMergeFloatsPerTerm);
+    } else if (parts > 1) {
+        us += kPackedUsPerTerm * parts;
     }
     return us;
 }
@@ -221,10 +239,12 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
             if ((parts - 1) * span >= p.k || (parts > 1 && span < 64)) {
                 continue;
             }
-            const uint64_t waves = (default_tiles * parts + sm_count - 1) / sm_count;
+            const uint64_t waves = fp32_waves(default_tiles, parts, sm_count);
             const uint64_t gemm = waves * ((uint64_t)span + kFp32WaveFixed);
             const uint64_t merge =
-                parts > 1 ? kMergeFixed + (uint64_t)(2 * parts + 2) * p.m * p.n / kMergeFloatsPerTerm : 0;
+                parts > kClusterMergeMax ? kMergeFixed + (uint64_t)(2 * parts + 2) * p.m * p.n / kMergeFloatsPerTerm
+                : parts > 1              ? (uint64_t)parts
+                                         : 0;
             if (gemm + merge < best) {
                 best = gemm + merge;
                 best_parts = parts;
@@ -354,8 +374,10 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     off = align_up(off + out.plane_b_elems * elem * out.planes, kRegionAlign);
     out.partial_pitch = (int)align_up((size_t)p.m, 32);
     out.partial_plane_elems = (size_t)out.partial_pitch * p.n;
+    out.cluster_merge = !tc && !out.rounding && out.parts > 1 && out.parts <= kClusterMergeMax &&
+                        out.tile_m == 128 && out.tile_n == 64;
     out.partial_off = off;
-    if (out.parts > 1) {
+    if (out.parts > 1 && !out.cluster_merge) {
         off = align_up(off + out.partial_plane_elems * 4 * 2 * out.parts, kRegionAlign);
     }
     out.round_off = off;

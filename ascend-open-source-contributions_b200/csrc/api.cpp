@@ -101,6 +101,16 @@ cg3mStatus_t workspace(cg3mContext* h, size_t bytes, void** out)
     return CG3M_STATUS_SUCCESS;
 }
 
+// Options of cg3mCgemm's three-product case: the FP32 drop-in arithmetic, no
+// rounding pass.
+cg3mOptions cgemm_unit_options()
+{
+    cg3mOptions o{};
+    o.form = CG3M_FORM_FP32;
+    o.rounding = CG3M_ROUNDING_OFF;
+    return o;
+}
+
 cg3mStatus_t to_status(cudaError_t e)
 {
     if (e == cudaSuccess) {
@@ -457,11 +467,34 @@ cg3mStatus_t cg3mCgemm(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t t
     const bool unit = alpha->real == 1.0f && alpha->imag == 0.0f && beta->real == 0.0f && beta->imag == 0.0f;
     const int mode = unit ? 0 : 1;
     Problem p{transa, transb, m, n, k, alpha->real, alpha->imag, beta->real, beta->imag, A, lda, B, ldb, C, ldc};
-    // One problem: the one-launch kernel of the on-chip family (K partitions
-    // merged in a cluster; no workspace).
+    if (unit) {
+        // Three products with the repair: the FP32 planner's engine.  The packed
+        // engine's products equal the on-chip family's bit for bit for the same
+        // K split, and with alpha = 1, beta = 0 C holds them unchanged, so the
+        // repair can run as a pass over the finished C.
+        Plan plan;
+        if (!make_plan(p, cgemm_unit_options(), h->sm_count, &plan)) {
+            return CG3M_STATUS_INVALID_VALUE;
+        }
+        if (plan.engine == 2) {
+            return to_status(launch_single(h->stream, p, 0, 1, plan.onchip_tile, plan.parts));
+        }
+        void* ws = nullptr;
+        const cg3mStatus_t wst = workspace(h, plan.total, &ws);
+        if (wst != CG3M_STATUS_SUCCESS) {
+            return wst;
+        }
+        cudaError_t err = enqueue(h->stream, p, plan, ws, h->status, nullptr);
+        if (err == cudaSuccess) {
+            err = launch_repair(h->stream, p);
+        }
+        return to_status(err);
+    }
+    // Four products: the one-launch kernel of the on-chip family (K
+    // partitions merged in a cluster; no workspace).
     int tile = 0, parts = 1;
     plan_single(m, n, k, mode, h->sm_count, -1, 0, &tile, &parts);
-    return to_status(launch_single(h->stream, p, mode, unit ? 1 : 0, tile, parts));
+    return to_status(launch_single(h->stream, p, mode, 0, tile, parts));
 }
 
 cg3mStatus_t cg3mCgemm3mHost(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
@@ -710,6 +743,25 @@ cg3mStatus_t cg3mPlanOnchip(int m, int n, int k, int mode, int batch, int sm_cou
 {
     if (info == nullptr) {
         return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (mode == 2) {  // cg3mCgemm with alpha = 1, beta = 0: the FP32 planner's engine, then the repair pass
+        if (batch != 1 || m <= 0 || n <= 0 || k <= 0) {
+            return CG3M_STATUS_INVALID_VALUE;
+        }
+        Problem p{CG3M_OP_N, CG3M_OP_N, m, n, k, 1.0f, 0.0f, 0.0f, 0.0f, nullptr, m, nullptr, k, nullptr, m};
+        Plan plan;
+        if (!make_plan(p, cgemm_unit_options(), sm_count > 0 ? sm_count : 148, &plan)) {
+            return CG3M_STATUS_INVALID_VALUE;
+        }
+        std::memset(info, 0, sizeof(*info));
+        info->path = plan.engine == 2 ? 4 : plan.parts > 1 ? 3 : 2;
+        info->tile_m = plan.tile_m;
+        info->tile_n = plan.tile_n;
+        info->k_partitions = plan.parts;
+        info->k_span = plan.span;
+        info->kernels = plan.engine == 2 ? 1 : 3 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0);
+        info->workspace_bytes = plan.total;
+        return CG3M_STATUS_SUCCESS;
     }
     Problem p{CG3M_OP_N, CG3M_OP_N, m, n, k, 1.0f, 0.0f, 0.0f, 0.0f, nullptr, m, nullptr, k, nullptr, m};
     StridedPlan plan;

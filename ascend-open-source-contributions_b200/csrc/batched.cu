@@ -765,6 +765,23 @@ cudaError_t launch_single_tile(cudaStream_t s, const BProblem& bp, int tile)
     }
 }
 
+// Non-finite repair of a finished three-product result with alpha = 1 and
+// beta = 0, where C holds the merged products unchanged: every output with a
+// non-finite component is recomputed with the explicit four-product FP32 sum,
+// as the kernels above do before their identity epilogue.
+__global__ void repair_kernel(const BProblem p)
+{
+    const size_t total = (size_t)p.m * p.n;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int col = (int)(idx / p.m), row = (int)(idx - (size_t)col * p.m);
+        float2* cp = p.C + (size_t)col * p.ldc + row;
+        if (!finite2(*cp)) {
+            *cp = repair_product(p, row, col);
+        }
+    }
+}
+
 }  // namespace
 }  // namespace cg3m
 
@@ -1181,6 +1198,26 @@ cudaError_t launch_single(cudaStream_t s, const Problem& p, int mode, int repair
     const cudaError_t e =
         mode == kMode3M ? launch_single_tile<kMode3M>(s, bp, tile) : launch_single_tile<kMode4M>(s, bp, tile);
     return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t launch_repair(cudaStream_t s, const Problem& p)
+{
+    BProblem bp{};
+    bp.ta = p.transa;
+    bp.tb = p.transb;
+    bp.m = p.m;
+    bp.n = p.n;
+    bp.k = p.k;
+    bp.A = static_cast<const float2*>(p.A);
+    bp.B = static_cast<const float2*>(p.B);
+    bp.C = static_cast<float2*>(p.C);
+    bp.lda = p.lda;
+    bp.ldb = p.ldb;
+    bp.ldc = p.ldc;
+    const long long total = (long long)p.m * p.n;
+    const int grid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 8));
+    repair_kernel<<<grid, 256, 0, s>>>(bp);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_strided(cudaStream_t s, const Problem& p, int mode, int repair, long long sA, long long sB,

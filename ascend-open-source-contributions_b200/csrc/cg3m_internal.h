@@ -118,6 +118,9 @@ bool make_strided_plan(const Problem& p, int mode, int batch, int sm_count, Stri
 // (parts <= 8, and (parts - 1) * span < k).  tile: 0 128x64, 1 64x64,
 // 2 128x32, 3 32x128, 4 64x32, 5 32x32.  No workspace.
 cudaError_t launch_single(cudaStream_t s, const Problem& p, int mode, int repair, int tile, int parts);
+// Recomputes, with the explicit four-product FP32 sum, every output of C that
+// a three-product call with alpha = 1, beta = 0 left non-finite.
+cudaError_t launch_repair(cudaStream_t s, const Problem& p);
 // The one-launch plan for an m x n x k problem in `mode`: tile and K
 // partitions (each forced when >= 0), chosen to minimise the estimated time,
 // which is returned in microseconds.

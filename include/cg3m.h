@@ -278,7 +278,10 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
  * one problem shape: mode 0 = three products, 1 = four; `batch` problems per
  * launch.  Fills tile_m, tile_n, k_partitions, k_span and workspace_bytes.
  * batch == 1 (cg3mCgemm, a strided batch of one, or overlapping outputs run
- * one per launch) reports the one-launch kernel: path 4, no workspace. */
+ * one per launch) reports the one-launch kernel: path 4, no workspace.
+ * mode 2 (batch 1 only) = cg3mCgemm with alpha = 1, beta = 0: three products
+ * with the non-finite repair on the FP32 planner's engine (the one-launch
+ * kernel, or the packed engine followed by a repair pass over C). */
 cg3mStatus_t cg3mPlanOnchip(int m, int n, int k, int mode, int batch, int sm_count, cg3mCallInfo* info);
 
 /* ---- diagnostics (not a compute path of cgemm3m) ------------------------- */

@@ -226,7 +226,8 @@ def test_cgemm_bit_exact_and_reference_criterion(cg3m, oracle, cuda, h, case):
     out = to_host(dC)
     unit = alpha == 1 and beta == 0
     mode = 0 if unit else 1
-    plan = cg3m.plan_onchip(m, n, k, mode, 1, torch.cuda.get_device_properties(cuda).multi_processor_count)
+    # unit: three products + repair on the FP32 planner's engine (plan mode 2)
+    plan = cg3m.plan_onchip(m, n, k, 2 if unit else 1, 1, torch.cuda.get_device_properties(cuda).multi_processor_count)
     want = c.copy()
     oracle.cgemm_modes_model(mode, 1 if unit else 0, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, want, ldc,
                              span=plan["k_span"] if plan["k_partitions"] > 1 else 0)
@@ -291,7 +292,7 @@ def test_cgemm_case_table_rows(cg3m, oracle, cuda, h, cases):
         if m and n and k and alpha != 0:
             unit = alpha == 1 and beta == 0
             mode = 0 if unit else 1
-            plan = cg3m.plan_onchip(m, n, k, mode, 1, sms)
+            plan = cg3m.plan_onchip(m, n, k, 2 if unit else 1, 1, sms)
             model = c.copy()
             oracle.cgemm_modes_model(mode, 1 if unit else 0, ta, tb, m, n, k, alpha, a, cs["lda"], b, cs["ldb"], beta,
                                      model, cs["ldc"], span=plan["k_span"] if plan["k_partitions"] > 1 else 0)

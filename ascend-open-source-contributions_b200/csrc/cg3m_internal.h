@@ -51,6 +51,7 @@ struct Plan {
     int engine = 1;          // 1 packed planes (pack + GEMM [+ merge]), 2 one cluster-merged launch
     int onchip_tile = 0;     // engine 2: tile index of the on-chip family (0 128x64 .. 5 32x32)
     bool cluster_merge = false;  // FP32 packed engine: the K partitions (2..8) merge inside their cluster
+    double est_us = 0.0;         // FP32 plans: the planner's time estimate (microseconds)
     // workspace layout (byte offsets from the workspace base)
     size_t planes_a_off = 0, planes_b_off = 0, partial_off = 0, round_off = 0, total = 0;
     int pitch_a = 0, pitch_b = 0;  // elements per plane row

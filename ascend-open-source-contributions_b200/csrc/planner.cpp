@@ -209,7 +209,7 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
             --parts;
         }
         int tile = 0;
-        plan_single(p.m, p.n, p.k, 0, sm_count, opts.onchip_tile - 1, parts, &tile, &parts);
+        out.est_us = plan_single(p.m, p.n, p.k, 0, sm_count, opts.onchip_tile - 1, parts, &tile, &parts);
         out.engine = 2;
         out.onchip_tile = tile;
         out.tile_m = single_tile_bm(tile);
@@ -306,7 +306,9 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
         const int forced = opts.k_partitions > 0 ? out.parts : narrow ? 8 : 0;
         int tile = 0, parts = 0;
         const double single = plan_single(p.m, p.n, p.k, 0, sm_count, -1, forced, &tile, &parts);
-        if (single < packed_time_us(p, out.parts, out.span, default_tiles, sm_count)) {
+        out.est_us = packed_time_us(p, out.parts, out.span, default_tiles, sm_count);
+        if (single < out.est_us) {
+            out.est_us = single;
             out.engine = 2;
             out.onchip_tile = tile;
             out.tile_m = single_tile_bm(tile);
@@ -321,24 +323,19 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
 
     // ---- tensor-core forms on small shapes ---------------------------------------
     // A tensor-core call carries a fixed cost of 12-13 us (pack, TMEM set-up,
-    // pipeline fill) that the one-launch FP32 kernel does not.  Where the FP32
-    // one-launch estimate is clearly lower (a 1.25x margin over the rougher
-    // tensor-core model), the call runs in plain FP32 -- its error is the
-    // plain form's, which every form promises not to exceed -- and reports
-    // form FP32.  engine 1 (or a forced K split) keeps the tensor-core path.
+    // pipeline fill) that the FP32 engines do not.  Where the FP32 planner's
+    // own plan is clearly faster (a 1.1x margin over the rougher tensor-core
+    // model), the call runs that plan in plain FP32 -- its error is the plain
+    // form's, which every form promises not to exceed -- and reports form
+    // FP32.  engine 1 (or a forced K split) keeps the tensor-core path.
     if (tc && !out.rounding && opts.engine == 0 && opts.k_partitions <= 0) {
-        int tile = 0, parts = 0;
-        const double single = plan_single(p.m, p.n, p.k, 0, sm_count, -1, 0, &tile, &parts);
-        if (single * 1.25 < tc_time_us(p, opts.form, out.parts, out.span, sm_count)) {
-            out.form = CG3M_FORM_FP32;
-            out.engine = 2;
-            out.onchip_tile = tile;
-            out.tile_m = single_tile_bm(tile);
-            out.tile_n = single_tile_bn(tile);
-            out.parts = parts;
-            out.span = parts > 1 ? k_span(p.k, parts) : p.k;
-            out.total = 0;
-            *plan = out;
+        cg3mOptions fo = opts;
+        fo.form = CG3M_FORM_FP32;
+        fo.rounding = CG3M_ROUNDING_OFF;
+        Plan fp;
+        if (make_plan(p, fo, sm_count, &fp) && fp.est_us * 1.1 < tc_time_us(p, opts.form, out.parts, out.span,
+                                                                              sm_count)) {
+            *plan = fp;
             return true;
         }
     }

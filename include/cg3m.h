@@ -86,9 +86,9 @@ typedef struct {
                          merges its K partitions (<= 8) inside a thread-block cluster.  For a given K
                          split both give the same bits.  2 is refused (INVALID_VALUE) for the
                          tensor-core forms, with the rounding pass, or with k_partitions > 8.
-                         Tensor-core forms: 0 may run a small problem as the plain FP32 one-launch
-                         product when that is clearly faster (the call info then reports form FP32;
-                         its error is the plain form's); 1 always uses the tensor cores. */
+                         Tensor-core forms: 0 may run a small problem as the plain FP32 product (the
+                         FP32 planner's plan) when that is clearly faster (the call info then reports
+                         form FP32; its error is the plain form's); 1 always uses the tensor cores. */
     int onchip_tile;  /* engine 2: 0 = planner, 1..6 = 128x64, 64x64, 128x32, 32x128, 64x32, 32x32 */
     int reserved[2];
 } cg3mOptions;

@@ -2,8 +2,8 @@
 
 The product shards with no exchange: C(:, j) needs all of op(A) and only
 column j of op(B), so rank r of G owns a contiguous block of columns and
-multiplies op(A) by its own block of op(B) (SURVEY's multi-GPU row; no
-collective is needed on the data path).  Timing across ranks takes the maximum
+multiplies op(A) by its own block of op(B) (no collective is needed on the
+data path).  Timing across ranks takes the maximum
 of the per-rank device times.
 """
 from __future__ import annotations

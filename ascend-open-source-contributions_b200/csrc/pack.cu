@@ -1,4 +1,4 @@
-// pack.cu -- deinterleave / pack kernel (north-star item (a)).
+// pack.cu -- deinterleave / pack kernel.
 //
 // Reference: gemm_cgemm_deinterleave_kernel, blas/gemm/arch35/cgemm_kernel.cpp
 // :137-157 and DeinterleaveElement, cgemm_deinterleave_common.h:18-52.  The

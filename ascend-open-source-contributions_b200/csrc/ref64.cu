@@ -1,6 +1,6 @@
 // ref64.cu -- FP64 reference product and error report (diagnostics only).
 //
-// The north star asks every result to report its normwise and worst
+// Every result can report its normwise and worst
 // componentwise errors (real and imaginary parts separately) against an FP64
 // zgemm.  For full-size problems that reference is computed here, on the
 // device, in complex128 with a plain 32x32 shared-memory tiling; it is never

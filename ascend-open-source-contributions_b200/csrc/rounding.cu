@@ -1,4 +1,4 @@
-// rounding.cu -- the rounding-correction pass (north-star item (d)).
+// rounding.cu -- the rounding-correction pass.
 //
 // Reference: gemm_cgemm3m_rounding_do, blas/gemm/arch35/cgemm3m_rounding_kernel.cpp
 // :474-497, run after the path-tracking GEMM when the call is a contiguous

@@ -1,4 +1,4 @@
-"""GPU parity of the rounding-correction pass (north-star item (d)).
+"""GPU parity of the rounding-correction pass.
 
 Reference: gemm_cgemm3m_rounding_do and its kernels (ops-blas/blas/gemm/arch35/
 cgemm3m_rounding_kernel.cpp:43-497), gated at cgemm_host.cpp:234-238, and the

@@ -5,8 +5,9 @@ forms are checked against FP64 rather than bit for bit (engine="packed" keeps
 every call on the tensor cores; the planner may otherwise run a small problem
 as plain FP32): the reference accuracy
 criterion (cgemm3m_verify.h:22-84) against the FP64 result rounded to FP32, a
-normwise-error bound, run-to-run bitwise determinism, and the north-star bar --
-normwise error vs FP64 no worse than the plain FP32 3M form on the same inputs.
+normwise-error bound, run-to-run bitwise determinism, and the precision forms'
+promise -- normwise error vs FP64 no worse than the plain FP32 3M form on the
+same inputs.
 """
 import numpy as np
 import pytest

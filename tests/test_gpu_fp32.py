@@ -125,6 +125,28 @@ def test_forced_k_partitions_bit_exact(cg3m, oracle, cuda, h, parts):
     assert same_bits(out, model)
 
 
+@pytest.mark.parametrize("parts", [2, 3, 5, 8, 12])
+def test_packed_engine_split_merges_bit_exact(cg3m, oracle, cuda, h, parts):
+    """The packed engine's K split: 2..8 partitions merge inside the GEMM through
+    the tile's cluster (two launches), deeper splits through the merge kernel
+    (three); both give the model's bits, on ragged tiles with padded ld."""
+    import torch
+
+    m, n, k = 300, 130, 1500
+    alpha, beta = complex(0.3, -1.25), complex(0.5, 0.5)
+    a, lda, b, ldb, c, ldc = _operands(oracle, "N", "T", m, n, k, 5, "RANDOM_NORM_5_5", 700 + parts)
+    out, info = run(cg3m, h, torch, cuda, "N", "T", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                    k_partitions=parts, engine="packed", rounding="off")
+    assert info["k_partitions"] == parts and info["path"] == 3
+    assert info["kernels"] == (2 if parts <= 8 else 3)
+    again, _ = run(cg3m, h, torch, cuda, "N", "T", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                   k_partitions=parts, engine="packed", rounding="off")
+    assert out.tobytes() == again.tobytes()
+    model = c.copy()
+    oracle.cgemm3m_fp32_model("N", "T", m, n, k, alpha, a, lda, b, ldb, beta, model, ldc, span=info["k_span"])
+    assert same_bits(out, model)
+
+
 def _fixture_cases(cases, limit=3e6):
     out = []
     for c in cases["cases"]:

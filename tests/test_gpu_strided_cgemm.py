@@ -344,3 +344,35 @@ def test_strided_case_table_rows(cg3m, oracle, cuda, h, cases):
                 if not same_bits(ot, model):
                     failures.append((cs["name"], t, "model"))
     assert not failures, failures[:10]
+
+
+def test_cgemm_unit_packed_engine_repair_pass(cg3m, oracle, cuda, h):
+    """cg3mCgemm with alpha = 1, beta = 0 on a shape the planner gives to the
+    packed engine: entries near the FP32 maximum make some three-product sums
+    overflow, and the repair pass over C recomputes exactly those outputs with
+    the four-product sum -- the same bits as the on-chip family's model."""
+    import torch
+
+    m, n, k = 600, 400, 500
+    plan = cg3m.plan_onchip(m, n, k, 2, 1, torch.cuda.get_device_properties(cuda).multi_processor_count)
+    assert plan["path"] in (2, 3)  # pack + GEMM (+ merge) + repair pass
+    rng = np.random.default_rng(17)
+    a = (rng.uniform(-1, 1, m * k) + 1j * rng.uniform(-1, 1, m * k)).astype(np.complex64)
+    b = (rng.uniform(-1, 1, k * n) + 1j * rng.uniform(-1, 1, k * n)).astype(np.complex64)
+    hot = rng.choice(m * k, 40, replace=False)
+    a[hot] = np.complex64(complex(2.5e38, 2.5e38))
+    b *= np.float32(1e-6)
+    c = np.zeros(m * n, np.complex64)
+    dC = to_dev(c, torch, cuda)
+    assert h.cgemm("N", "N", m, n, k, 1.0, to_dev(a, torch, cuda), m, to_dev(b, torch, cuda), k, 0.0, dC,
+                   m) == cg3m.SUCCESS
+    torch.cuda.synchronize()
+    out = to_host(dC)
+    span = plan["k_span"] if plan["k_partitions"] > 1 else 0
+    want = c.copy()
+    oracle.cgemm_modes_model(0, 1, "N", "N", m, n, k, 1.0, a, m, b, k, 0.0, want, m, span=span)
+    assert same_bits(out, want)
+    plain = c.copy()
+    oracle.cgemm_modes_model(0, 0, "N", "N", m, n, k, 1.0, a, m, b, k, 0.0, plain, m, span=span)
+    assert not np.all(np.isfinite(plain.view(np.float32)))  # the three-product sums overflow ...
+    assert np.all(np.isfinite(out.view(np.float32)))        # ... the repaired outputs do not

@@ -144,7 +144,22 @@ struct TcParams {
     int* status;
     int seg_blocks;  // K-blocks per accumulation segment
     float* path;     // risk plane (path-tracking variant), ld = ldc
+    int cluster_merge;  // pair kernel: the `parts` pairs of a tile form one cluster and merge on chip
 };
+
+// Loads from a shared::cluster address (a peer block's shared memory).
+__device__ __forceinline__ float ld_dsmem_f32(uint32_t addr)
+{
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_dsmem_s32(uint32_t addr)
+{
+    int v;
+    asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
 
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle (layout type 2),
 // 8-row groups 8 x 128 = 1024 bytes apart (SBO), leading offset unused (1),
@@ -475,6 +490,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr int KSTEPS = ROW_BYTES / 32;
     constexpr int COLS = G::COLS;
     constexpr int BN = PAIR_BN;
+    static_assert((size_t)2 * TILE_M * BN * sizeof(float) <= (size_t)STAGES * STAGE_BYTES,
+                  "merge partials must fit the ring below the barriers");
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -488,8 +505,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const uint32_t rank = cluster_ctarank();
+    // The cluster is the CTA pair (1 x 2), or with an on-chip K merge the pairs
+    // of all partitions of the tile (2 x parts): ranks 2q and 2q + 1 are the
+    // pair of partition q, so the pair role is rank bit 0.
+    const uint32_t crank = cluster_ctarank();
+    const uint32_t rank = crank & 1u;     // role in the pair: 0 even (MMA issuer), 1 odd
+    const uint32_t base = crank & ~1u;    // cluster rank of this pair's even CTA
+    const uint16_t pair_mask = (uint16_t)(0x3u << base);
     const bool leader = rank == 0;
+    __shared__ int merge_fail;
 
     constexpr int GM = 4;  // pair tiles per L2 group along m
     const int pid = blockIdx.x >> 1;
@@ -519,6 +543,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         mbar_init(mma_done, 1);
         *abort_flag = 0;
+        merge_fail = 0;
         fence_mbar_init();
     }
     if (warp == 1) {
@@ -549,7 +574,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                             break;
                         }
                         uint8_t* st = ring + s * STAGE_BYTES;
-                        const uint32_t bar = mapa_shared(smem_u32(&full[s]), 0);
+                        const uint32_t bar = mapa_shared(smem_u32(&full[s]), base);
                         if (leader) {
                             mbar_arrive_expect_tx(&full[s], 2 * STAGE_BYTES);
                         }
@@ -609,14 +634,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                                 }
                             }
                         }
-                        umma_commit_pair(&empty[s], 0x3);
+                        umma_commit_pair(&empty[s], pair_mask);
                     }
                     if (!stop && c > 0) {
-                        umma_commit_pair(&acc_full[c], 0x3);
+                        umma_commit_pair(&acc_full[c], pair_mask);
                     }
                 }
             }
-            umma_commit_pair(mma_done, 0x3);
+            umma_commit_pair(mma_done, pair_mask);
             mbar_wait(mma_done, 0, p.status);  // nothing may still write TMEM when it is freed
         }
     } else {
@@ -626,9 +651,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int row = m0 + quad * 32 + lane;
         const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * COLS);
         const uint32_t spare = lane_addr + (uint32_t)(3 * BN);
-        const uint32_t free0 = mapa_shared(smem_u32(&acc_free[0]), 0);
-        const uint32_t free1 = mapa_shared(smem_u32(&acc_free[1]), 0);
-        const uint32_t free2 = mapa_shared(smem_u32(&acc_free[2]), 0);
+        const uint32_t free0 = mapa_shared(smem_u32(&acc_free[0]), base);
+        const uint32_t free1 = mapa_shared(smem_u32(&acc_free[1]), base);
+        const uint32_t free2 = mapa_shared(smem_u32(&acc_free[2]), base);
         float re[COLS], im[COLS];
         bool go = true;
         for (int seg = 0; seg < segments && go; ++seg) {
@@ -679,7 +704,24 @@ __global__ void __launch_bounds__(kThreads, 1)
                 mbar_arrive_cluster(free2);
             }
         }
-        if (go && row < p.m) {
+        if (p.cluster_merge) {
+            // This partition's (Re, Im) of the CTA's 128 rows x 128 columns go to
+            // the ring, free once the last segment's products are read (every
+            // MMA, and so every copy into the ring, is complete by then).
+            if (!go) {
+                merge_fail = 1;
+            } else {
+                float* part_re = reinterpret_cast<float*>(ring);
+                float* part_im = part_re + TILE_M * BN;
+                const int rl = quad * 32 + lane;
+#pragma unroll
+                for (int j = 0; j < COLS; ++j) {
+                    const int cl = half * COLS + j;
+                    part_re[cl * TILE_M + rl] = re[j];
+                    part_im[cl * TILE_M + rl] = im[j];
+                }
+            }
+        } else if (go && row < p.m) {
 #pragma unroll
             for (int j = 0; j < COLS; ++j) {
                 const int col = n0 + half * COLS + j;
@@ -699,6 +741,41 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_fence_before();
     __syncthreads();
     cluster_sync();  // the even CTA's MMAs are complete; neither CTA's memory is used any more
+    if (p.cluster_merge) {
+        // K merge across the tile's pairs: CTA (pair role r, partition q) sums
+        // the q-th slice of its 128 x 128 half-tile over partitions 0, 1, ... in
+        // order (the merge kernel's arithmetic), reading the same role's CTA of
+        // every partition (cluster rank r + 2q'), then applies alpha/beta.
+        // Every thread of every CTA reaches both cluster barriers.
+        const uint32_t re_local = smem_u32(ring), im_local = re_local + 4u * TILE_M * BN;
+        int bad = 0;
+        for (int q = 0; q < p.parts; ++q) {
+            const uint32_t peer = rank + 2u * (uint32_t)q;
+            bad |= ld_dsmem_s32(mapa_shared(smem_u32(&merge_fail), peer));
+            bad |= ld_dsmem_s32(mapa_shared(smem_u32((const void*)abort_flag), peer));
+        }
+        if (!bad) {
+            const int per = (TILE_M * BN + p.parts - 1) / p.parts;
+            const int e_end = min(TILE_M * BN, (part + 1) * per);
+            for (int e = part * per + tid; e < e_end; e += kThreads) {
+                const int rl = e % TILE_M, cl = e / TILE_M;
+                const int row = m0 + rl, col = n0 + cl;
+                if (row >= p.m || col >= p.n) {
+                    continue;
+                }
+                float vre = ld_dsmem_f32(mapa_shared(re_local + 4u * e, rank));
+                float vim = ld_dsmem_f32(mapa_shared(im_local + 4u * e, rank));
+                for (int q = 1; q < p.parts; ++q) {
+                    const uint32_t peer = rank + 2u * (uint32_t)q;
+                    vre = __fadd_rn(vre, ld_dsmem_f32(mapa_shared(re_local + 4u * e, peer)));
+                    vim = __fadd_rn(vim, ld_dsmem_f32(mapa_shared(im_local + 4u * e, peer)));
+                }
+                float2* cp = p.C + (size_t)col * p.ldc + row;
+                *cp = epilogue_value(vre, vim, p.epi, cp);
+            }
+        }
+        cluster_sync();  // no CTA leaves while others may still read its shared memory
+    }
     if (warp == 1) {
         tc_fence_after();
         tmem_dealloc_pair(tmem, G::TMEM_COLS);
@@ -751,6 +828,12 @@ cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan
         p.seg_blocks = 1;
     }
     p.path = nullptr;
+    p.cluster_merge = plan.cluster_merge ? 1 : 0;
+    if (p.cluster_merge && (plan.parts < 2 || plan.parts > 4)) {
+        return cudaErrorInvalidValue;  // clusters of at most 8 CTAs: up to 4 pairs
+    }
+    static_assert((size_t)2 * TILE_M * PAIR_BN * sizeof(float) <= (size_t)PAIR_RING,
+                  "merge partials exceed the ring");
     auto kernel = gemm3m_tc_pair_kernel<FORM>;
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
     if (err != cudaSuccess) {
@@ -764,7 +847,7 @@ cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = 2;
-    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.y = p.cluster_merge ? (unsigned)plan.parts : 1u;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;

@@ -371,8 +371,22 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     off = align_up(off + out.plane_b_elems * elem * out.planes, kRegionAlign);
     out.partial_pitch = (int)align_up((size_t)p.m, 32);
     out.partial_plane_elems = (size_t)out.partial_pitch * p.n;
-    out.cluster_merge = !tc && !out.rounding && out.parts > 1 && out.parts <= kClusterMergeMax &&
-                        out.tile_m == 128 && out.tile_n == 64;
+    // K splits merged on chip through the tile's cluster: the FP32 GEMM (up to 8
+    // partitions) and the tensor-core CTA-pair kernel (used for m > 128; up to 4
+    // partitions, two CTAs each).  The pair kernel merges on chip only when all
+    // of its clusters of 2 x parts CTAs are resident at once: a grid that one
+    // wave holds as loose CTAs but not as clusters runs a second wave, which
+    // costs more than the merge launch it saves (1.3-1.6x on 128..144-CTA grids).
+    bool tc_merge = false;
+    if (tc && p.m > 128 && out.parts <= 4) {
+        const uint64_t pair_tiles = (uint64_t)ceil_div(p.m, 256) * ceil_div(p.n, 128);
+        const uint64_t cap =
+            std::max<uint64_t>(1, kClusterCapOneBlock[2 * out.parts - 1] * (uint64_t)sm_count / 148);
+        tc_merge = pair_tiles <= cap;
+    }
+    out.cluster_merge = !out.rounding && out.parts > 1 &&
+                        (tc ? tc_merge
+                            : (out.parts <= kClusterMergeMax && out.tile_m == 128 && out.tile_n == 64));
     out.partial_off = off;
     if (out.parts > 1 && !out.cluster_merge) {
         off = align_up(off + out.partial_plane_elems * 4 * 2 * out.parts, kRegionAlign);

@@ -94,17 +94,24 @@ def test_tc_nine_ops_padded(cg3m, oracle, cuda, h, form, ta, tb):
 
 
 @pytest.mark.parametrize("form", FORMS)
-@pytest.mark.parametrize("parts", [2, 3])
+@pytest.mark.parametrize("parts", [2, 3, 4, 5])
 def test_tc_forced_partitions(cg3m, oracle, cuda, h, form, parts):
+    """CTA-pair kernel with a forced K split: 2..4 partitions merge inside the
+    kernel through the tile's cluster (pack + GEMM), 5 through the merge kernel."""
     import torch
 
-    m, n, k = 200, 150, 1000
+    m, n, k = 200, 150, 1500  # 24 blocks of 64: splits into 2, 3, 4 and 5 spans come out exact
     alpha, beta = complex(0.3, -1.25), complex(0.5, 0.5)
     a, lda, b, ldb, c, ldc = _operands(oracle, "T", "N", m, n, k, 2, "RANDOM_NORM_5_5", 77)
     out, info = run(cg3m, h, torch, cuda, "T", "N", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form,
                     k_partitions=parts, engine="packed")
     assert info["k_partitions"] == parts and info["k_span"] % 64 == 0
+    assert info["kernels"] == (2 if parts <= 4 else 3)
+    again, _ = run(cg3m, h, torch, cuda, "T", "N", m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, form=form,
+                   k_partitions=parts, engine="packed")
+    assert out.tobytes() == again.tobytes()
     _check(oracle, out, c, "T", "N", m, n, k, alpha, a, lda, b, ldb, beta, ldc, 2e-6)
+    assert h.device_status() == 0
 
 
 @pytest.mark.parametrize("form", FORMS)

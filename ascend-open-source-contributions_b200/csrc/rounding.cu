@@ -22,9 +22,9 @@
 // recompute works on
 // output tiles so operand rows are staged once per tile instead of once per
 // output, and skips tiles with no flagged output.  FP32 form: the reference's
-// segmented replay, one output per thread over 16 x 16 tiles, with the 64
-// lane sums in shared memory and the lane reductions and the inclusive lane
-// scan in fixed orders.  Tensor-core forms: flagged outputs are recomputed
+// segmented replay over 16 x 16 tiles, 2 x 2 outputs per thread for 8 of the
+// 64 lanes, with the 64 lane sums in shared memory and the lane reductions
+// and the inclusive lane scan in fixed orders.  Tensor-core forms: flagged outputs are recomputed
 // in FP64 over 64 x 64 tiles (K in order) and rounded once to FP32.
 #include <cstring>
 #include <functional>
@@ -119,28 +119,22 @@ __device__ __forceinline__ bool flagged(const uint32_t* bits, size_t idx)
 
 // ---- 4a. FP32 segmented replay (FastSegmentDot) ---------------------------------------
 
-struct Cf {
-    float r, i;
-};
-
-// One 3M term with the fused identity (ThreeProductTerms, :192-208).
-__device__ __forceinline__ Cf term(float2 x, float2 y)
-{
-    const float p = __fmul_rn(__fadd_rn(x.x, x.y), y.x);
-    const float q = __fmul_rn(x.x, __fsub_rn(y.y, y.x));
-    const float rr = __fmul_rn(x.y, __fadd_rn(y.x, y.y));
-    return Cf{__fsub_rn(p, rr), __fadd_rn(p, q)};
-}
-
-// FP32 segmented replay of one 16 x 16 output tile with 512 threads: two per
-// output, the lower half of the block summing K lanes 0..31 and the upper half
-// lanes 32..63 (lane l holds k in [l*span, (l+1)*span)), both halves on the
-// same lane step at a time while the next step's op(A) rows and op(B) columns
-// are copied into shared memory.  The 64 lane sums of each output sit in
-// shared memory (S[l][output]); the lower-half thread computes the reduction,
-// the inclusive scan and the final selection, and both halves replay their
-// lanes seeded with the scanned prefixes -- all in the oracle's fixed orders.
-// Only flagged outputs are written.
+// FP32 segmented replay of one 16 x 16 output tile with 512 threads.  Warps
+// 2g and 2g + 1 hold the K lanes 8g .. 8g + 7 (lane l holds k in
+// [l*span, (l+1)*span)); each of their threads owns the 2 x 2 outputs of one
+// micro-tile (rows 2*mr, 2*mr + 1, columns 2*mc, 2*mc + 1).  So every op(A)
+// and op(B) value a thread loads from shared memory feeds two outputs, and the
+// operand sums of the fused identity (xr + xi, yi - yr, yr + yi) are formed
+// once per load rather than once per output.  A lane is walked in kChunks
+// chunks of ch = ceil(span / kChunks) terms; one step stages chunk c of lane
+// 8g + s for all eight groups (the next step's copies in flight during this
+// one), so every thread takes the same barriers.  The 64 lane sums of each
+// output sit in shared memory (S[l][output]); one thread per output and part
+// (real or imaginary) computes the direct reduction, the inclusive scan and
+// the final selection with the 64 values in registers, and the groups replay
+// their lanes seeded with the scanned prefixes -- all in the
+// oracle's fixed orders, with each output's K terms of a lane added one at a
+// time in increasing k.  Only flagged outputs are written.
 __device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes)
 {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
@@ -151,14 +145,46 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_by
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Shared memory of recompute_fp32_tiled: the 64 lane sums (real, imaginary)
-// of the tile's 256 outputs, then two staging buffers, each with the operand
-// slices (16 rows of op(A) and 16 columns of op(B), span K terms each) of two
-// lanes, one for each half of the block.
+constexpr int kGroups = 8;                                   // lane groups, two warps each
+constexpr int kGroupLanes = kLanes / kGroups;                // 8 lanes per group
+constexpr int kChunks = 4;                                   // chunks per lane
+constexpr int kChunk = (kMaxSpan + kChunks - 1) / kChunks;   // 17: the longest chunk
+constexpr int kRow = kChunk;                                 // staged row stride in float2
+static_assert(kRow % 2 == 1, "an odd row stride keeps a warp's 16 rows in distinct banks");
+constexpr int kSteps = kGroupLanes * kChunks;                // 32 staging steps per pass
 constexpr size_t kLaneSumBytes = (size_t)2 * kLanes * 256 * sizeof(float);
-constexpr size_t kStageElems = (size_t)kMaxSpan * kTile;  // float2 per operand per buffer
-constexpr int kStageIters = (kTile * kMaxSpan + 511) / 512;  // staging elements per thread
-constexpr size_t kRecomputeSmem = kLaneSumBytes + 2 * 2 * 2 * kStageElems * sizeof(float2);
+constexpr size_t kGroupSlice = (size_t)kTile * kRow;             // float2 per operand per group
+constexpr size_t kBufElems = (size_t)kGroups * 2 * kGroupSlice;  // float2 per staging buffer
+constexpr size_t kRecomputeSmem = kLaneSumBytes + 2 * kBufElems * sizeof(float2);
+constexpr int kStageIters = (2 * kTile * kChunk + 63) / 64;     // copies per staging thread per step
+
+// Accumulate terms [0, len) of one staged chunk into the 2 x 2 outputs: X holds
+// rows ra, ra + 1 of op(A), Y columns cb, cb + 1 of op(B), kRow apart.  Output
+// (a, b) is acc[a + 2b].  Each term is the fused identity of ThreeProductTerms
+// (:192-208): p = (xr + xi) yr, re = p - xi (yr + yi), im = p + xr (yi - yr).
+__device__ __forceinline__ void replay_chunk(const float2* X, const float2* Y, int len, float* acc_r, float* acc_i)
+{
+#pragma unroll 4
+    for (int q = 0; q < len; ++q) {
+        const float2 x0 = X[q], x1 = X[kRow + q];
+        const float2 y0 = Y[q], y1 = Y[kRow + q];
+        const float sx[2] = {__fadd_rn(x0.x, x0.y), __fadd_rn(x1.x, x1.y)};
+        const float dy[2] = {__fsub_rn(y0.y, y0.x), __fsub_rn(y1.y, y1.x)};
+        const float ey[2] = {__fadd_rn(y0.x, y0.y), __fadd_rn(y1.x, y1.y)};
+        const float xr[2] = {x0.x, x1.x}, xi[2] = {x0.y, x1.y}, yr[2] = {y0.x, y1.x};
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const float p = __fmul_rn(sx[a], yr[b]);
+                const float qq = __fmul_rn(xr[a], dy[b]);
+                const float rr = __fmul_rn(xi[a], ey[b]);
+                acc_r[a + 2 * b] = __fadd_rn(acc_r[a + 2 * b], __fsub_rn(p, rr));
+                acc_i[a + 2 * b] = __fadd_rn(acc_i[a + 2 * b], __fadd_rn(p, qq));
+            }
+        }
+    }
+}
 
 __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, const float2* __restrict__ rows_a,
                                                             const float2* __restrict__ rows_b,
@@ -166,180 +192,204 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
                                                             const uint32_t* __restrict__ tile_flags,
                                                             float2* __restrict__ C)
 {
-    extern __shared__ __align__(16) float lane_sums[];  // [2][64][256]: real then imaginary
+    // Lane sums, real then imaginary: S[l][o] for output o = ti + 16 tj of the tile.
+    extern __shared__ __align__(16) float lane_sums[];
     float* sr = lane_sums;
     float* si = lane_sums + kLanes * 256;
-    float2* stage_base = reinterpret_cast<float2*>(reinterpret_cast<char*>(lane_sums) + kLaneSumBytes);
+    float2* stage = reinterpret_cast<float2*>(reinterpret_cast<char*>(lane_sums) + kLaneSumBytes);
     const int tiles = (n + kTile - 1) / kTile;
     if (tile_flags[blockIdx.x] == 0) {
         return;
     }
     const int i0 = (blockIdx.x % tiles) * kTile, j0 = (blockIdx.x / tiles) * kTile;
     const int tid = threadIdx.x;
-    // Thread (o, half): output o of the 16 x 16 tile, K lanes [32*half, 32*half + 32).
-    // A warp covers 8 rows x 4 columns of the tile, so each of its operand
-    // reads touches at most 8 distinct shared addresses.
-    const int o = tid & 255, half = tid >> 8;
-    const int ti = (o & 7) | (((o >> 5) & 1) << 3), tj = ((o >> 3) & 3) | ((o >> 6) << 2);
-    const int i = i0 + ti, j = j0 + tj;
-    // Buffer b holds, for both halves h, xs[r][q] and ys[r][q] of lane
-    // 32h + step at slot(b, h, 0) and slot(b, h, 1), rows span apart: span is
-    // odd, so the rows a warp reads at one q fall in distinct bank pairs, and
-    // consecutive threads stage consecutive q of one row.
-    auto slot = [&](int b, int h, int op) { return stage_base + (size_t)((b * 2 + h) * 2 + op) * kStageElems; };
+    const int ch = (span + kChunks - 1) / kChunks;
     auto lane_count = [&](int l) { return max(0, min(span, n - l * span)); };
-    // Staging element e = tid + 512u of a lane slice (u < staged): row
-    // r = e / span, K offset q = e % span, shared offset e.  These are fixed for
-    // the launch; a step only moves the source by the lane's K start.  A row
-    // outside the matrix gets q = span, which fails every q < count test.
-    const int slice = kTile * span;
-    const int staged = tid < slice ? (slice - tid + 511) / 512 : 0;
-    const float2* src_a[kStageIters];
-    const float2* src_b[kStageIters];
-    int qa[kStageIters], qb[kStageIters];
+    auto chunk_len = [&](int l, int c) { return max(0, min(ch, lane_count(l) - c * ch)); };
+
+    // Compute role: group g = warp / 2; the warp's 32 micro-tiles cover all 16
+    // rows (mr = lane % 8) and 8 of the 16 columns, so one operand load of a
+    // warp touches 8 distinct op(A) rows or 4 distinct op(B) columns.
+    const int warp = tid >> 5, wl = tid & 31;
+    const int g = warp >> 1;
+    const int ra = 2 * (wl & 7), cb = 2 * (((warp & 1) << 2) | (wl >> 3));
+    int out[4];  // o of output (a, b) at out[a + 2b]
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            out[a + 2 * b] = (ra + a) + kTile * (cb + b);
+        }
+    }
+
+    // Staging role: the 64 threads of group sg copy its 32 rows (16 of op(A),
+    // then 16 of op(B)) of one chunk.  Element e = st + 64u is row e / ch at
+    // offset e % ch, so the copies of one warp run along one or two rows; the
+    // offsets are fixed for the launch, a step only moves the source by the
+    // chunk's K start.  Rows past the matrix read as zero.
+    const int sg = tid >> 6, st = tid & 63;
+    const float2* src[kStageIters];
+    int dst[kStageIters], qs[kStageIters];
 #pragma unroll
     for (int u = 0; u < kStageIters; ++u) {
-        const int e = tid + 512 * u;
-        const int r = e / span, q = e - r * span;
-        const bool in_a = u < staged && i0 + r < n, in_b = u < staged && j0 + r < n;
-        src_a[u] = in_a ? rows_a + (size_t)(i0 + r) * n + q : rows_a;
-        src_b[u] = in_b ? rows_b + (size_t)(j0 + r) * n + q : rows_b;
-        qa[u] = in_a ? q : span;
-        qb[u] = in_b ? q : span;
+        const int e = st + 64 * u;
+        const int ro = e / ch, q = e - ro * ch;
+        const int op = ro >> 4, r = ro & 15;
+        const int row = (op ? j0 : i0) + r;
+        const bool staged = e < 2 * kTile * ch;
+        src[u] = staged && row < n ? (op ? rows_b : rows_a) + (size_t)row * n + q : nullptr;
+        dst[u] = staged ? (sg * 2 + op) * (int)kGroupSlice + r * kRow + q : 0;
+        qs[u] = staged ? q : kChunk;  // kChunk fails every q < len test
     }
-    // Asynchronous copy of lanes step and 32 + step into buffer b; positions
-    // past the end of K or past the matrix read as zero.
-    auto issue = [&](int step, int b) {
+    auto issue = [&](int t, int b) {
+        const int l = kGroupLanes * sg + t / kChunks, c = t % kChunks;
+        const int len = chunk_len(l, c);
+        const int k0 = l * span + c * ch;
+        float2* base = stage + (size_t)b * kBufElems;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int l = step + 32 * h;
-            const int k0 = l * span;
-            const int cnt = lane_count(l);
-            float2* X = slot(b, h, 0) + tid;
-            float2* Y = slot(b, h, 1) + tid;
-#pragma unroll
-            for (int u = 0; u < kStageIters; ++u) {
-                if (u < staged) {
-                    const bool okx = qa[u] < cnt, oky = qb[u] < cnt;
-                    cp_async8(X + 512 * u, okx ? (const void*)(src_a[u] + k0) : rows_a, okx ? 8 : 0);
-                    cp_async8(Y + 512 * u, oky ? (const void*)(src_b[u] + k0) : rows_b, oky ? 8 : 0);
-                }
+        for (int u = 0; u < kStageIters; ++u) {
+            if (qs[u] < len) {
+                cp_async8(base + dst[u], src[u] != nullptr ? (const void*)(src[u] + k0) : (const void*)rows_a,
+                          src[u] != nullptr ? 8 : 0);
             }
         }
         cp_async_commit();
     };
-    // pass 1: lane sums (the next lane pair is copied while this one is summed)
+    auto slab = [&](int t, int which) {
+        return stage + (size_t)(t & 1) * kBufElems + (size_t)(g * 2 + which) * kGroupSlice;
+    };
+
+    // pass 1: lane sums (the next step's chunks are copied while this one is summed)
+    float acc_r[4], acc_i[4];
     issue(0, 0);
-    for (int step = 0; step < kLanes / 2; ++step) {
+    for (int t = 0; t < kSteps; ++t) {
         cp_async_wait_all();
         __syncthreads();  // this step staged by every thread; the previous step's buffer is free
-        if (step + 1 < kLanes / 2) {
-            issue(step + 1, (step + 1) & 1);
+        if (t + 1 < kSteps) {
+            issue(t + 1, (t + 1) & 1);
         }
-        const int l = step + 32 * half;
-        const int cnt = lane_count(l);
-        const float2* X = slot(step & 1, half, 0);
-        const float2* Y = slot(step & 1, half, 1);
-        Cf acc{0.0f, 0.0f};
-#pragma unroll 8
-        for (int q = 0; q < cnt; ++q) {
-            const Cf t = term(X[ti * span + q], Y[tj * span + q]);
-            acc.r = __fadd_rn(acc.r, t.r);
-            acc.i = __fadd_rn(acc.i, t.i);
+        const int l = kGroupLanes * g + t / kChunks, c = t % kChunks;
+        if (c == 0) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                acc_r[u] = 0.0f;
+                acc_i[u] = 0.0f;
+            }
         }
-        sr[l * 256 + o] = acc.r;
-        si[l * 256 + o] = acc.i;
+        replay_chunk(slab(t, 0) + ra * kRow, slab(t, 1) + cb * kRow, chunk_len(l, c), acc_r, acc_i);
+        if (c == kChunks - 1) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                sr[l * 256 + out[u]] = acc_r[u];
+                si[l * 256 + out[u]] = acc_i[u];
+            }
+        }
     }
     __syncthreads();  // all 64 lane sums of every output are in place
-    float direct_r = 0.0f, direct_i = 0.0f, max_r = 0.0f, max_i = 0.0f;
-    if (half == 0) {
-        // direct reduction (pairwise, stride 32 .. 1) in registers
-        float vr[kLanes], vi[kLanes];
+    // Lane reductions and the scan: thread t takes the real (t < 256) or the
+    // imaginary part of output o = t % 256, with its 64 lane values in
+    // registers.
+    const int o = tid & 255;
+    float* const part = tid < 256 ? sr : si;
+    float direct, peak = 0.0f;
+    {
+        float v[kLanes];
 #pragma unroll
         for (int l = 0; l < kLanes; ++l) {
-            vr[l] = sr[l * 256 + o];
-            vi[l] = si[l * 256 + o];
+            v[l] = part[l * 256 + o];
         }
+        // direct reduction (pairwise, stride 32 .. 1)
 #pragma unroll
         for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
 #pragma unroll
             for (int l = 0; l < stride; ++l) {
-                vr[l] = __fadd_rn(vr[l], vr[l + stride]);
-                vi[l] = __fadd_rn(vi[l], vi[l + stride]);
+                v[l] = __fadd_rn(v[l], v[l + stride]);
             }
         }
-        direct_r = vr[0];
-        direct_i = vi[0];
-        // inclusive Hillis-Steele scan in place: new[l] = s[l] + s[l-d] for l >= d
-        for (int d = 1; d < kLanes; d *= 2) {
-            for (int l = kLanes - 1; l >= d; --l) {
-                sr[l * 256 + o] = __fadd_rn(sr[l * 256 + o], sr[(l - d) * 256 + o]);
-                si[l * 256 + o] = __fadd_rn(si[l * 256 + o], si[(l - d) * 256 + o]);
-            }
-        }
+        direct = v[0];
+#pragma unroll
         for (int l = 0; l < kLanes; ++l) {
-            const float ar = fabsf(sr[l * 256 + o]), ai = fabsf(si[l * 256 + o]);
-            max_r = ar > max_r ? ar : max_r;
-            max_i = ai > max_i ? ai : max_i;
+            v[l] = part[l * 256 + o];
+        }
+        // inclusive Hillis-Steele scan in place: new[l] = s[l] + s[l-d] for l >= d
+#pragma unroll
+        for (int d = 1; d < kLanes; d *= 2) {
+#pragma unroll
+            for (int l = kLanes - 1; l >= d; --l) {
+                v[l] = __fadd_rn(v[l], v[l - d]);
+            }
+        }
+#pragma unroll
+        for (int l = 0; l < kLanes; ++l) {
+            const float a = fabsf(v[l]);
+            peak = a > peak ? a : peak;
+            part[l * 256 + o] = v[l];
         }
     }
     __syncthreads();  // scanned prefixes in place; every thread is done with the last buffer
-    // pass 2: replay each lane seeded with the previous lanes' prefix.  The
-    // upper half starts from the prefix of lane 31, read before the lower half
-    // overwrites it (after at least 31 more barriers).
-    float prev_r = half == 0 ? 0.0f : sr[31 * 256 + o];
-    float prev_i = half == 0 ? 0.0f : si[31 * 256 + o];
+    // pass 2: replay each lane seeded with the previous lane's prefix.  Group g
+    // starts from the prefix of lane 8g - 1, read here, before group g - 1
+    // overwrites it at the last step; each lane's own prefix is read at the
+    // lane's first chunk, before its replayed value replaces it.
+    float prev_r[4], prev_i[4], init_r[4], init_i[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        prev_r[u] = g == 0 ? 0.0f : sr[(kGroupLanes * g - 1) * 256 + out[u]];
+        prev_i[u] = g == 0 ? 0.0f : si[(kGroupLanes * g - 1) * 256 + out[u]];
+        init_r[u] = 0.0f;
+        init_i[u] = 0.0f;
+    }
     issue(0, 0);
-    for (int step = 0; step < kLanes / 2; ++step) {
+    for (int t = 0; t < kSteps; ++t) {
         cp_async_wait_all();
         __syncthreads();
-        if (step + 1 < kLanes / 2) {
-            issue(step + 1, (step + 1) & 1);
+        if (t + 1 < kSteps) {
+            issue(t + 1, (t + 1) & 1);
         }
-        const int l = step + 32 * half;
-        const int cnt = lane_count(l);
-        const float2* X = slot(step & 1, half, 0);
-        const float2* Y = slot(step & 1, half, 1);
-        const float init_r = prev_r, init_i = prev_i;
-        prev_r = sr[l * 256 + o];
-        prev_i = si[l * 256 + o];
-        float r = __fadd_rn(init_r, 0.0f), im = __fadd_rn(init_i, 0.0f);
-#pragma unroll 8
-        for (int q = 0; q < cnt; ++q) {
-            const Cf t = term(X[ti * span + q], Y[tj * span + q]);
-            r = __fadd_rn(r, t.r);
-            im = __fadd_rn(im, t.i);
+        const int l = kGroupLanes * g + t / kChunks, c = t % kChunks;
+        if (c == 0) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                init_r[u] = prev_r[u];
+                init_i[u] = prev_i[u];
+                prev_r[u] = sr[l * 256 + out[u]];
+                prev_i[u] = si[l * 256 + out[u]];
+                acc_r[u] = __fadd_rn(init_r[u], 0.0f);
+                acc_i[u] = __fadd_rn(init_i[u], 0.0f);
+            }
         }
-        sr[l * 256 + o] = __fsub_rn(r, init_r);
-        si[l * 256 + o] = __fsub_rn(im, init_i);
+        replay_chunk(slab(t, 0) + ra * kRow, slab(t, 1) + cb * kRow, chunk_len(l, c), acc_r, acc_i);
+        if (c == kChunks - 1) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                sr[l * 256 + out[u]] = __fsub_rn(acc_r[u], init_r[u]);
+                si[l * 256 + out[u]] = __fsub_rn(acc_i[u], init_i[u]);
+            }
+        }
     }
     __syncthreads();  // every replayed lane is in place
-    if (half == 0) {
-        float vr[kLanes], vi[kLanes];
+    {
+        float v[kLanes];
 #pragma unroll
         for (int l = 0; l < kLanes; ++l) {
-            vr[l] = sr[l * 256 + o];
-            vi[l] = si[l * 256 + o];
+            v[l] = part[l * 256 + o];
         }
 #pragma unroll
         for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
 #pragma unroll
             for (int l = 0; l < stride; ++l) {
-                vr[l] = __fadd_rn(vr[l], vr[l + stride]);
-                vi[l] = __fadd_rn(vi[l], vi[l + stride]);
+                v[l] = __fadd_rn(v[l], v[l + stride]);
             }
         }
-        float bridged_r = vr[0], bridged_i = vi[0];
-        if (max_r >= __fmul_rn(fabsf(direct_r), 32.0f)) {
-            bridged_r = direct_r;
+        float bridged = v[0];
+        if (peak >= __fmul_rn(fabsf(direct), 32.0f)) {
+            bridged = direct;
         }
-        if (max_i >= __fmul_rn(fabsf(direct_i), 32.0f)) {
-            bridged_i = direct_i;
-        }
+        const int i = i0 + (o & (kTile - 1)), j = j0 + o / kTile;
         if (i < n && j < n) {
             const size_t idx = (size_t)j * n + i;
             if (flagged(flag_bits, idx)) {
-                C[idx] = make_float2(bridged_r, bridged_i);
+                reinterpret_cast<float*>(C)[2 * idx + (tid < 256 ? 0 : 1)] = bridged;
             }
         }
     }
@@ -554,6 +604,9 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
     }
     if (err == cudaSuccess) {
         if (plan.form == CG3M_FORM_FP32) {
+            if (span > kChunks * kChunk) {
+                return cudaErrorInvalidValue;  // lanes longer than the staged chunks (n > 4096)
+            }
             const int tiles = (n + kTile - 1) / kTile;
             const size_t smem = kRecomputeSmem;
             err = cudaFuncSetAttribute(recompute_fp32_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -157,6 +157,7 @@ constexpr size_t kGroupSlice = (size_t)kTile * kRow;             // float2 per o
 constexpr size_t kBufElems = (size_t)kGroups * 2 * kGroupSlice;  // float2 per staging buffer
 constexpr size_t kRecomputeSmem = kLaneSumBytes + 2 * kBufElems * sizeof(float2);
 constexpr int kStageIters = (2 * kTile * kChunk + 63) / 64;     // copies per staging thread per step
+constexpr int kBand = 16;                                        // tile rows per band of the launch order
 
 // Accumulate terms [0, len) of one staged chunk into the 2 x 2 outputs: X holds
 // rows ra, ra + 1 of op(A), Y columns cb, cb + 1 of op(B), kRow apart.  Output
@@ -197,11 +198,17 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
     float* sr = lane_sums;
     float* si = lane_sums + kLanes * 256;
     float2* stage = reinterpret_cast<float2*>(reinterpret_cast<char*>(lane_sums) + kLaneSumBytes);
+    // Tiles run in bands of kBand tile rows, rows fastest within a band: the
+    // op(A) rows of a band stay in L2 while its columns go by, so op(A) is read
+    // from DRAM about once and op(B) once per band.
     const int tiles = (n + kTile - 1) / kTile;
-    if (tile_flags[blockIdx.x] == 0) {
+    const int band = blockIdx.x / (kBand * tiles), first = band * kBand;
+    const int rows_in_band = min(kBand, tiles - first), in_band = blockIdx.x - band * kBand * tiles;
+    const int ti_tile = first + in_band % rows_in_band, tj_tile = in_band / rows_in_band;
+    if (tile_flags[(size_t)tj_tile * tiles + ti_tile] == 0) {
         return;
     }
-    const int i0 = (blockIdx.x % tiles) * kTile, j0 = (blockIdx.x / tiles) * kTile;
+    const int i0 = ti_tile * kTile, j0 = tj_tile * kTile;
     const int tid = threadIdx.x;
     const int ch = (span + kChunks - 1) / kChunks;
     auto lane_count = [&](int l) { return max(0, min(span, n - l * span)); };

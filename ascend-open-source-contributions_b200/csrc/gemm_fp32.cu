@@ -484,7 +484,12 @@ __global__ void __launch_bounds__(288, 1)
     uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * B_STAGE);
     uint64_t* empty = full + STAGES;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tm = blockIdx.x % p.tiles, tn = blockIdx.x / p.tiles;
+    // Tiles run in bands of BAND tile rows, rows fastest within a band, so the
+    // band's op(A) planes stay in L2 while its columns go by.
+    constexpr int BAND = 8;
+    const int band = blockIdx.x / (BAND * p.tiles), first = band * BAND;
+    const int rows_in_band = min(BAND, p.tiles - first), in_band = blockIdx.x - band * BAND * p.tiles;
+    const int tm = first + in_band % rows_in_band, tn = in_band / rows_in_band;
     const int m0 = tm * BM, n0 = tn * BN;
     const int ktiles = (p.n + BK - 1) / BK;
     if (tid == 0) {
@@ -517,14 +522,22 @@ __global__ void __launch_bounds__(288, 1)
         const int wm = warp & 1, wn = warp >> 1;
         const int tm0 = wm * 32 + (lane & 7) * 4;
         const int tn0 = wn * 16 + (lane >> 3) * 4;
-        float p0[4][4], p1[4][4], p2[4][4], sr[4][4], si[4][4], ir[4][4], ii[4][4];
+        // Product accumulators in column pairs: p0[i][jj] = (P0(row i, col 2jj),
+        // P0(row i, col 2jj + 1)), updated by one packed FMA (__ffma2_rn: two
+        // independent round-to-nearest FMAs).
+        float2 p0[4][2], p1[4][2], p2[4][2];
+        float sr[4][4], si[4][4], ir[4][4], ii[4][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i) {
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj) {
+                p0[i][jj] = p1[i][jj] = p2[i][jj] = make_float2(0.0f, 0.0f);
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                p0[i][j] = p1[i][j] = p2[i][j] = 0.0f;
                 sr[i][j] = si[i][j] = ir[i][j] = ii[i][j] = 0.0f;
             }
+        }
         bool ok = true;
         int seg_terms = 0;
         for (int kt = 0; kt < ktiles; ++kt) {
@@ -538,7 +551,8 @@ __global__ void __launch_bounds__(288, 1)
             const int kvalid = min(BK, p.n - kt * BK);
 #pragma unroll
             for (int kk = 0; kk < BK; ++kk) {
-                float x0[4], x1[4], x2[4], y0[4], y1[4], y2[4];
+                float x0[4], x1[4], x2[4];
+                float2 y0[2], y1[2], y2[2];
                 *reinterpret_cast<float4*>(x0) = *reinterpret_cast<const float4*>(a + kk * BM);
                 *reinterpret_cast<float4*>(x1) = *reinterpret_cast<const float4*>(a + (BK + kk) * BM);
                 *reinterpret_cast<float4*>(x2) = *reinterpret_cast<const float4*>(a + (2 * BK + kk) * BM);
@@ -546,13 +560,16 @@ __global__ void __launch_bounds__(288, 1)
                 *reinterpret_cast<float4*>(y1) = *reinterpret_cast<const float4*>(b + (BK + kk) * BN);
                 *reinterpret_cast<float4*>(y2) = *reinterpret_cast<const float4*>(b + (2 * BK + kk) * BN);
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < 4; ++i) {
+                    const float2 a0 = make_float2(x0[i], x0[i]), a1 = make_float2(x1[i], x1[i]),
+                                 a2 = make_float2(x2[i], x2[i]);
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        p0[i][j] = __fmaf_rn(x0[i], y0[j], p0[i][j]);
-                        p1[i][j] = __fmaf_rn(x1[i], y1[j], p1[i][j]);
-                        p2[i][j] = __fmaf_rn(x2[i], y2[j], p2[i][j]);
+                    for (int jj = 0; jj < 2; ++jj) {
+                        p0[i][jj] = __ffma2_rn(a0, y0[jj], p0[i][jj]);
+                        p1[i][jj] = __ffma2_rn(a1, y1[jj], p1[i][jj]);
+                        p2[i][jj] = __ffma2_rn(a2, y2[jj], p2[i][jj]);
                     }
+                }
             }
             __syncwarp();
             if (lane == 0) {
@@ -566,8 +583,11 @@ __global__ void __launch_bounds__(288, 1)
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
-                        const float nr = __fadd_rn(sr[i][j], __fsub_rn(p0[i][j], p1[i][j]));
-                        const float ni = __fadd_rn(si[i][j], __fsub_rn(__fsub_rn(p2[i][j], p0[i][j]), p1[i][j]));
+                        const float q0 = (j & 1) ? p0[i][j >> 1].y : p0[i][j >> 1].x;
+                        const float q1 = (j & 1) ? p1[i][j >> 1].y : p1[i][j >> 1].x;
+                        const float q2 = (j & 1) ? p2[i][j >> 1].y : p2[i][j >> 1].x;
+                        const float nr = __fadd_rn(sr[i][j], __fsub_rn(q0, q1));
+                        const float ni = __fadd_rn(si[i][j], __fsub_rn(__fsub_rn(q2, q0), q1));
                         float t = __fmul_rn(sr[i][j], sr[i][j]);
                         t = __fmaf_rn(sr[i][j], nr, t);
                         t = __fmaf_rn(nr, nr, t);
@@ -578,7 +598,12 @@ __global__ void __launch_bounds__(288, 1)
                         ii[i][j] = __fadd_rn(ii[i][j], __fmul_rn(t, w));
                         sr[i][j] = nr;
                         si[i][j] = ni;
-                        p0[i][j] = p1[i][j] = p2[i][j] = 0.0f;
+                    }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int jj = 0; jj < 2; ++jj) {
+                        p0[i][jj] = p1[i][jj] = p2[i][jj] = make_float2(0.0f, 0.0f);
                     }
                 seg_terms = 0;
             }

@@ -163,7 +163,7 @@ constexpr int kBand = 16;                                        // tile rows pe
 // rows ra, ra + 1 of op(A), Y columns cb, cb + 1 of op(B), kRow apart.  Output
 // (a, b) is acc[a + 2b].  Each term is the fused identity of ThreeProductTerms
 // (:192-208): p = (xr + xi) yr, re = p - xi (yr + yi), im = p + xr (yi - yr).
-__device__ __forceinline__ void replay_chunk(const float2* X, const float2* Y, int len, float* acc_r, float* acc_i)
+__device__ __forceinline__ void replay_chunk(const float2* X, const float2* Y, int len, float2* acc)
 {
 #pragma unroll 4
     for (int q = 0; q < len; ++q) {
@@ -180,8 +180,10 @@ __device__ __forceinline__ void replay_chunk(const float2* X, const float2* Y, i
                 const float p = __fmul_rn(sx[a], yr[b]);
                 const float qq = __fmul_rn(xr[a], dy[b]);
                 const float rr = __fmul_rn(xi[a], ey[b]);
-                acc_r[a + 2 * b] = __fadd_rn(acc_r[a + 2 * b], __fsub_rn(p, rr));
-                acc_i[a + 2 * b] = __fadd_rn(acc_i[a + 2 * b], __fadd_rn(p, qq));
+                // (re, im) of the term, added to the output's (re, im) by one
+                // packed add: two independent round-to-nearest adds of sums,
+                // no product feeds it.
+                acc[a + 2 * b] = __fadd2_rn(acc[a + 2 * b], make_float2(__fsub_rn(p, rr), __fadd_rn(p, qq)));
             }
         }
     }
@@ -267,7 +269,7 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
     };
 
     // pass 1: lane sums (the next step's chunks are copied while this one is summed)
-    float acc_r[4], acc_i[4];
+    float2 acc[4];  // (re, im) of output (a, b) at acc[a + 2b]
     issue(0, 0);
     for (int t = 0; t < kSteps; ++t) {
         cp_async_wait_all();
@@ -279,16 +281,15 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
         if (c == 0) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                acc_r[u] = 0.0f;
-                acc_i[u] = 0.0f;
+                acc[u] = make_float2(0.0f, 0.0f);
             }
         }
-        replay_chunk(slab(t, 0) + ra * kRow, slab(t, 1) + cb * kRow, chunk_len(l, c), acc_r, acc_i);
+        replay_chunk(slab(t, 0) + ra * kRow, slab(t, 1) + cb * kRow, chunk_len(l, c), acc);
         if (c == kChunks - 1) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                sr[l * 256 + out[u]] = acc_r[u];
-                si[l * 256 + out[u]] = acc_i[u];
+                sr[l * 256 + out[u]] = acc[u].x;
+                si[l * 256 + out[u]] = acc[u].y;
             }
         }
     }
@@ -361,16 +362,15 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
                 init_i[u] = prev_i[u];
                 prev_r[u] = sr[l * 256 + out[u]];
                 prev_i[u] = si[l * 256 + out[u]];
-                acc_r[u] = __fadd_rn(init_r[u], 0.0f);
-                acc_i[u] = __fadd_rn(init_i[u], 0.0f);
+                acc[u] = make_float2(__fadd_rn(init_r[u], 0.0f), __fadd_rn(init_i[u], 0.0f));
             }
         }
-        replay_chunk(slab(t, 0) + ra * kRow, slab(t, 1) + cb * kRow, chunk_len(l, c), acc_r, acc_i);
+        replay_chunk(slab(t, 0) + ra * kRow, slab(t, 1) + cb * kRow, chunk_len(l, c), acc);
         if (c == kChunks - 1) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                sr[l * 256 + out[u]] = __fsub_rn(acc_r[u], init_r[u]);
-                si[l * 256 + out[u]] = __fsub_rn(acc_i[u], init_i[u]);
+                sr[l * 256 + out[u]] = __fsub_rn(acc[u].x, init_r[u]);
+                si[l * 256 + out[u]] = __fsub_rn(acc[u].y, init_i[u]);
             }
         }
     }

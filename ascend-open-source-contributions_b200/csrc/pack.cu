@@ -155,7 +155,7 @@ unsigned pack_blocks(const PackSide& a, const PackSide& b)
 
 }  // namespace
 
-cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a, void* rows_b)
+cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a, void* rows_b, int pitch)
 {
     auto side = [&](bool isA) {
         PackSide s{};
@@ -171,7 +171,7 @@ cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a
         // K-major rows: A row i holds op(A)(i, :), B row j holds op(B)(:, j).
         s.trans = isA ? (normal ? 1 : 0) : (normal ? 0 : 1);
         s.out = isA ? rows_a : rows_b;
-        s.pitch = p.k;
+        s.pitch = pitch;  // row stride in complex elements (>= k)
         s.plane_elems = 0;
         return s;
     };

@@ -30,10 +30,11 @@
 #include <functional>
 
 #include "cg3m_internal.h"
+#include "ptx.cuh"
 
 namespace cg3m {
 
-cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a, void* rows_b);
+cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a, void* rows_b, int pitch);
 cudaError_t launch_gemm_fp32_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, float* path,
                                   int* status);
 cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, float* path,
@@ -49,13 +50,13 @@ constexpr float kConfidence = 3.75f;  // CGEMM_ROUNDING_CONFIDENCE, cgemm_host.c
 // ---- 2. energies ----------------------------------------------------------------
 
 __global__ void __launch_bounds__(kLanes) energy_kernel(const float2* __restrict__ rows_a,
-                                                        const float2* __restrict__ rows_b, int n, int span,
-                                                        float* __restrict__ energy)
+                                                        const float2* __restrict__ rows_b, int n, int pitch,
+                                                        int span, float* __restrict__ energy)
 {
     extern __shared__ float2 row[];
     __shared__ float lanes[kLanes];
     const int r = blockIdx.x;
-    const float2* src = r < n ? rows_a + (size_t)r * n : rows_b + (size_t)(r - n) * n;
+    const float2* src = r < n ? rows_a + (size_t)r * pitch : rows_b + (size_t)(r - n) * pitch;
     for (int k = threadIdx.x; k < n; k += kLanes) {
         row[k] = src[k];
     }
@@ -122,53 +123,59 @@ __device__ __forceinline__ bool flagged(const uint32_t* bits, size_t idx)
 // FP32 segmented replay of one 16 x 16 output tile with 512 threads.  Warps
 // 2g and 2g + 1 hold the K lanes 8g .. 8g + 7 (lane l holds k in
 // [l*span, (l+1)*span)); each of their threads owns the 2 x 2 outputs of one
-// micro-tile (rows 2*mr, 2*mr + 1, columns 2*mc, 2*mc + 1).  So every op(A)
-// and op(B) value a thread loads from shared memory feeds two outputs, and the
+// micro-tile (rows mr, mr + 8, columns 2*mc, 2*mc + 1).  So every op(A) and
+// op(B) value a thread loads from shared memory feeds two outputs, and the
 // operand sums of the fused identity (xr + xi, yi - yr, yr + yi) are formed
 // once per load rather than once per output.  A lane is walked in kChunks
-// chunks of ch = ceil(span / kChunks) terms; one step stages chunk c of lane
-// 8g + s for all eight groups (the next step's copies in flight during this
-// one), so every thread takes the same barriers.  The 64 lane sums of each
-// output sit in shared memory (S[l][output]); one thread per output and part
-// (real or imaginary) computes the direct reduction, the inclusive scan and
-// the final selection with the 64 values in registers, and the groups replay
-// their lanes seeded with the scanned prefixes -- all in the
-// oracle's fixed orders, with each output's K terms of a lane added one at a
-// time in increasing k.  Only flagged outputs are written.
-__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
-                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-                 "l"(src), "r"(src_bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
+// chunks of ch = ceil(span / kChunks) terms.  One step stages chunk c of lane
+// 8g + s for all eight groups: one thread issues two 2-D tensor copies per
+// group (16 rows of op(A), 16 of op(B), w columns from the even K offset at or
+// below the chunk's start), completing on the buffer's mbarrier, while the
+// block sums the previous step.  The 64 lane sums of each output sit in shared
+// memory (S[l][output]); one thread per output and part (real or imaginary)
+// computes the direct reduction, the inclusive scan and the final selection
+// with the 64 values in registers, and the groups replay their lanes seeded
+// with the scanned prefixes -- all in the oracle's fixed orders, with each
+// output's K terms of a lane added one at a time in increasing k.  Only
+// flagged outputs are written.
 constexpr int kGroups = 8;                                   // lane groups, two warps each
 constexpr int kGroupLanes = kLanes / kGroups;                // 8 lanes per group
 constexpr int kChunks = 4;                                   // chunks per lane
 constexpr int kChunk = (kMaxSpan + kChunks - 1) / kChunks;   // 17: the longest chunk
-constexpr int kRow = kChunk;                                 // staged row stride in float2
-static_assert(kRow % 2 == 1, "an odd row stride keeps a warp's 16 rows in distinct banks");
 constexpr int kSteps = kGroupLanes * kChunks;                // 32 staging steps per pass
+constexpr int kBoxMax = 18;                                  // widest staged row (float2)
 constexpr size_t kLaneSumBytes = (size_t)2 * kLanes * 256 * sizeof(float);
-constexpr size_t kGroupSlice = (size_t)kTile * kRow;             // float2 per operand per group
-constexpr size_t kBufElems = (size_t)kGroups * 2 * kGroupSlice;  // float2 per staging buffer
-constexpr size_t kRecomputeSmem = kLaneSumBytes + 2 * kBufElems * sizeof(float2);
-constexpr int kStageIters = (2 * kTile * kChunk + 63) / 64;     // copies per staging thread per step
-constexpr int kBand = 16;                                        // tile rows per band of the launch order
+constexpr size_t kBoxElems = (size_t)kTile * kBoxMax;               // float2 per staged box
+constexpr size_t kBufElems = (size_t)kGroups * 2 * kBoxElems;       // float2 per staging buffer
+constexpr size_t kRecomputeSmem = 128 + kLaneSumBytes + 2 * kBufElems * sizeof(float2) + 2 * sizeof(uint64_t);
+constexpr int kBand = 16;                                           // tile rows per band of the launch order
+static_assert(kBoxElems * sizeof(float2) % 128 == 0, "staged boxes start on 128-byte boundaries");
 
-// Accumulate terms [0, len) of one staged chunk into the 2 x 2 outputs: X holds
-// rows ra, ra + 1 of op(A), Y columns cb, cb + 1 of op(B), kRow apart.  Output
-// (a, b) is acc[a + 2b].  Each term is the fused identity of ThreeProductTerms
-// (:192-208): p = (xr + xi) yr, re = p - xi (yr + yi), im = p + xr (yi - yr).
-__device__ __forceinline__ void replay_chunk(const float2* X, const float2* Y, int len, float2* acc)
+// Staged row width for chunks of ch terms: at least ch + 1 (the copy starts at
+// the even K offset at or below the chunk's start), even (16-byte rows) and
+// 2 mod 4, so the 8 rows (or 4 columns) a warp reads at one K offset fall in
+// distinct shared-memory bank pairs.
+static int box_width(int ch)
+{
+    int w = ch + 1;
+    while (w % 4 != 2) {
+        ++w;
+    }
+    return w;
+}
+
+// Accumulate terms [0, len) of one staged chunk into the 2 x 2 outputs: x0, x1
+// are the two op(A) rows, y0, y1 the two op(B) columns, all at the chunk's
+// first term.  Output (a, b) is acc[a + 2b].  Each term is the fused identity
+// of ThreeProductTerms (:192-208): p = (xr + xi) yr, re = p - xi (yr + yi),
+// im = p + xr (yi - yr).
+__device__ __forceinline__ void replay_chunk(const float2* X0, const float2* X1, const float2* Y0,
+                                             const float2* Y1, int len, float2* acc)
 {
 #pragma unroll 4
     for (int q = 0; q < len; ++q) {
-        const float2 x0 = X[q], x1 = X[kRow + q];
-        const float2 y0 = Y[q], y1 = Y[kRow + q];
+        const float2 x0 = X0[q], x1 = X1[q];
+        const float2 y0 = Y0[q], y1 = Y1[q];
         const float sx[2] = {__fadd_rn(x0.x, x0.y), __fadd_rn(x1.x, x1.y)};
         const float dy[2] = {__fsub_rn(y0.y, y0.x), __fsub_rn(y1.y, y1.x)};
         const float ey[2] = {__fadd_rn(y0.x, y0.y), __fadd_rn(y1.x, y1.y)};
@@ -189,17 +196,20 @@ __device__ __forceinline__ void replay_chunk(const float2* X, const float2* Y, i
     }
 }
 
-__global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, const float2* __restrict__ rows_a,
-                                                            const float2* __restrict__ rows_b,
+__global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constant__ CUtensorMap tm_a,
+                                                            const __grid_constant__ CUtensorMap tm_b, int n,
+                                                            int span, int ch, int w,
                                                             const uint32_t* __restrict__ flag_bits,
                                                             const uint32_t* __restrict__ tile_flags,
-                                                            float2* __restrict__ C)
+                                                            float2* __restrict__ C, int* status)
 {
+    extern __shared__ uint8_t replay_smem[];
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(replay_smem) + 127) & ~uintptr_t(127));
     // Lane sums, real then imaginary: S[l][o] for output o = ti + 16 tj of the tile.
-    extern __shared__ __align__(16) float lane_sums[];
-    float* sr = lane_sums;
-    float* si = lane_sums + kLanes * 256;
-    float2* stage = reinterpret_cast<float2*>(reinterpret_cast<char*>(lane_sums) + kLaneSumBytes);
+    float* sr = reinterpret_cast<float*>(base);
+    float* si = sr + kLanes * 256;
+    float2* stage = reinterpret_cast<float2*>(base + kLaneSumBytes);
+    uint64_t* full = reinterpret_cast<uint64_t*>(stage + 2 * kBufElems);
     // Tiles run in bands of kBand tile rows, rows fastest within a band: the
     // op(A) rows of a band stay in L2 while its columns go by, so op(A) is read
     // from DRAM about once and op(B) once per band.
@@ -212,71 +222,83 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
     }
     const int i0 = ti_tile * kTile, j0 = tj_tile * kTile;
     const int tid = threadIdx.x;
-    const int ch = (span + kChunks - 1) / kChunks;
     auto lane_count = [&](int l) { return max(0, min(span, n - l * span)); };
     auto chunk_len = [&](int l, int c) { return max(0, min(ch, lane_count(l) - c * ch)); };
 
     // Compute role: group g = warp / 2; the warp's 32 micro-tiles cover all 16
-    // rows (mr = lane % 8) and 8 of the 16 columns, so one operand load of a
-    // warp touches 8 distinct op(A) rows or 4 distinct op(B) columns.
+    // rows (mr = lane % 8, rows mr and mr + 8) and 8 of the 16 columns, so one
+    // operand load of a warp touches 8 distinct op(A) rows or 4 distinct op(B)
+    // columns.
     const int warp = tid >> 5, wl = tid & 31;
     const int g = warp >> 1;
-    const int ra = 2 * (wl & 7), cb = 2 * (((warp & 1) << 2) | (wl >> 3));
+    const int mr = wl & 7, cb = 2 * (((warp & 1) << 2) | (wl >> 3));
     int out[4];  // o of output (a, b) at out[a + 2b]
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
 #pragma unroll
         for (int a = 0; a < 2; ++a) {
-            out[a + 2 * b] = (ra + a) + kTile * (cb + b);
+            out[a + 2 * b] = (mr + 8 * a) + kTile * (cb + b);
         }
     }
 
-    // Staging role: the 64 threads of group sg copy its 32 rows (16 of op(A),
-    // then 16 of op(B)) of one chunk.  Element e = st + 64u is row e / ch at
-    // offset e % ch, so the copies of one warp run along one or two rows; the
-    // offsets are fixed for the launch, a step only moves the source by the
-    // chunk's K start.  Rows past the matrix read as zero.
-    const int sg = tid >> 6, st = tid & 63;
-    const float2* src[kStageIters];
-    int dst[kStageIters], qs[kStageIters];
-#pragma unroll
-    for (int u = 0; u < kStageIters; ++u) {
-        const int e = st + 64 * u;
-        const int ro = e / ch, q = e - ro * ch;
-        const int op = ro >> 4, r = ro & 15;
-        const int row = (op ? j0 : i0) + r;
-        const bool staged = e < 2 * kTile * ch;
-        src[u] = staged && row < n ? (op ? rows_b : rows_a) + (size_t)row * n + q : nullptr;
-        dst[u] = staged ? (sg * 2 + op) * (int)kGroupSlice + r * kRow + q : 0;
-        qs[u] = staged ? q : kChunk;  // kChunk fails every q < len test
+    // Staging: thread 0 arms buffer T % 2 with the step's bytes and issues, per
+    // group, the op(A) box (rows i0 .., x) and the op(B) box (rows j0 .., x),
+    // x = the chunk's K start rounded down to even.  Boxes past the matrix or
+    // past K read as zero.  T counts steps over both passes: buffer T % 2,
+    // phase parity (T / 2) % 2.
+    const uint32_t step_bytes = (uint32_t)(kGroups * 2 * kTile * w * sizeof(float2));
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+        tma_prefetch_desc(&tm_a);
+        tma_prefetch_desc(&tm_b);
     }
-    auto issue = [&](int t, int b) {
-        const int l = kGroupLanes * sg + t / kChunks, c = t % kChunks;
-        const int len = chunk_len(l, c);
-        const int k0 = l * span + c * ch;
-        float2* base = stage + (size_t)b * kBufElems;
-#pragma unroll
-        for (int u = 0; u < kStageIters; ++u) {
-            if (qs[u] < len) {
-                cp_async8(base + dst[u], src[u] != nullptr ? (const void*)(src[u] + k0) : (const void*)rows_a,
-                          src[u] != nullptr ? 8 : 0);
+    __syncthreads();
+    auto issue = [&](int T) {
+        if (tid == 0) {
+            const int t = T % kSteps, b = T & 1;
+            mbar_arrive_expect_tx(&full[b], step_bytes);
+#pragma unroll 1
+            for (int gg = 0; gg < kGroups; ++gg) {
+                const int l = kGroupLanes * gg + t / kChunks;
+                const int x = (l * span + (t % kChunks) * ch) & ~1;
+                float2* dst = stage + (size_t)b * kBufElems + (size_t)(gg * 2) * kBoxElems;
+                tma_load_2d(dst, &tm_a, &full[b], x, i0);
+                tma_load_2d(dst + kBoxElems, &tm_b, &full[b], x, j0);
             }
         }
-        cp_async_commit();
     };
-    auto slab = [&](int t, int which) {
-        return stage + (size_t)(t & 1) * kBufElems + (size_t)(g * 2 + which) * kGroupSlice;
+    // Bounded waits: a thread whose wait gave up (status flagged) stops
+    // waiting and runs on, so the block ends; the call's result is then
+    // reported as failed.
+    bool ok = true;
+    auto wait_step = [&](int T) {
+        if (ok) {
+            ok = mbar_wait(&full[T & 1], (uint32_t)((T >> 1) & 1), status);
+        }
+    };
+    // Operand pointers of this thread's rows and columns in buffer b for the
+    // step's lane l and chunk c (the copy started at an even K offset).
+    auto chunk_ptrs = [&](int T, int l, int c, const float2** xp) {
+        const int off = (l * span + c * ch) & 1;
+        const float2* a = stage + (size_t)(T & 1) * kBufElems + (size_t)(g * 2) * kBoxElems + off;
+        const float2* bb = a + kBoxElems;
+        xp[0] = a + mr * w;
+        xp[1] = a + (mr + 8) * w;
+        xp[2] = bb + cb * w;
+        xp[3] = bb + (cb + 1) * w;
     };
 
-    // pass 1: lane sums (the next step's chunks are copied while this one is summed)
+    // pass 1: lane sums (the next step's boxes are copied while this one is summed)
     float2 acc[4];  // (re, im) of output (a, b) at acc[a + 2b]
-    issue(0, 0);
+    issue(0);
     for (int t = 0; t < kSteps; ++t) {
-        cp_async_wait_all();
-        __syncthreads();  // this step staged by every thread; the previous step's buffer is free
+        __syncthreads();  // every thread is done with the previous step's buffer
         if (t + 1 < kSteps) {
-            issue(t + 1, (t + 1) & 1);
+            issue(t + 1);
         }
+        wait_step(t);
         const int l = kGroupLanes * g + t / kChunks, c = t % kChunks;
         if (c == 0) {
 #pragma unroll
@@ -284,7 +306,9 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
                 acc[u] = make_float2(0.0f, 0.0f);
             }
         }
-        replay_chunk(slab(t, 0) + ra * kRow, slab(t, 1) + cb * kRow, chunk_len(l, c), acc);
+        const float2* xp[4];
+        chunk_ptrs(t, l, c, xp);
+        replay_chunk(xp[0], xp[1], xp[2], xp[3], chunk_len(l, c), acc);
         if (c == kChunks - 1) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -347,13 +371,14 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
         init_r[u] = 0.0f;
         init_i[u] = 0.0f;
     }
-    issue(0, 0);
+    issue(kSteps);
     for (int t = 0; t < kSteps; ++t) {
-        cp_async_wait_all();
+        const int T = kSteps + t;
         __syncthreads();
         if (t + 1 < kSteps) {
-            issue(t + 1, (t + 1) & 1);
+            issue(T + 1);
         }
+        wait_step(T);
         const int l = kGroupLanes * g + t / kChunks, c = t % kChunks;
         if (c == 0) {
 #pragma unroll
@@ -365,7 +390,9 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
                 acc[u] = make_float2(__fadd_rn(init_r[u], 0.0f), __fadd_rn(init_i[u], 0.0f));
             }
         }
-        replay_chunk(slab(t, 0) + ra * kRow, slab(t, 1) + cb * kRow, chunk_len(l, c), acc);
+        const float2* xp[4];
+        chunk_ptrs(T, l, c, xp);
+        replay_chunk(xp[0], xp[1], xp[2], xp[3], chunk_len(l, c), acc);
         if (c == kChunks - 1) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -400,6 +427,12 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(int n, int span, con
             }
         }
     }
+    // A block in which a wait gave up drains its last copies (bounded) before
+    // it exits, so no copy lands in shared memory after the block is gone.
+    if (__syncthreads_or(!ok) && tid == 0) {
+        mbar_wait(&full[0], (uint32_t)(((2 * kSteps - 2) >> 1) & 1), status);
+        mbar_wait(&full[1], (uint32_t)(((2 * kSteps - 1) >> 1) & 1), status);
+    }
 }
 
 // ---- 4b. FP64 recompute (tensor-core forms) -----------------------------------------
@@ -415,7 +448,7 @@ constexpr int kT64 = 64;
 constexpr size_t kFp64Slab = (size_t)16 * kT64;  // double2 per operand per buffer
 constexpr size_t kFp64Smem = 2 * 2 * kFp64Slab * sizeof(double2);
 
-__global__ void __launch_bounds__(256, 2) recompute_fp64_tiled(int n, const float2* __restrict__ rows_a,
+__global__ void __launch_bounds__(256, 2) recompute_fp64_tiled(int n, int pitch, const float2* __restrict__ rows_a,
                                                             const float2* __restrict__ rows_b,
                                                             const uint32_t* __restrict__ flag_bits,
                                                             const uint32_t* __restrict__ tile_flags,
@@ -455,8 +488,8 @@ __global__ void __launch_bounds__(256, 2) recompute_fp64_tiled(int n, const floa
             const int e = tid + 256 * u;
             const int r = e >> 4, q = e & 15;
             const int k = k0 + q;
-            vx[u] = (k < n && i0 + r < n) ? rows_a[(size_t)(i0 + r) * n + k] : make_float2(0.0f, 0.0f);
-            vy[u] = (k < n && j0 + r < n) ? rows_b[(size_t)(j0 + r) * n + k] : make_float2(0.0f, 0.0f);
+            vx[u] = (k < n && i0 + r < n) ? rows_a[(size_t)(i0 + r) * pitch + k] : make_float2(0.0f, 0.0f);
+            vy[u] = (k < n && j0 + r < n) ? rows_b[(size_t)(j0 + r) * pitch + k] : make_float2(0.0f, 0.0f);
         }
     };
     load(0);
@@ -546,18 +579,24 @@ static size_t tile_words(int n)
     return t * t;
 }
 
+// Row stride of the packed op(A) rows and op(B) columns: n rounded up to even,
+// so that every row starts on a 16-byte boundary (the replay stages them with
+// 2-D tensor copies, whose row stride must be a multiple of 16 bytes).
+static int row_pitch(int n) { return n + (n & 1); }
+
 static RoundLayout round_layout(const Plan& plan, void* ws, int n)
 {
     uint8_t* b = static_cast<uint8_t*>(ws) + plan.round_off;
     const size_t nn = (size_t)n * n;
+    const size_t rows = (size_t)n * row_pitch(n);
     RoundLayout L;
     size_t off = 0;
     L.path = reinterpret_cast<float*>(b + off);
     off = align_up(off + nn * 4, kRegionAlign);
     L.rows_a = reinterpret_cast<float2*>(b + off);
-    off = align_up(off + nn * 8, kRegionAlign);
+    off = align_up(off + rows * 8, kRegionAlign);
     L.rows_b = reinterpret_cast<float2*>(b + off);
-    off = align_up(off + nn * 8, kRegionAlign);
+    off = align_up(off + rows * 8, kRegionAlign);
     L.energy = reinterpret_cast<float*>(b + off);
     off = align_up(off + (size_t)2 * n * 4, kRegionAlign);
     L.flag_bits = reinterpret_cast<uint32_t*>(b + off);
@@ -570,10 +609,11 @@ static RoundLayout round_layout(const Plan& plan, void* ws, int n)
 size_t rounding_bytes(int n)
 {
     const size_t nn = (size_t)n * n;
+    const size_t rows = (size_t)n * row_pitch(n);
     size_t off = 0;
     off = align_up(off + nn * 4, kRegionAlign);
-    off = align_up(off + nn * 8, kRegionAlign);
-    off = align_up(off + nn * 8, kRegionAlign);
+    off = align_up(off + rows * 8, kRegionAlign);
+    off = align_up(off + rows * 8, kRegionAlign);
     off = align_up(off + (size_t)2 * n * 4, kRegionAlign);
     off = align_up(off + (flag_words(n) + tile_words(n) + 1) * 4, kRegionAlign);
     return off;
@@ -586,17 +626,31 @@ cudaError_t launch_gemm_with_path(cudaStream_t s, const Problem& p, const Plan& 
                                        : launch_gemm_tc_path(s, p, plan, ws, L.path, status);
 }
 
-cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int*, int* launched,
-                            const std::function<void(int)>& mark)
+// The replay's staging copies: op(A) rows or op(B) columns as an n x n array of
+// 8-byte complex elements with the even row pitch; a box is w K terms of 16
+// rows.
+static bool replay_tensor_map(CUtensorMap* map, const float2* rows, int n, int w)
+{
+    const uint64_t dims[2] = {(uint64_t)n, (uint64_t)n};
+    const uint64_t strides[1] = {(uint64_t)row_pitch(n) * sizeof(float2)};
+    const uint32_t box[2] = {(uint32_t)w, (uint32_t)kTile};
+    return encode_tensor_map(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, dims, strides, box,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, rows);
+}
+
+cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status,
+                            int* launched, const std::function<void(int)>& mark)
 {
     const int n = p.n;
+    const int pitch = row_pitch(n);
     const RoundLayout L = round_layout(plan, ws, n);
     const int span = ((n + kLanes - 1) / kLanes) | 1;
     int count = 0;
-    cudaError_t err = launch_pack_rows(s, p, L.rows_a, L.rows_b);
+    cudaError_t err = launch_pack_rows(s, p, L.rows_a, L.rows_b, pitch);
     mark(++count);
     if (err == cudaSuccess) {
-        energy_kernel<<<2 * n, kLanes, (size_t)n * sizeof(float2), s>>>(L.rows_a, L.rows_b, n, span, L.energy);
+        energy_kernel<<<2 * n, kLanes, (size_t)n * sizeof(float2), s>>>(L.rows_a, L.rows_b, n, pitch, span,
+                                                                        L.energy);
         err = cudaGetLastError();
         mark(++count);
     }
@@ -611,22 +665,28 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
     }
     if (err == cudaSuccess) {
         if (plan.form == CG3M_FORM_FP32) {
-            if (span > kChunks * kChunk) {
-                return cudaErrorInvalidValue;  // lanes longer than the staged chunks (n > 4096)
+            const int ch = (span + kChunks - 1) / kChunks;
+            const int w = box_width(ch);
+            if (ch > kChunk || w > kBoxMax) {
+                return cudaErrorInvalidValue;  // lanes longer than the staged boxes (n > 4096)
+            }
+            CUtensorMap tm_a, tm_b;
+            if (!replay_tensor_map(&tm_a, L.rows_a, n, w) || !replay_tensor_map(&tm_b, L.rows_b, n, w)) {
+                return cudaErrorInvalidValue;
             }
             const int tiles = (n + kTile - 1) / kTile;
-            const size_t smem = kRecomputeSmem;
-            err = cudaFuncSetAttribute(recompute_fp32_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            err = cudaFuncSetAttribute(recompute_fp32_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kRecomputeSmem);
             if (err == cudaSuccess) {
-                recompute_fp32_tiled<<<tiles * tiles, 512, smem, s>>>(n, span, L.rows_a, L.rows_b, L.flag_bits,
-                                                                     L.tile_flags, static_cast<float2*>(p.C));
+                recompute_fp32_tiled<<<tiles * tiles, 512, kRecomputeSmem, s>>>(
+                    tm_a, tm_b, n, span, ch, w, L.flag_bits, L.tile_flags, static_cast<float2*>(p.C), status);
             }
         } else {
             const int tiles = (n + kT64 - 1) / kT64;
             err = cudaFuncSetAttribute(recompute_fp64_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kFp64Smem);
             if (err == cudaSuccess) {
-                recompute_fp64_tiled<<<tiles * tiles, 256, kFp64Smem, s>>>(n, L.rows_a, L.rows_b, L.flag_bits,
+                recompute_fp64_tiled<<<tiles * tiles, 256, kFp64Smem, s>>>(n, pitch, L.rows_a, L.rows_b, L.flag_bits,
                                                                             L.tile_flags, static_cast<float2*>(p.C));
             }
         }

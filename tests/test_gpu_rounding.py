@@ -34,11 +34,12 @@ def _square(oracle, fill, seed, scale=1.0, n=N):
     return a, b
 
 
-@pytest.mark.parametrize("ops,N", [(("N", "N"), 2048), (("C", "T"), 2048), (("N", "N"), 3000), (("T", "C"), 4096)])
+@pytest.mark.parametrize("ops,N", [(("N", "N"), 2048), (("C", "T"), 2048), (("N", "N"), 3000), (("T", "C"), 4096),
+                                   (("C", "N"), 2049)])
 def test_fp32_rounding_pass_bit_exact_blocks(cg3m, oracle, cuda, h, ops, N):
     """Orders 2048, 3000 and 4096 give lane widths of 33, 47 and 65 K terms
     (ceil(n/64) | 1), replayed in chunks of 9, 12 and 17, with short or empty
-    last lanes."""
+    last lanes; the odd order 2049 stores the packed rows with a padded pitch."""
     import torch
 
     ta, tb = ops

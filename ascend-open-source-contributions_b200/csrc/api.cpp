@@ -470,12 +470,14 @@ cg3mStatus_t cg3mCgemm(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t t
     if (unit) {
         // Three products with the repair: the FP32 planner's engine.  The packed
         // engine's products equal the on-chip family's bit for bit for the same
-        // K split, and with alpha = 1, beta = 0 C holds them unchanged, so the
-        // repair can run as a pass over the finished C.
+        // K split, and its epilogues (GEMM, cluster merge or merge kernel)
+        // recompute a non-finite output with the four-product sum before
+        // storing it, as the on-chip kernels do.
         Plan plan;
         if (!make_plan(p, cgemm_unit_options(), h->sm_count, &plan)) {
             return CG3M_STATUS_INVALID_VALUE;
         }
+        plan.repair = true;
         if (plan.engine == 2) {
             return to_status(launch_single(h->stream, p, 0, 1, plan.onchip_tile, plan.parts));
         }
@@ -484,11 +486,7 @@ cg3mStatus_t cg3mCgemm(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperation_t t
         if (wst != CG3M_STATUS_SUCCESS) {
             return wst;
         }
-        cudaError_t err = enqueue(h->stream, p, plan, ws, h->status, nullptr);
-        if (err == cudaSuccess) {
-            err = launch_repair(h->stream, p);
-        }
-        return to_status(err);
+        return to_status(enqueue(h->stream, p, plan, ws, h->status, nullptr));
     }
     // Four products: the one-launch kernel of the on-chip family (K
     // partitions merged in a cluster; no workspace).
@@ -744,7 +742,7 @@ cg3mStatus_t cg3mPlanOnchip(int m, int n, int k, int mode, int batch, int sm_cou
     if (info == nullptr) {
         return CG3M_STATUS_INVALID_VALUE;
     }
-    if (mode == 2) {  // cg3mCgemm with alpha = 1, beta = 0: the FP32 planner's engine, then the repair pass
+    if (mode == 2) {  // cg3mCgemm with alpha = 1, beta = 0: the FP32 planner's engine, repair in its epilogue
         if (batch != 1 || m <= 0 || n <= 0 || k <= 0) {
             return CG3M_STATUS_INVALID_VALUE;
         }
@@ -759,7 +757,7 @@ cg3mStatus_t cg3mPlanOnchip(int m, int n, int k, int mode, int batch, int sm_cou
         info->tile_n = plan.tile_n;
         info->k_partitions = plan.parts;
         info->k_span = plan.span;
-        info->kernels = plan.engine == 2 ? 1 : 3 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0);
+        info->kernels = plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0);
         info->workspace_bytes = plan.total;
         return CG3M_STATUS_SUCCESS;
     }

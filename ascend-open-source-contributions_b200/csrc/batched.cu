@@ -235,28 +235,10 @@ __device__ __forceinline__ float2 beta_scaled(const EpiParams& e, const float2* 
                        __fadd_rn(__fmul_rn(e.br, c.y), __fmul_rn(e.bi, c.x)));
 }
 
-// Non-finite repair (RepairNonFiniteOutput, cgemm_compute_kernel.cpp:672-706):
-// the product op(A)(row, :) . op(B)(:, col) recomputed over the whole K in
-// increasing order with each FP32 product materialised (rr, ii, ri, ir) and
-// re += rr - ii, im += ri + ir, one rounding per operation.  A 3M product that
-// overflowed before cancelling gets the four-product value scalar BLAS gives.
+// Non-finite repair of one output (repair_four_product, epilogue.cuh).
 __device__ float2 repair_product(const BProblem& p, int row, int col)
 {
-    const bool na = p.ta == CG3M_OP_N || p.ta == CG3M_OP_R;
-    const bool nb = p.tb == CG3M_OP_N || p.tb == CG3M_OP_R;
-    const float ca = (p.ta == CG3M_OP_C || p.ta == CG3M_OP_R) ? -1.0f : 1.0f;
-    const float cb = (p.tb == CG3M_OP_C || p.tb == CG3M_OP_R) ? -1.0f : 1.0f;
-    float re = 0.0f, im = 0.0f;
-    for (int k = 0; k < p.k; ++k) {
-        const float2 a = p.A[na ? (size_t)row + (size_t)k * p.lda : (size_t)k + (size_t)row * p.lda];
-        const float2 b = p.B[nb ? (size_t)k + (size_t)col * p.ldb : (size_t)col + (size_t)k * p.ldb];
-        const float av = a.y * ca, bv = b.y * cb;
-        const float rr = __fmul_rn(a.x, b.x), ii = __fmul_rn(av, bv);
-        const float ri = __fmul_rn(a.x, bv), ir = __fmul_rn(av, b.x);
-        re = __fadd_rn(re, __fsub_rn(rr, ii));
-        im = __fadd_rn(im, __fadd_rn(ri, ir));
-    }
-    return make_float2(re, im);
+    return repair_four_product(p.A, p.lda, p.ta, p.B, p.ldb, p.tb, p.k, row, col);
 }
 
 // Partition product (before alpha/beta) of the accumulators of one output.
@@ -765,23 +747,6 @@ cudaError_t launch_single_tile(cudaStream_t s, const BProblem& bp, int tile)
     }
 }
 
-// Non-finite repair of a finished three-product result with alpha = 1 and
-// beta = 0, where C holds the merged products unchanged: every output with a
-// non-finite component is recomputed with the explicit four-product FP32 sum,
-// as the kernels above do before their identity epilogue.
-__global__ void repair_kernel(const BProblem p)
-{
-    const size_t total = (size_t)p.m * p.n;
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (size_t)gridDim.x * blockDim.x) {
-        const int col = (int)(idx / p.m), row = (int)(idx - (size_t)col * p.m);
-        float2* cp = p.C + (size_t)col * p.ldc + row;
-        if (!finite2(*cp)) {
-            *cp = repair_product(p, row, col);
-        }
-    }
-}
-
 }  // namespace
 }  // namespace cg3m
 
@@ -1198,26 +1163,6 @@ cudaError_t launch_single(cudaStream_t s, const Problem& p, int mode, int repair
     const cudaError_t e =
         mode == kMode3M ? launch_single_tile<kMode3M>(s, bp, tile) : launch_single_tile<kMode4M>(s, bp, tile);
     return e != cudaSuccess ? e : cudaGetLastError();
-}
-
-cudaError_t launch_repair(cudaStream_t s, const Problem& p)
-{
-    BProblem bp{};
-    bp.ta = p.transa;
-    bp.tb = p.transb;
-    bp.m = p.m;
-    bp.n = p.n;
-    bp.k = p.k;
-    bp.A = static_cast<const float2*>(p.A);
-    bp.B = static_cast<const float2*>(p.B);
-    bp.C = static_cast<float2*>(p.C);
-    bp.lda = p.lda;
-    bp.ldb = p.ldb;
-    bp.ldc = p.ldc;
-    const long long total = (long long)p.m * p.n;
-    const int grid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 8));
-    repair_kernel<<<grid, 256, 0, s>>>(bp);
-    return cudaGetLastError();
 }
 
 cudaError_t launch_strided(cudaStream_t s, const Problem& p, int mode, int repair, long long sA, long long sB,

@@ -51,6 +51,7 @@ struct Plan {
     int engine = 1;          // 1 packed planes (pack + GEMM [+ merge]), 2 one cluster-merged launch
     int onchip_tile = 0;     // engine 2: tile index of the on-chip family (0 128x64 .. 5 32x32)
     bool cluster_merge = false;  // FP32 packed engine: the K partitions (2..8) merge inside their cluster
+    bool repair = false;         // cg3mCgemm, alpha = 1, beta = 0: non-finite outputs repaired in the epilogue
     double est_us = 0.0;         // FP32 plans: the planner's time estimate (microseconds)
     // workspace layout (byte offsets from the workspace base)
     size_t planes_a_off = 0, planes_b_off = 0, partial_off = 0, round_off = 0, total = 0;
@@ -119,9 +120,6 @@ bool make_strided_plan(const Problem& p, int mode, int batch, int sm_count, Stri
 // (parts <= 8, and (parts - 1) * span < k).  tile: 0 128x64, 1 64x64,
 // 2 128x32, 3 32x128, 4 64x32, 5 32x32.  No workspace.
 cudaError_t launch_single(cudaStream_t s, const Problem& p, int mode, int repair, int tile, int parts);
-// Recomputes, with the explicit four-product FP32 sum, every output of C that
-// a three-product call with alpha = 1, beta = 0 left non-finite.
-cudaError_t launch_repair(cudaStream_t s, const Problem& p);
 // The one-launch plan for an m x n x k problem in `mode`: tile and K
 // partitions (each forced when >= 0), chosen to minimise the estimated time,
 // which is returned in microseconds.

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(Fp32Cfg<BM, BN>::THREADS, 1)
                     const float im = __fsub_rn(__fsub_rn(p2[i][j], p0[i][j]), p1[i][j]);
                     if (p.parts == 1) {
                         float2* cp = p.C + (size_t)col * p.ldc + row;
-                        *cp = epilogue_value(re, im, p.epi, cp);
+                        *cp = epilogue_at(re, im, p.epi, cp, row, col);
                     } else {
                         const size_t o = (size_t)col * p.ppitch + row;
                         p.partial[(size_t)(2 * part) * p.pplane + o] = re;
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(ws::THREADS, 1)
             const float im = __fsub_rn(__fsub_rn(q2, q0), q1);
             if (p.parts == 1) {
                 float2* cp = p.C + (size_t)col * p.ldc + row;
-                *cp = epilogue_value(re, im, p.epi, cp);
+                *cp = epilogue_at(re, im, p.epi, cp, row, col);
             } else {
                 const size_t o = (size_t)col * p.ppitch + row;
                 p.partial[(size_t)(2 * part) * p.pplane + o] = re;
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(ws::THREADS, 1)
                 im = __fadd_rn(im, ld_dsmem_f32(mapa_shared(im_local + 4u * e, q)));
             }
             float2* cp = p.C + (size_t)col * p.ldc + row;
-            *cp = epilogue_value(re, im, p.epi, cp);
+            *cp = epilogue_at(re, im, p.epi, cp, row, col);
         }
     }
     cluster_sync();  // no block leaves while others may still read its shared memory
@@ -642,7 +642,7 @@ __global__ void merge_kernel(int m, int n, int parts, const float* __restrict__ 
             im = __fadd_rn(im, partial[(size_t)(2 * q + 1) * pplane + o]);
         }
         float2* cp = C + (size_t)col * ldc + row;
-        *cp = epilogue_value(re, im, e, cp);
+        *cp = epilogue_at(re, im, e, cp, row, col);
     }
 }
 
@@ -669,6 +669,24 @@ int elementwise_blocks(size_t total)
 {
     const size_t blocks = (total + 255) / 256;
     return (int)(blocks < 148 * 16 ? (blocks == 0 ? 1 : blocks) : 148 * 16);
+}
+
+// Epilogue parameters of an FP32 call; a cg3mCgemm call with alpha = 1,
+// beta = 0 (plan.repair) also carries what the non-finite repair reads.
+EpiParams fp32_epilogue(const Problem& pr, const Plan& plan)
+{
+    EpiParams e{pr.ar, pr.ai, pr.br, pr.bi, plan.unit ? 1 : 0, plan.beta_zero ? 1 : 0};
+    if (plan.repair) {
+        e.repair = 1;
+        e.ta = pr.transa;
+        e.tb = pr.transb;
+        e.k = pr.k;
+        e.lda = pr.lda;
+        e.ldb = pr.ldb;
+        e.A = static_cast<const float2*>(pr.A);
+        e.B = static_cast<const float2*>(pr.B);
+    }
+    return e;
 }
 
 template <int BM, int BN>
@@ -703,7 +721,7 @@ cudaError_t launch_fp32_tile(cudaStream_t stream, const Problem& pr, const Plan&
     p.parts = plan.parts;
     p.tiles_m = ceil_div(pr.m, BM);
     p.tiles_n = ceil_div(pr.n, BN);
-    p.epi = EpiParams{pr.ar, pr.ai, pr.br, pr.bi, plan.unit ? 1 : 0, plan.beta_zero ? 1 : 0};
+    p.epi = fp32_epilogue(pr, plan);
     p.C = static_cast<float2*>(pr.C);
     p.ldc = pr.ldc;
     p.partial = reinterpret_cast<float*>(w + plan.partial_off);
@@ -736,14 +754,16 @@ cudaError_t launch_fp32_tile(cudaStream_t stream, const Problem& pr, const Plan&
         cfg.numAttrs = 1;
         err = cudaLaunchKernelEx(&cfg, gemm3m_fp32_ws_kernel, ta, tb, p);
         return err != cudaSuccess ? err : cudaGetLastError();
+    } else {
+        auto kernel = gemm3m_fp32_kernel<BM, BN>;
+        cudaError_t err =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+        if (err != cudaSuccess) {
+            return err;
+        }
+        kernel<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(ta, tb, p);
+        return cudaGetLastError();
     }
-    auto kernel = gemm3m_fp32_kernel<BM, BN>;
-    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-    if (err != cudaSuccess) {
-        return err;
-    }
-    kernel<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(ta, tb, p);
-    return cudaGetLastError();
 }
 
 }  // namespace
@@ -800,7 +820,7 @@ cudaError_t launch_gemm_fp32_path(cudaStream_t stream, const Problem& pr, const 
 cudaError_t launch_merge(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws)
 {
     const float* partial = reinterpret_cast<const float*>(static_cast<uint8_t*>(ws) + plan.partial_off);
-    const EpiParams e{pr.ar, pr.ai, pr.br, pr.bi, plan.unit ? 1 : 0, plan.beta_zero ? 1 : 0};
+    const EpiParams e = fp32_epilogue(pr, plan);
     merge_kernel<<<elementwise_blocks((size_t)pr.m * pr.n), 256, 0, stream>>>(
         pr.m, pr.n, plan.parts, partial, plan.partial_pitch, plan.partial_plane_elems, e, static_cast<float2*>(pr.C),
         pr.ldc);

@@ -281,7 +281,8 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
  * one per launch) reports the one-launch kernel: path 4, no workspace.
  * mode 2 (batch 1 only) = cg3mCgemm with alpha = 1, beta = 0: three products
  * with the non-finite repair on the FP32 planner's engine (the one-launch
- * kernel, or the packed engine followed by a repair pass over C). */
+ * kernel, or the packed engine, whose epilogue repairs each non-finite
+ * output before storing it). */
 cg3mStatus_t cg3mPlanOnchip(int m, int n, int k, int mode, int batch, int sm_count, cg3mCallInfo* info);
 
 /* ---- diagnostics (not a compute path of cgemm3m) ------------------------- */

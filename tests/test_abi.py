@@ -302,7 +302,7 @@ def test_onchip_plan(cg3m):
     assert four["tile_m"] * four["tile_n"] <= 4096  # no 128x64 tile with four accumulators
     # cgemm with alpha = 1, beta = 0: the FP32 planner's engine plus the repair pass
     big_unit = cg3m.plan_onchip(2048, 2048, 2048, mode=2, batch=1)
-    assert big_unit["path"] in (2, 3) and big_unit["kernels"] >= 3  # pack, GEMM, repair
+    assert big_unit["path"] in (2, 3) and big_unit["kernels"] >= 2  # pack, GEMM (repair in its epilogue)
     small_unit = cg3m.plan_onchip(64, 64, 64, mode=2, batch=1)
     assert small_unit["path"] == 4 and small_unit["kernels"] == 1
     with pytest.raises(cg3m.Cg3mError):

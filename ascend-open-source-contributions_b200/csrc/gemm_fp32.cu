@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(Fp32Cfg<BM, BN>::THREADS, 1)
     using Cfg = Fp32Cfg<BM, BN>;
     constexpr int BK = Cfg::BK, STAGES = Cfg::STAGES;
     extern __shared__ uint8_t smem_raw[];
-    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* base = align_shared<1024>(smem_raw);
     float* sA = reinterpret_cast<float*>(base);
     float* sB = sA + STAGES * Cfg::A_STAGE;
     uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * Cfg::B_STAGE);
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(ws::THREADS, 1)
 {
     using namespace ws;
     extern __shared__ uint8_t smem_raw[];
-    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* base = align_shared<1024>(smem_raw);
     float* sA = reinterpret_cast<float*>(base);
     float* sB = sA + STAGES * A_STAGE;
     uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * B_STAGE);
@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(288, 1)
     constexpr int BM = 64, BN = 64, BK = 16, STAGES = 4, CONSUMER_WARPS = 8;
     constexpr int A_STAGE = 3 * BK * BM, B_STAGE = 3 * BK * BN;
     extern __shared__ uint8_t smem_raw[];
-    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* base = align_shared<1024>(smem_raw);
     float* sA = reinterpret_cast<float*>(base);
     float* sB = sA + STAGES * A_STAGE;
     uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * B_STAGE);

@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr int COLS = G::COLS;
 
     extern __shared__ uint8_t smem_raw[];
-    uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* ring = align_shared<1024>(smem_raw);
     uint64_t* full = reinterpret_cast<uint64_t*>(ring + STAGES * STAGE_BYTES);
     uint64_t* empty = full + STAGES;
     uint64_t* acc_full = empty + STAGES;  // [3] MMA -> epilogue: product c of the segment is in TMEM
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                   "merge partials must fit the ring below the barriers");
 
     extern __shared__ uint8_t smem_raw[];
-    uint8_t* ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* ring = align_shared<1024>(smem_raw);
     uint64_t* full = reinterpret_cast<uint64_t*>(ring + STAGES * STAGE_BYTES);
     uint64_t* empty = full + STAGES;
     uint64_t* acc_full = empty + STAGES;  // [3]

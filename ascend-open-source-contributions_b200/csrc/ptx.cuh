@@ -21,6 +21,16 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p)
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// The first ALIGN-byte boundary of shared memory at or above p (an extern
+// __shared__ array), reached by pointer arithmetic on that array so that the
+// result and everything derived from it stay shared-memory pointers: loads
+// through them are shared loads with 32-bit addresses, not generic ones.
+template <uint32_t ALIGN>
+__device__ __forceinline__ uint8_t* align_shared(uint8_t* p)
+{
+    return p + ((ALIGN - (smem_u32(p) & (ALIGN - 1u))) & (ALIGN - 1u));
+}
+
 __device__ __forceinline__ uint64_t globaltimer()
 {
     uint64_t t;

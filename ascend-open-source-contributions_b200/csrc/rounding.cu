@@ -204,10 +204,7 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constan
                                                             float2* __restrict__ C, int* status)
 {
     extern __shared__ uint8_t replay_smem[];
-    // 128-byte aligned base, reached by pointer arithmetic on the shared array
-    // so that every operand pointer below stays a shared-memory pointer (plain
-    // shared loads with 32-bit addresses, not generic ones).
-    uint8_t* base = replay_smem + ((128u - (smem_u32(replay_smem) & 127u)) & 127u);
+    uint8_t* base = align_shared<128>(replay_smem);
     // Lane sums, real then imaginary: S[l][o] for output o = ti + 16 tj of the tile.
     float* sr = reinterpret_cast<float*>(base);
     float* si = sr + kLanes * 256;

@@ -141,7 +141,8 @@ __device__ __forceinline__ bool flagged(const uint32_t* bits, size_t idx)
 constexpr int kGroups = 8;                                   // lane groups, two warps each
 constexpr int kGroupLanes = kLanes / kGroups;                // 8 lanes per group
 constexpr int kChunks = 4;                                   // chunks per lane
-constexpr int kChunk = (kMaxSpan + kChunks - 1) / kChunks;   // 17: the longest chunk
+constexpr int kChunk = (kMaxSpan + kChunks - 1) / kChunks;   // 17: the longest chunk (n = 4096)
+constexpr int kChunkMin = (((2048 + kLanes - 1) / kLanes | 1) + kChunks - 1) / kChunks;  // 9: n = 2048
 constexpr int kSteps = kGroupLanes * kChunks;                // 32 staging steps per pass
 constexpr int kBoxMax = 18;                                  // widest staged row (float2)
 constexpr size_t kLaneSumBytes = (size_t)2 * kLanes * 256 * sizeof(float);
@@ -155,7 +156,7 @@ static_assert(kBoxElems * sizeof(float2) % 128 == 0, "staged boxes start on 128-
 // the even K offset at or below the chunk's start), even (16-byte rows) and
 // 2 mod 4, so the 8 rows (or 4 columns) a warp reads at one K offset fall in
 // distinct shared-memory bank pairs.
-static int box_width(int ch)
+constexpr int box_width(int ch)
 {
     int w = ch + 1;
     while (w % 4 != 2) {
@@ -164,45 +165,65 @@ static int box_width(int ch)
     return w;
 }
 
-// Accumulate terms [0, len) of one staged chunk into the 2 x 2 outputs: x0, x1
-// are the two op(A) rows, y0, y1 the two op(B) columns, all at the chunk's
-// first term.  Output (a, b) is acc[a + 2b].  Each term is the fused identity
-// of ThreeProductTerms (:192-208): p = (xr + xi) yr, re = p - xi (yr + yi),
-// im = p + xr (yi - yr).
-__device__ __forceinline__ void replay_chunk(const float2* X0, const float2* X1, const float2* Y0,
-                                             const float2* Y1, int len, float2* acc)
+// One term at K offset q for the 2 x 2 outputs: X0, X1 are the two op(A) rows,
+// Y0, Y1 the two op(B) columns, all at the chunk's first term.  Output (a, b)
+// is acc[a + 2b].  The term is the fused identity of ThreeProductTerms
+// (:192-208): p = (xr + xi) yr, re = p - xi (yr + yi), im = p + xr (yi - yr).
+__device__ __forceinline__ void replay_term(const float2* X0, const float2* X1, const float2* Y0, const float2* Y1,
+                                            int q, float2* acc)
 {
-#pragma unroll 4
-    for (int q = 0; q < len; ++q) {
-        const float2 x0 = X0[q], x1 = X1[q];
-        const float2 y0 = Y0[q], y1 = Y1[q];
-        const float sx[2] = {__fadd_rn(x0.x, x0.y), __fadd_rn(x1.x, x1.y)};
-        const float dy[2] = {__fsub_rn(y0.y, y0.x), __fsub_rn(y1.y, y1.x)};
-        const float ey[2] = {__fadd_rn(y0.x, y0.y), __fadd_rn(y1.x, y1.y)};
-        const float xr[2] = {x0.x, x1.x}, xi[2] = {x0.y, x1.y}, yr[2] = {y0.x, y1.x};
+    const float2 x0 = X0[q], x1 = X1[q];
+    const float2 y0 = Y0[q], y1 = Y1[q];
+    const float sx[2] = {__fadd_rn(x0.x, x0.y), __fadd_rn(x1.x, x1.y)};
+    const float dy[2] = {__fsub_rn(y0.y, y0.x), __fsub_rn(y1.y, y1.x)};
+    const float ey[2] = {__fadd_rn(y0.x, y0.y), __fadd_rn(y1.x, y1.y)};
+    const float xr[2] = {x0.x, x1.x}, xi[2] = {x0.y, x1.y}, yr[2] = {y0.x, y1.x};
 #pragma unroll
-        for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < 2; ++b) {
 #pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                const float p = __fmul_rn(sx[a], yr[b]);
-                const float qq = __fmul_rn(xr[a], dy[b]);
-                const float rr = __fmul_rn(xi[a], ey[b]);
-                // (re, im) of the term, added to the output's (re, im) by one
-                // packed add: two independent round-to-nearest adds of sums,
-                // no product feeds it.
-                acc[a + 2 * b] = __fadd2_rn(acc[a + 2 * b], make_float2(__fsub_rn(p, rr), __fadd_rn(p, qq)));
-            }
+        for (int a = 0; a < 2; ++a) {
+            const float p = __fmul_rn(sx[a], yr[b]);
+            const float qq = __fmul_rn(xr[a], dy[b]);
+            const float rr = __fmul_rn(xi[a], ey[b]);
+            // (re, im) of the term, added to the output's (re, im) by one
+            // packed add: two independent round-to-nearest adds of sums, no
+            // product feeds it.
+            acc[a + 2 * b] = __fadd2_rn(acc[a + 2 * b], make_float2(__fsub_rn(p, rr), __fadd_rn(p, qq)));
         }
     }
 }
 
+// Terms [0, len) of one staged chunk, in increasing K: a full chunk (len = CH)
+// as one straight-line block, a shorter one (the last chunk of a lane) as a
+// loop.
+template <int CH>
+__device__ __forceinline__ void replay_chunk(const float2* X0, const float2* X1, const float2* Y0,
+                                             const float2* Y1, int len, float2* acc)
+{
+    if (len == CH) {
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            replay_term(X0, X1, Y0, Y1, q, acc);
+        }
+    } else {
+#pragma unroll 4
+        for (int q = 0; q < len; ++q) {
+            replay_term(X0, X1, Y0, Y1, q, acc);
+        }
+    }
+}
+
+// One instance per chunk length CH = ceil(span / kChunks) (9 at n = 2048 .. 17
+// at n = 4096), so the box width and the full-chunk loop are constants.
+template <int CH>
 __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constant__ CUtensorMap tm_a,
                                                             const __grid_constant__ CUtensorMap tm_b, int n,
-                                                            int span, int ch, int w,
-                                                            const uint32_t* __restrict__ flag_bits,
+                                                            int span, const uint32_t* __restrict__ flag_bits,
                                                             const uint32_t* __restrict__ tile_flags,
                                                             float2* __restrict__ C, int* status)
 {
+    constexpr int ch = CH;
+    constexpr int w = box_width(CH);
     extern __shared__ uint8_t replay_smem[];
     uint8_t* base = align_shared<128>(replay_smem);
     // Lane sums, real then imaginary: S[l][o] for output o = ti + 16 tj of the tile.
@@ -308,7 +329,7 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constan
         }
         const float2* xp[4];
         chunk_ptrs(t, l, c, xp);
-        replay_chunk(xp[0], xp[1], xp[2], xp[3], chunk_len(l, c), acc);
+        replay_chunk<CH>(xp[0], xp[1], xp[2], xp[3], chunk_len(l, c), acc);
         if (c == kChunks - 1) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -392,7 +413,7 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constan
         }
         const float2* xp[4];
         chunk_ptrs(T, l, c, xp);
-        replay_chunk(xp[0], xp[1], xp[2], xp[3], chunk_len(l, c), acc);
+        replay_chunk<CH>(xp[0], xp[1], xp[2], xp[3], chunk_len(l, c), acc);
         if (c == kChunks - 1) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -638,6 +659,34 @@ static bool replay_tensor_map(CUtensorMap* map, const float2* rows, int n, int w
                              CU_TENSOR_MAP_SWIZZLE_NONE, rows);
 }
 
+// The replay instance for this order's chunk length ch = ceil(span / kChunks).
+template <int CH>
+static cudaError_t launch_replay(cudaStream_t s, int n, int span, const RoundLayout& L, float2* C, int* status)
+{
+    if ((span + kChunks - 1) / kChunks != CH) {
+        if constexpr (CH < kChunk) {
+            return launch_replay<CH + 1>(s, n, span, L, C, status);
+        } else {
+            return cudaErrorInvalidValue;  // lanes longer than the staged boxes (n > 4096)
+        }
+    }
+    static_assert(box_width(CH) <= kBoxMax, "box wider than its staging slot");
+    CUtensorMap tm_a, tm_b;
+    if (!replay_tensor_map(&tm_a, L.rows_a, n, box_width(CH)) ||
+        !replay_tensor_map(&tm_b, L.rows_b, n, box_width(CH))) {
+        return cudaErrorInvalidValue;
+    }
+    const int tiles = (n + kTile - 1) / kTile;
+    cudaError_t err = cudaFuncSetAttribute(recompute_fp32_tiled<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kRecomputeSmem);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    recompute_fp32_tiled<CH><<<tiles * tiles, 512, kRecomputeSmem, s>>>(tm_a, tm_b, n, span, L.flag_bits,
+                                                                       L.tile_flags, C, status);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status,
                             int* launched, const std::function<void(int)>& mark)
 {
@@ -665,22 +714,7 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
     }
     if (err == cudaSuccess) {
         if (plan.form == CG3M_FORM_FP32) {
-            const int ch = (span + kChunks - 1) / kChunks;
-            const int w = box_width(ch);
-            if (ch > kChunk || w > kBoxMax) {
-                return cudaErrorInvalidValue;  // lanes longer than the staged boxes (n > 4096)
-            }
-            CUtensorMap tm_a, tm_b;
-            if (!replay_tensor_map(&tm_a, L.rows_a, n, w) || !replay_tensor_map(&tm_b, L.rows_b, n, w)) {
-                return cudaErrorInvalidValue;
-            }
-            const int tiles = (n + kTile - 1) / kTile;
-            err = cudaFuncSetAttribute(recompute_fp32_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kRecomputeSmem);
-            if (err == cudaSuccess) {
-                recompute_fp32_tiled<<<tiles * tiles, 512, kRecomputeSmem, s>>>(
-                    tm_a, tm_b, n, span, ch, w, L.flag_bits, L.tile_flags, static_cast<float2*>(p.C), status);
-            }
+            err = launch_replay<kChunkMin>(s, n, span, L, static_cast<float2*>(p.C), status);
         } else {
             const int tiles = (n + kT64 - 1) / kT64;
             err = cudaFuncSetAttribute(recompute_fp64_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,

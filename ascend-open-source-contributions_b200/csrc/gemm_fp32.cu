@@ -460,6 +460,10 @@ __global__ void __launch_bounds__(ws::THREADS, 1)
 // d/9 * (s_old^2 + s_old*s_new + s_new^2) to the real and imaginary integrals;
 // path = max(I_re, I_im).  Each thread keeps a 4 x 4 complex micro-tile (three
 // product accumulators, the running sums and both integrals), CTA tile 64 x 64.
+// Only the real and imaginary planes are staged: the third operand of the
+// identity (Re + Im) is formed in registers with the same round-to-nearest
+// add the pack kernel uses for that plane, so the products keep their bits
+// while shared-memory reads (this kernel's limit) drop by a third.
 // ---------------------------------------------------------------------------
 constexpr int kRiskSegment = 128;
 
@@ -476,7 +480,7 @@ __global__ void __launch_bounds__(288, 1)
                             const PathParams p)
 {
     constexpr int BM = 64, BN = 64, BK = 16, STAGES = 4, CONSUMER_WARPS = 8;
-    constexpr int A_STAGE = 3 * BK * BM, B_STAGE = 3 * BK * BN;
+    constexpr int A_STAGE = 2 * BK * BM, B_STAGE = 2 * BK * BN;  // planes 0 (Re) and 1 (Im)
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = align_shared<1024>(smem_raw);
     float* sA = reinterpret_cast<float*>(base);
@@ -555,10 +559,18 @@ __global__ void __launch_bounds__(288, 1)
                 float2 y0[2], y1[2], y2[2];
                 *reinterpret_cast<float4*>(x0) = *reinterpret_cast<const float4*>(a + kk * BM);
                 *reinterpret_cast<float4*>(x1) = *reinterpret_cast<const float4*>(a + (BK + kk) * BM);
-                *reinterpret_cast<float4*>(x2) = *reinterpret_cast<const float4*>(a + (2 * BK + kk) * BM);
                 *reinterpret_cast<float4*>(y0) = *reinterpret_cast<const float4*>(b + kk * BN);
                 *reinterpret_cast<float4*>(y1) = *reinterpret_cast<const float4*>(b + (BK + kk) * BN);
-                *reinterpret_cast<float4*>(y2) = *reinterpret_cast<const float4*>(b + (2 * BK + kk) * BN);
+                // Re + Im of each operand (the pack kernel's third plane, same rounding);
+                // packed adds of loaded values, so nothing can be contracted.
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float2 s = __fadd2_rn(make_float2(x0[2 * h], x0[2 * h + 1]),
+                                                make_float2(x1[2 * h], x1[2 * h + 1]));
+                    x2[2 * h] = s.x;
+                    x2[2 * h + 1] = s.y;
+                    y2[h] = __fadd2_rn(y0[h], y1[h]);
+                }
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const float2 a0 = make_float2(x0[i], x0[i]), a1 = make_float2(x1[i], x1[i]),
@@ -791,7 +803,7 @@ cudaError_t launch_gemm_fp32_path(cudaStream_t stream, const Problem& pr, const 
     {
         const uint64_t dims[3] = {(uint64_t)pr.m, (uint64_t)pr.k, 3};
         const uint64_t strides[2] = {(uint64_t)plan.pitch_a * 4, (uint64_t)plan.plane_a_elems * 4};
-        const uint32_t box[3] = {BM, BK, 3};
+        const uint32_t box[3] = {BM, BK, 2};  // planes 0 and 1; the kernel forms plane 2
         if (!encode_tensor_map(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, dims, strides, box,
                                CU_TENSOR_MAP_SWIZZLE_NONE, w + plan.planes_a_off)) {
             return cudaErrorInvalidValue;
@@ -800,14 +812,14 @@ cudaError_t launch_gemm_fp32_path(cudaStream_t stream, const Problem& pr, const 
     {
         const uint64_t dims[3] = {(uint64_t)pr.n, (uint64_t)pr.k, 3};
         const uint64_t strides[2] = {(uint64_t)plan.pitch_b * 4, (uint64_t)plan.plane_b_elems * 4};
-        const uint32_t box[3] = {BN, BK, 3};
+        const uint32_t box[3] = {BN, BK, 2};
         if (!encode_tensor_map(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, dims, strides, box,
                                CU_TENSOR_MAP_SWIZZLE_NONE, w + plan.planes_b_off)) {
             return cudaErrorInvalidValue;
         }
     }
     PathParams p{pr.n, ceil_div(pr.n, BM), static_cast<float2*>(pr.C), path, status};
-    const size_t smem = (size_t)STAGES * 3 * BK * (BM + BN) * 4 + 2 * STAGES * 8 + 1024;
+    const size_t smem = (size_t)STAGES * 2 * BK * (BM + BN) * 4 + 2 * STAGES * 8 + 1024;
     cudaError_t err =
         cudaFuncSetAttribute(gemm3m_fp32_path_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) {

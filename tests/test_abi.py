@@ -300,7 +300,7 @@ def test_onchip_plan(cg3m):
     assert (one4["tile_m"], one4["tile_n"]) != (128, 64)  # four accumulators: no 128x64 tile
     four = cg3m.plan_onchip(1024, 1024, 1024, mode=1, batch=8)
     assert four["tile_m"] * four["tile_n"] <= 4096  # no 128x64 tile with four accumulators
-    # cgemm with alpha = 1, beta = 0: the FP32 planner's engine plus the repair pass
+    # cgemm with alpha = 1, beta = 0: the FP32 planner's engine, non-finite repair in its epilogues
     big_unit = cg3m.plan_onchip(2048, 2048, 2048, mode=2, batch=1)
     assert big_unit["path"] in (2, 3) and big_unit["kernels"] >= 2  # pack, GEMM (repair in its epilogue)
     small_unit = cg3m.plan_onchip(64, 64, 64, mode=2, batch=1)

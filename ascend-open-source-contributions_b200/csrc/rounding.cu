@@ -458,29 +458,33 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constan
 
 // ---- 4b. FP64 recompute (tensor-core forms) -----------------------------------------
 
-// FP64 product of one 64 x 64 output tile (each thread 4 x 4 outputs, K in
+// FP64 product of one 64 x 128 output tile (each thread 4 x 8 outputs, K in
 // order), computed only when one of its 16 x 16 flag granules is set; flagged
-// outputs are rounded once to FP32 and written.
-constexpr int kT64 = 64;
+// outputs are rounded once to FP32 and written.  Per K term a thread reads 12
+// complex operands for 32 complex products (128 DFMA): 1.5 bytes of shared
+// memory per DFMA, below the rate at which the FP64 pipe consumes them.
+constexpr int kT64 = 64;    // tile rows (op(A) rows)
+constexpr int kT128 = 128;  // tile columns (op(B) columns)
 
 // Operand slabs of 16 K terms, converted to FP64 once while staging (each
 // value feeds 16 threads), double-buffered with the next slab held in
 // registers during the current slab's DFMAs.
-constexpr size_t kFp64Slab = (size_t)16 * kT64;  // double2 per operand per buffer
-constexpr size_t kFp64Smem = 2 * 2 * kFp64Slab * sizeof(double2);
+constexpr size_t kFp64SlabX = (size_t)16 * kT64;   // double2 per buffer, op(A)
+constexpr size_t kFp64SlabY = (size_t)16 * kT128;  // double2 per buffer, op(B)
+constexpr size_t kFp64Smem = 2 * (kFp64SlabX + kFp64SlabY) * sizeof(double2);
 
-__global__ void __launch_bounds__(256, 2) recompute_fp64_tiled(int n, int pitch, const float2* __restrict__ rows_a,
+__global__ void __launch_bounds__(256, 1) recompute_fp64_tiled(int n, int pitch, const float2* __restrict__ rows_a,
                                                             const float2* __restrict__ rows_b,
                                                             const uint32_t* __restrict__ flag_bits,
                                                             const uint32_t* __restrict__ tile_flags,
                                                             float2* __restrict__ C)
 {
-    extern __shared__ __align__(16) double2 slabs[];  // [buffer][x | y][16][64]
+    extern __shared__ __align__(16) double2 slabs[];  // [buffer][x: 16 x 64 | y: 16 x 128]
     const int tiles16 = (n + kTile - 1) / kTile;
-    const int tiles64 = (n + kT64 - 1) / kT64;
-    const int i0 = (blockIdx.x % tiles64) * kT64, j0 = (blockIdx.x / tiles64) * kT64;
+    const int tiles_i = (n + kT64 - 1) / kT64;
+    const int i0 = (blockIdx.x % tiles_i) * kT64, j0 = (blockIdx.x / tiles_i) * kT128;
     uint32_t any = 0;
-    for (int q = 0; q < 16; ++q) {
+    for (int q = 0; q < (kT64 / kTile) * (kT128 / kTile); ++q) {
         const int gi = i0 / kTile + (q & 3), gj = j0 / kTile + (q >> 2);
         if (gi < tiles16 && gj < tiles16) {
             any |= tile_flags[gj * tiles16 + gi];
@@ -490,40 +494,45 @@ __global__ void __launch_bounds__(256, 2) recompute_fp64_tiled(int n, int pitch,
         return;
     }
     const int tid = threadIdx.x;
-    // Thread (ti, tj) owns rows ti + 16a and columns tj + 16b (a, b < 4): for a
-    // fixed a the 16 row values a warp reads are 256 consecutive bytes.
+    // Thread (ti, tj) owns rows ti + 16a (a < 4) and columns tj + 16b (b < 8):
+    // for a fixed a the 16 row values a warp reads are 256 consecutive bytes.
     const int ti = tid & 15, tj = tid >> 4;
-    double ar[4][4], ai[4][4];
+    double ar[4][8], ai[4][8];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < 8; ++b) {
             ar[a][b] = 0.0;
             ai[a][b] = 0.0;
         }
-    // Element e = tid + 256*u of a slab: row r = e >> 4, K offset q = e & 15.
-    float2 vx[4], vy[4];
+    // Element e = tid + 256*u of a slab: row r = e >> 4, K offset q = e & 15
+    // (4 elements per thread of the op(A) slab, 8 of the op(B) slab).
+    float2 vx[4], vy[8];
     auto load = [&](int k0) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 8; ++u) {
             const int e = tid + 256 * u;
             const int r = e >> 4, q = e & 15;
             const int k = k0 + q;
-            vx[u] = (k < n && i0 + r < n) ? rows_a[(size_t)(i0 + r) * pitch + k] : make_float2(0.0f, 0.0f);
+            if (u < 4) {
+                vx[u] = (k < n && i0 + r < n) ? rows_a[(size_t)(i0 + r) * pitch + k] : make_float2(0.0f, 0.0f);
+            }
             vy[u] = (k < n && j0 + r < n) ? rows_b[(size_t)(j0 + r) * pitch + k] : make_float2(0.0f, 0.0f);
         }
     };
     load(0);
     const int slabs_n = (n + 15) / 16;
     for (int t = 0; t < slabs_n; ++t) {
-        double2* xs = slabs + (size_t)(t & 1) * 2 * kFp64Slab;
-        double2* ys = xs + kFp64Slab;
+        double2* xs = slabs + (size_t)(t & 1) * (kFp64SlabX + kFp64SlabY);
+        double2* ys = xs + kFp64SlabX;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 8; ++u) {
             const int e = tid + 256 * u;
             const int r = e >> 4, q = e & 15;
-            xs[q * kT64 + r] = make_double2((double)vx[u].x, (double)vx[u].y);
-            ys[q * kT64 + r] = make_double2((double)vy[u].x, (double)vy[u].y);
+            if (u < 4) {
+                xs[q * kT64 + r] = make_double2((double)vx[u].x, (double)vx[u].y);
+            }
+            ys[q * kT128 + r] = make_double2((double)vy[u].x, (double)vy[u].y);
         }
         // Buffer t&1 was last read in slab t-2; this barrier also orders slab
         // t-1's reads before slab t+1's writes.
@@ -531,25 +540,28 @@ __global__ void __launch_bounds__(256, 2) recompute_fp64_tiled(int n, int pitch,
         if (t + 1 < slabs_n) {
             load((t + 1) * 16);
         }
-#pragma unroll 2
+#pragma unroll 1
         for (int q = 0; q < 16; ++q) {
-            double2 x[4], y[4];
+            double2 x[4], y[8];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
                 x[a] = xs[q * kT64 + ti + 16 * a];
-                y[a] = ys[q * kT64 + tj + 16 * a];
+            }
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                y[b] = ys[q * kT128 + tj + 16 * b];
             }
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
+                for (int b = 0; b < 8; ++b) {
                     ar[a][b] = fma(x[a].x, y[b].x, fma(-x[a].y, y[b].y, ar[a][b]));
                     ai[a][b] = fma(x[a].x, y[b].y, fma(x[a].y, y[b].x, ai[a][b]));
                 }
         }
     }
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
+    for (int b = 0; b < 8; ++b) {
         const int j = j0 + tj + 16 * b;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
@@ -716,11 +728,11 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
         if (plan.form == CG3M_FORM_FP32) {
             err = launch_replay<kChunkMin>(s, n, span, L, static_cast<float2*>(p.C), status);
         } else {
-            const int tiles = (n + kT64 - 1) / kT64;
+            const int tiles = ((n + kT64 - 1) / kT64) * ((n + kT128 - 1) / kT128);
             err = cudaFuncSetAttribute(recompute_fp64_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kFp64Smem);
             if (err == cudaSuccess) {
-                recompute_fp64_tiled<<<tiles * tiles, 256, kFp64Smem, s>>>(n, pitch, L.rows_a, L.rows_b, L.flag_bits,
+                recompute_fp64_tiled<<<tiles, 256, kFp64Smem, s>>>(n, pitch, L.rows_a, L.rows_b, L.flag_bits,
                                                                             L.tile_flags, static_cast<float2*>(p.C));
             }
         }

@@ -307,3 +307,23 @@ def test_onchip_plan(cg3m):
     assert small_unit["path"] == 4 and small_unit["kernels"] == 1
     with pytest.raises(cg3m.Cg3mError):
         cg3m.plan_onchip(64, 64, 64, mode=2, batch=2)
+
+
+@pytest.mark.parametrize("m,n,parts,merged", [
+    (512, 2048, 2, True),    # 32 pair tiles: 32 clusters of 4 CTAs fit at once (33)
+    (768, 1536, 2, False),   # 36 clusters of 4 do not: pack + GEMM + merge kernel
+    (512, 1408, 3, True),    # 22 clusters of 6 fit (22)
+    (512, 1536, 3, False),   # 24 do not
+    (768, 640, 4, True),     # 15 clusters of 8 fit (15)
+    (512, 1792, 4, False),   # 28 do not
+    (128, 1024, 2, False),   # one row tile: the single-CTA kernel, which writes partials
+])
+def test_tc_cluster_merge_gate(cg3m, m, n, parts, merged):
+    """Tensor-core K splits of 2..4 merge inside the tile's cluster (pack +
+    GEMM, no merge kernel) only when every cluster of 2 x parts CTAs of the
+    grid is resident at once on 148 SMs; a grid that one wave holds as loose
+    CTAs but not as clusters keeps the merge kernel."""
+    for form in ("tf32x3", "bf16x6"):
+        p = cg3m.plan("N", "N", m, n, 2048, form=form, rounding="off", k_partitions=parts)
+        assert p["k_partitions"] == parts and p["path"] == 3
+        assert p["kernels"] == (2 if merged else 3), (form, m, n, parts, p)

@@ -24,8 +24,9 @@
 // output, and skips tiles with no flagged output.  FP32 form: the reference's
 // segmented replay over 16 x 16 tiles, 2 x 2 outputs per thread for 8 of the
 // 64 lanes, with the 64 lane sums in shared memory and the lane reductions
-// and the inclusive lane scan in fixed orders.  Tensor-core forms: flagged outputs are recomputed
-// in FP64 over 64 x 64 tiles (K in order) and rounded once to FP32.
+// and the inclusive lane scan in fixed orders.  Tensor-core forms: flagged
+// outputs are recomputed in FP64 over 64 x 128 tiles (K in order) and rounded
+// once to FP32.
 #include <cstring>
 #include <functional>
 

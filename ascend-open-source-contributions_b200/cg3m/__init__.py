@@ -92,6 +92,9 @@ SIGNATURES = {
     "cg3mBatchPlanDestroy": [_P],
     "cg3mBatchPlanDescribe": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "cg3mGetDeviceStatus": [_P, ctypes.POINTER(_I)],
+    "cg3mDiagFailAllocations": [_I],
+    "cg3mGetRoundingStats": [_P, ctypes.POINTER(ctypes.c_longlong), _I],
+    "cg3mDiagBoundedWait": [_P, ctypes.c_longlong, ctypes.POINTER(_I)],
     "cg3mCgemm3mNoAlloc": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I],
     "cg3mSetStageEvents": [_P, ctypes.POINTER(_P), _I],
     "cg3mValidate": [_I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I, _I, ctypes.POINTER(_I)],
@@ -182,6 +185,16 @@ class Handle:
         f = ctypes.c_int()
         _check(_lib.cg3mGetDeviceStatus(self.h, ctypes.byref(f)), "cg3mGetDeviceStatus")
         return f.value
+
+    def rounding_stats(self):
+        """Counters of the last call's rounding pass (synchronizes): flagged
+        outputs, those recomputed by the tile kernels and those recomputed one
+        by one; None when the last call ran no rounding pass."""
+        v = (ctypes.c_longlong * 3)()
+        _check(_lib.cg3mGetRoundingStats(self.h, v, 3), "cg3mGetRoundingStats")
+        if v[0] < 0:
+            return None
+        return {"flagged": v[0], "dense_outputs": v[1], "sparse_outputs": v[2]}
 
     def cgemm3m(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, form="fp32", rounding="auto",
                 k_partitions=0, raw=False, tc_segment=0, engine="auto", onchip_tile=0):
@@ -323,6 +336,22 @@ def plan(transa, transb, m, n, k, alpha=1, beta=0, lda=None, ldb=None, ldc=None,
     _check(_lib.cg3mPlan(ta, tb, m, n, k, ctypes.byref(cx(alpha)), lda, ldb, ctypes.byref(cx(beta)), ldc,
                          ctypes.byref(opts), sm_count, ctypes.byref(info)), "cg3mPlan")
     return info.as_dict()
+
+
+def stage_names(info):
+    """Names of the kernels one call launched, in launch order, from its call
+    info (the order cg3mSetStageEvents records them in)."""
+    k = int(info["kernels"])
+    if info["path"] == 4:
+        return ["onchip"][:k]
+    if info["rounding"]:
+        fp32 = info["form"] == FORM["fp32"]
+        tail = ["replay_tiles", "replay_outputs"] if fp32 else ["recompute_fp64_tiles", "recompute_fp64_outputs"]
+        names = ["pack", "gemm_path", "pack_rows", "energy", "select"] + tail
+    else:
+        names = ["pack", "gemm", "merge"]
+    names = names[:k]
+    return names + [f"kernel{i}" for i in range(len(names), k)]
 
 
 def plan_onchip(m, n, k, mode=0, batch=1, sm_count=148):

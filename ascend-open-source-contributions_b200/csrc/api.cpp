@@ -7,6 +7,7 @@
 // nothing here synchronizes except Destroy, GetDeviceStatus and the
 // host-buffer entry point (which returns with C on the host).
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -40,6 +41,9 @@ void log_call(const char* what, const Plan& plan, const Problem& p)
                  plan.rounding ? 1 : 0, plan.total);
 }
 
+// Allocations still to fail on purpose (cg3mDiagFailAllocations).
+std::atomic<int> g_fail_allocs{0};
+
 cg3mStatus_t bind_device(cg3mContext* h)
 {
     if (h->device >= 0) {
@@ -54,7 +58,7 @@ cg3mStatus_t bind_device(cg3mContext* h)
         return CG3M_STATUS_INTERNAL_ERROR;
     }
     int* status = nullptr;
-    if (cudaMalloc(&status, 64) != cudaSuccess) {
+    if (device_malloc(reinterpret_cast<void**>(&status), 64) != cudaSuccess) {
         return CG3M_STATUS_ALLOC_FAILED;
     }
     if (cudaMemset(status, 0, 64) != cudaSuccess) {
@@ -62,7 +66,7 @@ cg3mStatus_t bind_device(cg3mContext* h)
         return CG3M_STATUS_INTERNAL_ERROR;
     }
     void* ws = nullptr;
-    if (cudaMalloc(&ws, kDefaultWorkspaceBytes) != cudaSuccess) {
+    if (device_malloc(&ws, kDefaultWorkspaceBytes) != cudaSuccess) {
         cudaFree(status);
         return CG3M_STATUS_ALLOC_FAILED;
     }
@@ -91,7 +95,7 @@ cg3mStatus_t workspace(cg3mContext* h, size_t bytes, void** out)
             h->default_ws_bytes = 0;
         }
         const size_t grow = align_up(bytes, size_t(2) << 20);
-        if (cudaMalloc(&h->default_ws, grow) != cudaSuccess) {
+        if (device_malloc(&h->default_ws, grow) != cudaSuccess) {
             h->default_ws = nullptr;
             return CG3M_STATUS_ALLOC_FAILED;
         }
@@ -169,6 +173,7 @@ cg3mStatus_t run_one(cg3mContext* h, int transa, int transb, int m, int n, int k
     int kernels = 0;
     const cudaError_t err = enqueue(h->stream, p, plan, ws, h->status, &kernels, h->stage_events,
                                     h->stage_event_count);
+    h->round_stats = plan.rounding ? rounding_stats_ptr(plan, ws, p.n) : nullptr;
     if (info != nullptr) {
         info->path = plan.engine == 2 ? 4 : plan.parts > 1 ? 3 : 2;
         info->form = plan.form;
@@ -186,6 +191,18 @@ cg3mStatus_t run_one(cg3mContext* h, int transa, int transb, int m, int n, int k
 }  // namespace
 
 namespace cg3m {
+
+cudaError_t device_malloc(void** p, size_t bytes)
+{
+    int pending = g_fail_allocs.load();
+    while (pending > 0) {
+        if (g_fail_allocs.compare_exchange_weak(pending, pending - 1)) {
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
 
 cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status, int* kernels,
                     const cudaEvent_t* events, int nevents)
@@ -561,7 +578,7 @@ cg3mStatus_t cg3mCgemm3mHost(cg3mHandle_t h, cg3mOperation_t transa, cg3mOperati
         cudaFree(h->host_arena);  // synchronizes with work that may still use it
         h->host_arena = nullptr;
         h->host_arena_bytes = 0;
-        if (cudaMalloc(&h->host_arena, bytes) != cudaSuccess) {
+        if (device_malloc(&h->host_arena, bytes) != cudaSuccess) {
             h->host_arena = nullptr;
             return CG3M_STATUS_ALLOC_FAILED;
         }
@@ -674,13 +691,27 @@ cg3mStatus_t cg3mSetStageEvents(cg3mHandle_t h, void* const* events, int count)
 
 cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t h, int* flags)
 {
-    if (h == nullptr) {
-        return CG3M_STATUS_HANDLE_IS_NULLPTR;
-    }
     if (flags == nullptr) {
-        return CG3M_STATUS_INVALID_VALUE;
+        return h == nullptr ? CG3M_STATUS_HANDLE_IS_NULLPTR : CG3M_STATUS_INVALID_VALUE;
     }
     *flags = 0;
+    if (h == nullptr) {
+        // The allocation-free entry point's word on the current device: its
+        // calls may be on any stream of the device, so the device is drained.
+        int* word = nullptr;
+        const cg3mStatus_t st = noalloc_status_word(&word);
+        if (st != CG3M_STATUS_SUCCESS) {
+            return st;
+        }
+        int v = 0;
+        if (cudaDeviceSynchronize() != cudaSuccess ||
+            cudaMemcpy(&v, word, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemset(word, 0, sizeof(int)) != cudaSuccess) {
+            return CG3M_STATUS_EXECUTION_FAILED;
+        }
+        *flags = v;
+        return CG3M_STATUS_SUCCESS;
+    }
     if (h->device < 0) {
         return CG3M_STATUS_SUCCESS;
     }
@@ -693,6 +724,74 @@ cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t h, int* flags)
         return CG3M_STATUS_EXECUTION_FAILED;
     }
     *flags = v;
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mGetRoundingStats(cg3mHandle_t h, long long* stats, int count)
+{
+    if (h == nullptr) {
+        return CG3M_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (stats == nullptr || count < 0) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    for (int i = 0; i < count; ++i) {
+        stats[i] = -1;
+    }
+    if (h->round_stats == nullptr) {
+        return CG3M_STATUS_SUCCESS;
+    }
+    uint32_t v[8] = {};
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(v, h->round_stats, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        return CG3M_STATUS_EXECUTION_FAILED;
+    }
+    for (int i = 0; i < count && i < 8; ++i) {
+        stats[i] = (long long)v[i];
+    }
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mDiagFailAllocations(int count)
+{
+    if (count < 0) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    g_fail_allocs.store(count);
+    return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mDiagBoundedWait(cg3mHandle_t h, long long limit_ns, int* gave_up)
+{
+    if (gave_up == nullptr || limit_ns <= 0 || limit_ns > 10000000000ll) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    *gave_up = 0;
+    int* word = nullptr;
+    cudaStream_t s = nullptr;
+    if (h == nullptr) {
+        const cg3mStatus_t st = noalloc_status_word(&word);
+        if (st != CG3M_STATUS_SUCCESS) {
+            return st;
+        }
+    } else {
+        const cg3mStatus_t bs = bind_device(h);
+        if (bs != CG3M_STATUS_SUCCESS) {
+            return bs;
+        }
+        word = h->status;
+        s = h->stream;
+    }
+    // word[1] is spare in both status blocks (64 and 256 bytes): the probe's
+    // result slot.
+    int v = 0;
+    if (cudaMemsetAsync(word + 1, 0, sizeof(int), s) != cudaSuccess ||
+        launch_wait_probe(s, word, (unsigned long long)limit_ns, word + 1) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess ||
+        cudaMemcpy(&v, word + 1, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        return CG3M_STATUS_EXECUTION_FAILED;
+    }
+    *gave_up = v;
     return CG3M_STATUS_SUCCESS;
 }
 
@@ -732,7 +831,7 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
     info->k_span = plan.span;
     info->rounding = plan.rounding ? 1 : 0;
     info->kernels =
-        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? 4 : 0);
+        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? 5 : 0);
     info->workspace_bytes = plan.total;
     return CG3M_STATUS_SUCCESS;
 }

@@ -20,6 +20,7 @@ struct cg3mContext {
     void* user_ws = nullptr;     // borrowed (cg3mSetWorkspace), never freed here
     size_t user_ws_bytes = 0;
     int* status = nullptr;       // device status word (bounded-wait failures)
+    uint32_t* round_stats = nullptr;  // counters of the last call's rounding pass (null if it had none)
     cudaEvent_t stage_events[16] = {};
     int stage_event_count = 0;
     // host-buffer entry point: device copies of A, B, C and its copy streams
@@ -98,7 +99,18 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
 cudaError_t launch_gemm_with_path(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
 // Bytes of the rounding-correction region for a square problem of order n.
 size_t rounding_bytes(int n);
+// Device address of the pass's counters (flagged, recomputed as tiles, one by
+// one) inside a planned call's workspace.
+uint32_t* rounding_stats_ptr(const Plan& plan, void* ws, int n);
 cudaError_t launch_zgemm_ref(cudaStream_t s, const Problem& p, const void* Cin, void* out64);
+// Diagnostics: one thread waits on an mbarrier nothing arrives on, with the
+// given limit; *gave_up (device) becomes 1 when the wait gave up.
+cudaError_t launch_wait_probe(cudaStream_t s, int* status, unsigned long long limit_ns, int* gave_up);
+// The allocation-free entry point's status word on the current device.
+cg3mStatus_t noalloc_status_word(int** word);
+// Every device allocation the handle API makes goes through this: it fails
+// like cudaMalloc out of memory while a diagnostics failure count is pending.
+cudaError_t device_malloc(void** p, size_t bytes);
 cudaError_t launch_error_report(cudaStream_t s, int m, int n, const void* C, int ldc, const void* out64,
                                 double* dev_report);
 

@@ -14,6 +14,11 @@
 // address, so the device address is looked up once per device with
 // cudaGetSymbolAddress (with that device current) and cached.  That lookup
 // happens inside the first call made on each device.
+//
+// The first 256 bytes of the array hold the status word the kernels set when
+// a bounded wait gives up.  The word is sticky: calls only add bits to it, and
+// cg3mGetDeviceStatus(NULL, ...) reads and clears it (the call itself returns
+// before its kernels run, so it cannot report them).
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -23,7 +28,7 @@
 namespace {
 
 constexpr size_t kScratchBytes = size_t(32) << 20;
-constexpr size_t kStatusBytes = 256;  // bounded-wait status word, cleared every call
+constexpr size_t kStatusBytes = 256;  // bounded-wait status word (sticky) and a probe slot
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
@@ -72,6 +77,15 @@ extern "C" cg3mStatus_t cg3mCgemm3mNoAlloc(void* stream, cg3mOperation_t transa,
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         return CG3M_STATUS_INTERNAL_ERROR;
     }
+    // The scratch address is per device: a stream of another device would get
+    // this device's array, so such a stream is refused.
+    int stream_dev = dev;
+    if (cudaStreamGetDevice(s, &stream_dev) != cudaSuccess) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    if (stream_dev != dev) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
     void* base = nullptr;
     int sms = 0;
     const cg3mStatus_t su = setup_device(dev, &base, &sms);
@@ -96,13 +110,32 @@ extern "C" cg3mStatus_t cg3mCgemm3mNoAlloc(void* stream, cg3mOperation_t transa,
         }
         return CG3M_STATUS_INVALID_VALUE;
     }
+    // Kernels only OR bits into the status word (zero when the library is
+    // loaded, cleared when it is read); the planes and partials are fully
+    // rewritten before they are read, so nothing else needs clearing.
     int* status = static_cast<int*>(base);
     void* ws = static_cast<unsigned char*>(base) + kStatusBytes;
-    // The status word must start each call at zero; the planes and partials
-    // are fully rewritten before they are read, so the rest is left as is.
-    if (cudaMemsetAsync(status, 0, sizeof(int), s) != cudaSuccess) {
-        return CG3M_STATUS_EXECUTION_FAILED;
-    }
     const cudaError_t err = enqueue(s, p, plan, ws, status, nullptr);
     return err == cudaSuccess ? CG3M_STATUS_SUCCESS : CG3M_STATUS_EXECUTION_FAILED;
 }
+
+namespace cg3m {
+
+// The status word of the allocation-free entry point on the current device
+// (its address resolved if no call has done so yet).
+cg3mStatus_t noalloc_status_word(int** word)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        return CG3M_STATUS_INTERNAL_ERROR;
+    }
+    void* base = nullptr;
+    int sms = 0;
+    const cg3mStatus_t st = setup_device(dev, &base, &sms);
+    if (st == CG3M_STATUS_SUCCESS) {
+        *word = static_cast<int*>(base);
+    }
+    return st;
+}
+
+}  // namespace cg3m

@@ -84,7 +84,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity)
 
 // Waits for the phase with the given parity to complete.  Returns false (and
 // sets kStatusTimeout in *status) when the wall-time limit expires.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status,
+                                          uint64_t limit_ns = CG3M_WAIT_LIMIT_NS)
 {
     const uint32_t addr = smem_u32(bar);
     if (mbar_try_wait(addr, parity)) {
@@ -95,7 +96,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* s
         if (mbar_try_wait(addr, parity)) {
             return true;
         }
-        if ((spin & 255u) == 0 && globaltimer() - start > CG3M_WAIT_LIMIT_NS) {
+        if ((spin & 255u) == 0 && globaltimer() - start > limit_ns) {
             if (status != nullptr) {
                 atomicOr(status, kStatusTimeout);
             }

@@ -47,6 +47,12 @@ constexpr int kLanes = 64;
 constexpr int kTile = 16;             // flag granule: 16 x 16 outputs
 constexpr int kMaxSpan = 65;          // ceil(4096/64) | 1
 constexpr float kConfidence = 3.75f;  // CGEMM_ROUNDING_CONFIDENCE, cgemm_host.cpp:37
+// A 16 x 16 tile with more flagged outputs than this is recomputed as a tile
+// (operands staged once for all its outputs); sparser tiles have each flagged
+// output recomputed on its own, so a handful of flags no longer costs a tile.
+constexpr uint32_t kSparseMax = 64;
+// Counters the pass leaves beside the flags (cg3mGetRoundingStats).
+enum : int { kStatFlagged = 0, kStatDenseOutputs = 1, kStatSparseOutputs = 2, kStatWords = 8 };
 
 // ---- 2. energies ----------------------------------------------------------------
 
@@ -88,30 +94,49 @@ __global__ void __launch_bounds__(kLanes) energy_kernel(const float2* __restrict
 
 // ---- 3. selection -----------------------------------------------------------------
 
+// One warp handles 32 consecutive outputs (idx = j*n + i) per step, so each
+// 32-bit word of the flag bitmap is the warp's ballot and is stored whole (no
+// memset, no atomics); flagged outputs are counted per 16 x 16 tile (the
+// warp's lanes of one tile add their count once) and in total.
 __global__ void select_kernel(int n, const float2* __restrict__ C, const float* __restrict__ energy,
                               const float* __restrict__ path, float bridge, uint32_t* __restrict__ flag_bits,
-                              uint32_t* __restrict__ tile_flags, uint32_t* __restrict__ count)
+                              uint32_t* __restrict__ tile_count, uint32_t* __restrict__ stats)
 {
     const size_t total = (size_t)n * n;
     const int tiles = (n + kTile - 1) / kTile;
     const float conf2 = __fmul_rn(kConfidence, kConfidence);
+    const int lane = threadIdx.x & 31;
     uint32_t local = 0;
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (size_t)gridDim.x * blockDim.x) {
-        const int j = (int)(idx / n), i = (int)(idx - (size_t)j * n);
-        const float2 c = C[idx];
-        const float re = fabsf(c.x), im = fabsf(c.y);
-        const float magnitude = re > im ? re : im;
-        const float variance =
-            __fmul_rn(0x1p-48f, __fadd_rn(path[idx], __fmul_rn(__fmul_rn(energy[i], energy[n + j]), bridge)));
-        const bool sel = !isfinite(magnitude) || !isfinite(variance) || __fmul_rn(conf2, variance) >= 0.0001f;
-        if (sel) {
-            atomicOr(&flag_bits[idx >> 5], 1u << (idx & 31));
-            atomicOr(&tile_flags[(j / kTile) * tiles + i / kTile], 1u);
-            ++local;
+    const size_t warps = (size_t)gridDim.x * (blockDim.x >> 5);
+    for (size_t base = (blockIdx.x * (size_t)(blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < total;
+         base += warps * 32) {
+        const size_t idx = base + lane;
+        bool sel = false;
+        int tile = -1;
+        if (idx < total) {
+            const int j = (int)(idx / n), i = (int)(idx - (size_t)j * n);
+            const float2 c = C[idx];
+            const float re = fabsf(c.x), im = fabsf(c.y);
+            const float magnitude = re > im ? re : im;
+            const float variance =
+                __fmul_rn(0x1p-48f, __fadd_rn(path[idx], __fmul_rn(__fmul_rn(energy[i], energy[n + j]), bridge)));
+            sel = !isfinite(magnitude) || !isfinite(variance) || __fmul_rn(conf2, variance) >= 0.0001f;
+            tile = (j / kTile) * tiles + i / kTile;
         }
+        const uint32_t word = __ballot_sync(0xffffffffu, sel);
+        if (lane == 0) {
+            flag_bits[base >> 5] = word;
+        }
+        const uint32_t peers = __match_any_sync(0xffffffffu, sel ? tile : -1);
+        if (sel && lane == __ffs(peers) - 1) {
+            atomicAdd(&tile_count[tile], (uint32_t)__popc(peers));
+        }
+        local += sel ? 1u : 0u;
     }
-    atomicAdd(count, local);
+    local = __reduce_add_sync(0xffffffffu, local);
+    if (lane == 0 && local != 0) {
+        atomicAdd(&stats[kStatFlagged], local);
+    }
 }
 
 __device__ __forceinline__ bool flagged(const uint32_t* bits, size_t idx)
@@ -220,8 +245,9 @@ template <int CH>
 __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constant__ CUtensorMap tm_a,
                                                             const __grid_constant__ CUtensorMap tm_b, int n,
                                                             int span, const uint32_t* __restrict__ flag_bits,
-                                                            const uint32_t* __restrict__ tile_flags,
-                                                            float2* __restrict__ C, int* status)
+                                                            const uint32_t* __restrict__ tile_count,
+                                                            uint32_t* __restrict__ stats, float2* __restrict__ C,
+                                                            int* status)
 {
     constexpr int ch = CH;
     constexpr int w = box_width(CH);
@@ -239,11 +265,15 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constan
     const int band = blockIdx.x / (kBand * tiles), first = band * kBand;
     const int rows_in_band = min(kBand, tiles - first), in_band = blockIdx.x - band * kBand * tiles;
     const int ti_tile = first + in_band % rows_in_band, tj_tile = in_band / rows_in_band;
-    if (tile_flags[(size_t)tj_tile * tiles + ti_tile] == 0) {
-        return;
+    const uint32_t tile_flagged = tile_count[(size_t)tj_tile * tiles + ti_tile];
+    if (tile_flagged <= kSparseMax) {
+        return;  // no flags, or few enough for the per-output kernel
     }
     const int i0 = ti_tile * kTile, j0 = tj_tile * kTile;
     const int tid = threadIdx.x;
+    if (tid == 0) {
+        atomicAdd(&stats[kStatDenseOutputs], tile_flagged);
+    }
     auto lane_count = [&](int l) { return max(0, min(span, n - l * span)); };
     auto chunk_len = [&](int l, int c) { return max(0, min(ch, lane_count(l) - c * ch)); };
 
@@ -477,24 +507,33 @@ constexpr size_t kFp64Smem = 2 * (kFp64SlabX + kFp64SlabY) * sizeof(double2);
 __global__ void __launch_bounds__(256, 1) recompute_fp64_tiled(int n, int pitch, const float2* __restrict__ rows_a,
                                                             const float2* __restrict__ rows_b,
                                                             const uint32_t* __restrict__ flag_bits,
-                                                            const uint32_t* __restrict__ tile_flags,
+                                                            const uint32_t* __restrict__ tile_count,
+                                                            uint32_t* __restrict__ stats,
                                                             float2* __restrict__ C)
 {
     extern __shared__ __align__(16) double2 slabs[];  // [buffer][x: 16 x 64 | y: 16 x 128]
     const int tiles16 = (n + kTile - 1) / kTile;
     const int tiles_i = (n + kT64 - 1) / kT64;
     const int i0 = (blockIdx.x % tiles_i) * kT64, j0 = (blockIdx.x / tiles_i) * kT128;
-    uint32_t any = 0;
+    // Recomputed as a tile when any of its 16 x 16 tiles is dense; then every
+    // flagged output of the tile is written here (recompute_sparse skips it).
+    bool dense = false;
+    uint32_t flagged_here = 0;
     for (int q = 0; q < (kT64 / kTile) * (kT128 / kTile); ++q) {
         const int gi = i0 / kTile + (q & 3), gj = j0 / kTile + (q >> 2);
         if (gi < tiles16 && gj < tiles16) {
-            any |= tile_flags[gj * tiles16 + gi];
+            const uint32_t c = tile_count[gj * tiles16 + gi];
+            dense |= c > kSparseMax;
+            flagged_here += c;
         }
     }
-    if (any == 0) {
+    if (!dense) {
         return;
     }
     const int tid = threadIdx.x;
+    if (tid == 0) {
+        atomicAdd(&stats[kStatDenseOutputs], flagged_here);
+    }
     // Thread (ti, tj) owns rows ti + 16a (a < 4) and columns tj + 16b (b < 8):
     // for a fixed a the 16 row values a warp reads are 256 consecutive bytes.
     const int ti = tid & 15, tj = tid >> 4;
@@ -577,6 +616,202 @@ __global__ void __launch_bounds__(256, 1) recompute_fp64_tiled(int n, int pitch,
     }
 }
 
+// ---- 4c. per-output recompute of sparse tiles ----------------------------------
+
+// Whether the 64 x 128 FP64 recompute tile holding 16 x 16 tile (gi, gj) runs
+// as a tile (recompute_fp64_tiled's predicate).
+__device__ __forceinline__ bool fp64_tile_dense(const uint32_t* tile_count, int tiles16, int gi, int gj)
+{
+    const int bi = gi / (kT64 / kTile) * (kT64 / kTile), bj = gj / (kT128 / kTile) * (kT128 / kTile);
+    bool dense = false;
+    for (int q = 0; q < (kT64 / kTile) * (kT128 / kTile); ++q) {
+        const int qi = bi + q % (kT64 / kTile), qj = bj + q / (kT64 / kTile);
+        if (qi < tiles16 && qj < tiles16) {
+            dense |= tile_count[qj * tiles16 + qi] > kSparseMax;
+        }
+    }
+    return dense;
+}
+
+// Pairwise reduction over the 64 values of v (stride 32, 16, ..., 1: the
+// oracle's lane_reduce order); every thread of the block calls it.
+__device__ __forceinline__ void lane_reduce_shared(float* v, int l)
+{
+#pragma unroll
+    for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
+        float x = 0.0f;
+        if (l < stride) {
+            x = __fadd_rn(v[l], v[l + stride]);
+        }
+        __syncthreads();
+        if (l < stride) {
+            v[l] = x;
+        }
+        __syncthreads();
+    }
+}
+
+// One block of 64 threads per 16 x 16 output tile that holds between 1 and
+// kSparseMax flagged outputs (and, for the FP64 recompute, lies in no dense
+// 64 x 128 tile).  Its flagged outputs are recomputed one after another: the
+// output's op(A) row and op(B) column are staged in shared memory, then
+//   FP32 (FastSegmentDot, cgemm3m_rounding_kernel.cpp:264-309): thread l is
+//     K lane l (k in [l*span, (l+1)*span)); its direct sum, the pairwise lane
+//     reduction, the inclusive Hillis-Steele scan, the replay seeded with the
+//     previous lane's prefix and the 32x fallback follow the oracle's order
+//     exactly (one rounding per operation, no contraction);
+//   FP64: thread l sums the same lane's complex products in FP64, the lane
+//     sums are reduced in FP64 and the result is rounded once to FP32.
+// Staged reads: thread l reads element l*span + s, so a warp's 8-byte reads
+// fall in distinct bank pairs (span is odd).
+template <bool FP64>
+__global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int span,
+                                                          const float2* __restrict__ rows_a,
+                                                          const float2* __restrict__ rows_b,
+                                                          const uint32_t* __restrict__ flag_bits,
+                                                          const uint32_t* __restrict__ tile_count,
+                                                          uint32_t* __restrict__ stats, float2* __restrict__ C)
+{
+    extern __shared__ __align__(16) float2 vec[];  // op(A) row at [0, pitch), op(B) column at [pitch, 2 pitch)
+    __shared__ float sr[kLanes], si[kLanes], tr[kLanes], ti[kLanes];
+    __shared__ double dr[kLanes], di[kLanes];
+    __shared__ int list[kTile * kTile];
+    __shared__ int listed;
+    __shared__ float peak_r[2], peak_i[2];
+    const int tiles = (n + kTile - 1) / kTile;
+    const int gi = blockIdx.x % tiles, gj = blockIdx.x / tiles;
+    const uint32_t count = tile_count[(size_t)gj * tiles + gi];
+    if (count == 0 || count > kSparseMax) {
+        return;
+    }
+    if (FP64 && fp64_tile_dense(tile_count, tiles, gi, gj)) {
+        return;
+    }
+    const int l = threadIdx.x;
+    const int i0 = gi * kTile, j0 = gj * kTile;
+    if (l == 0) {
+        listed = 0;
+        atomicAdd(&stats[kStatSparseOutputs], count);
+    }
+    __syncthreads();
+    for (int o = l; o < kTile * kTile; o += kLanes) {
+        const int i = i0 + o % kTile, j = j0 + o / kTile;
+        if (i < n && j < n && flagged(flag_bits, (size_t)j * n + i)) {
+            list[atomicAdd(&listed, 1)] = o;
+        }
+    }
+    __syncthreads();
+    const int outputs = listed;
+    const int kbeg = min(n, l * span), kend = min(n, kbeg + span);
+    for (int u = 0; u < outputs; ++u) {
+        const int o = list[u];
+        const int i = i0 + o % kTile, j = j0 + o / kTile;
+        const float4* ra = reinterpret_cast<const float4*>(rows_a + (size_t)i * pitch);
+        const float4* rb = reinterpret_cast<const float4*>(rows_b + (size_t)j * pitch);
+        float4* va = reinterpret_cast<float4*>(vec);
+        float4* vb = reinterpret_cast<float4*>(vec + pitch);
+        for (int e = l; e < pitch / 2; e += kLanes) {
+            va[e] = ra[e];
+            vb[e] = rb[e];
+        }
+        __syncthreads();
+        const float2* X = vec;
+        const float2* Y = vec + pitch;
+        float out_r, out_i;
+        if constexpr (FP64) {
+            double ar = 0.0, ai = 0.0;
+            for (int k = kbeg; k < kend; ++k) {
+                const float2 x = X[k], y = Y[k];
+                ar = fma((double)x.x, (double)y.x, fma(-(double)x.y, (double)y.y, ar));
+                ai = fma((double)x.x, (double)y.y, fma((double)x.y, (double)y.x, ai));
+            }
+            dr[l] = ar;
+            di[l] = ai;
+            __syncthreads();
+            for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
+                if (l < stride) {
+                    dr[l] += dr[l + stride];
+                    di[l] += di[l + stride];
+                }
+                __syncthreads();
+            }
+            out_r = (float)dr[0];
+            out_i = (float)di[0];
+        } else {
+            // pass 1: the lane's direct sum
+            float r = 0.0f, im = 0.0f;
+            for (int k = kbeg; k < kend; ++k) {
+                const float2 x = X[k], y = Y[k];
+                const float p = __fmul_rn(__fadd_rn(x.x, x.y), y.x);
+                const float q = __fmul_rn(x.x, __fsub_rn(y.y, y.x));
+                const float rr = __fmul_rn(x.y, __fadd_rn(y.x, y.y));
+                r = __fadd_rn(r, __fsub_rn(p, rr));
+                im = __fadd_rn(im, __fadd_rn(p, q));
+            }
+            sr[l] = r;
+            si[l] = im;
+            tr[l] = r;
+            ti[l] = im;
+            __syncthreads();
+            lane_reduce_shared(tr, l);
+            lane_reduce_shared(ti, l);
+            const float direct_r = tr[0], direct_i = ti[0];
+            // inclusive Hillis-Steele scan of the lane sums (each step reads the previous one)
+            for (int d = 1; d < kLanes; d *= 2) {
+                const float nr = l >= d ? __fadd_rn(sr[l], sr[l - d]) : sr[l];
+                const float ni = l >= d ? __fadd_rn(si[l], si[l - d]) : si[l];
+                __syncthreads();
+                sr[l] = nr;
+                si[l] = ni;
+                __syncthreads();
+            }
+            // largest |inclusive prefix| per part (max is order-free)
+            float mr = fabsf(sr[l]), mi = fabsf(si[l]);
+#pragma unroll
+            for (int off = 16; off >= 1; off /= 2) {
+                mr = fmaxf(mr, __shfl_xor_sync(0xffffffffu, mr, off));
+                mi = fmaxf(mi, __shfl_xor_sync(0xffffffffu, mi, off));
+            }
+            if ((l & 31) == 0) {
+                peak_r[l >> 5] = mr;
+                peak_i[l >> 5] = mi;
+            }
+            // pass 2: replay seeded with the previous lane's prefix
+            const float init_r = l >= 1 ? sr[l - 1] : 0.0f;
+            const float init_i = l >= 1 ? si[l - 1] : 0.0f;
+            r = __fadd_rn(init_r, 0.0f);
+            im = __fadd_rn(init_i, 0.0f);
+            for (int k = kbeg; k < kend; ++k) {
+                const float2 x = X[k], y = Y[k];
+                const float p = __fmul_rn(__fadd_rn(x.x, x.y), y.x);
+                const float q = __fmul_rn(x.x, __fsub_rn(y.y, y.x));
+                const float rr = __fmul_rn(x.y, __fadd_rn(y.x, y.y));
+                r = __fadd_rn(r, __fsub_rn(p, rr));
+                im = __fadd_rn(im, __fadd_rn(p, q));
+            }
+            __syncthreads();  // tr/ti (direct) read by every thread
+            tr[l] = __fsub_rn(r, init_r);
+            ti[l] = __fsub_rn(im, init_i);
+            __syncthreads();
+            lane_reduce_shared(tr, l);
+            lane_reduce_shared(ti, l);
+            out_r = tr[0];
+            out_i = ti[0];
+            const float pr = fmaxf(peak_r[0], peak_r[1]), pi = fmaxf(peak_i[0], peak_i[1]);
+            if (pr >= __fmul_rn(fabsf(direct_r), 32.0f)) {
+                out_r = direct_r;
+            }
+            if (pi >= __fmul_rn(fabsf(direct_i), 32.0f)) {
+                out_i = direct_i;
+            }
+        }
+        if (l == 0) {
+            C[(size_t)j * n + i] = make_float2(out_r, out_i);
+        }
+        __syncthreads();  // every read of this output's staged vectors and sums is done
+    }
+}
+
 }  // namespace
 
 // bridge = (floor(n/128)*128^2 + (n mod 128)^2) / (18 n^2), in FP32 as the
@@ -593,17 +828,17 @@ static float bridge_term(int n)
 
 // Layout of the rounding region (Plan::round_off): path n^2 floats | rows of
 // op(A) n^2 complex | columns of op(B) n^2 complex | energies 2n floats |
-// flags (one bit per output, then one word per 16 x 16 tile, then the flagged
-// count), zeroed before every selection.
+// flags: one bit per output (written whole by the selection), then one count
+// per 16 x 16 tile and kStatWords counters (zeroed before every selection).
 struct RoundLayout {
     float* path;
     float2* rows_a;
     float2* rows_b;
     float* energy;
     uint32_t* flag_bits;
-    uint32_t* tile_flags;
-    uint32_t* count;
-    size_t flag_bytes;  // flag_bits + tile_flags + count, one memset
+    uint32_t* tile_count;
+    uint32_t* stats;
+    size_t zero_bytes;  // tile_count + stats, one memset
 };
 
 static size_t flag_words(int n) { return ((size_t)n * n + 31) / 32; }
@@ -634,11 +869,13 @@ static RoundLayout round_layout(const Plan& plan, void* ws, int n)
     L.energy = reinterpret_cast<float*>(b + off);
     off = align_up(off + (size_t)2 * n * 4, kRegionAlign);
     L.flag_bits = reinterpret_cast<uint32_t*>(b + off);
-    L.tile_flags = L.flag_bits + flag_words(n);
-    L.count = L.tile_flags + tile_words(n);
-    L.flag_bytes = (flag_words(n) + tile_words(n) + 1) * 4;
+    L.tile_count = L.flag_bits + flag_words(n);
+    L.stats = L.tile_count + tile_words(n);
+    L.zero_bytes = (tile_words(n) + kStatWords) * 4;
     return L;
 }
+
+uint32_t* rounding_stats_ptr(const Plan& plan, void* ws, int n) { return round_layout(plan, ws, n).stats; }
 
 size_t rounding_bytes(int n)
 {
@@ -649,7 +886,7 @@ size_t rounding_bytes(int n)
     off = align_up(off + rows * 8, kRegionAlign);
     off = align_up(off + rows * 8, kRegionAlign);
     off = align_up(off + (size_t)2 * n * 4, kRegionAlign);
-    off = align_up(off + (flag_words(n) + tile_words(n) + 1) * 4, kRegionAlign);
+    off = align_up(off + (flag_words(n) + tile_words(n) + kStatWords) * 4, kRegionAlign);
     return off;
 }
 
@@ -696,7 +933,7 @@ static cudaError_t launch_replay(cudaStream_t s, int n, int span, const RoundLay
         return err;
     }
     recompute_fp32_tiled<CH><<<tiles * tiles, 512, kRecomputeSmem, s>>>(tm_a, tm_b, n, span, L.flag_bits,
-                                                                       L.tile_flags, C, status);
+                                                                       L.tile_count, L.stats, C, status);
     return cudaGetLastError();
 }
 
@@ -717,14 +954,17 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
         mark(++count);
     }
     if (err == cudaSuccess) {
-        err = cudaMemsetAsync(L.flag_bits, 0, L.flag_bytes, s);
+        err = cudaMemsetAsync(L.tile_count, 0, L.zero_bytes, s);
     }
     if (err == cudaSuccess) {
         select_kernel<<<148 * 8, 256, 0, s>>>(n, static_cast<const float2*>(p.C), L.energy, L.path, bridge_term(n),
-                                              L.flag_bits, L.tile_flags, L.count);
+                                              L.flag_bits, L.tile_count, L.stats);
         err = cudaGetLastError();
         mark(++count);
     }
+    // Dense tiles, then the flagged outputs of sparse tiles one by one; both
+    // kernels read the same per-tile counts, so each flagged output is
+    // recomputed by exactly one of them.
     if (err == cudaSuccess) {
         if (plan.form == CG3M_FORM_FP32) {
             err = launch_replay<kChunkMin>(s, n, span, L, static_cast<float2*>(p.C), status);
@@ -734,10 +974,23 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
                                        (int)kFp64Smem);
             if (err == cudaSuccess) {
                 recompute_fp64_tiled<<<tiles, 256, kFp64Smem, s>>>(n, pitch, L.rows_a, L.rows_b, L.flag_bits,
-                                                                            L.tile_flags, static_cast<float2*>(p.C));
+                                                                   L.tile_count, L.stats, static_cast<float2*>(p.C));
             }
         }
         if (err == cudaSuccess) {
+            err = cudaGetLastError();
+        }
+        mark(++count);
+    }
+    if (err == cudaSuccess) {
+        const int tiles16 = (n + kTile - 1) / kTile;
+        const size_t smem = (size_t)2 * pitch * sizeof(float2);
+        const bool fp64 = plan.form != CG3M_FORM_FP32;
+        auto kernel = fp64 ? recompute_sparse<true> : recompute_sparse<false>;
+        err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err == cudaSuccess) {
+            kernel<<<tiles16 * tiles16, kLanes, smem, s>>>(n, pitch, span, L.rows_a, L.rows_b, L.flag_bits,
+                                                           L.tile_count, L.stats, static_cast<float2*>(p.C));
             err = cudaGetLastError();
         }
         mark(++count);

@@ -5,16 +5,19 @@
 Workload (one step = one cgemm3m call): C <- A*B, complex64, M = N = K = 4096,
 column-major, op N/N, alpha = 1, beta = 0, contiguous; Re(A), Re(B) ~ N(0,1),
 Im ~ N(0,1)*2^e with an integer e in [-8, 8] drawn per column; seeded
-synthetic data (the reference publishes no dataset).  The timed calls run the
-3M product path with the rounding-correction pass off (--rounding auto turns
-it on); the same calls with the pass as the reference gates it are timed and
-reported beside them.  Metric: c64 TFLOP/s counted as 8*M*N*K per call.  Under torchrun every rank runs its own independent
-problem on its own GPU (no data-path collective; weak scaling) and the value is
-the whole job's throughput over the max-over-ranks time.
+synthetic data (the reference publishes no dataset).  This is the precision
+form's configuration as stated: the rounding-correction pass is ON (the
+drop-in's default gate admits this shape), for the tensor-core form (value)
+and for the plain FP32 drop-in (plain_fp32), both timed with the same steps
+and warm-up; the same calls with the pass off are reported beside them.
+Metric: c64 TFLOP/s counted as 8*M*N*K per call.  Under torchrun every rank
+runs its own independent problem on its own GPU (no data-path collective; weak
+scaling) and the value is the whole job's throughput over the max-over-ranks
+time.
 
---impl reference times the reference's CPU algorithm (the oracle restatement of
-reference-BLAS cgemm, scalar C) on all host cores on a bounded column sample of
-the same workload; under torchrun only rank 0 runs it.
+--impl reference times the reference's CPU algorithm (the oracle's
+reference-order cgemm, timing build) on all host cores on a bounded column
+sample of the same workload; under torchrun only rank 0 runs it.
 """
 from __future__ import annotations
 
@@ -57,15 +60,15 @@ PASSES = {"fp32": 1, "tf32x3": 3, "bf16x6": 6, "bf16x9": 9}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="bf16x6", choices=["fp32", "tf32x3", "bf16x6", "bf16x9"])
     ap.add_argument("--size", type=int, default=SIZE)
     ap.add_argument("--tc-segment", type=int, default=0)
-    ap.add_argument("--rounding", default="off", choices=["off", "auto"],
-                    help="rounding-correction pass for the timed calls (reported both ways)")
-    ap.add_argument("--no-rounding-report", action="store_true")
+    ap.add_argument("--rounding", default="auto", choices=["off", "auto"],
+                    help="rounding-correction pass for the headline calls (the other setting is reported beside)")
+    ap.add_argument("--no-rounding-report", action="store_true", help="skip the calls with the other setting")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batching-report", action="store_true")
     ap.add_argument("--batching-only", action="store_true",
@@ -246,8 +249,9 @@ def host_operands(n):
 
 
 def cpu_sample(cols, n, seed_offset=0):
-    """Reference-order FP32 cgemm (the oracle) on op(A) (n x n) times the first
-    `cols` columns of B: (seconds, flops8)."""
+    """Reference-order FP32 cgemm (the oracle's timing build: same bytes as the
+    checker) on op(A) (n x n) times the first `cols` columns of B:
+    (seconds, flops8)."""
     import numpy as np
 
     import oracle as O
@@ -255,8 +259,9 @@ def cpu_sample(cols, n, seed_offset=0):
     a = O.precision_matrix(n, n, SEED_A)
     b = O.precision_matrix(n, n, SEED_B)[: n * cols]
     c = np.zeros(n * cols, np.complex64)
+    O.cgemm_timing("N", "N", n, 2, n, 1 + 0j, a, n, b, n, 0j, c, n)  # page in A
     t0 = time.perf_counter()
-    O.cgemm("N", "N", n, cols, n, 1 + 0j, a, n, b, n, 0j, c, n)
+    O.cgemm_timing("N", "N", n, cols, n, 1 + 0j, a, n, b, n, 0j, c, n)
     dt = time.perf_counter() - t0
     return dt, 8.0 * n * cols * n
 
@@ -266,34 +271,67 @@ def _cpu_worker(args):
     return cpu_sample(cols, n)
 
 
+def cpu_parallel_sample(n, cols_per_worker, steps=1, warmup=0):
+    """The oracle on every host core (one spawned process per core, each its
+    own column block): per-step wall times and the cores used."""
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(cores) as pool:
+        for step in range(warmup + steps):
+            t0 = time.perf_counter()
+            pool.map(_cpu_worker, [(cols_per_worker, n)] * cores)
+            dt = time.perf_counter() - t0
+            if step >= warmup:
+                times.append(dt)
+    return times, cores
+
+
+def openblas_cgemm(n):
+    """OpenBLAS cgemm (numpy/scipy's bundled build) at full n^3 on all host
+    cores: (TFLOP/s at 8n^3, threads, seconds)."""
+    import numpy as np
+
+    import oracle as O
+    import scipy.linalg.blas as sb
+
+    try:
+        from threadpoolctl import threadpool_info
+
+        threads = max((x.get("num_threads", 0) for x in threadpool_info() if x.get("internal_api") == "openblas"),
+                      default=0)
+    except Exception:
+        threads = 0
+    a = np.asfortranarray(O.precision_matrix(n, n, SEED_A).reshape(n, n).T)
+    b = np.asfortranarray(O.precision_matrix(n, n, SEED_B).reshape(n, n).T)
+    sb.cgemm(1.0, a, b)
+    t0 = time.perf_counter()
+    sb.cgemm(1.0, a, b)
+    dt = time.perf_counter() - t0
+    return 8.0 * n ** 3 / dt / 1e12, threads or (os.cpu_count() or 1), dt
+
+
 # ----------------------------------------------------------------------------- reference arm
 
 def run_reference(args, rank):
     if rank != 0:
         return
-    import multiprocessing as mp
-
     n = args.size
-    cores = os.cpu_count() or 1
-    cols_per_worker = 4  # ~2 s of scalar work per step, so a 50-step run stays near two minutes
-    ctx = mp.get_context("spawn")
-    times = []
-    with ctx.Pool(cores) as pool:
-        for step in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            res = pool.map(_cpu_worker, [(cols_per_worker, n)] * cores)
-            dt = time.perf_counter() - t0
-            if step >= args.warmup:
-                times.append(dt)
+    cols_per_worker = 16  # a few hundred ms of vectorised scalar work per step
+    times, cores = cpu_parallel_sample(n, cols_per_worker, args.steps, args.warmup)
     flops = 8.0 * n * n * cols_per_worker * cores
     t = statistics.median(times)
     value = flops / t / 1e12
-    sample = f"{n}x{cols_per_worker * cores}x{n} column sample of the {n}^3 workload per step ({cores} processes)"
+    sample = (f"{n}x{cols_per_worker * cores}x{n} column sample of the {n}^3 workload per step "
+              f"({cores} processes, one column block each)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload(args.size), "form": "reference-BLAS order FP32 (oracle port)", "sample": sample},
+        "config": {"workload": workload(args.size), "form": "reference-BLAS order FP32 (oracle port, timing build)",
+                   "sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -447,6 +485,41 @@ def pf_cases_report(h, stream, dev, forms=("fp32", "bf16x6"), per_case=False):
 
 # ----------------------------------------------------------------------------- our arm
 
+def kernel_roofline(name, ms, n, form, sm_count, sgemm, stats, mhz):
+    """Roofline entry of one kernel of the 4096^3 call from its mean in-loop
+    duration: algorithmic work per launch over the time, against the pipe or
+    memory peak that bounds it."""
+    pk, src = peaks()
+    p = PASSES[form]
+    if name in ("gemm", "gemm_path"):
+        work = 6.0 * n ** 3 * p
+        peak, peak_src = pipe_peak(form, sm_count, sgemm)
+        return {"bound": "tensor" if form != "fp32" else "fp32-pipe", "achieved": work / (ms * 1e-3) / 1e12,
+                "peak": peak, "unit": "TFLOP/s", "work_per_launch": work,
+                "work_model": f"6*n^3 real flop x {p} pass(es)", "peak_source": peak_src}
+    if name.startswith("recompute_fp64"):
+        key = "dense_outputs" if name.endswith("tiles") else "sparse_outputs"
+        outs = float(stats[key]) if stats and stats.get(key) is not None else float(n * n)
+        work = 8.0 * outs * n
+        peak = sm_count * 64 * 2 * mhz * 1e6 / 1e12
+        return {"bound": "fp64-pipe", "achieved": work / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "work_per_launch": work,
+                "work_model": f"8 flop (4 DFMA) x n per flagged output it recomputes ({key})",
+                "peak_source": f"nominal: {sm_count} SMs x 64 FP64 lanes x 2 x {mhz:.0f} MHz"}
+    if name.startswith("replay"):
+        key = "dense_outputs" if name.endswith("tiles") else "sparse_outputs"
+        outs = float(stats[key]) if stats and stats.get(key) is not None else float(n * n)
+        work = 20.0 * outs * n
+        peak = sm_count * 128 * mhz * 1e6 / 1e12
+        return {"bound": "fp32-pipe", "achieved": work / (ms * 1e-3) / 1e12, "peak": peak, "unit": "Top/s",
+                "work_per_launch": work,
+                "work_model": f"2 passes x 10 FP32 ops (operand sums, 3 products, term, accumulate) x n per flagged "
+                              f"output it recomputes ({key})",
+                "peak_source": f"nominal: {sm_count} SMs x 128 FP32 lanes x {mhz:.0f} MHz (one op per lane)"}
+    return {"bound": "hbm", "achieved": None, "peak": pk.get("hbm_gbs"), "unit": "GB/s", "work_per_launch": None,
+            "work_model": "not modelled", "peak_source": f"{src} copy bandwidth"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -456,12 +529,22 @@ def main():
         run_reference(args, rank)
         return
 
-    # CPU baseline sample first: its processes must not fork after CUDA is up.
+    # CPU legs first: the spawned processes must start before CUDA is up.
     cpu = None
+    cpu_openblas = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        dt, fl = cpu_sample(96, args.size)
-        cpu = {"value": fl / dt / 1e12, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{args.size}x96x{args.size} column sample, reference-BLAS order FP32 (oracle), 1 thread"}
+        cols = 16
+        times, cores = cpu_parallel_sample(args.size, cols, steps=1)
+        fl = 8.0 * args.size * args.size * cols * cores
+        cpu = {"value": fl / times[0] / 1e12, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{args.size}x{cols * cores}x{args.size} column sample of the workload, reference-BLAS "
+                         f"order FP32 (oracle timing build, bit-identical to the checker), {cores} processes"}
+        try:
+            tf, threads, dt = openblas_cgemm(args.size)
+            cpu_openblas = {"value": tf, "unit": UNIT, "threads": threads, "seconds": dt,
+                            "what": f"OpenBLAS cgemm (scipy's bundled build) at full {args.size}^3 on this host"}
+        except Exception as e:  # scipy missing on the host: report why
+            cpu_openblas = {"unavailable": str(e)[:200]}
 
     import torch
     import torch.distributed as dist
@@ -502,87 +585,70 @@ def main():
     C = torch.zeros(n * n, dtype=torch.complex64, device=dev)
     stream = torch.cuda.Stream(device=dev)
     h = cg3m.Handle(stream=stream.cuda_stream)
-    sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+    props = torch.cuda.get_device_properties(dev)
+    sm_count = props.multi_processor_count
 
-    def call(form, rounding=None):
+    def call(form, rounding):
         return h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, tc_segment=args.tc_segment,
-                         rounding=rounding or args.rounding)
+                         rounding=rounding)
 
-    def timed(form, steps, warmup, rounding=None):
+    def timed(form, rounding, steps, warmup):
+        """Mean ms per call over `steps` calls after `warmup`, and the mean
+        duration of each of the call's kernels from events the library records
+        between its launches inside the same timed loop."""
         with torch.cuda.stream(stream):
             for _ in range(warmup):
                 info = call(form, rounding)
             torch.cuda.synchronize()
             if world > 1:
                 dist.barrier()
+            nk = info["kernels"]
+            evsets = [[torch.cuda.Event(enable_timing=True) for _ in range(nk + 1)] for _ in range(steps)]
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for _ in range(steps):
+            for i in range(steps):
+                h.set_stage_events(evsets[i])
                 info = call(form, rounding)
             e1.record(stream)
-            torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms, info
-
-    def stage_times(form, steps):
-        return stage_times_mode(form, None, steps)
-
-    def stage_times_mode(form, rounding, steps=1):
-        """Per-kernel durations from events the library records between its launches."""
-        info = call(form, rounding)
-        nk = info["kernels"]
-        per = []
-        with torch.cuda.stream(stream):
-            for _ in range(steps):
-                evs = [torch.cuda.Event(enable_timing=True) for _ in range(nk + 1)]
-                h.set_stage_events(evs)
-                call(form, rounding)
-                per.append(evs)
             h.set_stage_events([])
             torch.cuda.synchronize()
-        out = []
-        for i in range(nk):
-            out.append(sum(e[i].elapsed_time(e[i + 1]) for e in per) / steps)
-        return out, info
+        ms = e0.elapsed_time(e1) / steps
+        per = [sum(ev[j].elapsed_time(ev[j + 1]) for ev in evsets) / steps for j in range(nk)]
+        if world > 1:
+            t = torch.tensor([ms] + per, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms, per = float(t[0].item()), [float(x) for x in t[1:].tolist()]
+        return ms, info, per
 
     flops8 = 8.0 * n ** 3
-    flops6 = 6.0 * n ** 3
+    other = "off" if args.rounding == "auto" else "auto"
 
-    sampler = ClockSampler(local, pci_bus_id(torch.cuda.get_device_properties(dev)))
+    sampler = ClockSampler(local, pci_bus_id(props))
     sampler.start()
-    ms, info = timed(args.form, args.steps, args.warmup)
+    ms, info, stages = timed(args.form, args.rounding, args.steps, args.warmup)
+    stats = h.rounding_stats() if info["rounding"] else None
+    if args.form != "fp32":
+        pms, pinfo, pstages = timed("fp32", args.rounding, args.steps, args.warmup)
+        pstats = h.rounding_stats() if pinfo["rounding"] else None
     clocks = sampler.stop()
     value = world * flops8 / (ms * 1e-3) / 1e12
+    names = cg3m.stage_names(info)
+    mhz = (clocks or {}).get("sm_mhz") or peaks()[0].get("sm_max_mhz", 1965.0)
 
-    # per-kernel times of the same call (instrumented, separate loop)
-    stages, _ = stage_times(args.form, max(3, min(args.steps, 10)))
-    # the GEMM is the second launch after the pack kernel, or the only one (one-launch engine)
-    gemm_ms = stages[1] if len(stages) > 1 else stages[0]
-    p = PASSES[args.form]
     sgemm = sgemm_tflops(torch, dev)
-    peak, peak_src = pipe_peak(args.form, sm_count, sgemm)
-    achieved = flops6 * p / (gemm_ms * 1e-3) / 1e12
-    pk_all, _src = peaks()
-    sustained = pk_all.get("bf16_tflops_sustained")
-    if sustained and args.form != "fp32":
-        sustained = sustained / 2.0 if args.form == "tf32x3" else sustained
-    roofline = {"bound": "tensor" if args.form != "fp32" else "fp32-pipe", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "kernel": "gemm",
-                "frac_vs_sustained_peak": (achieved / sustained) if sustained and args.form != "fp32" else None,
-                "peak_source": peak_src, "flops_per_launch": flops6 * p, "kernel_ms": gemm_ms,
-                "stage_ms": stages}
+    dom = max(range(len(stages)), key=lambda i: stages[i])
+    roofline = kernel_roofline(names[dom], stages[dom], n, args.form, sm_count, sgemm, stats, mhz)
+    roofline.update({"kernel": names[dom], "kernel_ms": stages[dom], "share_of_step": stages[dom] / ms,
+                     "traffic": None})
+    roofline["frac"] = (roofline["achieved"] / roofline["peak"]) if roofline.get("achieved") else None
     traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(traffic_file):
         with open(traffic_file) as f:
-            roofline["traffic"] = json.load(f).get(f"gemm_{args.form}_{n}")
+            roofline["traffic"] = json.load(f).get(f"{names[dom]}_{args.form}_{n}")
 
     # End to end through the public host-buffer entry point (cg3mCgemm3mHost):
     # A and B uploaded from page-locked host memory and C read back inside
-    # every step; the call pipelines the copies with the panels' compute.
+    # every step (with the rounding pass the call runs as one panel).
     a_pin = torch.from_numpy(a_host).pin_memory()
     b_pin = torch.from_numpy(b_host).pin_memory()
     c_pin = torch.empty(n * n, dtype=torch.complex64).pin_memory()
@@ -603,63 +669,49 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
-    # the same with the copies issued around one device call (no overlap)
-    with torch.cuda.stream(stream):
-        for it in range(args.warmup + args.steps):
-            if it == args.warmup:
-                torch.cuda.synchronize()
-                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                s0.record(stream)
-            A.copy_(a_pin, non_blocking=True)
-            B.copy_(b_pin, non_blocking=True)
-            call(args.form)
-            c_pin.copy_(C, non_blocking=True)
-        s1.record(stream)
-        torch.cuda.synchronize()
-    seq_ms = s0.elapsed_time(s1) / args.steps
     if world > 1:
-        t = torch.tensor([e2e_ms, seq_ms], device=dev)
+        t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms, seq_ms = (float(x) for x in t.tolist())
+        e2e_ms = float(t.item())
     e2e = {"value": world * flops8 / (e2e_ms * 1e-3) / 1e12, "unit": UNIT, "h2d_bytes_per_step": 2 * n * n * 8,
            "d2h_bytes_per_step": n * n * 8, "ms_per_step": e2e_ms,
-           "api": "cg3mCgemm3mHost (page-locked host A, B, C; copies pipelined with column panels)",
-           "kernels_per_step": host_info["kernels"],
-           "copy_then_call": {"value": world * flops8 / (seq_ms * 1e-3) / 1e12, "ms_per_step": seq_ms}}
+           "api": f"cg3mCgemm3mHost (page-locked host A, B, C; rounding {args.rounding})",
+           "kernels_per_step": host_info["kernels"]}
 
-    # accuracy vs FP64 (device reference), for this form and the plain FP32 form
-    errors = {}
-    plain = None
+    # accuracy vs FP64 (device reference) for every timed call
     out64 = torch.empty(n * n, dtype=torch.complex128, device=dev)
+    errors = {}
     with torch.cuda.stream(stream):
         h.zgemm_reference("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, out64)
         for form in sorted({args.form, "fp32"}):
-            call(form)
+            call(form, args.rounding)
             errors[form] = h.error_report(n, n, C, n, out64)
+    plain = None
     if args.form != "fp32":
-        pms, _ = timed("fp32", max(3, args.steps // 2), 2)
-        pst, _ = stage_times("fp32", 3)
-        pgemm = pst[1] if len(pst) > 1 else pst[0]
-        plain = {"value": world * flops8 / (pms * 1e-3) / 1e12, "ms_per_step": pms, "gemm_ms": pgemm,
-                 "gemm_fp32_tflops": flops6 / (pgemm * 1e-3) / 1e12, "sgemm_tflops_measured": sgemm,
-                 "gemm_frac_of_sgemm": flops6 / (pgemm * 1e-3) / 1e12 / sgemm,
-                 "what": "plain FP32 3M GEMM kernel: 6MNK FFMA flop over its time, against cuBLAS FP32 SGEMM "
-                         "(TF32 off) timed on the same GPU in this run"}
-    # The same calls with the rounding-correction pass as the reference gates it
-    # (this shape qualifies): time, flagged-output recompute share, errors.
-    rounding_report = None
+        plain = {"value": world * flops8 / (pms * 1e-3) / 1e12, "ms_per_step": pms, "rounding": args.rounding,
+                 "kernels": pinfo["kernels"], "stage_names": cg3m.stage_names(pinfo), "stage_ms": pstages,
+                 "rounding_stats": pstats, "errors_vs_fp64": errors["fp32"],
+                 "what": "the plain FP32 drop-in (cg3mCgemm3m arithmetic) on the same call, same steps and warm-up"}
+    # the same calls with the pass set the other way (same steps and warm-up)
+    other_report = None
     if not args.no_rounding_report:
-        rounding_report = {}
-        other = "auto" if args.rounding == "off" else "off"
+        other_report = {"rounding": other}
         for form in sorted({args.form, "fp32"}):
-            rms, rinfo = timed(form, 1, 1, rounding=other)
+            oms, oinfo, ost = timed(form, other, args.steps, args.warmup)
             with torch.cuda.stream(stream):
                 call(form, other)
                 err = h.error_report(n, n, C, n, out64)
-            st, _ = stage_times_mode(form, other)
-            rounding_report[form] = {"rounding": other, "value": world * flops8 / (rms * 1e-3) / 1e12,
-                                     "ms_per_step": rms, "kernels": rinfo["kernels"], "stage_ms": st,
-                                     "errors_vs_fp64": err}
+            other_report[form] = {"value": world * flops8 / (oms * 1e-3) / 1e12, "ms_per_step": oms,
+                                  "kernels": oinfo["kernels"], "stage_names": cg3m.stage_names(oinfo),
+                                  "stage_ms": ost, "errors_vs_fp64": err}
+        if args.form != "fp32":
+            other_report["tc_over_plain"] = other_report[args.form]["value"] / other_report["fp32"]["value"]
+            other_report["fp32"]["sgemm_tflops_measured"] = sgemm
+            fp32_names = other_report["fp32"]["stage_names"]
+            if "gemm" in fp32_names:
+                gms = other_report["fp32"]["stage_ms"][fp32_names.index("gemm")]
+                other_report["fp32"]["gemm_fp32_tflops"] = 6.0 * n ** 3 / (gms * 1e-3) / 1e12
+                other_report["fp32"]["gemm_frac_of_sgemm"] = other_report["fp32"]["gemm_fp32_tflops"] / sgemm
     del out64
     batching = None if args.no_batching_report else batching_report(h, stream, dev, world, args)
     status = h.device_status()
@@ -674,20 +726,23 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.form == "fp32" else args.form, "data": "synthetic",
         "config": {"workload": workload(n), "form": args.form, "rounding": args.rounding, "m": n, "n": n, "k": n,
-                   "transa": "N", "transb": "N",
-                   "alpha": [1, 0], "beta": [0, 0], "parallelism": f"replica x{world} (independent problems)",
-                   "l2": l2_note(n),
+                   "transa": "N", "transb": "N", "alpha": [1, 0], "beta": [0, 0],
+                   "parallelism": f"replica x{world} (independent problems)", "l2": l2_note(n),
                    "plan": {k_: info[k_] for k_ in ("tile_m", "tile_n", "k_partitions", "k_span", "rounding",
                                                     "kernels", "workspace_bytes")}},
         "roofline": roofline,
         "cpu_baseline": cpu,
+        "cpu_openblas": cpu_openblas,
         "e2e": e2e,
         "gpu_launches": args.steps * info["kernels"],
         "clocks": clocks,
+        "stage_names": names,
+        "stage_ms": stages,
+        "rounding_stats": stats,
         "errors_vs_fp64": errors,
         "plain_fp32": plain,
         "tc_over_plain": (value / plain["value"]) if plain else None,
-        "rounding_pass": rounding_report,
+        "rounding_" + other: other_report,
         "batching_form": batching,
         "device_status": status,
     }

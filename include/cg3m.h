@@ -221,8 +221,35 @@ cg3mStatus_t cg3mSetStageEvents(cg3mHandle_t handle, void* const* events, int co
 
 /* Device status word of the handle: synchronizes the stream, returns and
  * clears the error bits kernels set when a bounded wait gave up
- * (1: pipeline wait timed out).  0 means no device-side error. */
+ * (1: pipeline wait timed out).  0 means no device-side error.
+ * handle == NULL reads (and clears) the word of cg3mCgemm3mNoAlloc on the
+ * current device instead, after synchronizing the whole device. */
 cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t handle, int* flags);
+
+/* Counters of the rounding-correction pass of the last call made through the
+ * handle (synchronizes its stream): stats[0] = outputs flagged, stats[1] =
+ * flagged outputs recomputed by the tile kernels (16 x 16 tiles holding more
+ * than 64 flagged outputs; FP64 form: their 64 x 128 tiles), stats[2] =
+ * flagged outputs recomputed one by one (the other tiles); entries past 2
+ * are reserved.  All -1 when that call ran no rounding pass.  Valid until the
+ * next call through the handle (the counters live in its workspace). */
+cg3mStatus_t cg3mGetRoundingStats(cg3mHandle_t handle, long long* stats, int count);
+
+/* ---- diagnostics for failure handling (test use) -------------------------- */
+
+/* The next `count` device allocations the handle API attempts (status word,
+ * default workspace, workspace growth, host-buffer copies) fail as if the
+ * device were out of memory; the call that needed one returns
+ * CG3M_STATUS_ALLOC_FAILED without touching C.  0 turns it off. */
+cg3mStatus_t cg3mDiagFailAllocations(int count);
+
+/* Runs one bounded wait that cannot complete (an mbarrier nothing arrives on)
+ * through the wait every pipeline kernel uses, with a limit of limit_ns
+ * (0 < limit_ns <= 10 s), on the handle's stream, and synchronizes.  The
+ * wait gives up, sets bit 1 of the handle's status word (handle == NULL: the
+ * cg3mCgemm3mNoAlloc word of the current device) and the kernel returns;
+ * *gave_up is 1 when it did.  No fault, no hang: the context stays usable. */
+cg3mStatus_t cg3mDiagBoundedWait(cg3mHandle_t handle, long long limit_ns, int* gave_up);
 
 /* ---- allocation-free variant (no counterpart in the reference) ----------- */
 
@@ -235,9 +262,13 @@ cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t handle, int* flags);
  * instead of a handle.  The first call on each device resolves the array's
  * device address (cudaGetSymbolAddress), so make that first call before any
  * stream capture.  Problems whose scratch would exceed the array return
- * CG3M_STATUS_INVALID_VALUE with C untouched.  Every call shares the one
- * array, so calls whose work overlaps on the GPU (other streams, other host
- * threads) race on it; serialise them. */
+ * CG3M_STATUS_INVALID_VALUE with C untouched, and so is a stream that does
+ * not belong to the current device (the array's address is per device).
+ * Every call shares the one array, so calls whose work overlaps on the GPU
+ * (other streams, other host threads) race on it; serialise them.  The call
+ * returns before its kernels run, so a kernel whose bounded wait gave up
+ * (C then incomplete) cannot change its status: kernels set bit 1 of a status
+ * word that stays set until cg3mGetDeviceStatus(NULL, &flags) reads it. */
 cg3mStatus_t cg3mCgemm3mNoAlloc(void* stream, cg3mOperation_t transa, cg3mOperation_t transb, int m, int n, int k,
                                 const cg3mComplex* alpha, const cg3mComplex* A, int lda, const cg3mComplex* B,
                                 int ldb, const cg3mComplex* beta, cg3mComplex* C, int ldc);

@@ -45,9 +45,19 @@ typedef struct {
     double re, im;
 } c64;
 
+#ifdef ORACLE_TIMING_BUILD
+/* Timing build (the CPU baseline): the same operations in the same order.
+ * -ffp-contract=off and the absence of fast-math already forbid contraction
+ * and reassociation, so the compiler may only vectorise across independent
+ * outputs; tests check this build's bytes against the checker's. */
+static inline float fmul(float a, float b) { return a * b; }
+static inline float fadd(float a, float b) { return a + b; }
+static inline float fsub(float a, float b) { return a - b; }
+#else
 static inline float fmul(float a, float b) { volatile float r = a * b; return r; }
 static inline float fadd(float a, float b) { volatile float r = a + b; return r; }
 static inline float fsub(float a, float b) { volatile float r = a - b; return r; }
+#endif
 
 /* Element of op(X) at (row, col) for a column-major stored X. */
 static inline c32 op_elem(const c32* x, int ld, int op, int row, int col)

@@ -90,6 +90,25 @@ def cgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
     return c
 
 
+_timing_lib = None
+
+
+def cgemm_timing(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """oracle_cgemm from the timing build (no volatile stores; same bytes)."""
+    global _timing_lib
+    if _timing_lib is None:
+        lib()
+        L = ctypes.CDLL(_build.LIB_TIMING)
+        P, i = ctypes.c_void_p, ctypes.c_int
+        L.oracle_cgemm.argtypes = [i, i, i, i, i, P, P, i, P, i, P, P, i]
+        _timing_lib = L
+    al = np.array([complex(alpha).real, complex(alpha).imag], np.float32)
+    be = np.array([complex(beta).real, complex(beta).imag], np.float32)
+    _timing_lib.oracle_cgemm(_op(transa), _op(transb), m, n, k, _ptr(al), _ptr(_c64(a)), lda, _ptr(_c64(b)), ldb,
+                             _ptr(be), _ptr(c), ldc)
+    return c
+
+
 def zgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
     """FP64 product; returns an m x n complex128 array (column-major values)."""
     al = np.array([alpha.real, alpha.imag], dtype=np.float64)

@@ -49,7 +49,7 @@ def test_fp32_rounding_pass_bit_exact_blocks(cg3m, oracle, cuda, h, ops, N):
     b = oracle.precision_matrix(N, N, 12)
     c0 = np.zeros(N * N, np.complex64)
     out, info = run(cg3m, h, torch, cuda, ta, tb, N, N, N, 1.0, a, N, b, N, 0.0, c0, N)
-    assert info["rounding"] == 1 and info["kernels"] == 6
+    assert info["rounding"] == 1 and info["kernels"] == 7
     again, _ = run(cg3m, h, torch, cuda, ta, tb, N, N, N, 1.0, a, N, b, N, 0.0, c0, N)
     assert out.tobytes() == again.tobytes()
     e = oracle.energy(N, ta, tb, a, N, b, N)
@@ -69,6 +69,71 @@ def test_fp32_rounding_pass_bit_exact_blocks(cg3m, oracle, cuda, h, ops, N):
         expect[r, q] = oracle.recompute_dot(np.ascontiguousarray(opa[rows[r], :]), np.ascontiguousarray(opb[:, cols[q]]))
     got = oracle.unpack(out, N, N, N)[np.ix_(rows, cols)]
     assert got.tobytes() == expect.astype(np.complex64).tobytes()
+
+
+def _mixed_density_inputs(oracle, n):
+    """Uniform(-1,1) operands (nothing flagged) with five rows of op(A) and six
+    adjacent columns of op(B) scaled by 1024, which flags those whole rows and
+    columns through the energy term: 16 x 16 tiles crossed by one scaled row
+    hold 16 flagged outputs (recomputed one by one), tiles of the six columns
+    hold 96 or more (recomputed as tiles)."""
+    a = oracle.make_matrix(n, n, n, "UNIFORM_1", 91)
+    b = oracle.make_matrix(n, n, n, "UNIFORM_1", 92)
+    rows = [5, 100, 777, 1500, n - 3]
+    cols = list(range(160, 166))
+    A = a.reshape(n, n)  # [col][row]: column-major n x n
+    B = b.reshape(n, n)
+    for r in rows:
+        A[:, r] *= np.float32(1024.0)
+    for c in cols:
+        B[c, :] *= np.float32(1024.0)
+    return a, b, rows, cols
+
+
+@pytest.mark.parametrize("form", ["fp32", "bf16x6"])
+def test_rounding_pass_sparse_and_dense_tiles(cg3m, oracle, cuda, h, form):
+    """Tiles with few flagged outputs go to the per-output kernel, dense ones
+    to the tile kernel; each flagged output is recomputed exactly once.  FP32:
+    every checked block is bit-exact against the oracle (path GEMM value where
+    unflagged, segmented replay where flagged); FP64 recompute: flagged
+    outputs within one FP32 rounding of the FP64 product."""
+    import torch
+
+    n = 2048
+    a, b, srows, scols = _mixed_density_inputs(oracle, n)
+    c0 = np.zeros(n * n, np.complex64)
+    out, info = run(cg3m, h, torch, cuda, "N", "N", n, n, n, 1.0, a, n, b, n, 0.0, c0, n, form=form)
+    assert info["rounding"] == 1
+    st = h.rounding_stats()
+    assert st["dense_outputs"] > 0 and st["sparse_outputs"] > 0
+    assert st["dense_outputs"] + st["sparse_outputs"] == st["flagged"]
+    e = oracle.energy(n, "N", "N", a, n, b, n)
+    rows = np.r_[0:8, 96:104, 770:780, n - 8:n]
+    cols = np.r_[0:6, 156:170, 1500:1506, n - 6:n]
+    sa, slda = sub_problem(oracle, "N", a, n, n, n, rows, 0)
+    sb, sldb = sub_problem(oracle, "N", b, n, n, n, cols, 1)
+    opa = oracle.op_matrix(a, n, "N", n, n)
+    opb = oracle.op_matrix(b, n, "N", n, n)
+    got = oracle.unpack(out, n, n, n)[np.ix_(rows, cols)]
+    if form == "fp32":
+        path, cpath = oracle.risk_path_rect(len(rows), len(cols), n, "N", sa, slda, "N", sb, sldb)
+        P = path.reshape(len(cols), len(rows)).T
+        Cm = cpath.reshape(len(cols), len(rows)).T
+        flags = oracle.select_flags(P, Cm, e[rows], e[n + cols], oracle.bridge(n))
+        assert flags.any() and not flags.all()
+        expect = Cm.copy()
+        for (r, q) in zip(*np.nonzero(flags)):
+            expect[r, q] = oracle.recompute_dot(np.ascontiguousarray(opa[rows[r], :]),
+                                                np.ascontiguousarray(opb[:, cols[q]]))
+        assert got.tobytes() == expect.astype(np.complex64).tobytes()
+    else:
+        z = opa[rows, :].astype(np.complex128) @ opb[:, cols].astype(np.complex128)
+        for r in range(len(rows)):
+            for q in range(len(cols)):
+                if rows[r] in srows or cols[q] in scols:  # flagged through the energy term
+                    x = complex(got[r, q])
+                    assert abs(x.real - z[r, q].real) <= np.spacing(np.float32(abs(z[r, q].real)))
+                    assert abs(x.imag - z[r, q].imag) <= np.spacing(np.float32(abs(z[r, q].imag)))
 
 
 def _kat_inputs(residual):

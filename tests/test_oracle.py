@@ -216,3 +216,20 @@ def test_case_table_integrity(cases):
     pf = [r for r in rows if r["name"].startswith("TC_PF_")]
     assert all(r["alpha"] == [1.0, 0.0] and r["beta"] == [0.0, 0.0] for r in pf)
     assert sum(r["expect"] != "SUCCESS" for r in rows) == 16
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("C", "T"), ("T", "C"), ("R", "N"), ("N", "C")])
+def test_timing_build_gives_the_checkers_bytes(oracle, ta, tb):
+    """The CPU-baseline build of the reference-order cgemm (no volatile stores,
+    vectorised) computes the same bytes as the checker build."""
+    m, n, k = 97, 61, 130
+    al, be = complex(0.7, 0.3), complex(-1.0, 0.5)
+    ar, ac = oracle.stored_shape(ta, m, k)
+    br, bc = oracle.stored_shape(tb, k, n)
+    a = oracle.make_matrix(ar, ac, ar + 3, "UNIFORM_1", 11)
+    b = oracle.make_matrix(br, bc, br + 1, "UNIFORM_1", 12)
+    c = oracle.make_matrix(m, n, m + 2, "UNIFORM_1", 13)
+    c1, c2 = c.copy(), c.copy()
+    oracle.cgemm(ta, tb, m, n, k, al, a, ar + 3, b, br + 1, be, c1, m + 2)
+    oracle.cgemm_timing(ta, tb, m, n, k, al, a, ar + 3, b, br + 1, be, c2, m + 2)
+    assert c1.tobytes() == c2.tobytes()

@@ -55,6 +55,81 @@ def test_no_alloc_matches_drop_in_twice(cg3m, oracle, cuda):
         assert got.tobytes() == expect.tobytes()
 
 
+# Shapes whose plan puts packed planes (and split partials) in the fixed array:
+# config 1's 512^3 (K split merged in the GEMM's cluster), a fused square, a
+# conjugated split, and a long-K split whose partials go through the merge
+# kernel.
+SCRATCH_CASES = [
+    ("N", "N", 512, 512, 512, complex(1.5, -0.5), complex(0.25, 0.75)),
+    ("N", "N", 1024, 1024, 1024, 1.0, 0.0),
+    ("C", "N", 700, 600, 900, complex(0.7, 0.3), complex(-1.0, 0.5)),
+    ("N", "T", 64, 64, 16384, complex(0.5, 0.5), 0.0),
+]
+
+
+@pytest.mark.parametrize("ta,tb,m,n,k,alpha,beta", SCRATCH_CASES)
+def test_no_alloc_uses_its_scratch_and_matches_drop_in(cg3m, oracle, cuda, ta, tb, m, n, k, alpha, beta):
+    """The planner puts this call's packed planes (and any partials) in the
+    fixed array; two calls in a row give the drop-in's bytes."""
+    import torch
+
+    plan = cg3m.plan(ta, tb, m, n, k, alpha, beta)
+    assert plan["path"] in (2, 3) and 0 < plan["workspace_bytes"] <= (32 << 20) - 256
+    ar, ac = oracle.stored_shape(ta, m, k)
+    br, bc = oracle.stored_shape(tb, k, n)
+    lda, ldb, ldc = ar, br, m + 3
+    a = oracle.make_matrix(ar, ac, lda, "UNIFORM_1", 41)
+    b = oracle.make_matrix(br, bc, ldb, "UNIFORM_1", 42)
+    c = oracle.make_matrix(m, n, ldc, "UNIFORM_1", 43)
+    A = torch.from_numpy(a).to(cuda)
+    B = torch.from_numpy(b).to(cuda)
+    h = cg3m.Handle(stream=torch.cuda.current_stream().cuda_stream)
+    C_ref = torch.from_numpy(c.copy()).to(cuda)
+    assert h.cgemm3m(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C_ref, ldc, raw=True) == cg3m.SUCCESS
+    torch.cuda.synchronize()
+    expect = C_ref.cpu().numpy()
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        C = torch.from_numpy(c.copy()).to(cuda)
+        st = _call_no_alloc(cg3m, stream, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc)
+        torch.cuda.synchronize()
+        assert st == cg3m.SUCCESS
+        assert C.cpu().numpy().tobytes() == expect.tobytes()
+    flags = ctypes.c_int(-1)
+    assert cg3m.lib.cg3mGetDeviceStatus(None, ctypes.byref(flags)) == cg3m.SUCCESS
+    assert flags.value == 0
+
+
+def test_no_alloc_status_word_reports_a_wait_that_gave_up(cg3m, oracle, cuda):
+    """A bounded wait that runs out sets the allocation-free entry point's
+    status word; cg3mGetDeviceStatus(NULL) reports it once and clears it, and
+    the next call is unaffected."""
+    import torch
+
+    gave_up = ctypes.c_int(0)
+    assert cg3m.lib.cg3mDiagBoundedWait(None, 1_000_000, ctypes.byref(gave_up)) == cg3m.SUCCESS
+    assert gave_up.value == 1
+    flags = ctypes.c_int(0)
+    assert cg3m.lib.cg3mGetDeviceStatus(None, ctypes.byref(flags)) == cg3m.SUCCESS
+    assert flags.value == 1
+    assert cg3m.lib.cg3mGetDeviceStatus(None, ctypes.byref(flags)) == cg3m.SUCCESS
+    assert flags.value == 0
+    m = n = k = 512
+    a = oracle.make_matrix(m, k, m, "UNIFORM_1", 51)
+    b = oracle.make_matrix(k, n, k, "UNIFORM_1", 52)
+    A, B = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda)
+    C = torch.zeros(m * n, dtype=torch.complex64, device=cuda)
+    st = _call_no_alloc(cg3m, torch.cuda.current_stream().cuda_stream, "N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)
+    torch.cuda.synchronize()
+    assert st == cg3m.SUCCESS
+    model = np.zeros(m * n, np.complex64)
+    oracle.cgemm3m_fp32_model("N", "N", m, n, k, 1.0, a, m, b, k, 0.0, model, m,
+                              span=cg3m.plan("N", "N", m, n, k)["k_span"])
+    assert C.cpu().numpy().tobytes() == model.tobytes()
+    assert cg3m.lib.cg3mGetDeviceStatus(None, ctypes.byref(flags)) == cg3m.SUCCESS
+    assert flags.value == 0
+
+
 def test_no_alloc_rejects_oversized_problem(cg3m, cuda):
     import torch
 

@@ -190,11 +190,12 @@ class Handle:
         """Counters of the last call's rounding pass (synchronizes): flagged
         outputs, those recomputed by the tile kernels and those recomputed one
         by one; None when the last call ran no rounding pass."""
-        v = (ctypes.c_longlong * 3)()
-        _check(_lib.cg3mGetRoundingStats(self.h, v, 3), "cg3mGetRoundingStats")
+        v = (ctypes.c_longlong * 5)()
+        _check(_lib.cg3mGetRoundingStats(self.h, v, 5), "cg3mGetRoundingStats")
         if v[0] < 0:
             return None
-        return {"flagged": v[0], "dense_outputs": v[1], "sparse_outputs": v[2]}
+        return {"flagged": v[0], "dense_outputs": v[1], "sparse_outputs": v[2], "fallback_outputs": v[3],
+                "exact_tiles": v[4]}
 
     def cgemm3m(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, form="fp32", rounding="auto",
                 k_partitions=0, raw=False, tc_segment=0, engine="auto", onchip_tile=0):
@@ -346,7 +347,8 @@ def stage_names(info):
         return ["onchip"][:k]
     if info["rounding"]:
         fp32 = info["form"] == FORM["fp32"]
-        tail = ["replay_tiles", "replay_outputs"] if fp32 else ["recompute_fp64_tiles", "recompute_fp64_outputs"]
+        tail = ["replay_tiles", "replay_outputs"] if fp32 else \
+            ["exact_split", "exact_tiles", "recompute_fp64_outputs", "fallback_fp64"]
         names = ["pack", "gemm_path", "pack_rows", "energy", "select"] + tail
     else:
         names = ["pack", "gemm", "merge"]

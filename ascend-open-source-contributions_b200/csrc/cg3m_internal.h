@@ -97,8 +97,45 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
                             const std::function<void(int)>& mark);
 // GEMM that also writes the risk plane used by the rounding-correction pass.
 cudaError_t launch_gemm_with_path(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
+// Rounding pass: a 16 x 16 tile with more flagged outputs than this is
+// recomputed as part of a tile; sparser tiles have each flagged output
+// recomputed on its own.  Counters it leaves beside the flags:
+constexpr uint32_t kSparseMax = 64;
+enum : int {
+    kStatFlagged = 0,
+    kStatDenseOutputs = 1,
+    kStatSparseOutputs = 2,
+    kStatFallback = 3,
+    kStatExactTiles = 4,
+    kStatWords = 8
+};
+
+// Output rows and columns of the exact recompute's tile: it runs on every
+// such tile holding a 16 x 16 tile with more than kSparseMax flagged outputs.
+constexpr int kOzakiTile = 256;
+
+// Slices, exponents and FP64 partial sums of the tensor-core forms' exact
+// recompute (ozaki.cu), carved from the rounding region.
+struct OzLayout {
+    int* E = nullptr;          // op(A) row exponents
+    int* F = nullptr;          // op(B) column exponents
+    int8_t* planes_a = nullptr;
+    int8_t* planes_b = nullptr;
+    double2* partial = nullptr;
+    int kpitch = 0;
+    size_t plane_bytes = 0;
+    size_t bytes = 0;
+};
+OzLayout oz_layout(int n, uint8_t* base);
+// Slices op(A) rows and op(B) columns, then recomputes the flagged outputs of
+// every tile holding a dense 16 x 16 tile; outputs it cannot certify are
+// marked in fallback_bits.  mark(i) after the i-th launch (1-based).
+cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a, const float2* rows_b,
+                         const OzLayout& L, const uint32_t* flag_bits, const uint32_t* tile_count, uint32_t* stats,
+                         uint32_t* fallback_bits, float2* C, int* status, int* launched,
+                         const std::function<void(int)>& mark);
 // Bytes of the rounding-correction region for a square problem of order n.
-size_t rounding_bytes(int n);
+size_t rounding_bytes(int n, int form);
 // Device address of the pass's counters (flagged, recomputed as tiles, one by
 // one) inside a planned call's workspace.
 uint32_t* rounding_stats_ptr(const Plan& plan, void* ws, int n);

@@ -393,7 +393,7 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     }
     out.round_off = off;
     if (out.rounding) {
-        off = align_up(off + rounding_bytes(p.n), kRegionAlign);  // layout in rounding.cu
+        off = align_up(off + rounding_bytes(p.n, out.form), kRegionAlign);  // layout in rounding.cu
     }
     out.total = off;
     *plan = out;

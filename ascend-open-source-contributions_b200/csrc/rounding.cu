@@ -16,17 +16,19 @@
 //   4. recompute (:192-404) each flagged output again, in a fixed order.
 // B200 design: one CTA of 64 threads per row for the energies (the row is
 // staged in shared memory; span is odd so the strided lane reads are
-// conflict-free); a grid-stride select that sets one bit per flagged output
-// and one word per 16 x 16 output tile (each flagged output is recomputed
-// independently, so no ordering is needed to keep the result bits fixed); the
-// recompute works on
-// output tiles so operand rows are staged once per tile instead of once per
-// output, and skips tiles with no flagged output.  FP32 form: the reference's
-// segmented replay over 16 x 16 tiles, 2 x 2 outputs per thread for 8 of the
-// 64 lanes, with the 64 lane sums in shared memory and the lane reductions
-// and the inclusive lane scan in fixed orders.  Tensor-core forms: flagged
-// outputs are recomputed in FP64 over 64 x 128 tiles (K in order) and rounded
-// once to FP32.
+// conflict-free); a grid-stride select in which each warp writes one 32-bit
+// word of the flag bitmap (its ballot) and adds its flags to a count per
+// 16 x 16 output tile.  The recompute then splits by density, on the device,
+// from those counts: a tile with more than kSparseMax flagged outputs is
+// recomputed as a tile (operands staged once for all its outputs), every other
+// flagged output on its own by a 64-thread block (recompute_sparse), so a
+// handful of flags no longer costs a whole tile.  FP32 form: the reference's
+// segmented replay, bit for bit -- over 16 x 16 tiles with 2 x 2 outputs per
+// thread for 8 of the 64 lanes, or one lane per thread for a single output.
+// Tensor-core forms: flagged outputs come back within one FP32 rounding of
+// the exact product -- exact int8 slice products on the tensor cores for
+// 256 x 256 tiles holding a dense 16 x 16 tile (ozaki.cu), FP64 for sparse
+// tiles and for the few outputs the slice products cannot certify.
 #include <cstring>
 #include <functional>
 
@@ -47,12 +49,6 @@ constexpr int kLanes = 64;
 constexpr int kTile = 16;             // flag granule: 16 x 16 outputs
 constexpr int kMaxSpan = 65;          // ceil(4096/64) | 1
 constexpr float kConfidence = 3.75f;  // CGEMM_ROUNDING_CONFIDENCE, cgemm_host.cpp:37
-// A 16 x 16 tile with more flagged outputs than this is recomputed as a tile
-// (operands staged once for all its outputs); sparser tiles have each flagged
-// output recomputed on its own, so a handful of flags no longer costs a tile.
-constexpr uint32_t kSparseMax = 64;
-// Counters the pass leaves beside the flags (cg3mGetRoundingStats).
-enum : int { kStatFlagged = 0, kStatDenseOutputs = 1, kStatSparseOutputs = 2, kStatWords = 8 };
 
 // ---- 2. energies ----------------------------------------------------------------
 
@@ -487,145 +483,17 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constan
     }
 }
 
-// ---- 4b. FP64 recompute (tensor-core forms) -----------------------------------------
-
-// FP64 product of one 64 x 128 output tile (each thread 4 x 8 outputs, K in
-// order), computed only when one of its 16 x 16 flag granules is set; flagged
-// outputs are rounded once to FP32 and written.  Per K term a thread reads 12
-// complex operands for 32 complex products (128 DFMA): 1.5 bytes of shared
-// memory per DFMA, below the rate at which the FP64 pipe consumes them.
-constexpr int kT64 = 64;    // tile rows (op(A) rows)
-constexpr int kT128 = 128;  // tile columns (op(B) columns)
-
-// Operand slabs of 16 K terms, converted to FP64 once while staging (each
-// value feeds 16 threads), double-buffered with the next slab held in
-// registers during the current slab's DFMAs.
-constexpr size_t kFp64SlabX = (size_t)16 * kT64;   // double2 per buffer, op(A)
-constexpr size_t kFp64SlabY = (size_t)16 * kT128;  // double2 per buffer, op(B)
-constexpr size_t kFp64Smem = 2 * (kFp64SlabX + kFp64SlabY) * sizeof(double2);
-
-__global__ void __launch_bounds__(256, 1) recompute_fp64_tiled(int n, int pitch, const float2* __restrict__ rows_a,
-                                                            const float2* __restrict__ rows_b,
-                                                            const uint32_t* __restrict__ flag_bits,
-                                                            const uint32_t* __restrict__ tile_count,
-                                                            uint32_t* __restrict__ stats,
-                                                            float2* __restrict__ C)
-{
-    extern __shared__ __align__(16) double2 slabs[];  // [buffer][x: 16 x 64 | y: 16 x 128]
-    const int tiles16 = (n + kTile - 1) / kTile;
-    const int tiles_i = (n + kT64 - 1) / kT64;
-    const int i0 = (blockIdx.x % tiles_i) * kT64, j0 = (blockIdx.x / tiles_i) * kT128;
-    // Recomputed as a tile when any of its 16 x 16 tiles is dense; then every
-    // flagged output of the tile is written here (recompute_sparse skips it).
-    bool dense = false;
-    uint32_t flagged_here = 0;
-    for (int q = 0; q < (kT64 / kTile) * (kT128 / kTile); ++q) {
-        const int gi = i0 / kTile + (q & 3), gj = j0 / kTile + (q >> 2);
-        if (gi < tiles16 && gj < tiles16) {
-            const uint32_t c = tile_count[gj * tiles16 + gi];
-            dense |= c > kSparseMax;
-            flagged_here += c;
-        }
-    }
-    if (!dense) {
-        return;
-    }
-    const int tid = threadIdx.x;
-    if (tid == 0) {
-        atomicAdd(&stats[kStatDenseOutputs], flagged_here);
-    }
-    // Thread (ti, tj) owns rows ti + 16a (a < 4) and columns tj + 16b (b < 8):
-    // for a fixed a the 16 row values a warp reads are 256 consecutive bytes.
-    const int ti = tid & 15, tj = tid >> 4;
-    double ar[4][8], ai[4][8];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            ar[a][b] = 0.0;
-            ai[a][b] = 0.0;
-        }
-    // Element e = tid + 256*u of a slab: row r = e >> 4, K offset q = e & 15
-    // (4 elements per thread of the op(A) slab, 8 of the op(B) slab).
-    float2 vx[4], vy[8];
-    auto load = [&](int k0) {
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int e = tid + 256 * u;
-            const int r = e >> 4, q = e & 15;
-            const int k = k0 + q;
-            if (u < 4) {
-                vx[u] = (k < n && i0 + r < n) ? rows_a[(size_t)(i0 + r) * pitch + k] : make_float2(0.0f, 0.0f);
-            }
-            vy[u] = (k < n && j0 + r < n) ? rows_b[(size_t)(j0 + r) * pitch + k] : make_float2(0.0f, 0.0f);
-        }
-    };
-    load(0);
-    const int slabs_n = (n + 15) / 16;
-    for (int t = 0; t < slabs_n; ++t) {
-        double2* xs = slabs + (size_t)(t & 1) * (kFp64SlabX + kFp64SlabY);
-        double2* ys = xs + kFp64SlabX;
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int e = tid + 256 * u;
-            const int r = e >> 4, q = e & 15;
-            if (u < 4) {
-                xs[q * kT64 + r] = make_double2((double)vx[u].x, (double)vx[u].y);
-            }
-            ys[q * kT128 + r] = make_double2((double)vy[u].x, (double)vy[u].y);
-        }
-        // Buffer t&1 was last read in slab t-2; this barrier also orders slab
-        // t-1's reads before slab t+1's writes.
-        __syncthreads();
-        if (t + 1 < slabs_n) {
-            load((t + 1) * 16);
-        }
-#pragma unroll 1
-        for (int q = 0; q < 16; ++q) {
-            double2 x[4], y[8];
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                x[a] = xs[q * kT64 + ti + 16 * a];
-            }
-#pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                y[b] = ys[q * kT128 + tj + 16 * b];
-            }
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 8; ++b) {
-                    ar[a][b] = fma(x[a].x, y[b].x, fma(-x[a].y, y[b].y, ar[a][b]));
-                    ai[a][b] = fma(x[a].x, y[b].y, fma(x[a].y, y[b].x, ai[a][b]));
-                }
-        }
-    }
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-        const int j = j0 + tj + 16 * b;
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int i = i0 + ti + 16 * a;
-            if (i < n && j < n) {
-                const size_t idx = (size_t)j * n + i;
-                if (flagged(flag_bits, idx)) {
-                    C[idx] = make_float2((float)ar[a][b], (float)ai[a][b]);
-                }
-            }
-        }
-    }
-}
-
 // ---- 4c. per-output recompute of sparse tiles ----------------------------------
 
-// Whether the 64 x 128 FP64 recompute tile holding 16 x 16 tile (gi, gj) runs
-// as a tile (recompute_fp64_tiled's predicate).
-__device__ __forceinline__ bool fp64_tile_dense(const uint32_t* tile_count, int tiles16, int gi, int gj)
+// Whether the exact (int8 slice) recompute tile holding 16 x 16 tile (gi, gj)
+// runs, i.e. holds a dense 16 x 16 tile (ozaki_pair_kernel's predicate).
+__device__ __forceinline__ bool ozaki_tile_dense(const uint32_t* tile_count, int tiles16, int gi, int gj)
 {
-    const int bi = gi / (kT64 / kTile) * (kT64 / kTile), bj = gj / (kT128 / kTile) * (kT128 / kTile);
+    constexpr int G = kOzakiTile / kTile;
+    const int bi = gi / G * G, bj = gj / G * G;
     bool dense = false;
-    for (int q = 0; q < (kT64 / kTile) * (kT128 / kTile); ++q) {
-        const int qi = bi + q % (kT64 / kTile), qj = bj + q / (kT64 / kTile);
+    for (int q = 0; q < G * G; ++q) {
+        const int qi = bi + q % G, qj = bj + q / G;
         if (qi < tiles16 && qj < tiles16) {
             dense |= tile_count[qj * tiles16 + qi] > kSparseMax;
         }
@@ -651,9 +519,12 @@ __device__ __forceinline__ void lane_reduce_shared(float* v, int l)
     }
 }
 
-// One block of 64 threads per 16 x 16 output tile that holds between 1 and
-// kSparseMax flagged outputs (and, for the FP64 recompute, lies in no dense
-// 64 x 128 tile).  Its flagged outputs are recomputed one after another: the
+// Per-output recompute, one block of 64 threads per 16 x 16 output tile.
+//   kSparseFp32 / kSparseFp64: tiles holding between 1 and kSparseMax
+//     flagged outputs (FP64: outside every tile the exact recompute takes);
+//   kFallbackFp64: the outputs the exact recompute marked in `bits` (a
+//     non-finite operand, or a result it could not certify).
+// The tile's outputs are recomputed one after another: the
 // output's op(A) row and op(B) column are staged in shared memory, then
 //   FP32 (FastSegmentDot, cgemm3m_rounding_kernel.cpp:264-309): thread l is
 //     K lane l (k in [l*span, (l+1)*span)); its direct sum, the pairwise lane
@@ -664,14 +535,17 @@ __device__ __forceinline__ void lane_reduce_shared(float* v, int l)
 //     sums are reduced in FP64 and the result is rounded once to FP32.
 // Staged reads: thread l reads element l*span + s, so a warp's 8-byte reads
 // fall in distinct bank pairs (span is odd).
-template <bool FP64>
+enum { kSparseFp32 = 0, kSparseFp64 = 1, kFallbackFp64 = 2 };
+
+template <int MODE>
 __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int span,
                                                           const float2* __restrict__ rows_a,
                                                           const float2* __restrict__ rows_b,
-                                                          const uint32_t* __restrict__ flag_bits,
+                                                          const uint32_t* __restrict__ bits,
                                                           const uint32_t* __restrict__ tile_count,
                                                           uint32_t* __restrict__ stats, float2* __restrict__ C)
 {
+    constexpr bool FP64 = MODE != kSparseFp32;
     extern __shared__ __align__(16) float2 vec[];  // op(A) row at [0, pitch), op(B) column at [pitch, 2 pitch)
     __shared__ float sr[kLanes], si[kLanes], tr[kLanes], ti[kLanes];
     __shared__ double dr[kLanes], di[kLanes];
@@ -681,27 +555,37 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
     const int tiles = (n + kTile - 1) / kTile;
     const int gi = blockIdx.x % tiles, gj = blockIdx.x / tiles;
     const uint32_t count = tile_count[(size_t)gj * tiles + gi];
-    if (count == 0 || count > kSparseMax) {
+    if (count == 0) {
         return;
     }
-    if (FP64 && fp64_tile_dense(tile_count, tiles, gi, gj)) {
+    if (MODE != kFallbackFp64 && count > kSparseMax) {
+        return;
+    }
+    // The exact recompute writes (or marks) every flagged output of its tiles.
+    const bool in_exact_tile = FP64 && ozaki_tile_dense(tile_count, tiles, gi, gj);
+    if ((MODE == kSparseFp64 && in_exact_tile) || (MODE == kFallbackFp64 && !in_exact_tile)) {
         return;
     }
     const int l = threadIdx.x;
     const int i0 = gi * kTile, j0 = gj * kTile;
     if (l == 0) {
         listed = 0;
-        atomicAdd(&stats[kStatSparseOutputs], count);
     }
     __syncthreads();
     for (int o = l; o < kTile * kTile; o += kLanes) {
         const int i = i0 + o % kTile, j = j0 + o / kTile;
-        if (i < n && j < n && flagged(flag_bits, (size_t)j * n + i)) {
+        if (i < n && j < n && flagged(bits, (size_t)j * n + i)) {
             list[atomicAdd(&listed, 1)] = o;
         }
     }
     __syncthreads();
     const int outputs = listed;
+    if (outputs == 0) {
+        return;
+    }
+    if (l == 0 && MODE != kFallbackFp64) {
+        atomicAdd(&stats[kStatSparseOutputs], (uint32_t)outputs);
+    }
     const int kbeg = min(n, l * span), kend = min(n, kbeg + span);
     for (int u = 0; u < outputs; ++u) {
         const int o = list[u];
@@ -829,7 +713,9 @@ static float bridge_term(int n)
 // Layout of the rounding region (Plan::round_off): path n^2 floats | rows of
 // op(A) n^2 complex | columns of op(B) n^2 complex | energies 2n floats |
 // flags: one bit per output (written whole by the selection), then one count
-// per 16 x 16 tile and kStatWords counters (zeroed before every selection).
+// per 16 x 16 tile, kStatWords counters and the exact recompute's fallback
+// bits (one per output), all zeroed before every selection | tensor-core
+// forms: the exact recompute's slices and partial sums (OzLayout).
 struct RoundLayout {
     float* path;
     float2* rows_a;
@@ -838,7 +724,9 @@ struct RoundLayout {
     uint32_t* flag_bits;
     uint32_t* tile_count;
     uint32_t* stats;
-    size_t zero_bytes;  // tile_count + stats, one memset
+    uint32_t* fallback_bits;
+    size_t zero_bytes;  // tile_count + stats + fallback_bits, one memset
+    OzLayout oz;
 };
 
 static size_t flag_words(int n) { return ((size_t)n * n + 31) / 32; }
@@ -871,13 +759,18 @@ static RoundLayout round_layout(const Plan& plan, void* ws, int n)
     L.flag_bits = reinterpret_cast<uint32_t*>(b + off);
     L.tile_count = L.flag_bits + flag_words(n);
     L.stats = L.tile_count + tile_words(n);
-    L.zero_bytes = (tile_words(n) + kStatWords) * 4;
+    L.fallback_bits = L.stats + kStatWords;
+    L.zero_bytes = (tile_words(n) + kStatWords + flag_words(n)) * 4;
+    off = align_up(off + (2 * flag_words(n) + tile_words(n) + kStatWords) * 4, kRegionAlign);
+    if (plan.form != CG3M_FORM_FP32) {
+        L.oz = oz_layout(n, b + off);
+    }
     return L;
 }
 
 uint32_t* rounding_stats_ptr(const Plan& plan, void* ws, int n) { return round_layout(plan, ws, n).stats; }
 
-size_t rounding_bytes(int n)
+size_t rounding_bytes(int n, int form)
 {
     const size_t nn = (size_t)n * n;
     const size_t rows = (size_t)n * row_pitch(n);
@@ -886,7 +779,10 @@ size_t rounding_bytes(int n)
     off = align_up(off + rows * 8, kRegionAlign);
     off = align_up(off + rows * 8, kRegionAlign);
     off = align_up(off + (size_t)2 * n * 4, kRegionAlign);
-    off = align_up(off + (flag_words(n) + tile_words(n) + kStatWords) * 4, kRegionAlign);
+    off = align_up(off + (2 * flag_words(n) + tile_words(n) + kStatWords) * 4, kRegionAlign);
+    if (form != CG3M_FORM_FP32) {
+        off += oz_layout(n, nullptr).bytes;
+    }
     return off;
 }
 
@@ -963,37 +859,43 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
         mark(++count);
     }
     // Dense tiles, then the flagged outputs of sparse tiles one by one; both
-    // kernels read the same per-tile counts, so each flagged output is
-    // recomputed by exactly one of them.
-    if (err == cudaSuccess) {
-        if (plan.form == CG3M_FORM_FP32) {
-            err = launch_replay<kChunkMin>(s, n, span, L, static_cast<float2*>(p.C), status);
-        } else {
-            const int tiles = ((n + kT64 - 1) / kT64) * ((n + kT128 - 1) / kT128);
-            err = cudaFuncSetAttribute(recompute_fp64_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kFp64Smem);
-            if (err == cudaSuccess) {
-                recompute_fp64_tiled<<<tiles, 256, kFp64Smem, s>>>(n, pitch, L.rows_a, L.rows_b, L.flag_bits,
-                                                                   L.tile_count, L.stats, static_cast<float2*>(p.C));
-            }
-        }
-        if (err == cudaSuccess) {
-            err = cudaGetLastError();
+    // read the same per-tile counts, so each flagged output is recomputed by
+    // exactly one of them.
+    const int tiles16 = (n + kTile - 1) / kTile;
+    const size_t smem = (size_t)2 * pitch * sizeof(float2);
+    float2* C = static_cast<float2*>(p.C);
+    auto sparse = [&](auto kernel, const uint32_t* bits) {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) {
+            kernel<<<tiles16 * tiles16, kLanes, smem, s>>>(n, pitch, span, L.rows_a, L.rows_b, bits, L.tile_count,
+                                                           L.stats, C);
+            e = cudaGetLastError();
         }
         mark(++count);
-    }
-    if (err == cudaSuccess) {
-        const int tiles16 = (n + kTile - 1) / kTile;
-        const size_t smem = (size_t)2 * pitch * sizeof(float2);
-        const bool fp64 = plan.form != CG3M_FORM_FP32;
-        auto kernel = fp64 ? recompute_sparse<true> : recompute_sparse<false>;
-        err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return e;
+    };
+    if (plan.form == CG3M_FORM_FP32) {
         if (err == cudaSuccess) {
-            kernel<<<tiles16 * tiles16, kLanes, smem, s>>>(n, pitch, span, L.rows_a, L.rows_b, L.flag_bits,
-                                                           L.tile_count, L.stats, static_cast<float2*>(p.C));
-            err = cudaGetLastError();
+            err = launch_replay<kChunkMin>(s, n, span, L, C, status);
+            mark(++count);
         }
-        mark(++count);
+        if (err == cudaSuccess) {
+            err = sparse(recompute_sparse<kSparseFp32>, L.flag_bits);
+        }
+    } else {
+        if (err == cudaSuccess) {
+            int oz_launched = 0;
+            const int before = count;
+            err = launch_ozaki(s, n, pitch, L.rows_a, L.rows_b, L.oz, L.flag_bits, L.tile_count, L.stats,
+                               L.fallback_bits, C, status, &oz_launched, [&](int i) { mark(before + i); });
+            count += oz_launched;
+        }
+        if (err == cudaSuccess) {
+            err = sparse(recompute_sparse<kSparseFp64>, L.flag_bits);
+        }
+        if (err == cudaSuccess) {
+            err = sparse(recompute_sparse<kFallbackFp64>, L.fallback_bits);
+        }
     }
     if (launched != nullptr) {
         *launched = count;

@@ -62,7 +62,9 @@ typedef enum { CG3M_FORM_FP32 = 0, CG3M_FORM_TF32X3 = 1, CG3M_FORM_BF16X6 = 2, C
  * cgemm_host.cpp:234-238).
  *   AUTO -- as the reference: only for m==n==k in [2048,4096], lda==ldb==ldc==m,
  *           alpha==1, beta==0.  Flagged outputs are recomputed in FP32 fixed
- *           order (FP32 form) or in FP64 (tensor-core forms).
+ *           order (FP32 form, the reference's replay bit for bit) or to within
+ *           one FP32 rounding of the exact product (tensor-core forms: exact
+ *           int8 slice products on the tensor cores, FP64 where needed).
  *   OFF  -- never. */
 typedef enum { CG3M_ROUNDING_AUTO = 0, CG3M_ROUNDING_OFF = 1 } cg3mRounding_t;
 
@@ -229,9 +231,11 @@ cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t handle, int* flags);
 /* Counters of the rounding-correction pass of the last call made through the
  * handle (synchronizes its stream): stats[0] = outputs flagged, stats[1] =
  * flagged outputs recomputed by the tile kernels (16 x 16 tiles holding more
- * than 64 flagged outputs; FP64 form: their 64 x 128 tiles), stats[2] =
- * flagged outputs recomputed one by one (the other tiles); entries past 2
- * are reserved.  All -1 when that call ran no rounding pass.  Valid until the
+ * than 64 flagged outputs; tensor-core forms: every 256 x 256 tile holding
+ * one), stats[2] = flagged outputs recomputed one by one (the other tiles),
+ * stats[3] = tensor-core forms: outputs of those tiles the int8 slice
+ * products could not certify, recomputed in FP64, stats[4] = 256 x 256 tiles
+ * run on the int8 slice products; entries past 4 are reserved.  All -1 when that call ran no rounding pass.  Valid until the
  * next call through the handle (the counters live in its workspace). */
 cg3mStatus_t cg3mGetRoundingStats(cg3mHandle_t handle, long long* stats, int count);
 

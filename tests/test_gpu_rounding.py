@@ -107,6 +107,8 @@ def test_rounding_pass_sparse_and_dense_tiles(cg3m, oracle, cuda, h, form):
     st = h.rounding_stats()
     assert st["dense_outputs"] > 0 and st["sparse_outputs"] > 0
     assert st["dense_outputs"] + st["sparse_outputs"] == st["flagged"]
+    if form != "fp32":
+        assert st["exact_tiles"] > 0 and st["fallback_outputs"] <= st["dense_outputs"]
     e = oracle.energy(n, "N", "N", a, n, b, n)
     rows = np.r_[0:8, 96:104, 770:780, n - 8:n]
     cols = np.r_[0:6, 156:170, 1500:1506, n - 6:n]
@@ -183,6 +185,10 @@ def test_tc_rounding_pass_recomputes_in_fp64(cg3m, oracle, cuda, h, form):
     info = h.cgemm3m("N", "N", N, N, N, 1.0, A, N, B, N, 0.0, C, N, form=form)
     assert info["rounding"] == 1
     on = h.error_report(N, N, C, N, ref)
+    st = h.rounding_stats()
+    # every 256 x 256 tile is dense on this data: int8 slice products, few fallbacks
+    assert st["exact_tiles"] == (N // 256) ** 2 and st["sparse_outputs"] == 0
+    assert st["fallback_outputs"] < 0.05 * st["flagged"]
     got_on = C.clone()
     h.cgemm3m("N", "N", N, N, N, 1.0, A, N, B, N, 0.0, C, N, form=form, rounding="off")
     off = h.error_report(N, N, C, N, ref)

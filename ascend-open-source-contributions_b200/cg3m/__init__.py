@@ -93,6 +93,7 @@ SIGNATURES = {
     "cg3mBatchPlanDescribe": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "cg3mGetDeviceStatus": [_P, ctypes.POINTER(_I)],
     "cg3mDiagFailAllocations": [_I],
+    "cg3mDiagGuardStatus": [ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "cg3mGetRoundingStats": [_P, ctypes.POINTER(ctypes.c_longlong), _I],
     "cg3mDiagBoundedWait": [_P, ctypes.c_longlong, ctypes.POINTER(_I)],
     "cg3mCgemm3mNoAlloc": [_P, _I, _I, _I, _I, _I, _CP, _P, _I, _P, _I, _CP, _P, _I],

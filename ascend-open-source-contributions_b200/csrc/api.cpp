@@ -213,6 +213,12 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
             cudaEventRecord(events[i], s);
         }
     };
+    if (plan.guards > 0) {
+        const cudaError_t e = fill_guards(s, ws, plan.guard_off, plan.guards);
+        if (e != cudaSuccess) {
+            return e;
+        }
+    }
     mark(0);
     if (plan.engine == 2) {
         const cudaError_t e = launch_single(s, p, 0, 0, plan.onchip_tile, plan.parts);
@@ -242,6 +248,9 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
         const int before = count;
         err = launch_rounding(s, p, plan, ws, status, &launched, [&](int i) { mark(before + i); });
         count += launched;
+    }
+    if (err == cudaSuccess && plan.guards > 0) {
+        err = check_guards(s, ws, plan.guard_off, plan.guards);
     }
     if (kernels != nullptr) {
         *kernels = count;
@@ -750,6 +759,19 @@ cg3mStatus_t cg3mGetRoundingStats(cg3mHandle_t h, long long* stats, int count)
         stats[i] = (long long)v[i];
     }
     return CG3M_STATUS_SUCCESS;
+}
+
+cg3mStatus_t cg3mDiagGuardStatus(int* enabled, int* damaged)
+{
+    if (enabled == nullptr || damaged == nullptr) {
+        return CG3M_STATUS_INVALID_VALUE;
+    }
+    *enabled = guard_bands_on() ? 1 : 0;
+    *damaged = 0;
+    if (!guard_bands_on()) {
+        return CG3M_STATUS_SUCCESS;
+    }
+    return read_guard_damage(damaged) == cudaSuccess ? CG3M_STATUS_SUCCESS : CG3M_STATUS_EXECUTION_FAILED;
 }
 
 cg3mStatus_t cg3mDiagFailAllocations(int count)

@@ -8,6 +8,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <functional>
+#include <vector>
 
 #include "../../include/cg3m.h"
 
@@ -61,6 +62,10 @@ struct Plan {
     size_t plane_a_elems = 0, plane_b_elems = 0;
     size_t partial_plane_elems = 0;
     int partial_pitch = 0;
+    // guard-band offsets from the workspace base (guard bands on only)
+    static constexpr int kMaxGuards = 24;
+    size_t guard_off[kMaxGuards] = {};
+    int guards = 0;
 };
 
 struct Problem {
@@ -126,7 +131,7 @@ struct OzLayout {
     size_t plane_bytes = 0;
     size_t bytes = 0;
 };
-OzLayout oz_layout(int n, uint8_t* base);
+OzLayout oz_layout(int n, uint8_t* base, std::vector<size_t>* guards = nullptr);
 // Slices op(A) rows and op(B) columns, then recomputes the flagged outputs of
 // every tile holding a dense 16 x 16 tile; outputs it cannot certify are
 // marked in fallback_bits.  mark(i) after the i-th launch (1-based).
@@ -135,7 +140,7 @@ cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a,
                          uint32_t* fallback_bits, float2* C, int* status, int* launched,
                          const std::function<void(int)>& mark);
 // Bytes of the rounding-correction region for a square problem of order n.
-size_t rounding_bytes(int n, int form);
+size_t rounding_bytes(int n, int form, std::vector<size_t>* guards = nullptr);
 // Device address of the pass's counters (flagged, recomputed as tiles, one by
 // one) inside a planned call's workspace.
 uint32_t* rounding_stats_ptr(const Plan& plan, void* ws, int n);
@@ -186,6 +191,33 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
                     const cudaEvent_t* events = nullptr, int nevents = 0);
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Guard bands (diagnostics, the memory-safety check of the test suite): with
+// CG3M_GUARD_BANDS set in the environment when the library loads, every
+// workspace region is followed by kGuardBytes of a fixed byte pattern that
+// each call fills before its first kernel and checks after its last
+// (cg3mDiagGuardStatus reports a damaged band).  Off by default: no bands.
+constexpr size_t kGuardBytes = 4096;
+constexpr unsigned char kGuardByte = 0xA5;
+bool guard_bands_on();
+// End of a region of `bytes` bytes starting at `off`: aligned to kRegionAlign
+// and, with guard bands on, followed by a band whose offset goes to *guards.
+inline size_t next_region(size_t off, size_t bytes, std::vector<size_t>* guards)
+{
+    size_t end = align_up(off + bytes, kRegionAlign);
+    if (bytes != 0 && guard_bands_on()) {
+        if (guards != nullptr) {
+            guards->push_back(end);
+        }
+        end += kGuardBytes;
+    }
+    return end;
+}
+// Fills (before) and checks (after) a call's guard bands on stream s.
+cudaError_t fill_guards(cudaStream_t s, void* ws, const size_t* offs, int count);
+cudaError_t check_guards(cudaStream_t s, const void* ws, const size_t* offs, int count);
+// Synchronizes the device, returns and clears the damaged-band flag.
+cudaError_t read_guard_damage(int* damaged);
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
 }  // namespace cg3m

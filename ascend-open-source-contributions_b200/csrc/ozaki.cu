@@ -467,22 +467,22 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 
 }  // namespace
 
-OzLayout oz_layout(int n, uint8_t* base)
+OzLayout oz_layout(int n, uint8_t* base, std::vector<size_t>* guards)
 {
     OzLayout L;
     L.kpitch = (n + 63) / 64 * 64;
     L.plane_bytes = (size_t)n * L.kpitch;
     size_t off = 0;
     const size_t e_off = off;
-    off = align_up(off + (size_t)n * 4, kRegionAlign);
+    off = next_region(off, (size_t)n * 4, guards);
     const size_t f_off = off;
-    off = align_up(off + (size_t)n * 4, kRegionAlign);
+    off = next_region(off, (size_t)n * 4, guards);
     const size_t a_off = off;
-    off = align_up(off + 2 * kOzS * L.plane_bytes, kRegionAlign);
+    off = next_region(off, 2 * kOzS * L.plane_bytes, guards);
     const size_t b_off = off;
-    off = align_up(off + 3 * kOzS * L.plane_bytes, kRegionAlign);
+    off = next_region(off, 3 * kOzS * L.plane_bytes, guards);
     const size_t p_off = off;
-    off = align_up(off + (size_t)n * n * sizeof(double2), kRegionAlign);
+    off = next_region(off, (size_t)n * n * sizeof(double2), guards);
     L.bytes = off;
     if (base != nullptr) {
         L.E = reinterpret_cast<int*>(base + e_off);

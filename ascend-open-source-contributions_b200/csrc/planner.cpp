@@ -19,6 +19,8 @@
 #include <cstring>
 #include <limits>
 
+#include <vector>
+
 #include "cg3m_internal.h"
 
 namespace cg3m {
@@ -365,10 +367,11 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
         out.plane_b_elems = (size_t)out.pitch_b * p.k;
     }
     size_t off = 0;
+    std::vector<size_t> guards;
     out.planes_a_off = off;
-    off = align_up(off + out.plane_a_elems * elem * out.planes, kRegionAlign);
+    off = next_region(off, out.plane_a_elems * elem * out.planes, &guards);
     out.planes_b_off = off;
-    off = align_up(off + out.plane_b_elems * elem * out.planes, kRegionAlign);
+    off = next_region(off, out.plane_b_elems * elem * out.planes, &guards);
     out.partial_pitch = (int)align_up((size_t)p.m, 32);
     out.partial_plane_elems = (size_t)out.partial_pitch * p.n;
     // K splits merged on chip through the tile's cluster: the FP32 GEMM (up to 8
@@ -389,13 +392,24 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
                             : (out.parts <= kClusterMergeMax && out.tile_m == 128 && out.tile_n == 64));
     out.partial_off = off;
     if (out.parts > 1 && !out.cluster_merge) {
-        off = align_up(off + out.partial_plane_elems * 4 * 2 * out.parts, kRegionAlign);
+        off = next_region(off, out.partial_plane_elems * 4 * 2 * out.parts, &guards);
     }
     out.round_off = off;
     if (out.rounding) {
-        off = align_up(off + rounding_bytes(p.n, out.form), kRegionAlign);  // layout in rounding.cu
+        std::vector<size_t> inner;
+        off = next_region(off, rounding_bytes(p.n, out.form, &inner), &guards);  // layout in rounding.cu
+        for (size_t g : inner) {
+            guards.push_back(out.round_off + g);
+        }
     }
     out.total = off;
+    if (guards.size() > (size_t)Plan::kMaxGuards) {
+        return false;
+    }
+    out.guards = (int)guards.size();
+    for (size_t i = 0; i < guards.size(); ++i) {
+        out.guard_off[i] = guards[i];
+    }
     *plan = out;
     return true;
 }

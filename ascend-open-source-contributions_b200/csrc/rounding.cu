@@ -741,50 +741,64 @@ static size_t tile_words(int n)
 // 2-D tensor copies, whose row stride must be a multiple of 16 bytes).
 static int row_pitch(int n) { return n + (n & 1); }
 
+// Region offsets of the rounding region (shared by the layout and its size).
+struct RoundOffsets {
+    size_t path, rows_a, rows_b, energy, flags, oz, end;
+};
+
+static RoundOffsets round_offsets(int n, int form, std::vector<size_t>* guards)
+{
+    const size_t nn = (size_t)n * n;
+    const size_t rows = (size_t)n * row_pitch(n);
+    RoundOffsets o{};
+    size_t off = 0;
+    o.path = off;
+    off = next_region(off, nn * 4, guards);
+    o.rows_a = off;
+    off = next_region(off, rows * 8, guards);
+    o.rows_b = off;
+    off = next_region(off, rows * 8, guards);
+    o.energy = off;
+    off = next_region(off, (size_t)2 * n * 4, guards);
+    o.flags = off;
+    off = next_region(off, (2 * flag_words(n) + tile_words(n) + kStatWords) * 4, guards);
+    o.oz = off;
+    if (form != CG3M_FORM_FP32) {
+        std::vector<size_t> inner;
+        off += oz_layout(n, nullptr, &inner).bytes;
+        if (guards != nullptr) {
+            for (size_t g : inner) {
+                guards->push_back(o.oz + g);
+            }
+        }
+    }
+    o.end = off;
+    return o;
+}
+
 static RoundLayout round_layout(const Plan& plan, void* ws, int n)
 {
     uint8_t* b = static_cast<uint8_t*>(ws) + plan.round_off;
-    const size_t nn = (size_t)n * n;
-    const size_t rows = (size_t)n * row_pitch(n);
+    const RoundOffsets o = round_offsets(n, plan.form, nullptr);
     RoundLayout L;
-    size_t off = 0;
-    L.path = reinterpret_cast<float*>(b + off);
-    off = align_up(off + nn * 4, kRegionAlign);
-    L.rows_a = reinterpret_cast<float2*>(b + off);
-    off = align_up(off + rows * 8, kRegionAlign);
-    L.rows_b = reinterpret_cast<float2*>(b + off);
-    off = align_up(off + rows * 8, kRegionAlign);
-    L.energy = reinterpret_cast<float*>(b + off);
-    off = align_up(off + (size_t)2 * n * 4, kRegionAlign);
-    L.flag_bits = reinterpret_cast<uint32_t*>(b + off);
+    L.path = reinterpret_cast<float*>(b + o.path);
+    L.rows_a = reinterpret_cast<float2*>(b + o.rows_a);
+    L.rows_b = reinterpret_cast<float2*>(b + o.rows_b);
+    L.energy = reinterpret_cast<float*>(b + o.energy);
+    L.flag_bits = reinterpret_cast<uint32_t*>(b + o.flags);
     L.tile_count = L.flag_bits + flag_words(n);
     L.stats = L.tile_count + tile_words(n);
     L.fallback_bits = L.stats + kStatWords;
     L.zero_bytes = (tile_words(n) + kStatWords + flag_words(n)) * 4;
-    off = align_up(off + (2 * flag_words(n) + tile_words(n) + kStatWords) * 4, kRegionAlign);
     if (plan.form != CG3M_FORM_FP32) {
-        L.oz = oz_layout(n, b + off);
+        L.oz = oz_layout(n, b + o.oz);
     }
     return L;
 }
 
 uint32_t* rounding_stats_ptr(const Plan& plan, void* ws, int n) { return round_layout(plan, ws, n).stats; }
 
-size_t rounding_bytes(int n, int form)
-{
-    const size_t nn = (size_t)n * n;
-    const size_t rows = (size_t)n * row_pitch(n);
-    size_t off = 0;
-    off = align_up(off + nn * 4, kRegionAlign);
-    off = align_up(off + rows * 8, kRegionAlign);
-    off = align_up(off + rows * 8, kRegionAlign);
-    off = align_up(off + (size_t)2 * n * 4, kRegionAlign);
-    off = align_up(off + (2 * flag_words(n) + tile_words(n) + kStatWords) * 4, kRegionAlign);
-    if (form != CG3M_FORM_FP32) {
-        off += oz_layout(n, nullptr).bytes;
-    }
-    return off;
-}
+size_t rounding_bytes(int n, int form, std::vector<size_t>* guards) { return round_offsets(n, form, guards).end; }
 
 cudaError_t launch_gemm_with_path(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status)
 {

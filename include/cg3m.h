@@ -247,6 +247,15 @@ cg3mStatus_t cg3mGetRoundingStats(cg3mHandle_t handle, long long* stats, int cou
  * CG3M_STATUS_ALLOC_FAILED without touching C.  0 turns it off. */
 cg3mStatus_t cg3mDiagFailAllocations(int count);
 
+/* Guard bands around the workspace regions of cg3mCgemm3m / cg3mCgemm3mEx /
+ * cg3mCgemm3mNoAlloc calls, enabled only when CG3M_GUARD_BANDS is set in the
+ * environment before the library loads (a test-build switch: it adds 4 KB
+ * after every region of the planned workspace).  Each call then fills the
+ * bands with a byte pattern before its first kernel and checks them after
+ * its last.  *enabled = 1 when bands are on; *damaged = 1 when any call since
+ * the last query found a band overwritten (synchronizes the device, clears). */
+cg3mStatus_t cg3mDiagGuardStatus(int* enabled, int* damaged);
+
 /* Runs one bounded wait that cannot complete (an mbarrier nothing arrives on)
  * through the wait every pipeline kernel uses, with a limit of limit_ns
  * (0 < limit_ns <= 10 s), on the handle's stream, and synchronizes.  The

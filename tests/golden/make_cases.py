@@ -1,7 +1,7 @@
 """Regenerate ``cgemm3m_cases.json`` from the reference's case table.
 
 Reads ops-blas/test/gemm/cgemm3m/arch35/cgemm3m_test.csv under the reference
-checkout (default /root/reference, override with CG3M_REFERENCE) and keeps, per
+checkout, given as the first argument or in CG3M_REFERENCE and keeps, per
 row, the fields that pin behaviour: shapes, ops, scalars (``null`` kept as
 None), fill kinds, leading dimensions, expected status and seed.  The legacy
 ``mere_threshold`` / ``mare_multiplier`` columns are dropped (the reference's
@@ -9,15 +9,22 @@ own test README says they are unused).  Matrix values are not part of the
 table -- the reference generates them with an unshipped RNG -- so tests
 regenerate their own seeded values from the same seeds.
 
-Run from the repository root:  python tests/golden/make_cases.py
+Run from the repository root:  python tests/golden/make_cases.py <reference checkout>
 """
 import csv
 import hashlib
 import json
 import os
+import sys
 
-REF = os.environ.get("CG3M_REFERENCE", "/root/reference")
-SRC = os.path.join(REF, "ops-blas/test/gemm/cgemm3m/arch35/cgemm3m_test.csv")
+def _source():
+    """The reference's table: argv[1] or CG3M_REFERENCE names the checkout."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CG3M_REFERENCE")
+    if not ref:
+        sys.exit("usage: python %s <reference checkout>  (or set CG3M_REFERENCE)" % sys.argv[0])
+    return os.path.join(ref, "ops-blas/test/gemm/cgemm3m/arch35/cgemm3m_test.csv")
+
+
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cgemm3m_cases.json")
 
 OPS = {"ACLBLAS_OP_N": "N", "ACLBLAS_OP_T": "T", "ACLBLAS_OP_C": "C", "999": 999}
@@ -33,7 +40,7 @@ def scalar(value):
 
 
 def main():
-    with open(SRC, "rb") as f:
+    with open(_source(), "rb") as f:
         raw = f.read()
     rows = list(csv.DictReader(raw.decode().splitlines()))
     cases = []

@@ -1,27 +1,34 @@
 """Regenerate ``pf_gpu_baseline.json`` from the reference's performance table.
 
 Reads ops-blas/test/gemm/cgemm3m/arch35/gpu_baseline.csv under the reference
-checkout (default /root/reference, override with CG3M_REFERENCE): the 200
+checkout, given as the first argument or in CG3M_REFERENCE: the 200
 performance shapes of the reference's case table (alpha = 1, beta = 0, fills
 RANDOM_NORM_5_5) with the per-call time of the reference's GPU baseline, which
 its own performance gate divides by the NPU time.  Kept per row: id, ops,
 m, n, k, leading dimensions and gpu_ms; the sha256 of the source is recorded.
 
-Run from the repository root:  python tests/golden/make_pf_baseline.py
+Run from the repository root:  python tests/golden/make_pf_baseline.py <reference checkout>
 """
 import csv
 import hashlib
 import json
 import os
+import sys
 
-REF = os.environ.get("CG3M_REFERENCE", "/root/reference")
-SRC = os.path.join(REF, "ops-blas/test/gemm/cgemm3m/arch35/gpu_baseline.csv")
+def _source():
+    """The reference's table: argv[1] or CG3M_REFERENCE names the checkout."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CG3M_REFERENCE")
+    if not ref:
+        sys.exit("usage: python %s <reference checkout>  (or set CG3M_REFERENCE)" % sys.argv[0])
+    return os.path.join(ref, "ops-blas/test/gemm/cgemm3m/arch35/gpu_baseline.csv")
+
+
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pf_gpu_baseline.json")
 OPS = {"ACLBLAS_OP_N": "N", "ACLBLAS_OP_T": "T", "ACLBLAS_OP_C": "C"}
 
 
 def main():
-    with open(SRC, "rb") as f:
+    with open(_source(), "rb") as f:
         raw = f.read()
     rows = []
     for r in csv.DictReader(raw.decode().splitlines()):

@@ -129,12 +129,15 @@ def test_tc_long_k(cg3m, oracle, cuda, h, form):
 
 
 @pytest.mark.parametrize("form", FORMS)
-@pytest.mark.parametrize("size", [1024, 2048])
-def test_tc_error_no_worse_than_plain(cg3m, oracle, cuda, h, form, size):
+@pytest.mark.parametrize("size,rounding", [(1024, "off"), (2048, "off"), (3072, "off"), (4096, "off"),
+                                           (2048, "auto"), (3072, "auto"), (4096, "auto")])
+def test_tc_error_no_worse_than_plain(cg3m, oracle, cuda, h, form, size, rounding):
     """Precision-form data (Im scaled by 2^e, e in [-8, 8] per column, which
-    stresses the cancellation in Im = P2-P0-P1), alpha=1, beta=0, NN: the
-    tensor-core form's normwise error vs FP64 must not exceed the plain FP32
-    3M form's (rounding pass off in both, so only the products differ)."""
+    stresses the cancellation in Im = P2-P0-P1), alpha=1, beta=0, NN -- the
+    precision form's configuration at N = 2048, 3072, 4096: the tensor-core
+    form's normwise error vs FP64 must not exceed the plain FP32 3M form's,
+    with the rounding-correction pass off in both (only the products differ)
+    and on in both (the drop-in's default gate admits these squares)."""
     import torch
 
     n = size
@@ -143,14 +146,17 @@ def test_tc_error_no_worse_than_plain(cg3m, oracle, cuda, h, form, size):
     C = torch.zeros(n * n, dtype=torch.complex64, device=cuda)
     ref = torch.empty(n * n, dtype=torch.complex128, device=cuda)
     h.zgemm_reference("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, ref)
-    h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form="fp32", rounding="off")
+    info = h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form="fp32", rounding=rounding)
+    assert info["rounding"] == (1 if rounding == "auto" else 0)
     plain = h.error_report(n, n, C, n, ref)
-    h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, rounding="off", engine="packed")
+    h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, rounding=rounding, engine="packed")
     tc = h.error_report(n, n, C, n, ref)
     torch.cuda.synchronize()
-    print(form, n, "plain", plain, "tc", tc)
+    print(form, n, rounding, "plain", plain, "tc", tc)
     assert tc["normwise"] <= plain["normwise"], (plain, tc)
     assert tc["normwise"] < 1e-5
+    del A, B, C, ref
+    torch.cuda.empty_cache()
 
 
 @pytest.mark.parametrize("form", FORMS)

@@ -14,12 +14,12 @@
 //
 //   1. ozaki_split_kernel: every op(A) row i and op(B) column j gets a power
 //      of two 2^E > max |x| over the row (real and imaginary parts together),
-//      and each part x * 2^-E in (-1, 1) is cut into S = 7 slices of 7 bits:
+//      and each part x * 2^-E in (-1, 1) is cut into S = 8 slices of 7 bits:
 //      q_s = trunc(r_{s-1} * 2^7), r_s = r_{s-1} * 2^7 - q_s (exact steps), so
 //      x = 2^E (sum_s q_s 2^-7s + rho), |rho| < 2^-7S, q_s in [-127, 127].
 //   2. ozaki_pair_kernel: for each diagonal d = s + t (2 .. S+1) the int8
 //      products sum_k q_s(A) q_t(B) of all pairs on the diagonal are exact in
-//      the int32 TMEM accumulators (|sum| <= 2 * 7 * 4096 * 127^2 < 2^31):
+//      the int32 TMEM accumulators (|sum| <= 2 * 8 * 4096 * 127^2 < 2^31):
 //        Re_d = sum Ar_s Br_t + Ai_s (-Bi_t),  Im_d = sum Ar_s Bi_t + Ai_s Br_t;
 //      after each diagonal the epilogue adds Re_d 2^-7d, Im_d 2^-7d to FP64
 //      partial sums (global, L2-resident while the tile runs), and after the
@@ -48,7 +48,12 @@ namespace cg3m {
 
 namespace {
 
-constexpr int kOzS = 7;                      // slices per operand part
+// Slices per operand part.  The row exponent is shared by the real and the
+// imaginary part, so a part much smaller than the other spends its leading
+// slices on zeros; with 7 slices ~6 % of the flagged outputs of the precision
+// form's data (Im scaled by 2^e, |e| <= 8) could not be certified at n = 2048,
+// with 8 slices the bound is 2^7 tighter.
+constexpr int kOzS = 8;
 constexpr int kOzLastDiag = kOzS + 1;        // diagonals d = s + t in [2, S + 1]
 constexpr int OZ_TILE = kOzakiTile;          // output rows and columns of a pair tile
 constexpr int OZ_ROWS = 128;                 // A rows (or B columns) staged by one CTA

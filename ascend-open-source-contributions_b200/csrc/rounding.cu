@@ -543,7 +543,8 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
                                                           const float2* __restrict__ rows_b,
                                                           const uint32_t* __restrict__ bits,
                                                           const uint32_t* __restrict__ tile_count,
-                                                          uint32_t* __restrict__ stats, float2* __restrict__ C)
+                                                          uint32_t* __restrict__ stats, float2* __restrict__ C,
+                                                          int* status)
 {
     constexpr bool FP64 = MODE != kSparseFp32;
     extern __shared__ __align__(16) float2 vec[];  // op(A) row at [0, pitch), op(B) column at [pitch, 2 pitch)
@@ -552,6 +553,8 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
     __shared__ int list[kTile * kTile];
     __shared__ int listed;
     __shared__ float peak_r[2], peak_i[2];
+    __shared__ uint64_t staged;  // the output's two bulk copies have landed
+    __shared__ int give_up;
     const int tiles = (n + kTile - 1) / kTile;
     const int gi = blockIdx.x % tiles, gj = blockIdx.x / tiles;
     const uint32_t count = tile_count[(size_t)gj * tiles + gi];
@@ -561,13 +564,26 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
     if (MODE != kFallbackFp64 && count > kSparseMax) {
         return;
     }
-    // The exact recompute writes (or marks) every flagged output of its tiles.
-    const bool in_exact_tile = FP64 && ozaki_tile_dense(tile_count, tiles, gi, gj);
-    if ((MODE == kSparseFp64 && in_exact_tile) || (MODE == kFallbackFp64 && !in_exact_tile)) {
-        return;
-    }
     const int l = threadIdx.x;
     const int i0 = gi * kTile, j0 = gj * kTile;
+    if (MODE == kFallbackFp64) {
+        // Fallback bits are only ever set inside the exact recompute's tiles:
+        // look at this tile's bits first (one or two words per column).
+        bool any = false;
+        if (l < kTile && j0 + l < n) {
+            const size_t first = (size_t)(j0 + l) * n + i0, last = first + min(kTile, n - i0) - 1;
+            for (size_t w = first >> 5; w <= (last >> 5); ++w) {
+                any |= bits[w] != 0u;
+            }
+        }
+        if (!__syncthreads_or(any)) {
+            return;
+        }
+    }
+    // The exact recompute writes (or marks) every flagged output of its tiles.
+    if (MODE == kSparseFp64 && ozaki_tile_dense(tile_count, tiles, gi, gj)) {
+        return;
+    }
     if (l == 0) {
         listed = 0;
     }
@@ -586,19 +602,36 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
     if (l == 0 && MODE != kFallbackFp64) {
         atomicAdd(&stats[kStatSparseOutputs], (uint32_t)outputs);
     }
+    if (l == 0) {
+        mbar_init(&staged, 1);
+        fence_mbar_init();
+        give_up = 0;
+    }
+    __syncthreads();
+    const uint32_t row_bytes = (uint32_t)pitch * (uint32_t)sizeof(float2);  // pitch even: a multiple of 16
     const int kbeg = min(n, l * span), kend = min(n, kbeg + span);
     for (int u = 0; u < outputs; ++u) {
         const int o = list[u];
         const int i = i0 + o % kTile, j = j0 + o / kTile;
-        const float4* ra = reinterpret_cast<const float4*>(rows_a + (size_t)i * pitch);
-        const float4* rb = reinterpret_cast<const float4*>(rows_b + (size_t)j * pitch);
-        float4* va = reinterpret_cast<float4*>(vec);
-        float4* vb = reinterpret_cast<float4*>(vec + pitch);
-        for (int e = l; e < pitch / 2; e += kLanes) {
-            va[e] = ra[e];
-            vb[e] = rb[e];
+        // One thread stages the output's op(A) row and op(B) column with two
+        // bulk copies; every thread waits on the barrier (bounded; a wait that
+        // gives up leaves this block's outputs to the path GEMM's values).
+        if (l == 0) {
+            mbar_arrive_expect_tx(&staged, 2 * row_bytes);
+            bulk_load(vec, rows_a + (size_t)i * pitch, row_bytes, &staged);
+            bulk_load(vec + pitch, rows_b + (size_t)j * pitch, row_bytes, &staged);
         }
-        __syncthreads();
+        if (!mbar_wait(&staged, (uint32_t)(u & 1), status)) {
+            give_up = 1;
+        }
+        if (__syncthreads_or(give_up)) {
+            // The copies may still be in flight: wait once more (bounded)
+            // before the block's shared memory goes away.
+            if (l == 0) {
+                mbar_wait(&staged, (uint32_t)(u & 1), status);
+            }
+            break;
+        }
         const float2* X = vec;
         const float2* Y = vec + pitch;
         float out_r, out_i;
@@ -882,7 +915,7 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
         cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e == cudaSuccess) {
             kernel<<<tiles16 * tiles16, kLanes, smem, s>>>(n, pitch, span, L.rows_a, L.rows_b, bits, L.tile_count,
-                                                           L.stats, C);
+                                                           L.stats, C, status);
             e = cudaGetLastError();
         }
         mark(++count);

@@ -338,6 +338,48 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- the reference's own data
+
+# The reference's 4096^3 performance row with the rounding pass gated in
+# (gpu_baseline.csv:5, op C,N, alpha = 1, beta = 0, RANDOM_NORM_5_5 fills) and
+# the NPU time its perf gate implies: GPU baseline 10.8757 ms / worst ratio
+# 0.41465 (README.md:54).
+REF_ROW_BASELINE_MS = 10.8757
+REF_ROW_NPU_BOUND_MS = 10.8757 / 0.41465
+
+
+def reference_data_report(h, stream, dev, world, args, timed_fn):
+    """The drop-in exactly as called (cg3mCgemm3m arithmetic, rounding pass as
+    the reference gates it) on the reference's own fill -- entries uniform in
+    [-5, 5] -- at op C,N, n = --size: time with the same steps and warm-up,
+    per-kernel times and the rounding pass's counters."""
+    import torch
+
+    n = args.size
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(20262029)
+    with torch.cuda.stream(stream):
+        A = (torch.rand(2 * n * n, generator=gen, device=dev) * 10 - 5).view(torch.complex64)
+        B = (torch.rand(2 * n * n, generator=gen, device=dev) * 10 - 5).view(torch.complex64)
+        C = torch.zeros(n * n, dtype=torch.complex64, device=dev)
+    import cg3m
+
+    def call(form, rounding):
+        return h.cgemm3m("C", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, rounding=rounding)
+
+    out = {"workload": f"cgemm3m {n}^3 op C,N alpha=1 beta=0, entries uniform in [-5,5] (the reference's fill)"}
+    for form in ("fp32", args.form):
+        ms, info, stages = timed_fn(form, "auto", args.steps, args.warmup, call=call)
+        out[form] = {"value": world * 8.0 * n ** 3 / (ms * 1e-3) / 1e12, "ms_per_step": ms,
+                     "stage_names": cg3m.stage_names(info), "stage_ms": stages, "rounding_stats": h.rounding_stats()}
+    if n == 4096:
+        out["reference_gpu_baseline_ms"] = REF_ROW_BASELINE_MS
+        out["reference_npu_bound_ms"] = REF_ROW_NPU_BOUND_MS
+    del A, B, C
+    torch.cuda.empty_cache()
+    return out
+
+
 # ----------------------------------------------------------------------------- batching form
 
 def batching_report(h, stream, dev, world, args):
@@ -600,7 +642,7 @@ def main():
         return h.cgemm3m("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, form=form, tc_segment=args.tc_segment,
                          rounding=rounding)
 
-    def timed(form, rounding, steps, warmup):
+    def timed(form, rounding, steps, warmup, call=call):
         """Mean ms per call over `steps` calls after `warmup`, and the mean
         duration of each of the call's kernels from events the library records
         between its launches inside the same timed loop."""
@@ -721,6 +763,7 @@ def main():
                 other_report["fp32"]["gemm_fp32_tflops"] = 6.0 * n ** 3 / (gms * 1e-3) / 1e12
                 other_report["fp32"]["gemm_frac_of_sgemm"] = other_report["fp32"]["gemm_fp32_tflops"] / sgemm
     del out64
+    reference_data = None if args.no_rounding_report else reference_data_report(h, stream, dev, world, args, timed)
     batching = None if args.no_batching_report else batching_report(h, stream, dev, world, args)
     status = h.device_status()
 
@@ -751,6 +794,7 @@ def main():
         "plain_fp32": plain,
         "tc_over_plain": (value / plain["value"]) if plain else None,
         "rounding_" + other: other_report,
+        "reference_data": reference_data,
         "batching_form": batching,
         "device_status": status,
     }

@@ -33,7 +33,9 @@ def test_zgemm_reference_matches_numpy(cg3m, oracle, cuda, h, ta, tb):
     import torch
 
     m = n = k = 512
-    alpha, beta = complex(0.7, 0.3), complex(-1.0, 0.5)
+    # the API takes alpha and beta as FP32: the exact product is with those values
+    alpha = complex(np.float32(0.7), np.float32(0.3))
+    beta = complex(np.float32(-1.0), np.float32(0.5))
     ar, ac = oracle.stored_shape(ta, m, k)
     br, bc = oracle.stored_shape(tb, k, n)
     lda, ldb, ldc = ar + 13, br + 13, m + 13

@@ -501,24 +501,6 @@ __device__ __forceinline__ bool ozaki_tile_dense(const uint32_t* tile_count, int
     return dense;
 }
 
-// Pairwise reduction over the 64 values of v (stride 32, 16, ..., 1: the
-// oracle's lane_reduce order); every thread of the block calls it.
-__device__ __forceinline__ void lane_reduce_shared(float* v, int l)
-{
-#pragma unroll
-    for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
-        float x = 0.0f;
-        if (l < stride) {
-            x = __fadd_rn(v[l], v[l + stride]);
-        }
-        __syncthreads();
-        if (l < stride) {
-            v[l] = x;
-        }
-        __syncthreads();
-    }
-}
-
 // Per-output recompute, one block of 64 threads per 16 x 16 output tile.
 //   kSparseFp32 / kSparseFp64: tiles holding between 1 and kSparseMax
 //     flagged outputs (FP64: outside every tile the exact recompute takes);
@@ -634,7 +616,10 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
         }
         const float2* X = vec;
         const float2* Y = vec + pitch;
-        float out_r, out_i;
+        // Lane l's own terms; the 64 lane values then meet in warp 0, which
+        // holds lanes t and t + 32 in thread t and combines them with
+        // shuffles in the oracle's fixed orders (no block barrier inside).
+        const unsigned full = 0xffffffffu;
         if constexpr (FP64) {
             double ar = 0.0, ai = 0.0;
             for (int k = kbeg; k < kend; ++k) {
@@ -645,15 +630,17 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
             dr[l] = ar;
             di[l] = ai;
             __syncthreads();
-            for (int stride = kLanes / 2; stride >= 1; stride /= 2) {
-                if (l < stride) {
-                    dr[l] += dr[l + stride];
-                    di[l] += di[l + stride];
+            if (l < 32) {
+                double vr = dr[l] + dr[l + 32], vi = di[l] + di[l + 32];
+#pragma unroll
+                for (int stride = 16; stride >= 1; stride /= 2) {
+                    vr += __shfl_down_sync(full, vr, stride);
+                    vi += __shfl_down_sync(full, vi, stride);
                 }
-                __syncthreads();
+                if (l == 0) {
+                    C[(size_t)j * n + i] = make_float2((float)vr, (float)vi);
+                }
             }
-            out_r = (float)dr[0];
-            out_i = (float)di[0];
         } else {
             // pass 1: the lane's direct sum
             float r = 0.0f, im = 0.0f;
@@ -667,35 +654,65 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
             }
             sr[l] = r;
             si[l] = im;
-            tr[l] = r;
-            ti[l] = im;
             __syncthreads();
-            lane_reduce_shared(tr, l);
-            lane_reduce_shared(ti, l);
-            const float direct_r = tr[0], direct_i = ti[0];
-            // inclusive Hillis-Steele scan of the lane sums (each step reads the previous one)
-            for (int d = 1; d < kLanes; d *= 2) {
-                const float nr = l >= d ? __fadd_rn(sr[l], sr[l - d]) : sr[l];
-                const float ni = l >= d ? __fadd_rn(si[l], si[l - d]) : si[l];
-                __syncthreads();
-                sr[l] = nr;
-                si[l] = ni;
-                __syncthreads();
-            }
-            // largest |inclusive prefix| per part (max is order-free)
-            float mr = fabsf(sr[l]), mi = fabsf(si[l]);
+            if (l < 32) {
+                const float lo_r = sr[l], hi_r = sr[l + 32], lo_i = si[l], hi_i = si[l + 32];
+                // direct: pairwise reduction, stride 32, 16, ..., 1 (lane_reduce)
+                float wr = __fadd_rn(lo_r, hi_r), wi = __fadd_rn(lo_i, hi_i);
 #pragma unroll
-            for (int off = 16; off >= 1; off /= 2) {
-                mr = fmaxf(mr, __shfl_xor_sync(0xffffffffu, mr, off));
-                mi = fmaxf(mi, __shfl_xor_sync(0xffffffffu, mi, off));
+                for (int stride = 16; stride >= 1; stride /= 2) {
+                    const float xr = __shfl_down_sync(full, wr, stride), xi = __shfl_down_sync(full, wi, stride);
+                    if (l < stride) {
+                        wr = __fadd_rn(wr, xr);
+                        wi = __fadd_rn(wi, xi);
+                    }
+                }
+                const float direct_r = __shfl_sync(full, wr, 0), direct_i = __shfl_sync(full, wi, 0);
+                // inclusive Hillis-Steele scan, distances 1 .. 32, every step
+                // reading the previous one: new[x] = v[x] + v[x - d] for x >= d
+                float ar = lo_r, br = hi_r, ai = lo_i, bi = hi_i;  // lanes l and l + 32
+#pragma unroll
+                for (int d = 1; d < 32; d *= 2) {
+                    const float up_ar = __shfl_up_sync(full, ar, d), up_ai = __shfl_up_sync(full, ai, d);
+                    const float up_br = __shfl_up_sync(full, br, d), up_bi = __shfl_up_sync(full, bi, d);
+                    const int src = l + 32 - d;  // for l < d: lane l + 32 - d of the low half
+                    const float lo_wr = __shfl_sync(full, ar, src & 31), lo_wi = __shfl_sync(full, ai, src & 31);
+                    const float nbr = __fadd_rn(br, l >= d ? up_br : lo_wr);
+                    const float nbi = __fadd_rn(bi, l >= d ? up_bi : lo_wi);
+                    if (l >= d) {
+                        ar = __fadd_rn(ar, up_ar);
+                        ai = __fadd_rn(ai, up_ai);
+                    }
+                    br = nbr;
+                    bi = nbi;
+                }
+                br = __fadd_rn(br, ar);  // d = 32: lane l + 32 adds lane l
+                bi = __fadd_rn(bi, ai);
+                // largest |inclusive prefix| per part (max is order-free)
+                float mr = fmaxf(fabsf(ar), fabsf(br)), mi = fmaxf(fabsf(ai), fabsf(bi));
+#pragma unroll
+                for (int off = 16; off >= 1; off /= 2) {
+                    mr = fmaxf(mr, __shfl_xor_sync(full, mr, off));
+                    mi = fmaxf(mi, __shfl_xor_sync(full, mi, off));
+                }
+                // seeds: lane x starts from the inclusive prefix of lane x - 1
+                const float pa_r = __shfl_up_sync(full, ar, 1), pa_i = __shfl_up_sync(full, ai, 1);
+                const float pb_r = __shfl_up_sync(full, br, 1), pb_i = __shfl_up_sync(full, bi, 1);
+                const float last_r = __shfl_sync(full, ar, 31), last_i = __shfl_sync(full, ai, 31);
+                tr[l] = l >= 1 ? pa_r : 0.0f;
+                ti[l] = l >= 1 ? pa_i : 0.0f;
+                tr[l + 32] = l >= 1 ? pb_r : last_r;
+                ti[l + 32] = l >= 1 ? pb_i : last_i;
+                if (l == 0) {
+                    peak_r[0] = mr;
+                    peak_i[0] = mi;
+                    peak_r[1] = direct_r;
+                    peak_i[1] = direct_i;
+                }
             }
-            if ((l & 31) == 0) {
-                peak_r[l >> 5] = mr;
-                peak_i[l >> 5] = mi;
-            }
+            __syncthreads();
             // pass 2: replay seeded with the previous lane's prefix
-            const float init_r = l >= 1 ? sr[l - 1] : 0.0f;
-            const float init_i = l >= 1 ? si[l - 1] : 0.0f;
+            const float init_r = tr[l], init_i = ti[l];
             r = __fadd_rn(init_r, 0.0f);
             im = __fadd_rn(init_i, 0.0f);
             for (int k = kbeg; k < kend; ++k) {
@@ -706,24 +723,31 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
                 r = __fadd_rn(r, __fsub_rn(p, rr));
                 im = __fadd_rn(im, __fadd_rn(p, q));
             }
-            __syncthreads();  // tr/ti (direct) read by every thread
-            tr[l] = __fsub_rn(r, init_r);
-            ti[l] = __fsub_rn(im, init_i);
+            sr[l] = __fsub_rn(r, init_r);
+            si[l] = __fsub_rn(im, init_i);
             __syncthreads();
-            lane_reduce_shared(tr, l);
-            lane_reduce_shared(ti, l);
-            out_r = tr[0];
-            out_i = ti[0];
-            const float pr = fmaxf(peak_r[0], peak_r[1]), pi = fmaxf(peak_i[0], peak_i[1]);
-            if (pr >= __fmul_rn(fabsf(direct_r), 32.0f)) {
-                out_r = direct_r;
+            if (l < 32) {
+                float wr = __fadd_rn(sr[l], sr[l + 32]), wi = __fadd_rn(si[l], si[l + 32]);
+#pragma unroll
+                for (int stride = 16; stride >= 1; stride /= 2) {
+                    const float xr = __shfl_down_sync(full, wr, stride), xi = __shfl_down_sync(full, wi, stride);
+                    if (l < stride) {
+                        wr = __fadd_rn(wr, xr);
+                        wi = __fadd_rn(wi, xi);
+                    }
+                }
+                if (l == 0) {
+                    const float direct_r = peak_r[1], direct_i = peak_i[1];
+                    float out_r = wr, out_i = wi;
+                    if (peak_r[0] >= __fmul_rn(fabsf(direct_r), 32.0f)) {
+                        out_r = direct_r;
+                    }
+                    if (peak_i[0] >= __fmul_rn(fabsf(direct_i), 32.0f)) {
+                        out_i = direct_i;
+                    }
+                    C[(size_t)j * n + i] = make_float2(out_r, out_i);
+                }
             }
-            if (pi >= __fmul_rn(fabsf(direct_i), 32.0f)) {
-                out_i = direct_i;
-            }
-        }
-        if (l == 0) {
-            C[(size_t)j * n + i] = make_float2(out_r, out_i);
         }
         __syncthreads();  // every read of this output's staged vectors and sums is done
     }

@@ -37,7 +37,7 @@ def _large_rows(cases, limit=3e6):
     return out
 
 
-def _sample(size, take=8):
+def _sample(size, take=32):
     idx = np.r_[0:take, size // 2 - take // 2:size // 2 + take // 2, size - take:size]
     return np.unique(idx[(idx >= 0) & (idx < size)])
 

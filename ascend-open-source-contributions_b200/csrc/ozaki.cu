@@ -415,6 +415,16 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 if (row >= n) {
                     continue;
                 }
+                // The chunk's 16 partial sums are loaded before any is used
+                // (independent loads in flight together): the MMAs wait for
+                // this drain, so its memory latency must overlap.
+                double2 prev[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = n0 + half * 128 + cb + j;
+                    prev[j] = (d == 2 || col >= n) ? make_double2(0.0, 0.0)
+                                                   : __ldcg(&p.partial[(size_t)col * n + row]);
+                }
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const int col = n0 + half * 128 + cb + j;
@@ -422,11 +432,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                         break;
                     }
                     const size_t idx = (size_t)col * n + row;
-                    double2 v = d == 2 ? make_double2(0.0, 0.0) : p.partial[idx];
+                    double2 v = prev[j];
                     v.x = fma((double)vr[j], w, v.x);
                     v.y = fma((double)vi[j], w, v.y);
                     if (d < kOzLastDiag) {
-                        p.partial[idx] = v;
+                        __stcg(&p.partial[idx], v);
                         continue;
                     }
                     if (!flag_at(p.flag_bits, idx)) {

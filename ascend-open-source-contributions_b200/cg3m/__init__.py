@@ -350,7 +350,7 @@ def stage_names(info):
         fp32 = info["form"] == FORM["fp32"]
         tail = ["replay_tiles", "replay_outputs"] if fp32 else \
             ["exact_split", "exact_tiles", "recompute_fp64_outputs", "fallback_fp64"]
-        names = ["pack", "gemm_path", "pack_rows", "energy", "select"] + tail
+        names = ["pack", "gemm_path", "pack_rows", "energy", "select", "lane_major"] + tail
     else:
         names = ["pack", "gemm", "merge"]
     names = names[:k]

@@ -115,9 +115,11 @@ enum : int {
     kStatWords = 8
 };
 
-// Output rows and columns of the exact recompute's tile: it runs on every
-// such tile holding a 16 x 16 tile with more than kSparseMax flagged outputs.
+// Output rows of the exact recompute's tile; its width (ozaki_tile_n, 256 or
+// 192 columns) is chosen per order n.  It runs on every tile holding a
+// 16 x 16 tile with more than kSparseMax flagged outputs.
 constexpr int kOzakiTile = 256;
+int ozaki_tile_n(int n);
 
 // Slices, exponents and FP64 partial sums of the tensor-core forms' exact
 // recompute (ozaki.cu), carved from the rounding region.

@@ -55,24 +55,35 @@ namespace {
 // with 8 slices the bound is 2^7 tighter.
 constexpr int kOzS = 8;
 constexpr int kOzLastDiag = kOzS + 1;        // diagonals d = s + t in [2, S + 1]
-constexpr int OZ_TILE = kOzakiTile;          // output rows and columns of a pair tile
-constexpr int OZ_ROWS = 128;                 // A rows (or B columns) staged by one CTA
+constexpr int OZ_TILE_M = kOzakiTile;        // output rows of a pair tile (M of the pair MMA)
+constexpr int OZ_ROWS = 128;                 // A rows staged by one CTA
 constexpr int OZ_BK = 64;                    // K bytes per staged row (64-byte swizzle)
 constexpr int OZ_PLANE = OZ_ROWS * OZ_BK;    // 8 KB
-constexpr int OZ_STAGE = 5 * OZ_PLANE;       // Ar, Ai | Br, Bi, -Bi
-constexpr int OZ_STAGES = 5;
-constexpr size_t OZ_SMEM = (size_t)OZ_STAGES * OZ_STAGE + 1024 + 256;
 constexpr int kOzEpiWarps = 8;
 constexpr int kOzThreads = (2 + kOzEpiWarps) * 32;
-constexpr int kOzTileGranules = OZ_TILE / 16;  // 16 x 16 count tiles per pair-tile side
 constexpr int kOzNonFinite = 1 << 20;          // exponent marker: the row or column holds Inf/NaN
 constexpr int kOzZero = -(1 << 20);            // exponent marker: the row or column is all zero
-static_assert(kOzThreads >= kOzTileGranules * kOzTileGranules, "one thread per count tile in the density check");
+
+// A pair tile is 256 rows x TN columns (TN = N of the pair MMA, 256 or 192;
+// the launch picks the one whose waves fill the GPU best): each CTA stages
+// TN / 2 columns of the B slices; a stage holds Ar_s, Ai_s | Br_t, Bi_t, -Bi_t.
+template <int TN>
+struct OzGeom {
+    static constexpr int BCOLS = TN / 2;
+    static constexpr int B_PLANE = BCOLS * OZ_BK;
+    static constexpr int STAGE = 2 * OZ_PLANE + 3 * B_PLANE;
+    static constexpr int STAGES = (208 * 1024) / STAGE;
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 + 256;
+    static constexpr int GRAN_N = TN / 16;  // 16 x 16 count tiles across the pair tile
+    static_assert(STAGE % 1024 == 0 && B_PLANE % 1024 == 0, "plane tiles start on 1024-byte boundaries");
+    static_assert(kOzThreads >= 16 * GRAN_N, "one thread per count tile in the density check");
+    static_assert(BCOLS % 16 == 0, "epilogue chunks of 16 columns");
+};
 
 struct OzParams {
     int n;
     int kblocks;             // 64-byte K blocks
-    int tiles;               // pair tiles per side
+    int tiles_m, tiles_n;    // pair tiles along the rows and the columns
     const int* E;            // op(A) row exponents
     const int* F;            // op(B) column exponents
     const uint32_t* flag_bits;
@@ -216,10 +227,14 @@ __device__ __forceinline__ void tmem_ld16x2_s32(uint32_t ta, uint32_t tb, int* v
 __device__ __forceinline__ int diag_lo(int d) { return d - kOzS > 1 ? d - kOzS : 1; }
 __device__ __forceinline__ int diag_hi(int d) { return d - 1 < kOzS ? d - 1 : kOzS; }
 
+template <int TN>
 __global__ void __launch_bounds__(kOzThreads, 1)
     ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const OzParams p)
 {
+    using G = OzGeom<TN>;
+    constexpr int OZ_STAGES = G::STAGES;
+    constexpr int OZ_STAGE = G::STAGE;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* ring = align_shared<1024>(smem_raw);
     uint64_t* full = reinterpret_cast<uint64_t*>(ring + OZ_STAGES * OZ_STAGE);
@@ -241,13 +256,13 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     // stream come from L2.
     constexpr int GM = 8;
     const int pid = blockIdx.x >> 1;
-    const int in_group = GM * p.tiles;
+    const int in_group = GM * p.tiles_n;
     const int first_m = (pid / in_group) * GM;
-    const int gsz = min(p.tiles - first_m, GM);
+    const int gsz = min(p.tiles_m - first_m, GM);
     const int tm = first_m + (pid % in_group) % gsz;
     const int tn = (pid % in_group) / gsz;
-    const int m0 = tm * OZ_TILE + (int)rank * OZ_ROWS;  // this CTA's rows
-    const int n0 = tn * OZ_TILE;                        // the pair's columns
+    const int m0 = tm * OZ_TILE_M + (int)rank * OZ_ROWS;  // this CTA's rows
+    const int n0 = tn * TN;                               // the pair's columns
     const int n = p.n;
 
     // A tile runs here only when one of its 16 x 16 count tiles is dense; both
@@ -260,9 +275,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     }
     {
         const int g16 = (n + 15) / 16;
-        if (tid < kOzTileGranules * kOzTileGranules) {
-            const int gi = tm * kOzTileGranules + tid % kOzTileGranules;
-            const int gj = tn * kOzTileGranules + tid / kOzTileGranules;
+        if (tid < 16 * G::GRAN_N) {
+            const int gi = tm * 16 + tid % 16;
+            const int gj = tn * G::GRAN_N + tid / 16;
             if (gi < g16 && gj < g16) {
                 const uint32_t c = p.tile_count[(size_t)gj * g16 + gi];
                 dense = c > kSparseMax;
@@ -329,7 +344,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                         }
                         const int t = d - s;
                         tma_load_3d_pair(st, &tmA, bar, kb * OZ_BK, m0, 2 * (s - 1));
-                        tma_load_3d_pair(st + 2 * OZ_PLANE, &tmB, bar, kb * OZ_BK, n0 + (int)rank * OZ_ROWS,
+                        tma_load_3d_pair(st + 2 * OZ_PLANE, &tmB, bar, kb * OZ_BK, n0 + (int)rank * G::BCOLS,
                                          3 * (t - 1));
                     }
                 }
@@ -344,9 +359,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         // ---------------- MMA issuer (even CTA) ----------------
         if (leader && lane == 0) {
             // S32 accumulate, signed 8-bit A and B, both K-major, N = 256, M = 256.
-            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_TILE >> 3) << 17) |
-                                   ((uint32_t)(OZ_TILE >> 4) << 24);
-            const uint32_t d_re = tmem, d_im = tmem + (uint32_t)OZ_TILE;
+            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                                   ((uint32_t)(OZ_TILE_M >> 4) << 24);
+            const uint32_t d_re = tmem, d_im = tmem + (uint32_t)TN;
             int it = 0;
             bool stop = false;
             for (int d = 2; d <= kOzLastDiag && !stop; ++d) {
@@ -368,8 +383,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                         }
                         tc_fence_after();
                         const uint32_t ar = smem_u32(ring + slot * OZ_STAGE);
-                        const uint32_t ai = ar + OZ_PLANE, br = ar + 2 * OZ_PLANE, bi = ar + 3 * OZ_PLANE,
-                                       nbi = ar + 4 * OZ_PLANE;
+                        const uint32_t ai = ar + OZ_PLANE, br = ar + 2 * OZ_PLANE, bi = br + G::B_PLANE,
+                                       nbi = br + 2 * G::B_PLANE;
 #pragma unroll
                         for (int kk = 0; kk < OZ_BK / 32; ++kk) {
                             const uint32_t o = (uint32_t)(kk * 32);
@@ -393,11 +408,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     } else {
         // ---------------- epilogue warps 2..9 (both CTAs) ----------------
         // TMEM lane quadrant = warp % 4 (the warp's 32 rows); warps 2-5 take
-        // columns 0..127 of the tile, warps 6-9 columns 128..255.
+        // the first TN / 2 columns of the tile, warps 6-9 the rest.
         const int quad = warp & 3;
         const int half = (warp - 2) >> 2;
         const int row = m0 + quad * 32 + lane;
-        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * 128);
+        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * G::BCOLS);
         const uint32_t free_addr = mapa_shared(smem_u32(acc_free), 0);
         const int ei = row < n ? p.E[row] : 0;
         uint32_t fallbacks = 0;
@@ -409,9 +424,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             }
             const double w = ldexp(1.0, -7 * d);
 #pragma unroll 1
-            for (int cb = 0; cb < 128; cb += 16) {
+            for (int cb = 0; cb < G::BCOLS; cb += 16) {
                 int vr[16], vi[16];
-                tmem_ld16x2_s32(lane_addr + (uint32_t)cb, lane_addr + (uint32_t)(OZ_TILE + cb), vr, vi);
+                tmem_ld16x2_s32(lane_addr + (uint32_t)cb, lane_addr + (uint32_t)(TN + cb), vr, vi);
                 if (row >= n) {
                     continue;
                 }
@@ -421,13 +436,13 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 double2 prev[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const int col = n0 + half * 128 + cb + j;
+                    const int col = n0 + half * G::BCOLS + cb + j;
                     prev[j] = (d == 2 || col >= n) ? make_double2(0.0, 0.0)
                                                    : __ldcg(&p.partial[(size_t)col * n + row]);
                 }
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const int col = n0 + half * 128 + cb + j;
+                    const int col = n0 + half * G::BCOLS + cb + j;
                     if (col >= n) {
                         break;
                     }
@@ -509,6 +524,68 @@ OzLayout oz_layout(int n, uint8_t* base, std::vector<size_t>* guards)
     return L;
 }
 
+// Tile width of the exact recompute for order n: the one whose waves of
+// 2-CTA clusters (one per two SMs) cost least, counting a 192-column tile at
+// 3/4 of a 256-column one.  At n = 4096: 256 -> 256 tiles in 3.46 waves of
+// 74 (4 waves, 86 % full); 192 -> 352 tiles in 4.76 waves (5 x 3/4 = 3.75).
+int ozaki_tile_n(int n)
+{
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0, count = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && count > 0) {
+            sms = count;
+        } else {
+            sms = 148;
+        }
+    }
+    const long clusters = sms / 2 > 0 ? sms / 2 : 1;
+    const long tm = (n + OZ_TILE_M - 1) / OZ_TILE_M;
+    const long waves256 = (tm * ((n + 255) / 256) + clusters - 1) / clusters;
+    const long waves192 = (tm * ((n + 191) / 192) + clusters - 1) / clusters;
+    return 3 * waves192 < 4 * waves256 ? 192 : 256;
+}
+
+template <int TN>
+static cudaError_t launch_pair_tn(cudaStream_t s, int n, const OzLayout& L, OzParams p)
+{
+    using G = OzGeom<TN>;
+    CUtensorMap ta, tb;
+    const uint64_t dims_a[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(2 * kOzS)};
+    const uint64_t dims_b[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(3 * kOzS)};
+    const uint64_t strides[2] = {(uint64_t)L.kpitch, (uint64_t)L.plane_bytes};
+    const uint32_t box_a[3] = {(uint32_t)OZ_BK, (uint32_t)OZ_ROWS, 2u};
+    const uint32_t box_b[3] = {(uint32_t)OZ_BK, (uint32_t)G::BCOLS, 3u};
+    if (!encode_tensor_map(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims_a, strides, box_a, CU_TENSOR_MAP_SWIZZLE_64B,
+                           L.planes_a) ||
+        !encode_tensor_map(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims_b, strides, box_b, CU_TENSOR_MAP_SWIZZLE_64B,
+                           L.planes_b)) {
+        return cudaErrorInvalidValue;
+    }
+    p.tiles_m = (n + OZ_TILE_M - 1) / OZ_TILE_M;
+    p.tiles_n = (n + TN - 1) / TN;
+    auto kernel = ozaki_pair_kernel<TN>;
+    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(2 * p.tiles_m * p.tiles_n));
+    cfg.blockDim = dim3(kOzThreads);
+    cfg.dynamicSmemBytes = G::SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    err = cudaLaunchKernelEx(&cfg, kernel, ta, tb, p);
+    return err != cudaSuccess ? err : cudaGetLastError();
+}
+
 cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a, const float2* rows_b,
                          const OzLayout& L, const uint32_t* flag_bits, const uint32_t* tile_count, uint32_t* stats,
                          uint32_t* fallback_bits, float2* C, int* status, int* launched,
@@ -520,22 +597,9 @@ cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a,
     cudaError_t err = cudaGetLastError();
     mark(++count);
     if (err == cudaSuccess) {
-        CUtensorMap ta, tb;
-        const uint64_t dims_a[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(2 * kOzS)};
-        const uint64_t dims_b[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(3 * kOzS)};
-        const uint64_t strides[2] = {(uint64_t)L.kpitch, (uint64_t)L.plane_bytes};
-        const uint32_t box_a[3] = {(uint32_t)OZ_BK, (uint32_t)OZ_ROWS, 2u};
-        const uint32_t box_b[3] = {(uint32_t)OZ_BK, (uint32_t)OZ_ROWS, 3u};
-        if (!encode_tensor_map(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims_a, strides, box_a,
-                               CU_TENSOR_MAP_SWIZZLE_64B, L.planes_a) ||
-            !encode_tensor_map(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims_b, strides, box_b,
-                               CU_TENSOR_MAP_SWIZZLE_64B, L.planes_b)) {
-            return cudaErrorInvalidValue;
-        }
         OzParams p{};
         p.n = n;
         p.kblocks = (n + OZ_BK - 1) / OZ_BK;
-        p.tiles = (n + OZ_TILE - 1) / OZ_TILE;
         p.E = L.E;
         p.F = L.F;
         p.flag_bits = flag_bits;
@@ -546,25 +610,7 @@ cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a,
         p.C = C;
         p.thresh = ldexp(1.0 + ldexp(1.0, -20), 25) * (2.0 * n * (kOzS + 1)) * ldexp(1.0, -7 * kOzS);
         p.status = status;
-        err = cudaFuncSetAttribute(ozaki_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OZ_SMEM);
-        if (err == cudaSuccess) {
-            cudaLaunchConfig_t cfg{};
-            cfg.gridDim = dim3((unsigned)(2 * p.tiles * p.tiles));
-            cfg.blockDim = dim3(kOzThreads);
-            cfg.dynamicSmemBytes = OZ_SMEM;
-            cfg.stream = s;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeClusterDimension;
-            attr[0].val.clusterDim.x = 2;
-            attr[0].val.clusterDim.y = 1;
-            attr[0].val.clusterDim.z = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            err = cudaLaunchKernelEx(&cfg, ozaki_pair_kernel, ta, tb, p);
-            if (err == cudaSuccess) {
-                err = cudaGetLastError();
-            }
-        }
+        err = ozaki_tile_n(n) == 192 ? launch_pair_tn<192>(s, n, L, p) : launch_pair_tn<256>(s, n, L, p);
         mark(++count);
     }
     if (launched != nullptr) {

@@ -483,16 +483,44 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constan
     }
 }
 
+// ---- 4b. lane-major copies for the per-output recompute ---------------------------
+
+// Lane-major copies of the packed op(A) rows and op(B) columns, the layout of
+// the reference's PermuteSegments (cgemm3m_rounding_kernel.cpp:406-435):
+// element k = l * span + s of a row goes to s * 64 + l (zero past n), so the
+// 64 lanes of one K step are 512 contiguous bytes.  One block per row: the
+// row is staged with coalesced loads and written out coalesced (span is odd,
+// so the strided shared-memory reads of a half-warp hit distinct banks).
+__global__ void __launch_bounds__(256) lane_major_kernel(int n, int pitch, int span, const float2* __restrict__ rows_a,
+                                                         const float2* __restrict__ rows_b,
+                                                         float2* __restrict__ lanes_a, float2* __restrict__ lanes_b)
+{
+    extern __shared__ float2 row[];
+    const int r = blockIdx.x;
+    const size_t width = (size_t)kLanes * span;
+    const float2* src = r < n ? rows_a + (size_t)r * pitch : rows_b + (size_t)(r - n) * pitch;
+    float2* dst = r < n ? lanes_a + (size_t)r * width : lanes_b + (size_t)(r - n) * width;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        row[k] = src[k];
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < (int)width; f += blockDim.x) {
+        const int sidx = f / kLanes, l = f % kLanes;
+        const int k = l * span + sidx;
+        dst[f] = k < n ? row[k] : make_float2(0.0f, 0.0f);
+    }
+}
+
 // ---- 4c. per-output recompute of sparse tiles ----------------------------------
 
 // Whether the exact (int8 slice) recompute tile holding 16 x 16 tile (gi, gj)
 // runs, i.e. holds a dense 16 x 16 tile (ozaki_pair_kernel's predicate).
-__device__ __forceinline__ bool ozaki_tile_dense(const uint32_t* tile_count, int tiles16, int gi, int gj)
+__device__ __forceinline__ bool ozaki_tile_dense(const uint32_t* tile_count, int tiles16, int gi, int gj, int gn)
 {
-    constexpr int G = kOzakiTile / kTile;
-    const int bi = gi / G * G, bj = gj / G * G;
+    constexpr int G = kOzakiTile / kTile;  // count tiles down the exact tile; gn across it
+    const int bi = gi / G * G, bj = gj / gn * gn;
     bool dense = false;
-    for (int q = 0; q < G * G; ++q) {
+    for (int q = 0; q < G * gn; ++q) {
         const int qi = bi + q % G, qj = bj + q / G;
         if (qi < tiles16 && qj < tiles16) {
             dense |= tile_count[qj * tiles16 + qi] > kSparseMax;
@@ -506,8 +534,8 @@ __device__ __forceinline__ bool ozaki_tile_dense(const uint32_t* tile_count, int
 //     flagged outputs (FP64: outside every tile the exact recompute takes);
 //   kFallbackFp64: the outputs the exact recompute marked in `bits` (a
 //     non-finite operand, or a result it could not certify).
-// The tile's outputs are recomputed one after another: the
-// output's op(A) row and op(B) column are staged in shared memory, then
+// The tile's outputs are recomputed one after another, each from the
+// lane-major copies of its op(A) row and op(B) column:
 //   FP32 (FastSegmentDot, cgemm3m_rounding_kernel.cpp:264-309): thread l is
 //     K lane l (k in [l*span, (l+1)*span)); its direct sum, the pairwise lane
 //     reduction, the inclusive Hillis-Steele scan, the replay seeded with the
@@ -515,28 +543,23 @@ __device__ __forceinline__ bool ozaki_tile_dense(const uint32_t* tile_count, int
 //     exactly (one rounding per operation, no contraction);
 //   FP64: thread l sums the same lane's complex products in FP64, the lane
 //     sums are reduced in FP64 and the result is rounded once to FP32.
-// Staged reads: thread l reads element l*span + s, so a warp's 8-byte reads
-// fall in distinct bank pairs (span is odd).
 enum { kSparseFp32 = 0, kSparseFp64 = 1, kFallbackFp64 = 2 };
 
 template <int MODE>
-__global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int span,
-                                                          const float2* __restrict__ rows_a,
-                                                          const float2* __restrict__ rows_b,
+__global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int span,
+                                                          const float2* __restrict__ lanes_a,
+                                                          const float2* __restrict__ lanes_b,
                                                           const uint32_t* __restrict__ bits,
                                                           const uint32_t* __restrict__ tile_count,
                                                           uint32_t* __restrict__ stats, float2* __restrict__ C,
-                                                          int* status)
+                                                          int exact_gn)
 {
     constexpr bool FP64 = MODE != kSparseFp32;
-    extern __shared__ __align__(16) float2 vec[];  // op(A) row at [0, pitch), op(B) column at [pitch, 2 pitch)
     __shared__ float sr[kLanes], si[kLanes], tr[kLanes], ti[kLanes];
     __shared__ double dr[kLanes], di[kLanes];
     __shared__ int list[kTile * kTile];
     __shared__ int listed;
     __shared__ float peak_r[2], peak_i[2];
-    __shared__ uint64_t staged;  // the output's two bulk copies have landed
-    __shared__ int give_up;
     // Tiles in bands of kSparseBand tile rows, rows fastest within a band: the
     // op(A) rows of a band (1024 rows, 32 MB at n = 4096) stay in L2 while the
     // band's columns go by, so each staged row comes from L2, not HBM.
@@ -569,7 +592,7 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
         }
     }
     // The exact recompute writes (or marks) every flagged output of its tiles.
-    if (MODE == kSparseFp64 && ozaki_tile_dense(tile_count, tiles, gi, gj)) {
+    if (MODE == kSparseFp64 && ozaki_tile_dense(tile_count, tiles, gi, gj, exact_gn)) {
         return;
     }
     if (l == 0) {
@@ -590,46 +613,23 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
     if (l == 0 && MODE != kFallbackFp64) {
         atomicAdd(&stats[kStatSparseOutputs], (uint32_t)outputs);
     }
-    if (l == 0) {
-        mbar_init(&staged, 1);
-        fence_mbar_init();
-        give_up = 0;
-    }
-    __syncthreads();
-    const uint32_t row_bytes = (uint32_t)pitch * (uint32_t)sizeof(float2);  // pitch even: a multiple of 16
-    const int kbeg = min(n, l * span), kend = min(n, kbeg + span);
+    // Lane l's terms, read from the lane-major copies (element s of lane l at
+    // s * 64 + l): every warp load is 256 contiguous bytes, and no shared
+    // memory is staged, so many blocks share an SM.
+    const int kbeg = min(n, l * span), cnt = min(n, kbeg + span) - kbeg;
     for (int u = 0; u < outputs; ++u) {
         const int o = list[u];
         const int i = i0 + o % kTile, j = j0 + o / kTile;
-        // One thread stages the output's op(A) row and op(B) column with two
-        // bulk copies; every thread waits on the barrier (bounded; a wait that
-        // gives up leaves this block's outputs to the path GEMM's values).
-        if (l == 0) {
-            mbar_arrive_expect_tx(&staged, 2 * row_bytes);
-            bulk_load(vec, rows_a + (size_t)i * pitch, row_bytes, &staged);
-            bulk_load(vec + pitch, rows_b + (size_t)j * pitch, row_bytes, &staged);
-        }
-        if (!mbar_wait(&staged, (uint32_t)(u & 1), status)) {
-            give_up = 1;
-        }
-        if (__syncthreads_or(give_up)) {
-            // The copies may still be in flight: wait once more (bounded)
-            // before the block's shared memory goes away.
-            if (l == 0) {
-                mbar_wait(&staged, (uint32_t)(u & 1), status);
-            }
-            break;
-        }
-        const float2* X = vec;
-        const float2* Y = vec + pitch;
+        const float2* X = lanes_a + (size_t)i * (kLanes * span) + l;
+        const float2* Y = lanes_b + (size_t)j * (kLanes * span) + l;
         // Lane l's own terms; the 64 lane values then meet in warp 0, which
         // holds lanes t and t + 32 in thread t and combines them with
         // shuffles in the oracle's fixed orders (no block barrier inside).
         const unsigned full = 0xffffffffu;
         if constexpr (FP64) {
             double ar = 0.0, ai = 0.0;
-            for (int k = kbeg; k < kend; ++k) {
-                const float2 x = X[k], y = Y[k];
+            for (int step = 0; step < cnt; ++step) {
+                const float2 x = X[step * kLanes], y = Y[step * kLanes];
                 ar = fma((double)x.x, (double)y.x, fma(-(double)x.y, (double)y.y, ar));
                 ai = fma((double)x.x, (double)y.y, fma((double)x.y, (double)y.x, ai));
             }
@@ -650,8 +650,8 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
         } else {
             // pass 1: the lane's direct sum
             float r = 0.0f, im = 0.0f;
-            for (int k = kbeg; k < kend; ++k) {
-                const float2 x = X[k], y = Y[k];
+            for (int step = 0; step < cnt; ++step) {
+                const float2 x = X[step * kLanes], y = Y[step * kLanes];
                 const float p = __fmul_rn(__fadd_rn(x.x, x.y), y.x);
                 const float q = __fmul_rn(x.x, __fsub_rn(y.y, y.x));
                 const float rr = __fmul_rn(x.y, __fadd_rn(y.x, y.y));
@@ -721,8 +721,8 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int pitch, int
             const float init_r = tr[l], init_i = ti[l];
             r = __fadd_rn(init_r, 0.0f);
             im = __fadd_rn(init_i, 0.0f);
-            for (int k = kbeg; k < kend; ++k) {
-                const float2 x = X[k], y = Y[k];
+            for (int step = 0; step < cnt; ++step) {
+                const float2 x = X[step * kLanes], y = Y[step * kLanes];
                 const float p = __fmul_rn(__fadd_rn(x.x, x.y), y.x);
                 const float q = __fmul_rn(x.x, __fsub_rn(y.y, y.x));
                 const float rr = __fmul_rn(x.y, __fadd_rn(y.x, y.y));
@@ -783,6 +783,8 @@ struct RoundLayout {
     float* path;
     float2* rows_a;
     float2* rows_b;
+    float2* lanes_a;  // lane-major copies (per-output recompute)
+    float2* lanes_b;
     float* energy;
     uint32_t* flag_bits;
     uint32_t* tile_count;
@@ -806,7 +808,7 @@ static int row_pitch(int n) { return n + (n & 1); }
 
 // Region offsets of the rounding region (shared by the layout and its size).
 struct RoundOffsets {
-    size_t path, rows_a, rows_b, energy, flags, oz, end;
+    size_t path, rows_a, rows_b, lanes_a, lanes_b, energy, flags, oz, end;
 };
 
 static RoundOffsets round_offsets(int n, int form, std::vector<size_t>* guards)
@@ -821,6 +823,11 @@ static RoundOffsets round_offsets(int n, int form, std::vector<size_t>* guards)
     off = next_region(off, rows * 8, guards);
     o.rows_b = off;
     off = next_region(off, rows * 8, guards);
+    const size_t lanes = (size_t)n * kLanes * (((n + kLanes - 1) / kLanes) | 1);
+    o.lanes_a = off;
+    off = next_region(off, lanes * 8, guards);
+    o.lanes_b = off;
+    off = next_region(off, lanes * 8, guards);
     o.energy = off;
     off = next_region(off, (size_t)2 * n * 4, guards);
     o.flags = off;
@@ -847,6 +854,8 @@ static RoundLayout round_layout(const Plan& plan, void* ws, int n)
     L.path = reinterpret_cast<float*>(b + o.path);
     L.rows_a = reinterpret_cast<float2*>(b + o.rows_a);
     L.rows_b = reinterpret_cast<float2*>(b + o.rows_b);
+    L.lanes_a = reinterpret_cast<float2*>(b + o.lanes_a);
+    L.lanes_b = reinterpret_cast<float2*>(b + o.lanes_b);
     L.energy = reinterpret_cast<float*>(b + o.energy);
     L.flag_bits = reinterpret_cast<uint32_t*>(b + o.flags);
     L.tile_count = L.flag_bits + flag_words(n);
@@ -935,17 +944,23 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
         err = cudaGetLastError();
         mark(++count);
     }
+    if (err == cudaSuccess) {
+        lane_major_kernel<<<2 * n, 256, (size_t)n * sizeof(float2), s>>>(n, pitch, span, L.rows_a, L.rows_b,
+                                                                         L.lanes_a, L.lanes_b);
+        err = cudaGetLastError();
+        mark(++count);
+    }
     // Dense tiles, then the flagged outputs of sparse tiles one by one; both
     // read the same per-tile counts, so each flagged output is recomputed by
     // exactly one of them.
     const int tiles16 = (n + kTile - 1) / kTile;
-    const size_t smem = (size_t)2 * pitch * sizeof(float2);
     float2* C = static_cast<float2*>(p.C);
+    const int exact_gn = plan.form == CG3M_FORM_FP32 ? 1 : ozaki_tile_n(n) / kTile;
     auto sparse = [&](auto kernel, const uint32_t* bits) {
-        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) {
-            kernel<<<tiles16 * tiles16, kLanes, smem, s>>>(n, pitch, span, L.rows_a, L.rows_b, bits, L.tile_count,
-                                                           L.stats, C, status);
+        cudaError_t e = cudaSuccess;
+        {
+            kernel<<<tiles16 * tiles16, kLanes, 0, s>>>(n, span, L.lanes_a, L.lanes_b, bits, L.tile_count, L.stats,
+                                                        C, exact_gn);
             e = cudaGetLastError();
         }
         mark(++count);

@@ -191,12 +191,12 @@ class Handle:
         """Counters of the last call's rounding pass (synchronizes): flagged
         outputs, those recomputed by the tile kernels and those recomputed one
         by one; None when the last call ran no rounding pass."""
-        v = (ctypes.c_longlong * 5)()
-        _check(_lib.cg3mGetRoundingStats(self.h, v, 5), "cg3mGetRoundingStats")
+        v = (ctypes.c_longlong * 6)()
+        _check(_lib.cg3mGetRoundingStats(self.h, v, 6), "cg3mGetRoundingStats")
         if v[0] < 0:
             return None
         return {"flagged": v[0], "dense_outputs": v[1], "sparse_outputs": v[2], "fallback_outputs": v[3],
-                "exact_tiles": v[4]}
+                "exact_tiles": v[4], "exact_positions": v[5]}
 
     def cgemm3m(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, form="fp32", rounding="auto",
                 k_partitions=0, raw=False, tc_segment=0, engine="auto", onchip_tile=0):

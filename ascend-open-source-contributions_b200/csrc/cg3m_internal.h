@@ -112,12 +112,13 @@ enum : int {
     kStatSparseOutputs = 2,
     kStatFallback = 3,
     kStatExactTiles = 4,
+    kStatExactOutputs = 5,
     kStatWords = 8
 };
 
-// Output rows of the exact recompute's tile; its width (ozaki_tile_n, 256 or
-// 192 columns) is chosen per order n.  It runs on every tile holding a
-// 16 x 16 tile with more than kSparseMax flagged outputs.
+// Output rows of the exact recompute's tile; its width is ozaki_tile_n(n).
+// It runs on every tile holding a 16 x 16 tile with more than kSparseMax
+// flagged outputs.
 constexpr int kOzakiTile = 256;
 int ozaki_tile_n(int n);
 

@@ -64,9 +64,9 @@ constexpr int kOzThreads = (2 + kOzEpiWarps) * 32;
 constexpr int kOzNonFinite = 1 << 20;          // exponent marker: the row or column holds Inf/NaN
 constexpr int kOzZero = -(1 << 20);            // exponent marker: the row or column is all zero
 
-// A pair tile is 256 rows x TN columns (TN = N of the pair MMA, 256 or 192;
-// the launch picks the one whose waves fill the GPU best): each CTA stages
-// TN / 2 columns of the B slices; a stage holds Ar_s, Ai_s | Br_t, Bi_t, -Bi_t.
+// A pair tile is 256 rows x TN columns (TN = N of the pair MMA): each CTA
+// stages TN / 2 columns of the B slices; a stage holds Ar_s, Ai_s | Br_t,
+// Bi_t, -Bi_t.
 template <int TN>
 struct OzGeom {
     static constexpr int BCOLS = TN / 2;
@@ -300,6 +300,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         }
         if (leader) {
             atomicAdd(&p.stats[kStatExactTiles], 1u);
+            // output positions of the tile inside the matrix (the roofline's work)
+            const int rows = min(OZ_TILE_M, n - tm * OZ_TILE_M), cols = min(TN, n - n0);
+            atomicAdd(&p.stats[kStatExactOutputs], (uint32_t)(rows * cols));
         }
         for (int s = 0; s < OZ_STAGES; ++s) {
             mbar_init(&full[s], 1);
@@ -524,27 +527,14 @@ OzLayout oz_layout(int n, uint8_t* base, std::vector<size_t>* guards)
     return L;
 }
 
-// Tile width of the exact recompute for order n: the one whose waves of
-// 2-CTA clusters (one per two SMs) cost least, counting a 192-column tile at
-// 3/4 of a 256-column one.  At n = 4096: 256 -> 256 tiles in 3.46 waves of
-// 74 (4 waves, 86 % full); 192 -> 352 tiles in 4.76 waves (5 x 3/4 = 3.75).
+// Tile width of the exact recompute.  256 x 192 tiles fill the waves of 74
+// clusters better at n = 4096 (4.76 waves instead of 3.46) but measured no
+// faster (7.15 against 7.03 ms: the narrower MMA and the partial last column
+// cost what the fuller waves save), so every order uses 256 x 256.
 int ozaki_tile_n(int n)
 {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0, count = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && count > 0) {
-            sms = count;
-        } else {
-            sms = 148;
-        }
-    }
-    const long clusters = sms / 2 > 0 ? sms / 2 : 1;
-    const long tm = (n + OZ_TILE_M - 1) / OZ_TILE_M;
-    const long waves256 = (tm * ((n + 255) / 256) + clusters - 1) / clusters;
-    const long waves192 = (tm * ((n + 191) / 192) + clusters - 1) / clusters;
-    return 3 * waves192 < 4 * waves256 ? 192 : 256;
+    (void)n;
+    return 256;
 }
 
 template <int TN>
@@ -610,7 +600,7 @@ cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a,
         p.C = C;
         p.thresh = ldexp(1.0 + ldexp(1.0, -20), 25) * (2.0 * n * (kOzS + 1)) * ldexp(1.0, -7 * kOzS);
         p.status = status;
-        err = ozaki_tile_n(n) == 192 ? launch_pair_tn<192>(s, n, L, p) : launch_pair_tn<256>(s, n, L, p);
+        err = launch_pair_tn<256>(s, n, L, p);
         mark(++count);
     }
     if (launched != nullptr) {

@@ -235,7 +235,8 @@ cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t handle, int* flags);
  * one), stats[2] = flagged outputs recomputed one by one (the other tiles),
  * stats[3] = tensor-core forms: outputs of those tiles the int8 slice
  * products could not certify, recomputed in FP64, stats[4] = 256 x 256 tiles
- * run on the int8 slice products; entries past 4 are reserved.  All -1 when that call ran no rounding pass.  Valid until the
+ * run on the int8 slice products, stats[5] = the output positions inside the
+ * matrix those tiles cover; entries past 5 are reserved.  All -1 when that call ran no rounding pass.  Valid until the
  * next call through the handle (the counters live in its workspace). */
 cg3mStatus_t cg3mGetRoundingStats(cg3mHandle_t handle, long long* stats, int count);
 

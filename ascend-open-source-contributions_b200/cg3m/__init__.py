@@ -349,7 +349,7 @@ def stage_names(info):
     if info["rounding"]:
         fp32 = info["form"] == FORM["fp32"]
         tail = ["replay_tiles", "replay_outputs"] if fp32 else \
-            ["exact_split", "exact_tiles", "recompute_fp64_outputs", "fallback_fp64"]
+            ["exact_split", "exact_tiles", "exact_crt", "recompute_fp64_outputs", "fallback_fp64"]
         names = ["pack", "gemm_path", "pack_rows", "energy", "select", "lane_major"] + tail
     else:
         names = ["pack", "gemm", "merge"]

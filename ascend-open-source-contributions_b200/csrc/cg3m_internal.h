@@ -122,22 +122,29 @@ enum : int {
 constexpr int kOzakiTile = 256;
 int ozaki_tile_n(int n);
 
-// Slices, exponents and FP64 partial sums of the tensor-core forms' exact
-// recompute (ozaki.cu), carved from the rounding region.
+// Exponents, rounding counts, residue planes and product residues of the
+// tensor-core forms' exact recompute (ozaki.cu), carved from the rounding
+// region.
 struct OzLayout {
-    int* E = nullptr;          // op(A) row exponents
-    int* F = nullptr;          // op(B) column exponents
-    int8_t* planes_a = nullptr;
+    int* E = nullptr;            // op(A) row exponents
+    int* F = nullptr;            // op(B) column exponents
+    int* CA = nullptr;           // rounded parts per op(A) row
+    int* CB = nullptr;           // rounded parts per op(B) column
+    uint8_t* tile_ran = nullptr; // per exact tile: 1 when it ran
+    int8_t* planes_a = nullptr;  // operand residues, [modulus][part][row][kpitch]
     int8_t* planes_b = nullptr;
-    double2* partial = nullptr;
+    uint8_t* residues = nullptr; // product residues, [modulus][part][col / 16][y_pad][16]
     int kpitch = 0;
     size_t plane_bytes = 0;
+    int y_pad = 0;               // order rounded up to whole exact tiles
+    size_t y_plane = 0;
     size_t bytes = 0;
 };
 OzLayout oz_layout(int n, uint8_t* base, std::vector<size_t>* guards = nullptr);
-// Slices op(A) rows and op(B) columns, then recomputes the flagged outputs of
-// every tile holding a dense 16 x 16 tile; outputs it cannot certify are
-// marked in fallback_bits.  mark(i) after the i-th launch (1-based).
+// Residues of op(A) rows and op(B) columns, then the exact products of every
+// tile holding a dense 16 x 16 tile and their reconstruction into the flagged
+// outputs; outputs it cannot certify are marked in fallback_bits.  Three
+// launches; mark(i) after the i-th (1-based).
 cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a, const float2* rows_b,
                          const OzLayout& L, const uint32_t* flag_bits, const uint32_t* tile_count, uint32_t* stats,
                          uint32_t* fallback_bits, float2* C, int* status, int* launched,

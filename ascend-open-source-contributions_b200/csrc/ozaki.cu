@@ -5,42 +5,48 @@
 // (cgemm3m_rounding_kernel.cpp:192-404); the tensor-core forms of this library
 // promise instead that every flagged output is within one FP32 rounding of the
 // exact product.  Recomputing ~3/4 of a 4096^3 product in FP64 on the CUDA
-// cores takes ~24 ms at this GPU's FP64 rate, so the exact products run on the
-// int8 tensor cores as error-free slice products (the splitting scheme of
-// Ozaki, Ogita, Oishi and Rump, "Error-free transformations of matrix
-// multiplication by using fast routines of matrix multiplication and its
-// applications", Numer. Algorithms 59 (2012), with int8 slices as in Ootomo,
-// Ozaki and Yokota, "DGEMM on integer matrix multiplication unit", IJHPCA 2024):
+// cores takes ~24 ms at this GPU's FP64 rate, so the products run on the int8
+// tensor cores as exact integer products modulo small coprime moduli, put
+// back together by the Chinese remainder theorem (the modular form of the
+// Ozaki scheme: Ozaki, Uchino and Imamura, "Ozaki Scheme II: A GEMM-oriented
+// emulation of floating-point matrix multiplication using an integer modular
+// technique", 2025):
 //
 //   1. ozaki_split_kernel: every op(A) row i and op(B) column j gets a power
-//      of two 2^E > max |x| over the row (real and imaginary parts together),
-//      and each part x * 2^-E in (-1, 1) is cut into S = 8 slices of 7 bits:
-//      q_s = trunc(r_{s-1} * 2^7), r_s = r_{s-1} * 2^7 - q_s (exact steps), so
-//      x = 2^E (sum_s q_s 2^-7s + rho), |rho| < 2^-7S, q_s in [-127, 127].
-//   2. ozaki_pair_kernel: for each diagonal d = s + t (2 .. S+1) the int8
-//      products sum_k q_s(A) q_t(B) of all pairs on the diagonal are exact in
-//      the int32 TMEM accumulators (|sum| <= 2 * 8 * 4096 * 127^2 < 2^31):
-//        Re_d = sum Ar_s Br_t + Ai_s (-Bi_t),  Im_d = sum Ar_s Bi_t + Ai_s Br_t;
-//      after each diagonal the epilogue adds Re_d 2^-7d, Im_d 2^-7d to FP64
-//      partial sums (global, L2-resident while the tile runs), and after the
-//      last one scales by 2^(E_i + F_j).
-//   3. The dropped terms (pairs with s + t > S + 1 and the remainders rho)
-//      are bounded per real product and term by (S + 1) 2^-7S, so
-//        |error| <= 2^(E_i + F_j) * 2n (S + 1) 2^-7S  per component.
-//      An output is written only when both components exceed 2^25 times that
-//      bound (so the result, rounded to FP32, is within one FP32 rounding of
-//      the exact product); otherwise it is marked for the FP64 per-output
-//      kernel, as are outputs whose row or column holds a non-finite value.
+//      of two 2^E > max |x| over the row (real and imaginary parts together);
+//      each part becomes the integer a = rn(x 2^(beta - E)), |a| <= 2^beta,
+//      beta = 47, and the row counts its parts for which a != x 2^(beta - E)
+//      (cA_i; cB_j for the columns).  The planes hold a mod p_m for the
+//      kOzMods = 14 moduli p_m <= 256 (pairwise coprime, product M ~ 2^110.2)
+//      as int8 in [-(p-1)/2, (p-1)/2] ([-128, 127] for 256); the op(A)
+//      residues are multiplied by u_m = (M / p_m)^-1 mod p_m on the way.
+//   2. ozaki_pair_kernel: for each modulus the int8 products
+//        Re_m = sum Ar Br + Ai (-Bi),  Im_m = sum Ar Bi + Ai Br
+//      are exact in the int32 TMEM accumulators (|sum| <= 2 * 4096 * 128^2
+//      < 2^31); the epilogue stores y_m = sum mod p_m in [0, p_m) as one byte
+//      per output and part.  By construction y_m = u_m x mod p_m, x the exact
+//      integer product of the rounded parts.
+//   3. ozaki_crt_kernel: x = sum_m y_m (M / p_m) - k M with k the nearest
+//      integer to sum_m y_m / p_m (|x| <= 2 n 2^(2 beta) <= 2^107 < M / 8,
+//      so k is never in doubt), evaluated exactly in three 40-bit limbs of
+//      FP64.  Rounding a part moves each real product by at most 2^(beta - 1),
+//      so
+//        |error| <= (cA_i + cB_j) 2^(beta - 1)   (units of 2^(E_i + F_j - 2 beta)),
+//      zero for rows and columns that scaled exactly.  An output is written
+//      when the bound is zero or both parts exceed 2^25 times it (so the
+//      result, rounded to FP32, is within one FP32 rounding of the exact
+//      product); otherwise it is marked for the FP64 per-output kernel, as
+//      are outputs whose row or column holds a non-finite value.
 //
 // B200 design: a cluster of two CTAs per 256 x 256 output tile
 // (tcgen05.mma.cta_group::2.kind::i8, M = 256, N = 256, K = 32): CTA r stages
-// rows [128r, 128r + 128) of the A slices and columns [128r, 128r + 128) of
-// the B slices, 64-byte K rows with the 64-byte swizzle, 40 KB per stage
-// (Ar_s, Ai_s | Br_t, Bi_t, -Bi_t) in a 5-stage ring; each CTA's TMEM holds
-// its 128 rows x 256 columns of Re (columns 0..255) and Im (256..511).  Warp 0
-// of both CTAs issues the TMA copies (completion on the even CTA's barrier),
-// one thread of the even CTA issues every MMA, warps 2..9 of both CTAs drain
-// the accumulators after each diagonal.  Every wait is bounded.
+// rows [128r, 128r + 128) of the op(A) residues and columns [128r, 128r + 128)
+// of the op(B) residues, 64-byte K rows with the 64-byte swizzle, 40 KB per
+// stage (Ar, Ai | Br, Bi, -Bi) in a 5-stage ring; each CTA's TMEM holds its
+// 128 rows x 256 columns of Re (columns 0..255) and Im (256..511).  Warp 0 of
+// both CTAs issues the TMA copies (completion on the even CTA's barrier), one
+// thread of the even CTA issues every MMA, warps 2..9 of both CTAs drain the
+// accumulators after each modulus.  Every wait is bounded.
 #include "cg3m_internal.h"
 #include "ptx.cuh"
 
@@ -48,52 +54,77 @@ namespace cg3m {
 
 namespace {
 
-// Slices per operand part.  The row exponent is shared by the real and the
-// imaginary part, so a part much smaller than the other spends its leading
-// slices on zeros; with 7 slices ~6 % of the flagged outputs of the precision
-// form's data (Im scaled by 2^e, |e| <= 8) could not be certified at n = 2048,
-// with 8 slices the bound is 2^7 tighter.
-constexpr int kOzS = 8;
-constexpr int kOzLastDiag = kOzS + 1;        // diagonals d = s + t in [2, S + 1]
-constexpr int OZ_TILE_M = kOzakiTile;        // output rows of a pair tile (M of the pair MMA)
-constexpr int OZ_ROWS = 128;                 // A rows staged by one CTA
-constexpr int OZ_BK = 64;                    // K bytes per staged row (64-byte swizzle)
-constexpr int OZ_PLANE = OZ_ROWS * OZ_BK;    // 8 KB
+constexpr int kOzMods = 14;                    // moduli (planes per operand part)
+constexpr int kOzBeta = 47;                    // bits of the scaled integer parts
+constexpr int kOzMaxN = 4096;                  // 2 n 2^(2 beta) <= M / 8 up to this order
+constexpr int OZ_TILE_M = kOzakiTile;          // output rows of a pair tile (M of the pair MMA)
+constexpr int OZ_TN = kOzakiTile;              // output columns of a pair tile (N of the pair MMA)
+constexpr int OZ_ROWS = 128;                   // A rows staged by one CTA
+constexpr int OZ_BCOLS = OZ_TN / 2;            // B columns staged by one CTA
+constexpr int OZ_BK = 64;                      // K bytes per staged row (64-byte swizzle)
+constexpr int OZ_PLANE = OZ_ROWS * OZ_BK;      // 8 KB
+constexpr int OZ_B_PLANE = OZ_BCOLS * OZ_BK;   // 8 KB
+constexpr int OZ_STAGE = 2 * OZ_PLANE + 3 * OZ_B_PLANE;
+constexpr int OZ_STAGES = (208 * 1024) / OZ_STAGE;
+constexpr size_t OZ_SMEM = (size_t)OZ_STAGES * OZ_STAGE + 1024 + 256;
+constexpr int OZ_GRAN_N = OZ_TN / 16;          // 16 x 16 count tiles across the pair tile
 constexpr int kOzEpiWarps = 8;
 constexpr int kOzThreads = (2 + kOzEpiWarps) * 32;
 constexpr int kOzNonFinite = 1 << 20;          // exponent marker: the row or column holds Inf/NaN
 constexpr int kOzZero = -(1 << 20);            // exponent marker: the row or column is all zero
+constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52: x + kMagic rounds x to an integer
+constexpr float kMagicF = 12582912.0f;         // 1.5 * 2^23
+static_assert(OZ_STAGE % 1024 == 0 && OZ_B_PLANE % 1024 == 0, "plane tiles start on 1024-byte boundaries");
+static_assert(kOzThreads >= 16 * OZ_GRAN_N, "one thread per count tile in the density check");
+static_assert(OZ_BCOLS % 16 == 0, "epilogue chunks of 16 columns");
 
-// A pair tile is 256 rows x TN columns (TN = N of the pair MMA): each CTA
-// stages TN / 2 columns of the B slices; a stage holds Ar_s, Ai_s | Br_t,
-// Bi_t, -Bi_t.
-template <int TN>
-struct OzGeom {
-    static constexpr int BCOLS = TN / 2;
-    static constexpr int B_PLANE = BCOLS * OZ_BK;
-    static constexpr int STAGE = 2 * OZ_PLANE + 3 * B_PLANE;
-    static constexpr int STAGES = (208 * 1024) / STAGE;
-    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 + 256;
-    static constexpr int GRAN_N = TN / 16;  // 16 x 16 count tiles across the pair tile
-    static_assert(STAGE % 1024 == 0 && B_PLANE % 1024 == 0, "plane tiles start on 1024-byte boundaries");
-    static_assert(kOzThreads >= 16 * GRAN_N, "one thread per count tile in the density check");
-    static_assert(BCOLS % 16 == 0, "epilogue chunks of 16 columns");
+// Moduli, largest first: 256 and 13 odd numbers, pairwise coprime
+// (255 = 3 5 17, 253 = 11 23, 247 = 13 19, 217 = 7 31, the rest prime).
+constexpr int kOzModuli[kOzMods] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199};
+
+// Constants of the moduli (host-computed once, passed by value).
+struct OzCrt {
+    int p[kOzMods];
+    int u[kOzMods];          // (M / p)^-1 mod p, in [-(p-1)/2, (p-1)/2] ([-128, 127] for 256)
+    int c16[kOzMods];        // 2^16 mod p
+    float pf[kOzMods];
+    float inv_pf[kOzMods];   // rn(1 / p)
+    double pd[kOzMods];
+    double inv_pd[kOzMods];  // rn(1 / p)
+    double w[kOzMods][3];    // M / p in 40-bit limbs, low first
+    double m[3];             // M in 40-bit limbs, low first
 };
 
 struct OzParams {
     int n;
     int kblocks;             // 64-byte K blocks
     int tiles_m, tiles_n;    // pair tiles along the rows and the columns
-    const int* E;            // op(A) row exponents
-    const int* F;            // op(B) column exponents
-    const uint32_t* flag_bits;
     const uint32_t* tile_count;
     uint32_t* stats;
-    uint32_t* fallback_bits;
-    double2* partial;        // n x n, column-major
-    float2* C;
-    double thresh;           // 2^25 (1 + 2^-20) * 2n (S + 1) 2^-7S
+    uint8_t* tile_ran;       // per pair tile (tn * tiles_m + tm): 1 when it ran here
+    uint8_t* residues;       // [2 * kOzMods][y_pad / 16][y_pad][16]
+    int y_pad;
+    size_t y_plane;
+    OzCrt crt;
     int* status;
+};
+
+struct OzFinish {
+    int n;
+    int tiles_m;
+    const int* E;            // op(A) row exponents
+    const int* F;            // op(B) column exponents
+    const int* CA;           // rounded parts per op(A) row
+    const int* CB;           // rounded parts per op(B) column
+    const uint8_t* tile_ran;
+    const uint8_t* residues;
+    int y_pad;
+    size_t y_plane;
+    const uint32_t* flag_bits;
+    uint32_t* stats;
+    uint32_t* fallback_bits;
+    float2* C;
+    OzCrt crt;
 };
 
 __device__ __forceinline__ bool flag_at(const uint32_t* bits, size_t idx)
@@ -101,18 +132,41 @@ __device__ __forceinline__ bool flag_at(const uint32_t* bits, size_t idx)
     return (bits[idx >> 5] >> (idx & 31)) & 1u;
 }
 
-// ---- 1. slices ---------------------------------------------------------------------
+// t mod p in [-(p-1)/2, (p-1)/2] for odd p and an integer-valued t, |t| <= 2^47:
+// the nearest integer q to t * rn(1/p) is the nearest integer to t / p (their
+// distance, <= 2^-13.6, is below that of t / p to a half-integer, >= 1 / 2p),
+// and t - q p is exact.
+__device__ __forceinline__ int mod_odd_d(double t, double pd, double inv_pd)
+{
+    const double q = __dsub_rn(__fma_rn(t, inv_pd, kMagic), kMagic);
+    const double r = __fma_rn(-q, pd, t);
+    return __double2loint(__dadd_rn(r, kMagic));  // the low word of r + 1.5 * 2^52 is r
+}
+
+// v mod p in [-(p-1)/2, (p-1)/2] for odd p >= 199 and |v| <= 127^2 (|v / p| is
+// off by < 2^-17 in FP32, against a distance >= 1 / 2p to a half-integer).
+__device__ __forceinline__ int mod_odd_f(int v, float pf, float inv_pf)
+{
+    const float vf = __fsub_rn(__int_as_float(0x4B400000 + v), kMagicF);  // exact: v as a float
+    const float q = __fsub_rn(__fmaf_rn(vf, inv_pf, kMagicF), kMagicF);
+    const float r = __fmaf_rn(-q, pf, vf);
+    return __float_as_int(__fadd_rn(r, kMagicF)) - 0x4B400000;
+}
+
+// ---- 1. residues -------------------------------------------------------------------
 
 // One block per op(A) row (blockIdx.x < n) or op(B) column.  Plane layout:
-// [plane][row][kpitch] int8, A planes 2(s-1) + {0 re, 1 im}, B planes
-// 3(t-1) + {0 re, 1 im, 2 -im}.
-__global__ void __launch_bounds__(256) ozaki_split_kernel(int n, int pitch, const float2* __restrict__ rows_a,
-                                                          const float2* __restrict__ rows_b, int8_t* __restrict__ pa,
-                                                          int8_t* __restrict__ pb, int kpitch, size_t plane_bytes,
-                                                          int* __restrict__ E, int* __restrict__ F)
+// [plane][row][kpitch] int8, A planes 2m + {0 re, 1 im}, B planes
+// 3m + {0 re, 1 im, 2 -im}.
+__global__ void __launch_bounds__(256)
+    ozaki_split_kernel(int n, int pitch, const float2* __restrict__ rows_a, const float2* __restrict__ rows_b,
+                       int8_t* __restrict__ pa, int8_t* __restrict__ pb, int kpitch, size_t plane_bytes,
+                       int* __restrict__ E, int* __restrict__ F, int* __restrict__ CA, int* __restrict__ CB,
+                       const __grid_constant__ OzCrt crt)
 {
     __shared__ float wmax[8];
     __shared__ int wbad[8];
+    __shared__ int wcnt[8];
     const int r = blockIdx.x;
     const bool is_a = r < n;
     const int row = is_a ? r : r - n;
@@ -141,51 +195,72 @@ __global__ void __launch_bounds__(256) ozaki_split_kernel(int n, int pitch, cons
         amax = fmaxf(amax, wmax[w]);
         any_bad |= wbad[w];
     }
-    // 2^(e-1) <= amax < 2^e, so every part scaled by 2^-e lies in (-1, 1).
+    // 2^(e-1) <= amax < 2^e, so every part scaled by 2^(beta - e) lies in (-2^beta, 2^beta).
     const int e = any_bad ? kOzNonFinite : amax > 0.0f ? ilogbf(amax) + 1 : kOzZero;
-    if (tid == 0) {
-        (is_a ? E : F)[row] = e;
-    }
     const bool usable = !any_bad && amax > 0.0f;
-    const double scale = usable ? ldexp(1.0, -e) : 0.0;
+    const double scale = usable ? ldexp(1.0, kOzBeta - e) : 0.0;
     int8_t* dst = (is_a ? pa : pb) + (size_t)row * kpitch;
-    const int planes_per_slice = is_a ? 2 : 3;
+    const int planes_per_mod = is_a ? 2 : 3;
+    int rounded = 0;
     // Four consecutive K terms per thread: 4-byte stores into every plane.
     for (int k0 = tid * 4; k0 < n; k0 += 256 * 4) {
-        double xr[4], xi[4];
+        double t[8];  // re of terms 0..3, then im
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int k = k0 + u;
             const float2 x = (k < n && usable) ? src[k] : make_float2(0.0f, 0.0f);
-            xr[u] = (double)x.x * scale;  // exact: a power-of-two scaling in FP64
-            xi[u] = (double)x.y * scale;
+            const double sr = __dmul_rn((double)x.x, scale);  // exact: a power-of-two scaling in FP64
+            const double si = __dmul_rn((double)x.y, scale);
+            t[u] = __dsub_rn(__dadd_rn(sr, kMagic), kMagic);  // nearest integer, |t| <= 2^beta
+            t[4 + u] = __dsub_rn(__dadd_rn(si, kMagic), kMagic);
+            rounded += (t[u] != sr) + (t[4 + u] != si);
         }
 #pragma unroll
-        for (int s = 0; s < kOzS; ++s) {
-            signed char vr[4], vi[4];
+        for (int mi = 0; mi < kOzMods; ++mi) {
+            int v[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const double yr = xr[u] * 128.0, yi = xi[u] * 128.0;  // exact
-                const double tr = trunc(yr), ti = trunc(yi);         // |t| <= 127
-                xr[u] = yr - tr;                                      // exact: the fraction of y
-                xi[u] = yi - ti;
-                vr[u] = (signed char)(int)tr;
-                vi[u] = (signed char)(int)ti;
+            for (int q = 0; q < 8; ++q) {
+                if (mi == 0) {
+                    // mod 256: the low byte of the two's complement integer
+                    v[q] = (int)(signed char)(__double2loint(__dadd_rn(t[q], kMagic)) & 0xFF);
+                } else {
+                    v[q] = mod_odd_d(t[q], crt.pd[mi], crt.inv_pd[mi]);
+                }
+                if (is_a) {
+                    const int w = v[q] * crt.u[mi];
+                    v[q] = mi == 0 ? (int)(signed char)(w & 0xFF) : mod_odd_f(w, crt.pf[mi], crt.inv_pf[mi]);
+                }
             }
-            int8_t* base = dst + (size_t)(planes_per_slice * s) * plane_bytes;
+            int8_t* base = dst + (size_t)(planes_per_mod * mi) * plane_bytes;
             // K beyond n is never read (the tensor maps stop at n), so whole
             // 4-byte groups may be stored while k0 < n <= kpitch.
-            *reinterpret_cast<char4*>(base + k0) = make_char4(vr[0], vr[1], vr[2], vr[3]);
-            *reinterpret_cast<char4*>(base + plane_bytes + k0) = make_char4(vi[0], vi[1], vi[2], vi[3]);
+            *reinterpret_cast<char4*>(base + k0) =
+                make_char4((signed char)v[0], (signed char)v[1], (signed char)v[2], (signed char)v[3]);
+            *reinterpret_cast<char4*>(base + plane_bytes + k0) =
+                make_char4((signed char)v[4], (signed char)v[5], (signed char)v[6], (signed char)v[7]);
             if (!is_a) {
+                // -(-128) wraps to -128: the same residue mod 256
                 *reinterpret_cast<char4*>(base + 2 * plane_bytes + k0) =
-                    make_char4((signed char)-vi[0], (signed char)-vi[1], (signed char)-vi[2], (signed char)-vi[3]);
+                    make_char4((signed char)-v[4], (signed char)-v[5], (signed char)-v[6], (signed char)-v[7]);
             }
         }
     }
+    rounded = __reduce_add_sync(0xffffffffu, rounded);
+    if ((tid & 31) == 0) {
+        wcnt[tid >> 5] = rounded;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int total = 0;
+        for (int w = 0; w < 8; ++w) {
+            total += wcnt[w];
+        }
+        (is_a ? E : F)[row] = e;
+        (is_a ? CA : CB)[row] = total;
+    }
 }
 
-// ---- 2. slice products ----------------------------------------------------------------
+// ---- 2. residue products --------------------------------------------------------------
 
 // Shared-memory matrix descriptor: K-major, 64-byte swizzle (layout type 4),
 // 8-row groups 8 x 64 = 512 bytes apart (SBO), leading offset unused (1),
@@ -212,34 +287,46 @@ __device__ __forceinline__ void umma_i8_pair(uint32_t d_tmem, uint64_t a_desc, u
         : "memory");
 }
 
-// Warp-wide 32 lanes x 16 consecutive 32-bit TMEM columns, two blocks, one wait.
-__device__ __forceinline__ void tmem_ld16x2_s32(uint32_t ta, uint32_t tb, int* va, int* vb)
+// x mod p in [0, p) for odd p and |x| < 2^27: t = (x >> 16) c16 + (x & 0xFFFF)
+// is congruent to x with |t| < 2^20, exact in FP32, and t * rn(1/p) is off
+// t / p by < 2^-12 (the distance of t / p to a half-integer is >= 1 / 2p).
+__device__ __forceinline__ uint32_t residue_byte(int x, int c16, float pf, float inv_pf)
 {
-    float fa[16], fb[16];
-    tmem_ld16x2(ta, tb, fa, fb);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        va[i] = __float_as_int(fa[i]);
-        vb[i] = __float_as_int(fb[i]);
-    }
+    const int t = (x >> 16) * c16 + (x & 0xFFFF);
+    const float tf = __fsub_rn(__int_as_float(0x4B400000 + t), kMagicF);
+    const float q = __fsub_rn(__fmaf_rn(tf, inv_pf, kMagicF), kMagicF);
+    float r = __fmaf_rn(-q, pf, tf);
+    r = r < 0.0f ? __fadd_rn(r, pf) : r;
+    return (uint32_t)__float_as_int(__fadd_rn(r, kMagicF)) & 0xFFu;
 }
 
-__device__ __forceinline__ int diag_lo(int d) { return d - kOzS > 1 ? d - kOzS : 1; }
-__device__ __forceinline__ int diag_hi(int d) { return d - 1 < kOzS ? d - 1 : kOzS; }
+// 16 accumulator values (int32 bits) -> 16 residue bytes; x mod 256 is the low byte.
+__device__ __forceinline__ uint4 residue_bytes16(const float* v, bool pow2, int c16, float pf, float inv_pf)
+{
+    uint32_t w[4];
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+        uint32_t word = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int x = __float_as_int(v[4 * g + b]);
+            const uint32_t y = pow2 ? ((uint32_t)x & 0xFFu) : residue_byte(x, c16, pf, inv_pf);
+            word |= y << (8 * b);
+        }
+        w[g] = word;
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
 
-template <int TN>
 __global__ void __launch_bounds__(kOzThreads, 1)
     ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                      const OzParams p)
+                      const __grid_constant__ OzParams p)
 {
-    using G = OzGeom<TN>;
-    constexpr int OZ_STAGES = G::STAGES;
-    constexpr int OZ_STAGE = G::STAGE;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* ring = align_shared<1024>(smem_raw);
     uint64_t* full = reinterpret_cast<uint64_t*>(ring + OZ_STAGES * OZ_STAGE);
     uint64_t* empty = full + OZ_STAGES;
-    uint64_t* acc_full = empty + OZ_STAGES;  // MMA -> epilogue: the diagonal's sums are in TMEM
+    uint64_t* acc_full = empty + OZ_STAGES;  // MMA -> epilogue: the modulus's sums are in TMEM
     uint64_t* acc_free = acc_full + 1;       // epilogue -> MMA (even CTA): TMEM drained
     uint64_t* mma_done = acc_free + 1;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
@@ -252,8 +339,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     const bool leader = rank == 0;
     const uint16_t pair_mask = 0x3u;
     // Pair tiles in groups of 8 tile rows, rows fastest: the ~74 tiles in
-    // flight share a few A and B panels and walk K in step, so the slices they
-    // stream come from L2.
+    // flight share a few A and B panels and walk K in step, so the residues
+    // they stream come from L2.
     constexpr int GM = 8;
     const int pid = blockIdx.x >> 1;
     const int in_group = GM * p.tiles_n;
@@ -262,7 +349,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     const int tm = first_m + (pid % in_group) % gsz;
     const int tn = (pid % in_group) / gsz;
     const int m0 = tm * OZ_TILE_M + (int)rank * OZ_ROWS;  // this CTA's rows
-    const int n0 = tn * TN;                               // the pair's columns
+    const int n0 = tn * OZ_TN;                            // the pair's columns
     const int n = p.n;
 
     // A tile runs here only when one of its 16 x 16 count tiles is dense; both
@@ -275,9 +362,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     }
     {
         const int g16 = (n + 15) / 16;
-        if (tid < 16 * G::GRAN_N) {
+        if (tid < 16 * OZ_GRAN_N) {
             const int gi = tm * 16 + tid % 16;
-            const int gj = tn * G::GRAN_N + tid / 16;
+            const int gj = tn * OZ_GRAN_N + tid / 16;
             if (gi < g16 && gj < g16) {
                 const uint32_t c = p.tile_count[(size_t)gj * g16 + gi];
                 dense = c > kSparseMax;
@@ -287,7 +374,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             }
         }
     }
-    if (!__syncthreads_or(dense)) {
+    const bool run = __syncthreads_or(dense);
+    if (tid == 0 && leader) {
+        p.tile_ran[(size_t)tn * p.tiles_m + tm] = run ? 1 : 0;  // read by the reconstruction
+    }
+    if (!run) {
         return;
     }
     if (here != 0) {
@@ -301,7 +392,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         if (leader) {
             atomicAdd(&p.stats[kStatExactTiles], 1u);
             // output positions of the tile inside the matrix (the roofline's work)
-            const int rows = min(OZ_TILE_M, n - tm * OZ_TILE_M), cols = min(TN, n - n0);
+            const int rows = min(OZ_TILE_M, n - tm * OZ_TILE_M), cols = min(OZ_TN, n - n0);
             atomicAdd(&p.stats[kStatExactOutputs], (uint32_t)(rows * cols));
         }
         for (int s = 0; s < OZ_STAGES; ++s) {
@@ -330,26 +421,22 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             tma_prefetch_desc(&tmB);
             int it = 0;
             bool stop = false;
-            for (int d = 2; d <= kOzLastDiag && !stop; ++d) {
-                for (int kb = 0; kb < p.kblocks && !stop; ++kb) {
-                    for (int s = diag_lo(d); s <= diag_hi(d); ++s, ++it) {
-                        const int slot = it % OZ_STAGES;
-                        if ((it >= OZ_STAGES && !mbar_wait(&empty[slot], ((it / OZ_STAGES) - 1) & 1, p.status)) ||
-                            *abort_flag) {
-                            *abort_flag = 1;
-                            stop = true;
-                            break;
-                        }
-                        uint8_t* st = ring + slot * OZ_STAGE;
-                        const uint32_t bar = mapa_shared(smem_u32(&full[slot]), 0);
-                        if (leader) {
-                            mbar_arrive_expect_tx(&full[slot], 2 * OZ_STAGE);
-                        }
-                        const int t = d - s;
-                        tma_load_3d_pair(st, &tmA, bar, kb * OZ_BK, m0, 2 * (s - 1));
-                        tma_load_3d_pair(st + 2 * OZ_PLANE, &tmB, bar, kb * OZ_BK, n0 + (int)rank * G::BCOLS,
-                                         3 * (t - 1));
+            for (int mi = 0; mi < kOzMods && !stop; ++mi) {
+                for (int kb = 0; kb < p.kblocks; ++kb, ++it) {
+                    const int slot = it % OZ_STAGES;
+                    if ((it >= OZ_STAGES && !mbar_wait(&empty[slot], ((it / OZ_STAGES) - 1) & 1, p.status)) ||
+                        *abort_flag) {
+                        *abort_flag = 1;
+                        stop = true;
+                        break;
                     }
+                    uint8_t* st = ring + slot * OZ_STAGE;
+                    const uint32_t bar = mapa_shared(smem_u32(&full[slot]), 0);
+                    if (leader) {
+                        mbar_arrive_expect_tx(&full[slot], 2 * OZ_STAGE);
+                    }
+                    tma_load_3d_pair(st, &tmA, bar, kb * OZ_BK, m0, 2 * mi);
+                    tma_load_3d_pair(st + 2 * OZ_PLANE, &tmB, bar, kb * OZ_BK, n0 + (int)rank * OZ_BCOLS, 3 * mi);
                 }
             }
             if (leader) {
@@ -362,44 +449,40 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         // ---------------- MMA issuer (even CTA) ----------------
         if (leader && lane == 0) {
             // S32 accumulate, signed 8-bit A and B, both K-major, N = 256, M = 256.
-            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_TN >> 3) << 17) |
                                    ((uint32_t)(OZ_TILE_M >> 4) << 24);
-            const uint32_t d_re = tmem, d_im = tmem + (uint32_t)TN;
+            const uint32_t d_re = tmem, d_im = tmem + (uint32_t)OZ_TN;
             int it = 0;
             bool stop = false;
-            for (int d = 2; d <= kOzLastDiag && !stop; ++d) {
-                if (d > 2) {
-                    if (!mbar_wait_cluster(acc_free, (d - 3) & 1, p.status)) {
+            for (int mi = 0; mi < kOzMods && !stop; ++mi) {
+                if (mi > 0) {
+                    if (!mbar_wait_cluster(acc_free, (mi - 1) & 1, p.status)) {
                         *abort_flag = 1;
                         break;
                     }
                     tc_fence_after();
                 }
-                bool first = true;
-                for (int kb = 0; kb < p.kblocks && !stop; ++kb) {
-                    for (int s = diag_lo(d); s <= diag_hi(d); ++s, ++it) {
-                        const int slot = it % OZ_STAGES;
-                        if (!mbar_wait(&full[slot], (it / OZ_STAGES) & 1, p.status)) {
-                            *abort_flag = 1;
-                            stop = true;
-                            break;
-                        }
-                        tc_fence_after();
-                        const uint32_t ar = smem_u32(ring + slot * OZ_STAGE);
-                        const uint32_t ai = ar + OZ_PLANE, br = ar + 2 * OZ_PLANE, bi = br + G::B_PLANE,
-                                       nbi = br + 2 * G::B_PLANE;
-#pragma unroll
-                        for (int kk = 0; kk < OZ_BK / 32; ++kk) {
-                            const uint32_t o = (uint32_t)(kk * 32);
-                            const uint32_t acc = (first && kk == 0) ? 0u : 1u;
-                            umma_i8_pair(d_re, oz_desc(ar + o), oz_desc(br + o), idesc, acc);
-                            umma_i8_pair(d_re, oz_desc(ai + o), oz_desc(nbi + o), idesc, 1u);
-                            umma_i8_pair(d_im, oz_desc(ar + o), oz_desc(bi + o), idesc, acc);
-                            umma_i8_pair(d_im, oz_desc(ai + o), oz_desc(br + o), idesc, 1u);
-                        }
-                        first = false;
-                        umma_commit_pair(&empty[slot], pair_mask);
+                for (int kb = 0; kb < p.kblocks; ++kb, ++it) {
+                    const int slot = it % OZ_STAGES;
+                    if (!mbar_wait(&full[slot], (it / OZ_STAGES) & 1, p.status)) {
+                        *abort_flag = 1;
+                        stop = true;
+                        break;
                     }
+                    tc_fence_after();
+                    const uint32_t ar = smem_u32(ring + slot * OZ_STAGE);
+                    const uint32_t ai = ar + OZ_PLANE, br = ar + 2 * OZ_PLANE, bi = br + OZ_B_PLANE,
+                                   nbi = br + 2 * OZ_B_PLANE;
+#pragma unroll
+                    for (int kk = 0; kk < OZ_BK / 32; ++kk) {
+                        const uint32_t o = (uint32_t)(kk * 32);
+                        const uint32_t acc = (kb == 0 && kk == 0) ? 0u : 1u;
+                        umma_i8_pair(d_re, oz_desc(ar + o), oz_desc(br + o), idesc, acc);
+                        umma_i8_pair(d_re, oz_desc(ai + o), oz_desc(nbi + o), idesc, 1u);
+                        umma_i8_pair(d_im, oz_desc(ar + o), oz_desc(bi + o), idesc, acc);
+                        umma_i8_pair(d_im, oz_desc(ai + o), oz_desc(br + o), idesc, 1u);
+                    }
+                    umma_commit_pair(&empty[slot], pair_mask);
                 }
                 if (!stop) {
                     umma_commit_pair(acc_full, pair_mask);
@@ -411,82 +494,40 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     } else {
         // ---------------- epilogue warps 2..9 (both CTAs) ----------------
         // TMEM lane quadrant = warp % 4 (the warp's 32 rows); warps 2-5 take
-        // the first TN / 2 columns of the tile, warps 6-9 the rest.
+        // the first 128 columns of the tile, warps 6-9 the rest.  Every row
+        // and column of the tile lies inside the padded residue planes, so
+        // the stores need no bounds (rows and columns past n hold zeros).
         const int quad = warp & 3;
         const int half = (warp - 2) >> 2;
         const int row = m0 + quad * 32 + lane;
-        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * G::BCOLS);
+        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * OZ_BCOLS);
         const uint32_t free_addr = mapa_shared(smem_u32(acc_free), 0);
-        const int ei = row < n ? p.E[row] : 0;
-        uint32_t fallbacks = 0;
-        for (int d = 2; d <= kOzLastDiag; ++d) {
-            const bool ready = mbar_wait(acc_full, (d - 2) & 1, p.status);
+        const size_t strip = (size_t)p.y_pad * 16;  // bytes of one 16-column strip of a plane
+        uint8_t* const out0 = p.residues + (size_t)((n0 + half * OZ_BCOLS) >> 4) * strip + (size_t)row * 16;
+        for (int mi = 0; mi < kOzMods; ++mi) {
+            const bool ready = mbar_wait(acc_full, mi & 1, p.status);
             tc_fence_after();
             if (!__all_sync(0xffffffffu, ready && !*abort_flag)) {
                 break;
             }
-            const double w = ldexp(1.0, -7 * d);
+            const bool pow2 = mi == 0;
+            const int c16 = p.crt.c16[mi];
+            const float pf = p.crt.pf[mi], inv_pf = p.crt.inv_pf[mi];
+            uint8_t* const re_out = out0 + (size_t)(2 * mi) * p.y_plane;
+            uint8_t* const im_out = re_out + p.y_plane;
 #pragma unroll 1
-            for (int cb = 0; cb < G::BCOLS; cb += 16) {
-                int vr[16], vi[16];
-                tmem_ld16x2_s32(lane_addr + (uint32_t)cb, lane_addr + (uint32_t)(TN + cb), vr, vi);
-                if (row >= n) {
-                    continue;
-                }
-                // The chunk's 16 partial sums are loaded before any is used
-                // (independent loads in flight together): the MMAs wait for
-                // this drain, so its memory latency must overlap.
-                double2 prev[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int col = n0 + half * G::BCOLS + cb + j;
-                    prev[j] = (d == 2 || col >= n) ? make_double2(0.0, 0.0)
-                                                   : __ldcg(&p.partial[(size_t)col * n + row]);
-                }
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int col = n0 + half * G::BCOLS + cb + j;
-                    if (col >= n) {
-                        break;
-                    }
-                    const size_t idx = (size_t)col * n + row;
-                    double2 v = prev[j];
-                    v.x = fma((double)vr[j], w, v.x);
-                    v.y = fma((double)vi[j], w, v.y);
-                    if (d < kOzLastDiag) {
-                        __stcg(&p.partial[idx], v);
-                        continue;
-                    }
-                    if (!flag_at(p.flag_bits, idx)) {
-                        continue;  // not flagged: the GEMM's value stands
-                    }
-                    const int fj = p.F[col];
-                    bool ok = ei != kOzNonFinite && fj != kOzNonFinite;
-                    float2 out = make_float2(0.0f, 0.0f);
-                    if (ok && ei != kOzZero && fj != kOzZero) {
-                        const int sh = ei + fj;
-                        const double zr = ldexp(v.x, sh), zi = ldexp(v.y, sh);
-                        const double lim = ldexp(p.thresh, sh);
-                        ok = fabs(zr) >= lim && fabs(zi) >= lim;
-                        out = make_float2((float)zr, (float)zi);
-                    }
-                    if (ok) {
-                        p.C[idx] = out;
-                    } else {
-                        atomicOr(&p.fallback_bits[idx >> 5], 1u << (idx & 31));
-                        ++fallbacks;
-                    }
-                }
+            for (int cb = 0; cb < OZ_BCOLS; cb += 16) {
+                float vr[16], vi[16];
+                tmem_ld16x2(lane_addr + (uint32_t)cb, lane_addr + (uint32_t)(OZ_TN + cb), vr, vi);
+                const size_t o = (size_t)(cb >> 4) * strip;
+                __stcg(reinterpret_cast<uint4*>(re_out + o), residue_bytes16(vr, pow2, c16, pf, inv_pf));
+                __stcg(reinterpret_cast<uint4*>(im_out + o), residue_bytes16(vi, pow2, c16, pf, inv_pf));
             }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive_cluster(free_addr);
             }
-        }
-        fallbacks = __reduce_add_sync(0xffffffffu, fallbacks);
-        if (lane == 0 && fallbacks != 0) {
-            atomicAdd(&p.stats[kStatFallback], fallbacks);
         }
     }
     tc_fence_before();
@@ -498,6 +539,175 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     }
 }
 
+// ---- 3. reconstruction ---------------------------------------------------------------
+
+// 2^e as a double for -1022 <= e <= 1023.
+__device__ __forceinline__ double pow2d(int e)
+{
+    return __hiloint2double((e + 1023) << 20, 0);
+}
+
+// The exact integer products of one part for four outputs from their residue
+// bytes (word mi holds the four outputs' bytes for modulus mi).
+__device__ __forceinline__ void crt_part(const OzCrt& crt, const uint32_t* words, double* x)
+{
+    double s[4][3];
+    float ks[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        s[c][0] = s[c][1] = s[c][2] = 0.0;
+        ks[c] = 0.0f;
+    }
+#pragma unroll
+    for (int mi = 0; mi < kOzMods; ++mi) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const uint32_t y = (words[mi] >> (8 * c)) & 0xFFu;
+            const double yd = __dsub_rn(__hiloint2double(0x43300000, (int)y), 4503599627370496.0);  // exact
+            const float yf = __fsub_rn(__int_as_float(0x4B000000 | (int)y), 8388608.0f);            // exact
+            // every product and partial sum stays below 2^52: exact
+            s[c][0] = __fma_rn(yd, crt.w[mi][0], s[c][0]);
+            s[c][1] = __fma_rn(yd, crt.w[mi][1], s[c][1]);
+            s[c][2] = __fma_rn(yd, crt.w[mi][2], s[c][2]);
+            ks[c] = __fmaf_rn(yf, crt.inv_pf[mi], ks[c]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        // sum y / p = k + x / M with |x / M| < 1/8; the FP32 sum is off by < 2^-15
+        const double k = (double)rintf(ks[c]);
+        const double d0 = __fma_rn(-k, crt.m[0], s[c][0]);  // exact integers below 2^53
+        const double d1 = __fma_rn(-k, crt.m[1], s[c][1]);
+        const double d2 = __fma_rn(-k, crt.m[2], s[c][2]);
+        // x = (d2 2^40 + d1) 2^40 + d0: two roundings, relative error < 2^-52
+        x[c] = __fma_rn(__fma_rn(d2, 1099511627776.0, d1), 1099511627776.0, d0);
+    }
+}
+
+// One thread per op(A) row and four consecutive op(B) columns; a block holds 64
+// rows x 16 columns inside one pair tile.  Writes every flagged output whose
+// bound certifies it and marks the rest in fallback_bits.
+__global__ void __launch_bounds__(256) ozaki_crt_kernel(const __grid_constant__ OzFinish f)
+{
+    const int quad = threadIdx.x & 3;
+    const int row = blockIdx.y * 64 + (threadIdx.x >> 2);
+    const int col0 = blockIdx.x * 16 + quad * 4;
+    const int n = f.n;
+    const int tm = (blockIdx.y * 64) / OZ_TILE_M, tn = (blockIdx.x * 16) / OZ_TN;
+    if (!f.tile_ran[(size_t)tn * f.tiles_m + tm] || row >= n || col0 >= n) {
+        return;
+    }
+    uint32_t want = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int col = col0 + c;
+        if (col < n && flag_at(f.flag_bits, (size_t)col * n + row)) {
+            want |= 1u << c;
+        }
+    }
+    if (want == 0) {
+        return;
+    }
+    const uint8_t* src = f.residues + ((size_t)blockIdx.x * f.y_pad + row) * 16 + quad * 4;
+    double xr[4], xi[4];
+    {
+        uint32_t words[kOzMods];
+#pragma unroll
+        for (int mi = 0; mi < kOzMods; ++mi) {
+            words[mi] = __ldcs(reinterpret_cast<const uint32_t*>(src + (size_t)(2 * mi) * f.y_plane));
+        }
+        crt_part(f.crt, words, xr);
+#pragma unroll
+        for (int mi = 0; mi < kOzMods; ++mi) {
+            words[mi] = __ldcs(reinterpret_cast<const uint32_t*>(src + (size_t)(2 * mi + 1) * f.y_plane));
+        }
+        crt_part(f.crt, words, xi);
+    }
+    const int ei = f.E[row];
+    const int ca = f.CA[row];
+    uint32_t fallbacks = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        if (!((want >> c) & 1u)) {
+            continue;
+        }
+        const int col = col0 + c;
+        const size_t idx = (size_t)col * n + row;
+        const int fj = f.F[col];
+        bool ok = ei != kOzNonFinite && fj != kOzNonFinite;
+        float2 out = make_float2(0.0f, 0.0f);  // a zero row or column: the exact product is zero
+        if (ok && ei != kOzZero && fj != kOzZero) {
+            const int cnt = ca + f.CB[col];
+            if (cnt != 0) {
+                // |error| <= cnt 2^(beta - 1): both parts must exceed 2^25 (1 + 2^-20) times that
+                const double lim = (double)cnt * 0x1.00001p+71;
+                ok = fabs(xr[c]) >= lim && fabs(xi[c]) >= lim;
+            }
+            const double sc = pow2d(ei + fj - 2 * kOzBeta);  // exact: x is an integer, |x| >= 1 or x = 0
+            out = make_float2((float)(xr[c] * sc), (float)(xi[c] * sc));
+        }
+        if (ok) {
+            f.C[idx] = out;
+        } else {
+            atomicOr(&f.fallback_bits[idx >> 5], 1u << (idx & 31));
+            ++fallbacks;
+        }
+    }
+    if (fallbacks != 0) {
+        atomicAdd(&f.stats[kStatFallback], fallbacks);
+    }
+}
+
+// The constants of the moduli, exact in 128-bit integers.
+OzCrt make_crt()
+{
+    OzCrt c{};
+    unsigned __int128 M = 1;
+    for (int mi = 0; mi < kOzMods; ++mi) {
+        M *= (unsigned)kOzModuli[mi];
+    }
+    const unsigned __int128 mask40 = ((unsigned __int128)1 << 40) - 1;
+    auto limbs = [&](unsigned __int128 v, double* out) {
+        for (int l = 0; l < 3; ++l) {
+            out[l] = (double)(uint64_t)((v >> (40 * l)) & mask40);
+        }
+    };
+    for (int mi = 0; mi < kOzMods; ++mi) {
+        const int p = kOzModuli[mi];
+        const unsigned __int128 W = M / (unsigned)p;
+        const int wm = (int)(W % (unsigned)p);
+        int u = 0;
+        for (int v = 1; v < p; ++v) {
+            if ((wm * v) % p == 1) {
+                u = v;
+                break;
+            }
+        }
+        c.p[mi] = p;
+        c.u[mi] = u > p / 2 ? u - p : u;
+        c.c16[mi] = (1 << 16) % p;
+        c.pf[mi] = (float)p;
+        c.inv_pf[mi] = 1.0f / (float)p;
+        c.pd[mi] = (double)p;
+        c.inv_pd[mi] = 1.0 / (double)p;
+        limbs(W, c.w[mi]);
+    }
+    limbs(M, c.m);
+    return c;
+}
+
+// Whether every exact product of order <= kOzMaxN lies within M / 8 (the
+// reconstruction's margin).
+bool crt_range_ok()
+{
+    unsigned __int128 M = 1;
+    for (int mi = 0; mi < kOzMods; ++mi) {
+        M *= (unsigned)kOzModuli[mi];
+    }
+    const unsigned __int128 bound = (unsigned __int128)(2 * kOzMaxN) << (2 * kOzBeta);
+    return bound <= M / 8;
+}
+
 }  // namespace
 
 OzLayout oz_layout(int n, uint8_t* base, std::vector<size_t>* guards)
@@ -505,75 +715,44 @@ OzLayout oz_layout(int n, uint8_t* base, std::vector<size_t>* guards)
     OzLayout L;
     L.kpitch = (n + 63) / 64 * 64;
     L.plane_bytes = (size_t)n * L.kpitch;
+    L.y_pad = (n + kOzakiTile - 1) / kOzakiTile * kOzakiTile;
+    L.y_plane = (size_t)L.y_pad * L.y_pad;
+    const int tiles = L.y_pad / kOzakiTile;
     size_t off = 0;
     const size_t e_off = off;
     off = next_region(off, (size_t)n * 4, guards);
     const size_t f_off = off;
     off = next_region(off, (size_t)n * 4, guards);
+    const size_t ca_off = off;
+    off = next_region(off, (size_t)n * 4, guards);
+    const size_t cb_off = off;
+    off = next_region(off, (size_t)n * 4, guards);
+    const size_t t_off = off;
+    off = next_region(off, (size_t)tiles * tiles, guards);
     const size_t a_off = off;
-    off = next_region(off, 2 * kOzS * L.plane_bytes, guards);
+    off = next_region(off, 2 * kOzMods * L.plane_bytes, guards);
     const size_t b_off = off;
-    off = next_region(off, 3 * kOzS * L.plane_bytes, guards);
-    const size_t p_off = off;
-    off = next_region(off, (size_t)n * n * sizeof(double2), guards);
+    off = next_region(off, 3 * kOzMods * L.plane_bytes, guards);
+    const size_t y_off = off;
+    off = next_region(off, 2 * kOzMods * L.y_plane, guards);
     L.bytes = off;
     if (base != nullptr) {
         L.E = reinterpret_cast<int*>(base + e_off);
         L.F = reinterpret_cast<int*>(base + f_off);
+        L.CA = reinterpret_cast<int*>(base + ca_off);
+        L.CB = reinterpret_cast<int*>(base + cb_off);
+        L.tile_ran = base + t_off;
         L.planes_a = reinterpret_cast<int8_t*>(base + a_off);
         L.planes_b = reinterpret_cast<int8_t*>(base + b_off);
-        L.partial = reinterpret_cast<double2*>(base + p_off);
+        L.residues = base + y_off;
     }
     return L;
 }
 
-// Tile width of the exact recompute.  256 x 192 tiles fill the waves of 74
-// clusters better at n = 4096 (4.76 waves instead of 3.46) but measured no
-// faster (7.15 against 7.03 ms: the narrower MMA and the partial last column
-// cost what the fuller waves save), so every order uses 256 x 256.
 int ozaki_tile_n(int n)
 {
     (void)n;
-    return 256;
-}
-
-template <int TN>
-static cudaError_t launch_pair_tn(cudaStream_t s, int n, const OzLayout& L, OzParams p)
-{
-    using G = OzGeom<TN>;
-    CUtensorMap ta, tb;
-    const uint64_t dims_a[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(2 * kOzS)};
-    const uint64_t dims_b[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(3 * kOzS)};
-    const uint64_t strides[2] = {(uint64_t)L.kpitch, (uint64_t)L.plane_bytes};
-    const uint32_t box_a[3] = {(uint32_t)OZ_BK, (uint32_t)OZ_ROWS, 2u};
-    const uint32_t box_b[3] = {(uint32_t)OZ_BK, (uint32_t)G::BCOLS, 3u};
-    if (!encode_tensor_map(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims_a, strides, box_a, CU_TENSOR_MAP_SWIZZLE_64B,
-                           L.planes_a) ||
-        !encode_tensor_map(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims_b, strides, box_b, CU_TENSOR_MAP_SWIZZLE_64B,
-                           L.planes_b)) {
-        return cudaErrorInvalidValue;
-    }
-    p.tiles_m = (n + OZ_TILE_M - 1) / OZ_TILE_M;
-    p.tiles_n = (n + TN - 1) / TN;
-    auto kernel = ozaki_pair_kernel<TN>;
-    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
-    if (err != cudaSuccess) {
-        return err;
-    }
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3((unsigned)(2 * p.tiles_m * p.tiles_n));
-    cfg.blockDim = dim3(kOzThreads);
-    cfg.dynamicSmemBytes = G::SMEM;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 2;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    err = cudaLaunchKernelEx(&cfg, kernel, ta, tb, p);
-    return err != cudaSuccess ? err : cudaGetLastError();
+    return OZ_TN;
 }
 
 cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a, const float2* rows_b,
@@ -581,26 +760,88 @@ cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a,
                          uint32_t* fallback_bits, float2* C, int* status, int* launched,
                          const std::function<void(int)>& mark)
 {
+    static const OzCrt crt = make_crt();
+    static const bool range_ok = crt_range_ok();
     int count = 0;
+    if (launched != nullptr) {
+        *launched = 0;
+    }
+    if (n > kOzMaxN || !range_ok) {
+        return cudaErrorInvalidValue;  // the moduli cover the exact products up to order kOzMaxN
+    }
     ozaki_split_kernel<<<2 * n, 256, 0, s>>>(n, pitch, rows_a, rows_b, L.planes_a, L.planes_b, L.kpitch,
-                                              L.plane_bytes, L.E, L.F);
+                                              L.plane_bytes, L.E, L.F, L.CA, L.CB, crt);
     cudaError_t err = cudaGetLastError();
     mark(++count);
+    const int tiles = L.y_pad / kOzakiTile;
     if (err == cudaSuccess) {
+        CUtensorMap ta, tb;
+        const uint64_t dims_a[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(2 * kOzMods)};
+        const uint64_t dims_b[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(3 * kOzMods)};
+        const uint64_t strides[2] = {(uint64_t)L.kpitch, (uint64_t)L.plane_bytes};
+        const uint32_t box_a[3] = {(uint32_t)OZ_BK, (uint32_t)OZ_ROWS, 2u};
+        const uint32_t box_b[3] = {(uint32_t)OZ_BK, (uint32_t)OZ_BCOLS, 3u};
+        if (!encode_tensor_map(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims_a, strides, box_a,
+                               CU_TENSOR_MAP_SWIZZLE_64B, L.planes_a) ||
+            !encode_tensor_map(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims_b, strides, box_b,
+                               CU_TENSOR_MAP_SWIZZLE_64B, L.planes_b)) {
+            err = cudaErrorInvalidValue;
+        }
         OzParams p{};
         p.n = n;
         p.kblocks = (n + OZ_BK - 1) / OZ_BK;
-        p.E = L.E;
-        p.F = L.F;
-        p.flag_bits = flag_bits;
+        p.tiles_m = tiles;
+        p.tiles_n = tiles;
         p.tile_count = tile_count;
         p.stats = stats;
-        p.fallback_bits = fallback_bits;
-        p.partial = L.partial;
-        p.C = C;
-        p.thresh = ldexp(1.0 + ldexp(1.0, -20), 25) * (2.0 * n * (kOzS + 1)) * ldexp(1.0, -7 * kOzS);
+        p.tile_ran = L.tile_ran;
+        p.residues = L.residues;
+        p.y_pad = L.y_pad;
+        p.y_plane = L.y_plane;
+        p.crt = crt;
         p.status = status;
-        err = launch_pair_tn<256>(s, n, L, p);
+        if (err == cudaSuccess) {
+            err = cudaFuncSetAttribute(ozaki_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OZ_SMEM);
+        }
+        if (err == cudaSuccess) {
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3((unsigned)(2 * tiles * tiles));
+            cfg.blockDim = dim3(kOzThreads);
+            cfg.dynamicSmemBytes = OZ_SMEM;
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = 2;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            err = cudaLaunchKernelEx(&cfg, ozaki_pair_kernel, ta, tb, p);
+            if (err == cudaSuccess) {
+                err = cudaGetLastError();
+            }
+        }
+        mark(++count);
+    }
+    if (err == cudaSuccess) {
+        OzFinish f{};
+        f.n = n;
+        f.tiles_m = tiles;
+        f.E = L.E;
+        f.F = L.F;
+        f.CA = L.CA;
+        f.CB = L.CB;
+        f.tile_ran = L.tile_ran;
+        f.residues = L.residues;
+        f.y_pad = L.y_pad;
+        f.y_plane = L.y_plane;
+        f.flag_bits = flag_bits;
+        f.stats = stats;
+        f.fallback_bits = fallback_bits;
+        f.C = C;
+        f.crt = crt;
+        ozaki_crt_kernel<<<dim3((unsigned)(L.y_pad / 16), (unsigned)(L.y_pad / 64)), 256, 0, s>>>(f);
+        err = cudaGetLastError();
         mark(++count);
     }
     if (launched != nullptr) {

@@ -541,11 +541,11 @@ def kernel_roofline(name, ms, n, form, sm_count, sgemm, stats, mhz):
                 "work_model": f"6*n^3 real flop x {p} pass(es)", "peak_source": peak_src}
     if name == "exact_tiles":
         positions = float(stats.get("exact_positions", 0)) if stats else 0.0
-        work = 2.0 * 36 * 4 * positions * n  # int8 ops: 36 slice pairs x 4 real products per output and term
+        work = 2.0 * 14 * 4 * positions * n  # int8 ops: 14 moduli x 4 real products per output and term
         peak = 2.0 * pk["bf16_tflops"]
         return {"bound": "tensor", "achieved": work / (ms * 1e-3) / 1e12, "peak": peak, "unit": "Top/s",
                 "work_per_launch": work,
-                "work_model": "2 x 36 slice pairs x 4 real products x n int8 ops per output position of the tiles run",
+                "work_model": "2 x 14 moduli x 4 real products x n int8 ops per output position of the tiles run",
                 "peak_source": f"{src} bf16 burst x 2 (dense int8 is twice the dense bf16 rate)"}
     if name.startswith("recompute_fp64") or name.startswith("fallback"):
         key = "fallback_outputs" if name.startswith("fallback") else "sparse_outputs"

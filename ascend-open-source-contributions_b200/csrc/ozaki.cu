@@ -132,15 +132,15 @@ __device__ __forceinline__ bool flag_at(const uint32_t* bits, size_t idx)
     return (bits[idx >> 5] >> (idx & 31)) & 1u;
 }
 
-// t mod p in [-(p-1)/2, (p-1)/2] for odd p and an integer-valued t, |t| <= 2^47:
-// the nearest integer q to t * rn(1/p) is the nearest integer to t / p (their
-// distance, <= 2^-13.6, is below that of t / p to a half-integer, >= 1 / 2p),
-// and t - q p is exact.
-__device__ __forceinline__ int mod_odd_d(double t, double pd, double inv_pd)
+// t mod p in [-(p-1)/2, (p-1)/2] for odd p and an integer-valued t, |t| <= 2^47,
+// given tm = t + 1.5 * 2^52 (exact): the nearest integer q to t * rn(1/p) is
+// the nearest integer to t / p (their distance, <= 2^-13.6, is below that of
+// t / p to a half-integer, >= 1 / 2p), and tm - q p = 1.5 * 2^52 + (t - q p)
+// is exact, its low word the residue.
+__device__ __forceinline__ int mod_odd_d(double t, double tm, double pd, double inv_pd)
 {
     const double q = __dsub_rn(__fma_rn(t, inv_pd, kMagic), kMagic);
-    const double r = __fma_rn(-q, pd, t);
-    return __double2loint(__dadd_rn(r, kMagic));  // the low word of r + 1.5 * 2^52 is r
+    return __double2loint(__fma_rn(-q, pd, tm));
 }
 
 // v mod p in [-(p-1)/2, (p-1)/2] for odd p >= 199 and |v| <= 127^2 (|v / p| is
@@ -158,7 +158,7 @@ __device__ __forceinline__ int mod_odd_f(int v, float pf, float inv_pf)
 // One block per op(A) row (blockIdx.x < n) or op(B) column.  Plane layout:
 // [plane][row][kpitch] int8, A planes 2m + {0 re, 1 im}, B planes
 // 3m + {0 re, 1 im, 2 -im}.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     ozaki_split_kernel(int n, int pitch, const float2* __restrict__ rows_a, const float2* __restrict__ rows_b,
                        int8_t* __restrict__ pa, int8_t* __restrict__ pb, int kpitch, size_t plane_bytes,
                        int* __restrict__ E, int* __restrict__ F, int* __restrict__ CA, int* __restrict__ CB,
@@ -204,44 +204,45 @@ __global__ void __launch_bounds__(256)
     int rounded = 0;
     // Four consecutive K terms per thread: 4-byte stores into every plane.
     for (int k0 = tid * 4; k0 < n; k0 += 256 * 4) {
-        double t[8];  // re of terms 0..3, then im
+        // The real parts, then the imaginary parts, of four consecutive terms.
+#pragma unroll 1
+        for (int part = 0; part < 2; ++part) {
+            double t[4], tm[4];  // tm = t + 1.5 * 2^52
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int k = k0 + u;
-            const float2 x = (k < n && usable) ? src[k] : make_float2(0.0f, 0.0f);
-            const double sr = __dmul_rn((double)x.x, scale);  // exact: a power-of-two scaling in FP64
-            const double si = __dmul_rn((double)x.y, scale);
-            t[u] = __dsub_rn(__dadd_rn(sr, kMagic), kMagic);  // nearest integer, |t| <= 2^beta
-            t[4 + u] = __dsub_rn(__dadd_rn(si, kMagic), kMagic);
-            rounded += (t[u] != sr) + (t[4 + u] != si);
-        }
-#pragma unroll
-        for (int mi = 0; mi < kOzMods; ++mi) {
-            int v[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                if (mi == 0) {
-                    // mod 256: the low byte of the two's complement integer
-                    v[q] = (int)(signed char)(__double2loint(__dadd_rn(t[q], kMagic)) & 0xFF);
-                } else {
-                    v[q] = mod_odd_d(t[q], crt.pd[mi], crt.inv_pd[mi]);
-                }
-                if (is_a) {
-                    const int w = v[q] * crt.u[mi];
-                    v[q] = mi == 0 ? (int)(signed char)(w & 0xFF) : mod_odd_f(w, crt.pf[mi], crt.inv_pf[mi]);
-                }
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u;
+                const float2 x = (k < n && usable) ? src[k] : make_float2(0.0f, 0.0f);
+                const double sx = __dmul_rn((double)(part == 0 ? x.x : x.y), scale);  // exact: a power of two
+                tm[u] = __dadd_rn(sx, kMagic);    // rounds to an integer: |sx| < 2^51
+                t[u] = __dsub_rn(tm[u], kMagic);  // nearest integer, |t| <= 2^beta
+                rounded += t[u] != sx;
             }
-            int8_t* base = dst + (size_t)(planes_per_mod * mi) * plane_bytes;
-            // K beyond n is never read (the tensor maps stop at n), so whole
-            // 4-byte groups may be stored while k0 < n <= kpitch.
-            *reinterpret_cast<char4*>(base + k0) =
-                make_char4((signed char)v[0], (signed char)v[1], (signed char)v[2], (signed char)v[3]);
-            *reinterpret_cast<char4*>(base + plane_bytes + k0) =
-                make_char4((signed char)v[4], (signed char)v[5], (signed char)v[6], (signed char)v[7]);
-            if (!is_a) {
-                // -(-128) wraps to -128: the same residue mod 256
-                *reinterpret_cast<char4*>(base + 2 * plane_bytes + k0) =
-                    make_char4((signed char)-v[4], (signed char)-v[5], (signed char)-v[6], (signed char)-v[7]);
+#pragma unroll
+            for (int mi = 0; mi < kOzMods; ++mi) {
+                int v[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (mi == 0) {
+                        // mod 256: the low byte of the two's complement integer
+                        v[q] = (int)(signed char)(__double2loint(tm[q]) & 0xFF);
+                    } else {
+                        v[q] = mod_odd_d(t[q], tm[q], crt.pd[mi], crt.inv_pd[mi]);
+                    }
+                    if (is_a) {
+                        const int w = v[q] * crt.u[mi];
+                        v[q] = mi == 0 ? (int)(signed char)(w & 0xFF) : mod_odd_f(w, crt.pf[mi], crt.inv_pf[mi]);
+                    }
+                }
+                int8_t* plane = dst + (size_t)(planes_per_mod * mi + part) * plane_bytes;
+                // K beyond n is never read (the tensor maps stop at n), so whole
+                // 4-byte groups may be stored while k0 < n <= kpitch.
+                *reinterpret_cast<char4*>(plane + k0) =
+                    make_char4((signed char)v[0], (signed char)v[1], (signed char)v[2], (signed char)v[3]);
+                if (!is_a && part == 1) {
+                    // -(-128) wraps to -128: the same residue mod 256
+                    *reinterpret_cast<char4*>(plane + plane_bytes + k0) =
+                        make_char4((signed char)-v[0], (signed char)-v[1], (signed char)-v[2], (signed char)-v[3]);
+                }
             }
         }
     }
@@ -547,24 +548,27 @@ __device__ __forceinline__ double pow2d(int e)
     return __hiloint2double((e + 1023) << 20, 0);
 }
 
-// The exact integer products of one part for four outputs from their residue
-// bytes (word mi holds the four outputs' bytes for modulus mi).
-__device__ __forceinline__ void crt_part(const OzCrt& crt, const uint32_t* words, double* x)
+// The exact integer products of one part for outputs c0 and c0 + 1 of the
+// four whose residue bytes the words hold (word mi: byte c for modulus mi).
+__device__ __forceinline__ void crt_part2(const OzCrt& crt, const uint32_t* words, int c0, double* x)
 {
-    double s[4][3];
-    float ks[4];
+    double s[2][3];
+    float ks[2];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < 2; ++c) {
         s[c][0] = s[c][1] = s[c][2] = 0.0;
         ks[c] = 0.0f;
     }
 #pragma unroll
     for (int mi = 0; mi < kOzMods; ++mi) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const uint32_t y = (words[mi] >> (8 * c)) & 0xFFu;
-            const double yd = __dsub_rn(__hiloint2double(0x43300000, (int)y), 4503599627370496.0);  // exact
-            const float yf = __fsub_rn(__int_as_float(0x4B000000 | (int)y), 8388608.0f);            // exact
+        for (int c = 0; c < 2; ++c) {
+            // byte c0 + c of the word as the low byte of 2^52 + y (FP64) and 2^23 + y (FP32)
+            const unsigned sel = (unsigned)(c0 + c);
+            const int lo = (int)__byte_perm(words[mi], 0u, 0x4440u + sel);
+            const int fb = (int)__byte_perm(words[mi], 0x4B000000u, 0x7440u + sel);
+            const double yd = __dsub_rn(__hiloint2double(0x43300000, lo), 4503599627370496.0);  // exact
+            const float yf = __fsub_rn(__int_as_float(fb), 8388608.0f);                         // exact
             // every product and partial sum stays below 2^52: exact
             s[c][0] = __fma_rn(yd, crt.w[mi][0], s[c][0]);
             s[c][1] = __fma_rn(yd, crt.w[mi][1], s[c][1]);
@@ -573,14 +577,14 @@ __device__ __forceinline__ void crt_part(const OzCrt& crt, const uint32_t* words
         }
     }
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < 2; ++c) {
         // sum y / p = k + x / M with |x / M| < 1/8; the FP32 sum is off by < 2^-15
         const double k = (double)rintf(ks[c]);
         const double d0 = __fma_rn(-k, crt.m[0], s[c][0]);  // exact integers below 2^53
         const double d1 = __fma_rn(-k, crt.m[1], s[c][1]);
         const double d2 = __fma_rn(-k, crt.m[2], s[c][2]);
         // x = (d2 2^40 + d1) 2^40 + d0: two roundings, relative error < 2^-52
-        x[c] = __fma_rn(__fma_rn(d2, 1099511627776.0, d1), 1099511627776.0, d0);
+        x[c0 + c] = __fma_rn(__fma_rn(d2, 1099511627776.0, d1), 1099511627776.0, d0);
     }
 }
 
@@ -616,12 +620,14 @@ __global__ void __launch_bounds__(256) ozaki_crt_kernel(const __grid_constant__ 
         for (int mi = 0; mi < kOzMods; ++mi) {
             words[mi] = __ldcs(reinterpret_cast<const uint32_t*>(src + (size_t)(2 * mi) * f.y_plane));
         }
-        crt_part(f.crt, words, xr);
+        crt_part2(f.crt, words, 0, xr);
+        crt_part2(f.crt, words, 2, xr);
 #pragma unroll
         for (int mi = 0; mi < kOzMods; ++mi) {
             words[mi] = __ldcs(reinterpret_cast<const uint32_t*>(src + (size_t)(2 * mi + 1) * f.y_plane));
         }
-        crt_part(f.crt, words, xi);
+        crt_part2(f.crt, words, 0, xi);
+        crt_part2(f.crt, words, 2, xi);
     }
     const int ei = f.E[row];
     const int ca = f.CA[row];

@@ -175,7 +175,8 @@ class Handle:
             pass
 
     def set_stage_events(self, events):
-        """Record the given torch.cuda.Event objects around each kernel of later calls."""
+        """Record the given torch.cuda.Event objects around each kernel of later
+        calls: kernel j between events[2j] and events[2j + 1]."""
         for e in events:
             if not e.cuda_event:  # torch creates the CUDA event lazily on first record
                 e.record()
@@ -348,9 +349,10 @@ def stage_names(info):
         return ["onchip"][:k]
     if info["rounding"]:
         fp32 = info["form"] == FORM["fp32"]
-        tail = ["replay_tiles", "replay_outputs"] if fp32 else \
-            ["exact_split", "exact_tiles", "exact_crt", "recompute_fp64_outputs", "fallback_fp64"]
-        names = ["pack", "gemm_path", "pack_rows", "energy", "select", "lane_major"] + tail
+        prep = ["pack_rows", "energy", "lane_major"] + ([] if fp32 else ["exact_split"])
+        tail = ["select", "replay_tiles", "replay_outputs"] if fp32 else \
+            ["select", "gemm_form_tiles", "exact_tiles", "exact_crt", "recompute_fp64_outputs", "fallback_fp64"]
+        names = ["pack", "gemm_path"] + prep + tail
     else:
         names = ["pack", "gemm", "merge"]
     names = names[:k]

@@ -207,11 +207,22 @@ cudaError_t device_malloc(void** p, size_t bytes)
 cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status, int* kernels,
                     const cudaEvent_t* events, int nevents)
 {
-    int count = 0;
-    auto mark = [&](int i) {
-        if (events != nullptr && i < nevents && events[i] != nullptr) {
-            cudaEventRecord(events[i], s);
+    auto record = [&](int idx, cudaStream_t st) {
+        if (events != nullptr && idx >= 0 && idx < nevents && events[idx] != nullptr) {
+            cudaEventRecord(events[idx], st);
         }
+    };
+    // Marks for a run of `len` kernels with call indices first, first + 1, ...
+    // on stream st: the first one's begin now, and after the i-th (1-based)
+    // its end and the next one's begin.
+    auto run_marks = [&](int first, int len, cudaStream_t st) {
+        record(2 * first, st);
+        return [&record, first, len, st](int i) {
+            record(2 * (first + i - 1) + 1, st);
+            if (i < len) {
+                record(2 * (first + i), st);
+            }
+        };
     };
     if (plan.guards > 0) {
         const cudaError_t e = fill_guards(s, ws, plan.guard_off, plan.guards);
@@ -219,8 +230,8 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
             return e;
         }
     }
-    mark(0);
     if (plan.engine == 2) {
+        auto mark = run_marks(0, 1, s);
         const cudaError_t e = launch_single(s, p, 0, 0, plan.onchip_tile, plan.parts);
         mark(1);
         if (kernels != nullptr) {
@@ -228,26 +239,37 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
         }
         return e;
     }
-    cudaError_t err = launch_pack(s, p, plan, ws);
-    mark(++count);
-    if (err == cudaSuccess) {
-        if (plan.rounding) {
-            err = launch_gemm_with_path(s, p, plan, ws, status);
-        } else {
-            err = plan.form == CG3M_FORM_FP32 ? launch_gemm_fp32(s, p, plan, ws, status)
-                                              : launch_gemm_tc(s, p, plan, ws, status);
+    const int main_len = 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0);
+    const int prep_len = plan.rounding ? rounding_prep_kernels(plan.form) : 0;
+    cudaError_t err = cudaSuccess;
+    int prep_launched = 0;
+    int count = 0;
+    {
+        auto mark = run_marks(0, main_len, s);
+        err = launch_pack(s, p, plan, ws);
+        mark(++count);
+        if (err == cudaSuccess) {
+            if (plan.rounding) {
+                err = launch_gemm_with_path(s, p, plan, ws, status);
+            } else {
+                err = plan.form == CG3M_FORM_FP32 ? launch_gemm_fp32(s, p, plan, ws, status)
+                                                  : launch_gemm_tc(s, p, plan, ws, status);
+            }
+            mark(++count);
         }
-        mark(++count);
-    }
-    if (err == cudaSuccess && plan.parts > 1 && !plan.cluster_merge) {
-        err = launch_merge(s, p, plan, ws);
-        mark(++count);
+        if (err == cudaSuccess && plan.parts > 1 && !plan.cluster_merge) {
+            err = launch_merge(s, p, plan, ws);
+            mark(++count);
+        }
     }
     if (err == cudaSuccess && plan.rounding) {
-        int launched = 0;
-        const int before = count;
-        err = launch_rounding(s, p, plan, ws, status, &launched, [&](int i) { mark(before + i); });
-        count += launched;
+        err = launch_rounding_prep(s, p, plan, ws, &prep_launched, run_marks(count, prep_len, s));
+        count += prep_launched;
+        if (err == cudaSuccess) {
+            int launched = 0;
+            err = launch_rounding_finish(s, p, plan, ws, status, &launched, run_marks(count, 64, s));
+            count += launched;
+        }
     }
     if (err == cudaSuccess && plan.guards > 0) {
         err = check_guards(s, ws, plan.guard_off, plan.guards);
@@ -688,10 +710,10 @@ cg3mStatus_t cg3mSetStageEvents(cg3mHandle_t h, void* const* events, int count)
     if (h == nullptr) {
         return CG3M_STATUS_HANDLE_IS_NULLPTR;
     }
-    if (count < 0 || count > 16 || (count > 0 && events == nullptr)) {
+    if (count < 0 || count > 32 || (count > 0 && events == nullptr)) {
         return CG3M_STATUS_INVALID_VALUE;
     }
-    for (int i = 0; i < 16; ++i) {
+    for (int i = 0; i < 32; ++i) {
         h->stage_events[i] = i < count ? static_cast<cudaEvent_t>(events[i]) : nullptr;
     }
     h->stage_event_count = count;
@@ -853,7 +875,7 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
     info->k_span = plan.span;
     info->rounding = plan.rounding ? 1 : 0;
     info->kernels =
-        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? (plan.form == CG3M_FORM_FP32 ? 6 : 9) : 0);
+        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? (plan.form == CG3M_FORM_FP32 ? 6 : 10) : 0);
     info->workspace_bytes = plan.total;
     return CG3M_STATUS_SUCCESS;
 }

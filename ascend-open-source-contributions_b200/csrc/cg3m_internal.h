@@ -22,7 +22,7 @@ struct cg3mContext {
     size_t user_ws_bytes = 0;
     int* status = nullptr;       // device status word (bounded-wait failures)
     uint32_t* round_stats = nullptr;  // counters of the last call's rounding pass (null if it had none)
-    cudaEvent_t stage_events[16] = {};
+    cudaEvent_t stage_events[32] = {};
     int stage_event_count = 0;
     // host-buffer entry point: device copies of A, B, C and its copy streams
     void* host_arena = nullptr;
@@ -96,12 +96,25 @@ cudaError_t launch_pack(cudaStream_t s, const Problem& p, const Plan& plan, void
 cudaError_t launch_gemm_fp32(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
 cudaError_t launch_gemm_tc(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
 cudaError_t launch_merge(cudaStream_t s, const Problem& p, const Plan& plan, void* ws);
-// The rounding-correction kernels after the path GEMM; mark(i) is called after
-// the i-th of them (1-based) is enqueued.
-cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status, int* launched,
-                            const std::function<void(int)>& mark);
-// GEMM that also writes the risk plane used by the rounding-correction pass.
+// The rounding-correction pass in two halves: the preparation reads only
+// op(A) and op(B) (packed rows, energies, lane-major copies and, for the
+// tensor-core forms, the residues of the exact recompute); the finish needs
+// the GEMM's C and risk plane (selection, then the recomputes).  mark(i) is
+// called after the i-th kernel of each half (1-based) is enqueued.
+int rounding_prep_kernels(int form);
+cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* launched,
+                                 const std::function<void(int)>& mark);
+cudaError_t launch_rounding_finish(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status,
+                                   int* launched, const std::function<void(int)>& mark);
+// GEMM that also writes the risk plane used by the rounding-correction pass
+// (the tensor-core forms: one pass over the leading split planes, whose C the
+// pass then replaces everywhere).
 cudaError_t launch_gemm_with_path(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
+// Tensor-core forms in the rounding pass: the form's own products on every
+// 256 x 128 pair tile outside the tiles the exact recompute takes (tile_count:
+// the pass's per-16 x 16 flagged counts).
+cudaError_t launch_gemm_tc_tiles(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status,
+                                 const uint32_t* tile_count);
 // Rounding pass: a 16 x 16 tile with more flagged outputs than this is
 // recomputed as part of a tile; sparser tiles have each flagged output
 // recomputed on its own.  Counters it leaves beside the flags:
@@ -141,14 +154,14 @@ struct OzLayout {
     size_t bytes = 0;
 };
 OzLayout oz_layout(int n, uint8_t* base, std::vector<size_t>* guards = nullptr);
-// Residues of op(A) rows and op(B) columns, then the exact products of every
-// tile holding a dense 16 x 16 tile and their reconstruction into the flagged
-// outputs; outputs it cannot certify are marked in fallback_bits.  Three
-// launches; mark(i) after the i-th (1-based).
-cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a, const float2* rows_b,
-                         const OzLayout& L, const uint32_t* flag_bits, const uint32_t* tile_count, uint32_t* stats,
-                         uint32_t* fallback_bits, float2* C, int* status, int* launched,
-                         const std::function<void(int)>& mark);
+// Residues of op(A) rows and op(B) columns (needs only the packed rows).
+cudaError_t launch_ozaki_split(cudaStream_t s, int n, int pitch, const float2* rows_a, const float2* rows_b,
+                               const OzLayout& L);
+// The exact products of every tile holding a dense 16 x 16 tile and their
+// reconstruction into every output of those tiles; outputs it cannot certify
+// are marked in fallback_bits.  Two launches; mark(i) after the i-th (1-based).
+cudaError_t launch_ozaki_tiles(cudaStream_t s, int n, const OzLayout& L, const uint32_t* tile_count, uint32_t* stats, uint32_t* fallback_bits, float2* C,
+                               int* status, int* launched, const std::function<void(int)>& mark);
 // Bytes of the rounding-correction region for a square problem of order n.
 size_t rounding_bytes(int n, int form, std::vector<size_t>* guards = nullptr);
 // Device address of the pass's counters (flagged, recomputed as tiles, one by
@@ -195,8 +208,9 @@ cudaError_t launch_strided(cudaStream_t s, const Problem& p, int mode, int repai
                            long long sC, int batch, const StridedPlan& plan, void* ws, int sm_count);
 
 // Enqueue a fully planned call (pack + GEMM [+ merge] [+ rounding]); when
-// `events` is non-null, events[0] is recorded before the first launch and
-// events[i] after the i-th (i < nevents).
+// `events` is non-null, kernel j (in the order the call info names them) is
+// bracketed by events[2j] and events[2j + 1], recorded on the stream it runs
+// on (entries past nevents are skipped).
 cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status, int* kernels,
                     const cudaEvent_t* events = nullptr, int nevents = 0);
 

@@ -71,6 +71,7 @@ struct TcCfg;
 template <>
 struct TcCfg<CG3M_FORM_TF32X3> {
     static constexpr int S = 2;        // split planes per component (hi, lo)
+    static constexpr int ZS = 2;       // planes per component in the packed layout
     static constexpr int BK = 32;      // K elements per 128-byte row
     static constexpr int NPAIRS = 3;   // lo*hi, hi*lo, hi*hi
     static constexpr uint32_t FMT = 2; // TF32
@@ -80,6 +81,7 @@ struct TcCfg<CG3M_FORM_TF32X3> {
 template <>
 struct TcCfg<CG3M_FORM_BF16X6> {
     static constexpr int S = 3;        // b0, b1, b2
+    static constexpr int ZS = 3;
     static constexpr int BK = 64;
     static constexpr int NPAIRS = 6;   // b_i*b_j with i+j <= 2, smallest first
     static constexpr uint32_t FMT = 1; // BF16
@@ -99,6 +101,7 @@ struct TcCfg<CG3M_FORM_BF16X6> {
 template <>
 struct TcCfg<CG3M_FORM_BF16X9> {
     static constexpr int S = 3;
+    static constexpr int ZS = 3;
     static constexpr int BK = 64;
     static constexpr int NPAIRS = 9;   // all b_i*b_j, smallest first
     static constexpr uint32_t FMT = 1;
@@ -116,6 +119,34 @@ struct TcCfg<CG3M_FORM_BF16X9> {
             default: return make_int2(0, 0);
         }
     }
+};
+
+// The leading split plane alone (one tensor pass over the form's packed
+// planes, ZS of them per component): the risk plane of the tensor-core forms'
+// rounding pass.  The pass recomputes exactly every output of a tile it finds
+// dense and runs the form's own products on the other tiles, so this product
+// only feeds the selection, whose risk estimate needs a few significant bits.
+constexpr int kLeadTf32 = 100;
+constexpr int kLeadBf16 = 101;
+
+template <>
+struct TcCfg<kLeadTf32> {
+    static constexpr int S = 1;
+    static constexpr int ZS = 2;
+    static constexpr int BK = 32;
+    static constexpr int NPAIRS = 1;
+    static constexpr uint32_t FMT = 2;
+    __device__ static int2 pair(int) { return make_int2(0, 0); }
+};
+
+template <>
+struct TcCfg<kLeadBf16> {
+    static constexpr int S = 1;
+    static constexpr int ZS = 3;
+    static constexpr int BK = 64;
+    static constexpr int NPAIRS = 1;
+    static constexpr uint32_t FMT = 1;
+    __device__ static int2 pair(int) { return make_int2(0, 0); }
 };
 
 // Geometry of one instantiation: output tile 128 x BN.
@@ -145,6 +176,9 @@ struct TcParams {
     int seg_blocks;  // K-blocks per accumulation segment
     float* path;     // risk plane (path-tracking variant), ld = ldc
     int cluster_merge;  // pair kernel: the `parts` pairs of a tile form one cluster and merge on chip
+    // pair kernel in the rounding pass: the per-16 x 16 flagged counts; pair
+    // tiles inside a 256 x 256 tile the exact recompute takes are skipped
+    const uint32_t* skip_count;
 };
 
 // Loads from a shared::cluster address (a peer block's shared memory).
@@ -278,8 +312,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                         uint8_t* st = ring + s * STAGE_BYTES;
                         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-                        tma_load_3d(st, &tmA, &full[s], kbeg + kb * Cfg::BK, m0, c * Cfg::S);
-                        tma_load_3d(st + Cfg::S * A_PLANE, &tmB, &full[s], kbeg + kb * Cfg::BK, n0, c * Cfg::S);
+                        tma_load_3d(st, &tmA, &full[s], kbeg + kb * Cfg::BK, m0, c * Cfg::ZS);
+                        tma_load_3d(st + Cfg::S * A_PLANE, &tmB, &full[s], kbeg + kb * Cfg::BK, n0, c * Cfg::ZS);
                     }
                 }
             }
@@ -532,6 +566,26 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int seg_blocks = p.seg_blocks;
     const int segments = (kblocks + seg_blocks - 1) / seg_blocks;
 
+    if (p.skip_count != nullptr) {
+        // Rounding pass: the exact recompute writes every output of the
+        // 256 x 256 tile holding this pair tile when one of its 16 x 16 count
+        // tiles is dense (its own test, ozaki.cu); both CTAs read the same
+        // counts and leave together, before any barrier or TMEM is touched.
+        const int g16 = (p.n + 15) / 16;
+        const int et = (tn * BN) / kOzakiTile;
+        bool dense = false;
+        if (tid < 256) {
+            const int gi = tm * 16 + tid % 16;
+            const int gj = et * 16 + tid / 16;
+            if (gi < g16 && gj < g16) {
+                dense = p.skip_count[(size_t)gj * g16 + gi] > kSparseMax;
+            }
+        }
+        if (__syncthreads_or(dense)) {
+            return;
+        }
+    }
+
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
@@ -578,9 +632,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                         if (leader) {
                             mbar_arrive_expect_tx(&full[s], 2 * STAGE_BYTES);
                         }
-                        tma_load_3d_pair(st, &tmA, bar, kbeg + kb * Cfg::BK, m0, c * Cfg::S);
+                        tma_load_3d_pair(st, &tmA, bar, kbeg + kb * Cfg::BK, m0, c * Cfg::ZS);
                         tma_load_3d_pair(st + Cfg::S * A_PLANE, &tmB, bar, kbeg + kb * Cfg::BK,
-                                         n0 + (int)rank * PAIR_BHALF, c * Cfg::S);
+                                         n0 + (int)rank * PAIR_BHALF, c * Cfg::ZS);
                     }
                 }
             }
@@ -783,7 +837,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 template <int FORM>
-cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
+cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status,
+                        const uint32_t* skip_count = nullptr)
 {
     using Cfg = TcCfg<FORM>;
     using G = PairGeom<FORM>;
@@ -793,7 +848,7 @@ cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan
     CUtensorMap ta, tb;
     const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     {
-        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.m, (uint64_t)(3 * Cfg::S)};
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.m, (uint64_t)(3 * Cfg::ZS)};
         const uint64_t strides[2] = {(uint64_t)plan.pitch_a * elem, (uint64_t)plan.plane_a_elems * elem};
         const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)TILE_M, (uint32_t)Cfg::S};
         if (!encode_tensor_map(&ta, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_a_off)) {
@@ -801,7 +856,7 @@ cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan
         }
     }
     {
-        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.n, (uint64_t)(3 * Cfg::S)};
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.n, (uint64_t)(3 * Cfg::ZS)};
         const uint64_t strides[2] = {(uint64_t)plan.pitch_b * elem, (uint64_t)plan.plane_b_elems * elem};
         const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)PAIR_BHALF, (uint32_t)Cfg::S};
         if (!encode_tensor_map(&tb, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_b_off)) {
@@ -828,6 +883,7 @@ cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan
         p.seg_blocks = 1;
     }
     p.path = nullptr;
+    p.skip_count = skip_count;
     p.cluster_merge = plan.cluster_merge ? 1 : 0;
     if (p.cluster_merge && (plan.parts < 2 || plan.parts > 4)) {
         return cudaErrorInvalidValue;  // clusters of at most 8 CTAs: up to 4 pairs
@@ -866,7 +922,7 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
     CUtensorMap ta, tb;
     const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     {
-        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.m, (uint64_t)(3 * Cfg::S)};
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.m, (uint64_t)(3 * Cfg::ZS)};
         const uint64_t strides[2] = {(uint64_t)plan.pitch_a * elem, (uint64_t)plan.plane_a_elems * elem};
         const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)TILE_M, (uint32_t)Cfg::S};
         if (!encode_tensor_map(&ta, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_a_off)) {
@@ -874,7 +930,7 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
         }
     }
     {
-        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.n, (uint64_t)(3 * Cfg::S)};
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.n, (uint64_t)(3 * Cfg::ZS)};
         const uint64_t strides[2] = {(uint64_t)plan.pitch_b * elem, (uint64_t)plan.plane_b_elems * elem};
         const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)BN, (uint32_t)Cfg::S};
         if (!encode_tensor_map(&tb, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_b_off)) {
@@ -941,9 +997,23 @@ cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Pl
                                 int* status)
 {
     switch (plan.form) {
-        case CG3M_FORM_TF32X3: return launch_form<CG3M_FORM_TF32X3, 64, true>(stream, pr, plan, ws, status, path);
-        case CG3M_FORM_BF16X6: return launch_form<CG3M_FORM_BF16X6, 64, true>(stream, pr, plan, ws, status, path);
-        case CG3M_FORM_BF16X9: return launch_form<CG3M_FORM_BF16X9, 64, true>(stream, pr, plan, ws, status, path);
+        case CG3M_FORM_TF32X3: return launch_form<kLeadTf32, 64, true>(stream, pr, plan, ws, status, path);
+        case CG3M_FORM_BF16X6:
+        case CG3M_FORM_BF16X9: return launch_form<kLeadBf16, 64, true>(stream, pr, plan, ws, status, path);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_gemm_tc_tiles(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status,
+                                 const uint32_t* tile_count)
+{
+    if (!CG3M_TC_PAIR || pr.m <= TILE_M || plan.parts != 1 || tile_count == nullptr) {
+        return cudaErrorInvalidValue;  // the rounding pass's orders (2048..4096) always have two row tiles
+    }
+    switch (plan.form) {
+        case CG3M_FORM_TF32X3: return launch_pair<CG3M_FORM_TF32X3>(stream, pr, plan, ws, status, tile_count);
+        case CG3M_FORM_BF16X6: return launch_pair<CG3M_FORM_BF16X6>(stream, pr, plan, ws, status, tile_count);
+        case CG3M_FORM_BF16X9: return launch_pair<CG3M_FORM_BF16X9>(stream, pr, plan, ws, status, tile_count);
         default: return cudaErrorInvalidValue;
     }
 }

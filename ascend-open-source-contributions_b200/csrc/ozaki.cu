@@ -32,11 +32,12 @@
 //      FP64.  Rounding a part moves each real product by at most 2^(beta - 1),
 //      so
 //        |error| <= (cA_i + cB_j) 2^(beta - 1)   (units of 2^(E_i + F_j - 2 beta)),
-//      zero for rows and columns that scaled exactly.  An output is written
-//      when the bound is zero or both parts exceed 2^25 times it (so the
-//      result, rounded to FP32, is within one FP32 rounding of the exact
-//      product); otherwise it is marked for the FP64 per-output kernel, as
-//      are outputs whose row or column holds a non-finite value.
+//      zero for rows and columns that scaled exactly.  Every output of a tile
+//      that ran is written (flagged or not: the form's own products skip
+//      these tiles) when the bound is zero or both parts exceed 2^25 times it
+//      (so the result, rounded to FP32, is within one FP32 rounding of the
+//      exact product); otherwise it is marked for the FP64 per-output kernel,
+//      as are outputs whose row or column holds a non-finite value.
 //
 // B200 design: a cluster of two CTAs per 256 x 256 output tile
 // (tcgen05.mma.cta_group::2.kind::i8, M = 256, N = 256, K = 32): CTA r stages
@@ -120,17 +121,11 @@ struct OzFinish {
     const uint8_t* residues;
     int y_pad;
     size_t y_plane;
-    const uint32_t* flag_bits;
     uint32_t* stats;
     uint32_t* fallback_bits;
     float2* C;
     OzCrt crt;
 };
-
-__device__ __forceinline__ bool flag_at(const uint32_t* bits, size_t idx)
-{
-    return (bits[idx >> 5] >> (idx & 31)) & 1u;
-}
 
 // t mod p in [-(p-1)/2, (p-1)/2] for odd p and an integer-valued t, |t| <= 2^47,
 // given tm = t + 1.5 * 2^52 (exact): the nearest integer q to t * rn(1/p) is
@@ -589,8 +584,9 @@ __device__ __forceinline__ void crt_part2(const OzCrt& crt, const uint32_t* word
 }
 
 // One thread per op(A) row and four consecutive op(B) columns; a block holds 64
-// rows x 16 columns inside one pair tile.  Writes every flagged output whose
-// bound certifies it and marks the rest in fallback_bits.
+// rows x 16 columns inside one exact tile, and a warp (8 rows x 4 column
+// quads) reads 128 consecutive residue bytes per plane.  Writes every output of
+// the tile whose bound certifies it and marks the rest in fallback_bits.
 __global__ void __launch_bounds__(256) ozaki_crt_kernel(const __grid_constant__ OzFinish f)
 {
     const int quad = threadIdx.x & 3;
@@ -601,16 +597,14 @@ __global__ void __launch_bounds__(256) ozaki_crt_kernel(const __grid_constant__ 
     if (!f.tile_ran[(size_t)tn * f.tiles_m + tm] || row >= n || col0 >= n) {
         return;
     }
+    // Every output of a tile that ran is written here, flagged or not: the
+    // form's own products skipped these tiles.
     uint32_t want = 0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-        const int col = col0 + c;
-        if (col < n && flag_at(f.flag_bits, (size_t)col * n + row)) {
+        if (col0 + c < n) {
             want |= 1u << c;
         }
-    }
-    if (want == 0) {
-        return;
     }
     const uint8_t* src = f.residues + ((size_t)blockIdx.x * f.y_pad + row) * 16 + quad * 4;
     double xr[4], xi[4];
@@ -761,26 +755,38 @@ int ozaki_tile_n(int n)
     return OZ_TN;
 }
 
-cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a, const float2* rows_b,
-                         const OzLayout& L, const uint32_t* flag_bits, const uint32_t* tile_count, uint32_t* stats,
-                         uint32_t* fallback_bits, float2* C, int* status, int* launched,
-                         const std::function<void(int)>& mark)
+static const OzCrt& crt_constants()
 {
     static const OzCrt crt = make_crt();
+    return crt;
+}
+
+cudaError_t launch_ozaki_split(cudaStream_t s, int n, int pitch, const float2* rows_a, const float2* rows_b,
+                               const OzLayout& L)
+{
     static const bool range_ok = crt_range_ok();
-    int count = 0;
-    if (launched != nullptr) {
-        *launched = 0;
-    }
     if (n > kOzMaxN || !range_ok) {
         return cudaErrorInvalidValue;  // the moduli cover the exact products up to order kOzMaxN
     }
     ozaki_split_kernel<<<2 * n, 256, 0, s>>>(n, pitch, rows_a, rows_b, L.planes_a, L.planes_b, L.kpitch,
-                                              L.plane_bytes, L.E, L.F, L.CA, L.CB, crt);
-    cudaError_t err = cudaGetLastError();
-    mark(++count);
+                                              L.plane_bytes, L.E, L.F, L.CA, L.CB, crt_constants());
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ozaki_tiles(cudaStream_t s, int n, const OzLayout& L, const uint32_t* tile_count, uint32_t* stats, uint32_t* fallback_bits, float2* C,
+                               int* status, int* launched, const std::function<void(int)>& mark)
+{
+    const OzCrt& crt = crt_constants();
+    int count = 0;
+    if (launched != nullptr) {
+        *launched = 0;
+    }
+    if (n > kOzMaxN) {
+        return cudaErrorInvalidValue;
+    }
+    cudaError_t err = cudaSuccess;
     const int tiles = L.y_pad / kOzakiTile;
-    if (err == cudaSuccess) {
+    {
         CUtensorMap ta, tb;
         const uint64_t dims_a[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(2 * kOzMods)};
         const uint64_t dims_b[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)(3 * kOzMods)};
@@ -841,7 +847,6 @@ cudaError_t launch_ozaki(cudaStream_t s, int n, int pitch, const float2* rows_a,
         f.residues = L.residues;
         f.y_pad = L.y_pad;
         f.y_plane = L.y_plane;
-        f.flag_bits = flag_bits;
         f.stats = stats;
         f.fallback_bits = fallback_bits;
         f.C = C;

@@ -919,8 +919,13 @@ static cudaError_t launch_replay(cudaStream_t s, int n, int span, const RoundLay
     return cudaGetLastError();
 }
 
-cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status,
-                            int* launched, const std::function<void(int)>& mark)
+int rounding_prep_kernels(int form)
+{
+    return form == CG3M_FORM_FP32 ? 3 : 4;
+}
+
+cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* launched,
+                                 const std::function<void(int)>& mark)
 {
     const int n = p.n;
     const int pitch = row_pitch(n);
@@ -936,17 +941,32 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
         mark(++count);
     }
     if (err == cudaSuccess) {
-        err = cudaMemsetAsync(L.tile_count, 0, L.zero_bytes, s);
-    }
-    if (err == cudaSuccess) {
-        select_kernel<<<148 * 8, 256, 0, s>>>(n, static_cast<const float2*>(p.C), L.energy, L.path, bridge_term(n),
-                                              L.flag_bits, L.tile_count, L.stats);
+        lane_major_kernel<<<2 * n, 256, (size_t)n * sizeof(float2), s>>>(n, pitch, span, L.rows_a, L.rows_b,
+                                                                         L.lanes_a, L.lanes_b);
         err = cudaGetLastError();
         mark(++count);
     }
+    if (err == cudaSuccess && plan.form != CG3M_FORM_FP32) {
+        err = launch_ozaki_split(s, n, pitch, L.rows_a, L.rows_b, L.oz);
+        mark(++count);
+    }
+    if (launched != nullptr) {
+        *launched = count;
+    }
+    return err;
+}
+
+cudaError_t launch_rounding_finish(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status,
+                                   int* launched, const std::function<void(int)>& mark)
+{
+    const int n = p.n;
+    const RoundLayout L = round_layout(plan, ws, n);
+    const int span = ((n + kLanes - 1) / kLanes) | 1;
+    int count = 0;
+    cudaError_t err = cudaMemsetAsync(L.tile_count, 0, L.zero_bytes, s);
     if (err == cudaSuccess) {
-        lane_major_kernel<<<2 * n, 256, (size_t)n * sizeof(float2), s>>>(n, pitch, span, L.rows_a, L.rows_b,
-                                                                         L.lanes_a, L.lanes_b);
+        select_kernel<<<148 * 8, 256, 0, s>>>(n, static_cast<const float2*>(p.C), L.energy, L.path, bridge_term(n),
+                                              L.flag_bits, L.tile_count, L.stats);
         err = cudaGetLastError();
         mark(++count);
     }
@@ -957,12 +977,9 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
     float2* C = static_cast<float2*>(p.C);
     const int exact_gn = plan.form == CG3M_FORM_FP32 ? 1 : ozaki_tile_n(n) / kTile;
     auto sparse = [&](auto kernel, const uint32_t* bits) {
-        cudaError_t e = cudaSuccess;
-        {
-            kernel<<<tiles16 * tiles16, kLanes, 0, s>>>(n, span, L.lanes_a, L.lanes_b, bits, L.tile_count, L.stats,
-                                                        C, exact_gn);
-            e = cudaGetLastError();
-        }
+        kernel<<<tiles16 * tiles16, kLanes, 0, s>>>(n, span, L.lanes_a, L.lanes_b, bits, L.tile_count, L.stats, C,
+                                                    exact_gn);
+        const cudaError_t e = cudaGetLastError();
         mark(++count);
         return e;
     };
@@ -975,11 +992,18 @@ cudaError_t launch_rounding(cudaStream_t s, const Problem& p, const Plan& plan, 
             err = sparse(recompute_sparse<kSparseFp32>, L.flag_bits);
         }
     } else {
+        // The path GEMM's C came from the leading split planes alone: the
+        // form's own products now run on every tile the exact recompute does
+        // not take, and the exact recompute writes every output of its tiles.
+        if (err == cudaSuccess) {
+            err = launch_gemm_tc_tiles(s, p, plan, ws, status, L.tile_count);
+            mark(++count);
+        }
         if (err == cudaSuccess) {
             int oz_launched = 0;
             const int before = count;
-            err = launch_ozaki(s, n, pitch, L.rows_a, L.rows_b, L.oz, L.flag_bits, L.tile_count, L.stats,
-                               L.fallback_bits, C, status, &oz_launched, [&](int i) { mark(before + i); });
+            err = launch_ozaki_tiles(s, n, L.oz, L.tile_count, L.stats, L.fallback_bits, C, status,
+                                     &oz_launched, [&](int i) { mark(before + i); });
             count += oz_launched;
         }
         if (err == cudaSuccess) {

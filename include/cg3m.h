@@ -215,9 +215,11 @@ cg3mStatus_t cg3mBatchPlanDestroy(cg3mBatchPlan_t plan);
 /* Tile shape / K split the plan chose per problem (arrays of `count`). */
 cg3mStatus_t cg3mBatchPlanDescribe(cg3mBatchPlan_t plan, int* tile_m, int* tile_n, int* k_partitions);
 
-/* Instrumentation: when count > 0, every later call made through the handle
- * records events[0] on its stream before its first kernel and events[i] after
- * its i-th kernel (i < count); no work is skipped or reordered.  The events are
+/* Instrumentation: when count > 0 (at most 32), every later call made through
+ * the handle brackets its j-th kernel (0-based, in the order the call info's
+ * kernel count enumerates them) by events[2j] and events[2j + 1], both
+ * recorded on the stream that kernel runs on, for the entries below count; no
+ * work is skipped or reordered.  The events are
  * cudaEvent_t values owned by the caller.  count == 0 turns it off. */
 cg3mStatus_t cg3mSetStageEvents(cg3mHandle_t handle, void* const* events, int count);
 

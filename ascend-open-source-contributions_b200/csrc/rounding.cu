@@ -25,10 +25,11 @@
 // handful of flags no longer costs a whole tile.  FP32 form: the reference's
 // segmented replay, bit for bit -- over 16 x 16 tiles with 2 x 2 outputs per
 // thread for 8 of the 64 lanes, or one lane per thread for a single output.
-// Tensor-core forms: flagged outputs come back within one FP32 rounding of
-// the exact product -- exact int8 slice products on the tensor cores for
-// 256 x 256 tiles holding a dense 16 x 16 tile (ozaki.cu), FP64 for sparse
-// tiles and for the few outputs the slice products cannot certify.
+// Tensor-core forms: every output of a 256 x 256 tile holding a dense 16 x 16
+// tile comes back within one FP32 rounding of the exact product -- exact int8
+// products by residues on the tensor cores (ozaki.cu), FP64 for the few
+// outputs their bound cannot certify -- and the other tiles get the form's
+// own products, their flagged outputs recomputed in FP64 one by one.
 #include <cstring>
 #include <functional>
 
@@ -513,7 +514,7 @@ __global__ void __launch_bounds__(256) lane_major_kernel(int n, int pitch, int s
 
 // ---- 4c. per-output recompute of sparse tiles ----------------------------------
 
-// Whether the exact (int8 slice) recompute tile holding 16 x 16 tile (gi, gj)
+// Whether the exact (int8 residue) recompute tile holding 16 x 16 tile (gi, gj)
 // runs, i.e. holds a dense 16 x 16 tile (ozaki_pair_kernel's predicate).
 __device__ __forceinline__ bool ozaki_tile_dense(const uint32_t* tile_count, int tiles16, int gi, int gj, int gn)
 {
@@ -778,7 +779,8 @@ static float bridge_term(int n)
 // flags: one bit per output (written whole by the selection), then one count
 // per 16 x 16 tile, kStatWords counters and the exact recompute's fallback
 // bits (one per output), all zeroed before every selection | tensor-core
-// forms: the exact recompute's slices and partial sums (OzLayout).
+// forms: the exact recompute's exponents, residue planes and product residues
+// (OzLayout).
 struct RoundLayout {
     float* path;
     float2* rows_a;

@@ -61,10 +61,15 @@ typedef enum { CG3M_FORM_FP32 = 0, CG3M_FORM_TF32X3 = 1, CG3M_FORM_BF16X6 = 2, C
  * blas/gemm/arch35/cgemm3m_rounding_kernel.cpp:474-497, gated at
  * cgemm_host.cpp:234-238).
  *   AUTO -- as the reference: only for m==n==k in [2048,4096], lda==ldb==ldc==m,
- *           alpha==1, beta==0.  Flagged outputs are recomputed in FP32 fixed
- *           order (FP32 form, the reference's replay bit for bit) or to within
- *           one FP32 rounding of the exact product (tensor-core forms: exact
- *           int8 slice products on the tensor cores, FP64 where needed).
+ *           alpha==1, beta==0.  FP32 form: flagged outputs are recomputed in
+ *           FP32 fixed order (the reference's replay bit for bit).  Tensor-core
+ *           forms: the risk plane comes from one tensor pass over the leading
+ *           split planes; every output of a 256 x 256 tile holding a 16 x 16
+ *           tile with more than 64 flagged outputs is computed to within one
+ *           FP32 rounding of the exact product (exact int8 products by residues
+ *           on the tensor cores, FP64 where their bound does not certify it);
+ *           the other tiles get the form's own products, their flagged outputs
+ *           recomputed to within one FP32 rounding in FP64.
  *   OFF  -- never. */
 typedef enum { CG3M_ROUNDING_AUTO = 0, CG3M_ROUNDING_OFF = 1 } cg3mRounding_t;
 
@@ -235,9 +240,9 @@ cg3mStatus_t cg3mGetDeviceStatus(cg3mHandle_t handle, int* flags);
  * flagged outputs recomputed by the tile kernels (16 x 16 tiles holding more
  * than 64 flagged outputs; tensor-core forms: every 256 x 256 tile holding
  * one), stats[2] = flagged outputs recomputed one by one (the other tiles),
- * stats[3] = tensor-core forms: outputs of those tiles the int8 slice
+ * stats[3] = tensor-core forms: outputs of those tiles the exact int8
  * products could not certify, recomputed in FP64, stats[4] = 256 x 256 tiles
- * run on the int8 slice products, stats[5] = the output positions inside the
+ * run on the exact int8 products, stats[5] = the output positions inside the
  * matrix those tiles cover; entries past 5 are reserved.  All -1 when that call ran no rounding pass.  Valid until the
  * next call through the handle (the counters live in its workspace). */
 cg3mStatus_t cg3mGetRoundingStats(cg3mHandle_t handle, long long* stats, int count);

@@ -202,3 +202,46 @@ def test_tc_rounding_pass_recomputes_in_fp64(cg3m, oracle, cuda, h, form):
     assert np.all(np.abs(x.imag - z.imag) <= np.spacing(np.abs(z.imag).astype(np.float32)))
 
 
+
+
+@pytest.mark.parametrize("form", ["tf32x3", "bf16x6"])
+def test_tc_pass_tiles_taken_and_form_products(cg3m, oracle, cuda, h, form):
+    """Tensor-core forms: every output of a 256 x 256 tile the exact recompute
+    takes is within one FP32 rounding of the FP64 product, flagged or not;
+    outside those tiles the unflagged outputs are the form's own products byte
+    for byte (the same call with the pass off) and the flagged ones (the
+    scaled rows, recomputed one by one in FP64) are within one FP32 rounding."""
+    import torch
+
+    n = 2048
+    a, b, srows, scols = _mixed_density_inputs(oracle, n)
+    c0 = np.zeros(n * n, np.complex64)
+    on, info = run(cg3m, h, torch, cuda, "N", "N", n, n, n, 1.0, a, n, b, n, 0.0, c0, n, form=form)
+    assert info["rounding"] == 1
+    st = h.rounding_stats()
+    # the six scaled columns 160..165 make every 16 x 16 tile of columns 160..175 dense,
+    # so the exact recompute takes the 256-column strip 0..255 in every row band
+    assert st["exact_tiles"] == n // 256 and st["exact_positions"] == n * 256
+    # the pass's form products run unsplit over K: the comparison call too
+    off, _ = run(cg3m, h, torch, cuda, "N", "N", n, n, n, 1.0, a, n, b, n, 0.0, c0, n, form=form,
+                 rounding="off", k_partitions=1)
+    On = oracle.unpack(on, n, n, n)
+    Off = oracle.unpack(off, n, n, n)
+    opa = oracle.op_matrix(a, n, "N", n, n).astype(np.complex128)
+    opb = oracle.op_matrix(b, n, "N", n, n).astype(np.complex128)
+
+    def within_one_rounding(x, z):
+        x = x.astype(np.complex128)
+        sr = np.spacing(np.abs(z.real).astype(np.float32)).astype(np.float64)
+        si = np.spacing(np.abs(z.imag).astype(np.float32)).astype(np.float64)
+        return np.all(np.abs(x.real - z.real) <= sr) and np.all(np.abs(x.imag - z.imag) <= si)
+
+    # taken strip: sampled rows (scaled and plain), all 256 columns
+    rows = np.r_[0:8, srows, 1000:1008, n - 8:n]
+    z = opa[rows, :] @ opb[:, 0:256]
+    assert within_one_rounding(On[rows, 0:256], z)
+    # outside it: plain rows keep the form's products exactly, scaled rows are recomputed
+    plain = np.setdiff1d(np.arange(n), srows)
+    assert On[np.ix_(plain, np.arange(256, n))].tobytes() == Off[np.ix_(plain, np.arange(256, n))].tobytes()
+    z = opa[srows, :] @ opb[:, 256:]
+    assert within_one_rounding(On[srows, 256:], z)

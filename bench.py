@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--pf-forms", default="fp32,bf16x6",
                     help="forms for --pf-cases: fp32 (the drop-in as called), fp32-norounding, cgemm, tf32x3, bf16x6")
     ap.add_argument("--pf-per-case", action="store_true")
+    ap.add_argument("--shard-report", action="store_true",
+                    help="also time one problem split by output columns over the ranks (always on for N > 1)")
     return ap.parse_args()
 
 
@@ -346,6 +348,53 @@ def run_reference(args, rank):
 # 0.41465 (README.md:54).
 REF_ROW_BASELINE_MS = 10.8757
 REF_ROW_NPU_BOUND_MS = 10.8757 / 0.41465
+
+
+def column_shard_report(h, stream, dev, world, rank, A, B, n, form, steps, warmup):
+    """One n^3 problem split by output columns over the ranks (no exchange on
+    the data path: rank r multiplies all of op(A) by its own block of op(B)).
+    op(A) is broadcast once from rank 0 with NCCL before the timed steps (its
+    time is reported apart); the value is the whole problem's 8MNK over the
+    slowest rank's device time per step.  A column block is not square, so
+    the rounding-correction pass's gate leaves it off."""
+    import torch
+    import torch.distributed as dist
+    from cg3m import dist as cdist
+
+    C2 = torch.zeros(n * n, dtype=torch.complex64, device=dev)
+    first, cols = cdist.shard_columns(n, world, rank)
+    bcast_ms = None
+    with torch.cuda.stream(stream):
+        if world > 1:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dist.broadcast(torch.view_as_real(A), src=0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            bcast_ms = cdist.max_over_ranks(e0.elapsed_time(e1), dev)
+
+        def call():
+            return cdist.cgemm3m_local_block(h, "N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C2, n, world, rank,
+                                             form=form)
+
+        info = None
+        for _ in range(warmup):
+            info = call()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = cdist.max_over_ranks(e0.elapsed_time(e1) / steps, dev)
+    return {"workload": f"one cgemm3m {n}x{n}x{n} NN split by output columns over {world} rank(s), "
+                        f"op(A) resident on every rank", "form": form, "value": 8.0 * n ** 3 / (ms * 1e-3) / 1e12,
+            "unit": "TFLOP/s", "ms_per_step": ms, "scaling": "strong", "columns_per_rank": cols,
+            "rounding": info["rounding"] if info else None, "broadcast_a_ms": bcast_ms,
+            "timing": "max over ranks of CUDA-event time on each rank's stream"}
 
 
 def reference_data_report(h, stream, dev, world, args, timed_fn):
@@ -774,6 +823,8 @@ def main():
     del out64
     reference_data = None if args.no_rounding_report else reference_data_report(h, stream, dev, world, args, timed)
     batching = None if args.no_batching_report else batching_report(h, stream, dev, world, args)
+    shard = column_shard_report(h, stream, dev, world, rank, A, B, n, args.form, args.steps, args.warmup) \
+        if (world > 1 or args.shard_report) else None
     status = h.device_status()
 
     if world > 1:
@@ -805,6 +856,7 @@ def main():
         "rounding_" + other: other_report,
         "reference_data": reference_data,
         "batching_form": batching,
+        "column_shard": shard,
         "device_status": status,
     }
     print(json.dumps(line), flush=True)

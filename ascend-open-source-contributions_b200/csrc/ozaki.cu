@@ -583,55 +583,50 @@ __device__ __forceinline__ void crt_part2(const OzCrt& crt, const uint32_t* word
     }
 }
 
-// One thread per op(A) row and four consecutive op(B) columns; a block holds 64
-// rows x 16 columns inside one exact tile, and a warp (8 rows x 4 column
-// quads) reads 128 consecutive residue bytes per plane.  Writes every output of
-// the tile whose bound certifies it and marks the rest in fallback_bits.
-__global__ void __launch_bounds__(256) ozaki_crt_kernel(const __grid_constant__ OzFinish f)
+// One thread per op(A) row and two consecutive op(B) columns; a block holds 32
+// rows x 16 columns inside one exact tile, and a warp (4 rows x 8 column
+// pairs) reads 64 consecutive residue bytes per plane and writes whole 32-byte
+// sectors of C.  Two outputs per thread keep it near 64 registers, for twice
+// the resident warps of four.  Writes every output of the tile whose bound
+// certifies it and marks the rest in fallback_bits.
+constexpr int kCrtRows = 32;
+
+__global__ void __launch_bounds__(256, 4) ozaki_crt_kernel(const __grid_constant__ OzFinish f)
 {
-    const int quad = threadIdx.x & 3;
-    const int row = blockIdx.y * 64 + (threadIdx.x >> 2);
-    const int col0 = blockIdx.x * 16 + quad * 4;
+    const int pair = threadIdx.x & 7;
+    const int row = blockIdx.y * kCrtRows + (threadIdx.x >> 3);
+    const int col0 = blockIdx.x * 16 + pair * 2;
     const int n = f.n;
-    const int tm = (blockIdx.y * 64) / OZ_TILE_M, tn = (blockIdx.x * 16) / OZ_TN;
+    const int tm = (blockIdx.y * kCrtRows) / OZ_TILE_M, tn = (blockIdx.x * 16) / OZ_TN;
     if (!f.tile_ran[(size_t)tn * f.tiles_m + tm] || row >= n || col0 >= n) {
         return;
     }
     // Every output of a tile that ran is written here, flagged or not: the
     // form's own products skipped these tiles.
-    uint32_t want = 0;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        if (col0 + c < n) {
-            want |= 1u << c;
-        }
-    }
-    const uint8_t* src = f.residues + ((size_t)blockIdx.x * f.y_pad + row) * 16 + quad * 4;
-    double xr[4], xi[4];
+    const uint8_t* src = f.residues + ((size_t)blockIdx.x * f.y_pad + row) * 16 + pair * 2;
+    double xr[2], xi[2];
     {
         uint32_t words[kOzMods];
 #pragma unroll
         for (int mi = 0; mi < kOzMods; ++mi) {
-            words[mi] = __ldcs(reinterpret_cast<const uint32_t*>(src + (size_t)(2 * mi) * f.y_plane));
+            words[mi] = __ldcs(reinterpret_cast<const unsigned short*>(src + (size_t)(2 * mi) * f.y_plane));
         }
         crt_part2(f.crt, words, 0, xr);
-        crt_part2(f.crt, words, 2, xr);
 #pragma unroll
         for (int mi = 0; mi < kOzMods; ++mi) {
-            words[mi] = __ldcs(reinterpret_cast<const uint32_t*>(src + (size_t)(2 * mi + 1) * f.y_plane));
+            words[mi] = __ldcs(reinterpret_cast<const unsigned short*>(src + (size_t)(2 * mi + 1) * f.y_plane));
         }
         crt_part2(f.crt, words, 0, xi);
-        crt_part2(f.crt, words, 2, xi);
     }
     const int ei = f.E[row];
     const int ca = f.CA[row];
     uint32_t fallbacks = 0;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        if (!((want >> c) & 1u)) {
-            continue;
-        }
+    for (int c = 0; c < 2; ++c) {
         const int col = col0 + c;
+        if (col >= n) {
+            break;
+        }
         const size_t idx = (size_t)col * n + row;
         const int fj = f.F[col];
         bool ok = ei != kOzNonFinite && fj != kOzNonFinite;
@@ -851,7 +846,7 @@ cudaError_t launch_ozaki_tiles(cudaStream_t s, int n, const OzLayout& L, const u
         f.fallback_bits = fallback_bits;
         f.C = C;
         f.crt = crt;
-        ozaki_crt_kernel<<<dim3((unsigned)(L.y_pad / 16), (unsigned)(L.y_pad / 64)), 256, 0, s>>>(f);
+        ozaki_crt_kernel<<<dim3((unsigned)(L.y_pad / 16), (unsigned)(L.y_pad / kCrtRows)), 256, 0, s>>>(f);
         err = cudaGetLastError();
         mark(++count);
     }

@@ -245,3 +245,33 @@ def test_tc_pass_tiles_taken_and_form_products(cg3m, oracle, cuda, h, form):
     assert On[np.ix_(plain, np.arange(256, n))].tobytes() == Off[np.ix_(plain, np.arange(256, n))].tobytes()
     z = opa[srows, :] @ opb[:, 256:]
     assert within_one_rounding(On[srows, 256:], z)
+
+
+@pytest.mark.parametrize("form", ["tf32x3", "bf16x6"])
+def test_tc_pass_odd_order_edges(cg3m, oracle, cuda, h, form):
+    """Order 2077 (a rounding-gated size of the reference's performance table,
+    not a multiple of the 256 x 256 exact tile): the last row and column of
+    tiles are partial, the residue planes padded.  Precision-form data flags
+    every tile, so every output, edges included, is within one FP32 rounding
+    of the FP64 product."""
+    import torch
+
+    n = 2077
+    a = oracle.precision_matrix(n, n, 41)
+    b = oracle.precision_matrix(n, n, 42)
+    c0 = np.zeros(n * n, np.complex64)
+    out, info = run(cg3m, h, torch, cuda, "N", "N", n, n, n, 1.0, a, n, b, n, 0.0, c0, n, form=form)
+    assert info["rounding"] == 1
+    st = h.rounding_stats()
+    tiles = (n + 255) // 256
+    assert st["exact_tiles"] == tiles * tiles and st["exact_positions"] == n * n
+    got = oracle.unpack(out, n, n, n)
+    opa = oracle.op_matrix(a, n, "N", n, n).astype(np.complex128)
+    opb = oracle.op_matrix(b, n, "N", n, n).astype(np.complex128)
+    rows = np.r_[0:8, 2040:2077]   # the partial last row band and the rows before it
+    cols = np.r_[0:16, 2040:2077]
+    z = opa[rows, :] @ opb[:, cols]
+    x = got[np.ix_(rows, cols)].astype(np.complex128)
+    ur = np.spacing(np.abs(z.real).astype(np.float32)).astype(np.float64)
+    ui = np.spacing(np.abs(z.imag).astype(np.float32)).astype(np.float64)
+    assert np.all(np.abs(x.real - z.real) <= ur) and np.all(np.abs(x.imag - z.imag) <= ui)

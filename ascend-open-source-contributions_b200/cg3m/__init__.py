@@ -349,9 +349,10 @@ def stage_names(info):
         return ["onchip"][:k]
     if info["rounding"]:
         fp32 = info["form"] == FORM["fp32"]
-        prep = ["pack_rows", "energy", "lane_major"] + ([] if fp32 else ["exact_split"])
-        tail = ["select", "replay_tiles", "replay_outputs"] if fp32 else \
-            ["select", "gemm_form_tiles", "exact_tiles", "exact_crt", "recompute_fp64_outputs", "fallback_fp64"]
+        prep = ["pack_rows", "energy"] + ([] if fp32 else ["exact_split"])
+        tail = ["select", "replay_tiles", "lanes_needed", "lane_major", "replay_outputs"] if fp32 else \
+            ["select", "gemm_form_tiles", "exact_tiles", "exact_crt", "lanes_needed", "lane_major",
+             "recompute_fp64_outputs", "fallback_fp64"]
         names = ["pack", "gemm_path"] + prep + tail
     else:
         names = ["pack", "gemm", "merge"]

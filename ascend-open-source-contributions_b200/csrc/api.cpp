@@ -875,7 +875,7 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
     info->k_span = plan.span;
     info->rounding = plan.rounding ? 1 : 0;
     info->kernels =
-        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? (plan.form == CG3M_FORM_FP32 ? 6 : 10) : 0);
+        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? (plan.form == CG3M_FORM_FP32 ? 7 : 11) : 0);
     info->workspace_bytes = plan.total;
     return CG3M_STATUS_SUCCESS;
 }

@@ -494,10 +494,14 @@ __global__ void __launch_bounds__(512) recompute_fp32_tiled(const __grid_constan
 // so the strided shared-memory reads of a half-warp hit distinct banks).
 __global__ void __launch_bounds__(256) lane_major_kernel(int n, int pitch, int span, const float2* __restrict__ rows_a,
                                                          const float2* __restrict__ rows_b,
-                                                         float2* __restrict__ lanes_a, float2* __restrict__ lanes_b)
+                                                         float2* __restrict__ lanes_a, float2* __restrict__ lanes_b,
+                                                         const uint8_t* __restrict__ need)
 {
     extern __shared__ float2 row[];
     const int r = blockIdx.x;
+    if (!need[r]) {
+        return;  // no output the per-output kernels recompute lies in this row or column
+    }
     const size_t width = (size_t)kLanes * span;
     const float2* src = r < n ? rows_a + (size_t)r * pitch : rows_b + (size_t)(r - n) * pitch;
     float2* dst = r < n ? lanes_a + (size_t)r * width : lanes_b + (size_t)(r - n) * width;
@@ -509,6 +513,63 @@ __global__ void __launch_bounds__(256) lane_major_kernel(int n, int pitch, int s
         const int sidx = f / kLanes, l = f % kLanes;
         const int k = l * span + sidx;
         dst[f] = k < n ? row[k] : make_float2(0.0f, 0.0f);
+    }
+}
+
+// The op(A) rows (need[i]) and op(B) columns (need[n + j]) of the outputs the
+// per-output kernels recompute: flagged outputs of 16 x 16 tiles the tile
+// kernels leave (FP32: tiles with at most kSparseMax flagged outputs;
+// tensor-core forms: outside the 256 x 256 tiles the exact recompute took),
+// and, for the tensor-core forms, the outputs it marked for the FP64 fallback.
+// need[] starts zeroed; only those rows and columns get lane-major copies.
+__global__ void __launch_bounds__(256) lanes_needed_kernel(int n, int tc, const uint32_t* __restrict__ flag_bits,
+                                                           const uint32_t* __restrict__ fallback_bits,
+                                                           const uint32_t* __restrict__ tile_count,
+                                                           const uint8_t* __restrict__ tile_ran, int exact_tiles,
+                                                           uint8_t* __restrict__ need)
+{
+    const size_t words = ((size_t)n * n + 31) / 32;
+    const int tiles16 = (n + kTile - 1) / kTile;
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t fb = tc ? fallback_bits[w] : 0u;
+        uint32_t bits = flag_bits[w] | fb;
+        // Fast path: a word inside one column and one tile row band whose tile
+        // kernels take all its flags leaves only its fallback bits.
+        const size_t first = w * 32, last = min(first + 31, (size_t)n * n - 1);
+        const int j0 = (int)(first / n), j1 = (int)(last / n);
+        if (bits != 0 && j0 == j1) {
+            const int i0 = (int)(first - (size_t)j0 * n), i1 = (int)(last - (size_t)j1 * n);
+            if (tc) {
+                if (i0 / kOzakiTile == i1 / kOzakiTile &&
+                    tile_ran[(size_t)(j0 / kOzakiTile) * exact_tiles + i0 / kOzakiTile]) {
+                    bits = fb;
+                }
+            } else {
+                const size_t t = (size_t)(j0 / kTile) * tiles16;
+                if (tile_count[t + i0 / kTile] > kSparseMax && tile_count[t + i1 / kTile] > kSparseMax &&
+                    i1 / kTile - i0 / kTile <= 1) {
+                    bits = 0;
+                }
+            }
+        }
+        while (bits != 0) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const size_t idx = w * 32 + (size_t)b;
+            if (idx >= (size_t)n * n) {
+                break;  // bits past the last output are never set; bounds need[] all the same
+            }
+            const int j = (int)(idx / n), i = (int)(idx - (size_t)j * n);
+            bool want = (fb >> b) & 1u;
+            if (!want) {
+                want = tc ? !tile_ran[(size_t)(j / kOzakiTile) * exact_tiles + i / kOzakiTile]
+                          : tile_count[(size_t)(j / kTile) * tiles16 + i / kTile] <= kSparseMax;
+            }
+            if (want) {
+                need[i] = 1;
+                need[n + j] = 1;
+            }
+        }
     }
 }
 
@@ -777,8 +838,9 @@ static float bridge_term(int n)
 // Layout of the rounding region (Plan::round_off): path n^2 floats | rows of
 // op(A) n^2 complex | columns of op(B) n^2 complex | energies 2n floats |
 // flags: one bit per output (written whole by the selection), then one count
-// per 16 x 16 tile, kStatWords counters and the exact recompute's fallback
-// bits (one per output), all zeroed before every selection | tensor-core
+// per 16 x 16 tile, kStatWords counters, the exact recompute's fallback bits
+// (one per output) and a byte per op(A) row and op(B) column marking those the
+// per-output kernels read, all zeroed before every selection | tensor-core
 // forms: the exact recompute's exponents, residue planes and product residues
 // (OzLayout).
 struct RoundLayout {
@@ -792,11 +854,13 @@ struct RoundLayout {
     uint32_t* tile_count;
     uint32_t* stats;
     uint32_t* fallback_bits;
-    size_t zero_bytes;  // tile_count + stats + fallback_bits, one memset
+    uint8_t* need;      // rows of op(A), then columns of op(B), the per-output kernels read
+    size_t zero_bytes;  // tile_count + stats + fallback_bits + need, one memset
     OzLayout oz;
 };
 
 static size_t flag_words(int n) { return ((size_t)n * n + 31) / 32; }
+static size_t need_words(int n) { return ((size_t)2 * n + 3) / 4; }
 static size_t tile_words(int n)
 {
     const size_t t = (size_t)(n + kTile - 1) / kTile;
@@ -833,7 +897,7 @@ static RoundOffsets round_offsets(int n, int form, std::vector<size_t>* guards)
     o.energy = off;
     off = next_region(off, (size_t)2 * n * 4, guards);
     o.flags = off;
-    off = next_region(off, (2 * flag_words(n) + tile_words(n) + kStatWords) * 4, guards);
+    off = next_region(off, (2 * flag_words(n) + tile_words(n) + kStatWords + need_words(n)) * 4, guards);
     o.oz = off;
     if (form != CG3M_FORM_FP32) {
         std::vector<size_t> inner;
@@ -863,7 +927,8 @@ static RoundLayout round_layout(const Plan& plan, void* ws, int n)
     L.tile_count = L.flag_bits + flag_words(n);
     L.stats = L.tile_count + tile_words(n);
     L.fallback_bits = L.stats + kStatWords;
-    L.zero_bytes = (tile_words(n) + kStatWords + flag_words(n)) * 4;
+    L.need = reinterpret_cast<uint8_t*>(L.fallback_bits + flag_words(n));
+    L.zero_bytes = (tile_words(n) + kStatWords + flag_words(n) + need_words(n)) * 4;
     if (plan.form != CG3M_FORM_FP32) {
         L.oz = oz_layout(n, b + o.oz);
     }
@@ -923,7 +988,7 @@ static cudaError_t launch_replay(cudaStream_t s, int n, int span, const RoundLay
 
 int rounding_prep_kernels(int form)
 {
-    return form == CG3M_FORM_FP32 ? 3 : 4;
+    return form == CG3M_FORM_FP32 ? 2 : 3;
 }
 
 cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* launched,
@@ -939,12 +1004,6 @@ cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& p
     if (err == cudaSuccess) {
         energy_kernel<<<2 * n, kLanes, (size_t)n * sizeof(float2), s>>>(L.rows_a, L.rows_b, n, pitch, span,
                                                                         L.energy);
-        err = cudaGetLastError();
-        mark(++count);
-    }
-    if (err == cudaSuccess) {
-        lane_major_kernel<<<2 * n, 256, (size_t)n * sizeof(float2), s>>>(n, pitch, span, L.rows_a, L.rows_b,
-                                                                         L.lanes_a, L.lanes_b);
         err = cudaGetLastError();
         mark(++count);
     }
@@ -978,6 +1037,22 @@ cudaError_t launch_rounding_finish(cudaStream_t s, const Problem& p, const Plan&
     const int tiles16 = (n + kTile - 1) / kTile;
     float2* C = static_cast<float2*>(p.C);
     const int exact_gn = plan.form == CG3M_FORM_FP32 ? 1 : ozaki_tile_n(n) / kTile;
+    const int pitch = row_pitch(n);
+    // lane-major copies of the rows and columns the per-output kernels read
+    auto lanes = [&]() {
+        const bool tc = plan.form != CG3M_FORM_FP32;
+        lanes_needed_kernel<<<148 * 4, 256, 0, s>>>(n, tc ? 1 : 0, L.flag_bits, L.fallback_bits, L.tile_count,
+                                                    tc ? L.oz.tile_ran : nullptr, L.oz.y_pad / kOzakiTile, L.need);
+        cudaError_t e = cudaGetLastError();
+        mark(++count);
+        if (e == cudaSuccess) {
+            lane_major_kernel<<<2 * n, 256, (size_t)n * sizeof(float2), s>>>(n, pitch, span, L.rows_a, L.rows_b,
+                                                                             L.lanes_a, L.lanes_b, L.need);
+            e = cudaGetLastError();
+            mark(++count);
+        }
+        return e;
+    };
     auto sparse = [&](auto kernel, const uint32_t* bits) {
         kernel<<<tiles16 * tiles16, kLanes, 0, s>>>(n, span, L.lanes_a, L.lanes_b, bits, L.tile_count, L.stats, C,
                                                     exact_gn);
@@ -989,6 +1064,9 @@ cudaError_t launch_rounding_finish(cudaStream_t s, const Problem& p, const Plan&
         if (err == cudaSuccess) {
             err = launch_replay<kChunkMin>(s, n, span, L, C, status);
             mark(++count);
+        }
+        if (err == cudaSuccess) {
+            err = lanes();
         }
         if (err == cudaSuccess) {
             err = sparse(recompute_sparse<kSparseFp32>, L.flag_bits);
@@ -1007,6 +1085,9 @@ cudaError_t launch_rounding_finish(cudaStream_t s, const Problem& p, const Plan&
             err = launch_ozaki_tiles(s, n, L.oz, L.tile_count, L.stats, L.fallback_bits, C, status,
                                      &oz_launched, [&](int i) { mark(before + i); });
             count += oz_launched;
+        }
+        if (err == cudaSuccess) {
+            err = lanes();
         }
         if (err == cudaSuccess) {
             err = sparse(recompute_sparse<kSparseFp64>, L.flag_bits);

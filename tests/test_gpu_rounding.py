@@ -49,7 +49,7 @@ def test_fp32_rounding_pass_bit_exact_blocks(cg3m, oracle, cuda, h, ops, N):
     b = oracle.precision_matrix(N, N, 12)
     c0 = np.zeros(N * N, np.complex64)
     out, info = run(cg3m, h, torch, cuda, ta, tb, N, N, N, 1.0, a, N, b, N, 0.0, c0, N)
-    assert info["rounding"] == 1 and info["kernels"] == 8
+    assert info["rounding"] == 1 and info["kernels"] == 9
     again, _ = run(cg3m, h, torch, cuda, ta, tb, N, N, N, 1.0, a, N, b, N, 0.0, c0, N)
     assert out.tobytes() == again.tobytes()
     e = oracle.energy(N, ta, tb, a, N, b, N)

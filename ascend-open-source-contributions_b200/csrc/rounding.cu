@@ -57,22 +57,17 @@ __global__ void __launch_bounds__(kLanes) energy_kernel(const float2* __restrict
                                                         const float2* __restrict__ rows_b, int n, int pitch,
                                                         int span, float* __restrict__ energy)
 {
-    extern __shared__ float2 row[];
     __shared__ float lanes[kLanes];
     const int r = blockIdx.x;
     const float2* src = r < n ? rows_a + (size_t)r * pitch : rows_b + (size_t)(r - n) * pitch;
-    for (int k = threadIdx.x; k < n; k += kLanes) {
-        row[k] = src[k];
-    }
-    __syncthreads();
+    // Each lane reads its own span of consecutive terms straight from global
+    // memory (no staged row, so many rows are in flight per SM); the sector a
+    // thread fetches serves its next terms from L1.
     const int l = threadIdx.x;
     float e = 0.0f;
-    for (int s = 0; s < span; ++s) {
-        const int k = l * span + s;
-        if (k >= n) {
-            break;
-        }
-        const float2 x = row[k];
+    const int k0 = l * span, k1 = min(n, k0 + span);
+    for (int k = k0; k < k1; ++k) {
+        const float2 x = __ldg(src + k);
         e = __fmaf_rn(x.x, x.x, e);
         e = __fmaf_rn(x.y, x.y, e);
     }
@@ -99,36 +94,60 @@ __global__ void select_kernel(int n, const float2* __restrict__ C, const float* 
                               const float* __restrict__ path, float bridge, uint32_t* __restrict__ flag_bits,
                               uint32_t* __restrict__ tile_count, uint32_t* __restrict__ stats)
 {
-    const size_t total = (size_t)n * n;
+    // n <= 4096 (the gate), so output indices fit 32 bits.  Each warp takes
+    // kGroups consecutive 32-output words per trip and issues all their loads
+    // before any ballot, so several words' memory latency overlaps.
+    constexpr int kGroups = 4;
+    const uint32_t total = (uint32_t)n * (uint32_t)n;
+    const uint32_t un = (uint32_t)n;
     const int tiles = (n + kTile - 1) / kTile;
     const float conf2 = __fmul_rn(kConfidence, kConfidence);
     const int lane = threadIdx.x & 31;
     uint32_t local = 0;
-    const size_t warps = (size_t)gridDim.x * (blockDim.x >> 5);
-    for (size_t base = (blockIdx.x * (size_t)(blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < total;
-         base += warps * 32) {
-        const size_t idx = base + lane;
-        bool sel = false;
-        int tile = -1;
-        if (idx < total) {
-            const int j = (int)(idx / n), i = (int)(idx - (size_t)j * n);
-            const float2 c = C[idx];
-            const float re = fabsf(c.x), im = fabsf(c.y);
-            const float magnitude = re > im ? re : im;
-            const float variance =
-                __fmul_rn(0x1p-48f, __fadd_rn(path[idx], __fmul_rn(__fmul_rn(energy[i], energy[n + j]), bridge)));
-            sel = !isfinite(magnitude) || !isfinite(variance) || __fmul_rn(conf2, variance) >= 0.0001f;
-            tile = (j / kTile) * tiles + i / kTile;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * kGroups; base < total;
+         base += warps * 32 * kGroups) {
+        float2 c[kGroups];
+        float pth[kGroups], ei[kGroups], ej[kGroups];
+        uint32_t ii[kGroups], jj[kGroups];
+#pragma unroll
+        for (int g = 0; g < kGroups; ++g) {
+            const uint32_t idx = base + g * 32 + lane;
+            if (idx < total) {
+                jj[g] = idx / un;
+                ii[g] = idx - jj[g] * un;
+                c[g] = C[idx];
+                pth[g] = path[idx];
+                ei[g] = energy[ii[g]];
+                ej[g] = energy[n + jj[g]];
+            }
         }
-        const uint32_t word = __ballot_sync(0xffffffffu, sel);
-        if (lane == 0) {
-            flag_bits[base >> 5] = word;
+#pragma unroll
+        for (int g = 0; g < kGroups; ++g) {
+            const uint32_t wbase = base + g * 32;
+            if (wbase >= total) {
+                break;  // warp-uniform
+            }
+            const uint32_t idx = wbase + lane;
+            bool sel = false;
+            int tile = -1;
+            if (idx < total) {
+                const float re = fabsf(c[g].x), im = fabsf(c[g].y);
+                const float magnitude = re > im ? re : im;
+                const float variance = __fmul_rn(0x1p-48f, __fadd_rn(pth[g], __fmul_rn(__fmul_rn(ei[g], ej[g]), bridge)));
+                sel = !isfinite(magnitude) || !isfinite(variance) || __fmul_rn(conf2, variance) >= 0.0001f;
+                tile = (int)(jj[g] / kTile) * tiles + (int)(ii[g] / kTile);
+            }
+            const uint32_t word = __ballot_sync(0xffffffffu, sel);
+            if (lane == 0) {
+                flag_bits[wbase >> 5] = word;
+            }
+            const uint32_t peers = __match_any_sync(0xffffffffu, sel ? tile : -1);
+            if (sel && lane == __ffs(peers) - 1) {
+                atomicAdd(&tile_count[tile], (uint32_t)__popc(peers));
+            }
+            local += sel ? 1u : 0u;
         }
-        const uint32_t peers = __match_any_sync(0xffffffffu, sel ? tile : -1);
-        if (sel && lane == __ffs(peers) - 1) {
-            atomicAdd(&tile_count[tile], (uint32_t)__popc(peers));
-        }
-        local += sel ? 1u : 0u;
     }
     local = __reduce_add_sync(0xffffffffu, local);
     if (lane == 0 && local != 0) {
@@ -1002,7 +1021,7 @@ cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& p
     cudaError_t err = launch_pack_rows(s, p, L.rows_a, L.rows_b, pitch);
     mark(++count);
     if (err == cudaSuccess) {
-        energy_kernel<<<2 * n, kLanes, (size_t)n * sizeof(float2), s>>>(L.rows_a, L.rows_b, n, pitch, span,
+        energy_kernel<<<2 * n, kLanes, 0, s>>>(L.rows_a, L.rows_b, n, pitch, span,
                                                                         L.energy);
         err = cudaGetLastError();
         mark(++count);

@@ -11,7 +11,7 @@
 // while the accumulation stays FP32.
 //
 // B200 design.  One CTA per 128 x BN output tile (cta_group::1, M = 128,
-// N = BN = 128; BN = 64 for the path-tracking variant), 320 threads:
+// N = BN = 128), 320 threads:
 //   warp 0       TMA producer: per K-block and component c in {re, im, sum}
 //                one 3-D box for A (all split planes of c) and one for B,
 //                128-byte rows with the 128-byte swizzle, into a 192 KB
@@ -45,11 +45,10 @@
 #include "epilogue.cuh"
 #include "ptx.cuh"
 
-// Path-tracking variant (rounding-correction gate): with BN = 64 each epilogue
-// thread also keeps the two risk integrals of its 32 outputs and, after each
-// segment of depth d, adds d/9*(s_old^2 + s_old*s_new + s_new^2) as the
-// reference's MergeProductsWithPath does (cgemm_compute_kernel.cpp:432-474);
-// the risk plane max(I_re, I_im) is written beside C.
+// The rounding-correction gate's risk plane comes from gemm3m_lead_path_kernel
+// below: the leading split planes in the four-multiplication form, 128 x 128
+// tiles, the running sums in TMEM and both risk integrals per output in
+// registers (MergeProductsWithPath, cgemm_compute_kernel.cpp:432-474).
 namespace cg3m {
 namespace {
 
@@ -62,8 +61,7 @@ constexpr int kThreads = (2 + kEpilogueWarps) * 32;
 // 10 warps land 3/3/2/2 on the SM's four sub-partitions, whose register files
 // hold 16K registers each: 3 warps x 32 threads x 168 registers is the most
 // that still launches, so each epilogue thread keeps 2 x 64 running sums
-// (BN = 128) or 4 x 32 (BN = 64 with path tracking) and streams TMEM through
-// 8-column pieces.
+// (BN = 128) and streams TMEM through 8-column pieces.
 
 template <int FORM>
 struct TcCfg;
@@ -131,22 +129,16 @@ constexpr int kLeadBf16 = 101;
 
 template <>
 struct TcCfg<kLeadTf32> {
-    static constexpr int S = 1;
-    static constexpr int ZS = 2;
+    static constexpr int ZS = 2;       // planes per component in the packed layout (plane 0 is read)
     static constexpr int BK = 32;
-    static constexpr int NPAIRS = 1;
     static constexpr uint32_t FMT = 2;
-    __device__ static int2 pair(int) { return make_int2(0, 0); }
 };
 
 template <>
 struct TcCfg<kLeadBf16> {
-    static constexpr int S = 1;
     static constexpr int ZS = 3;
     static constexpr int BK = 64;
-    static constexpr int NPAIRS = 1;
     static constexpr uint32_t FMT = 1;
-    __device__ static int2 pair(int) { return make_int2(0, 0); }
 };
 
 // Geometry of one instantiation: output tile 128 x BN.
@@ -174,7 +166,7 @@ struct TcParams {
     size_t pplane;
     int* status;
     int seg_blocks;  // K-blocks per accumulation segment
-    float* path;     // risk plane (path-tracking variant), ld = ldc
+    float* path;     // risk plane (gemm3m_lead_path_kernel), ld = ldc
     int cluster_merge;  // pair kernel: the `parts` pairs of a tile form one cluster and merge on chip
     // pair kernel in the rounding pass: the per-16 x 16 flagged counts; pair
     // tiles inside a 256 x 256 tile the exact recompute takes are skipped
@@ -227,7 +219,62 @@ __device__ __forceinline__ float risk_step(float integral, float old, float nw, 
     return __fadd_rn(integral, __fmul_rn(t, w));
 }
 
-template <int FORM, int BN, bool PATH>
+// One segment of the risk integral summed by parts (gemm3m_lead_path_kernel):
+// before the last segment acc += s_new (2 s_new + s_old); the last one turns
+// acc into the integral, wfull (acc - s_old^2) + w (s_old^2 + s_old s_new + s_new^2).
+template <bool LAST>
+__device__ __forceinline__ float risk_part(float acc, float old, float nw, float w, float wfull)
+{
+    if constexpr (!LAST) {
+        return __fmaf_rn(nw, __fmaf_rn(nw, 2.0f, old), acc);
+    } else {
+        return risk_step(__fmul_rn(wfull, __fsub_rn(acc, __fmul_rn(old, old))), old, nw, w);
+    }
+}
+
+// One segment's drain of an epilogue thread's COLS columns: Re_s and Im_s
+// merge into the running sums in TMEM (round-to-nearest FP32) and both risk
+// integrals advance.  STEP 0: the first segment of several (the running sums
+// start at the segment's sums), 1: a middle one, 2: the last one, which
+// closes the integrals (first says whether it is also the first).
+template <int COLS, int STEP>
+__device__ __forceinline__ void lead_drain(uint32_t seg_re, uint32_t seg_im, uint32_t run_re, uint32_t run_im,
+                                           bool first, float w, float wfull, float* ir, float* ii)
+{
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+        const uint32_t sa = part == 0 ? seg_re : seg_im, ra = part == 0 ? run_re : run_im;
+        float* acc = part == 0 ? ir : ii;
+#pragma unroll
+        for (int cb = 0; cb < COLS; cb += 8) {
+            float v[8], r[8];
+            if constexpr (STEP == 0) {
+                tmem_ld8(sa + (uint32_t)cb, v);
+            } else {
+                tmem_ld8x2(sa + (uint32_t)cb, ra + (uint32_t)cb, v, r);
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if constexpr (STEP == 0) {
+                    acc[cb + j] = __fmul_rn(v[j], __fmul_rn(v[j], 2.0f));  // s_1 (2 s_1 + s_0), s_0 = 0
+                    r[j] = v[j];
+                } else if constexpr (STEP == 1) {
+                    const float nw = __fadd_rn(r[j], v[j]);
+                    acc[cb + j] = risk_part<false>(acc[cb + j], r[j], nw, w, wfull);
+                    r[j] = nw;
+                } else {
+                    const float old = first ? 0.0f : r[j];
+                    const float nw = first ? v[j] : __fadd_rn(r[j], v[j]);
+                    acc[cb + j] = risk_part<true>(first ? 0.0f : acc[cb + j], old, nw, w, wfull);
+                    r[j] = nw;
+                }
+            }
+            tmem_st8(ra + (uint32_t)cb, r);
+        }
+    }
+}
+
+template <int FORM, int BN>
 __global__ void __launch_bounds__(kThreads, 1)
     gemm3m_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const TcParams p)
@@ -386,13 +433,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * COLS);
         const uint32_t spare = lane_addr + (uint32_t)(3 * BN);
         float re[COLS], im[COLS];
-        float ir[PATH ? COLS : 1], ii[PATH ? COLS : 1];
         bool go = true;
         for (int seg = 0; seg < segments && go; ++seg) {
-            // Depth of this segment in K terms (the last one may be short).
-            const int t0 = kbeg + seg * seg_blocks * Cfg::BK;
-            const int depth = min(kend, t0 + seg_blocks * Cfg::BK) - t0;
-            const float w = __fdiv_rn((float)depth, 9.0f);
             // P0 and P1 complete: Re_s = P0 - P1 joins the running sum; P0 + P1
             // parks in the spare columns so both accumulators can be reused.
             bool ready = mbar_wait(&acc_full[1], seg & 1, p.status);
@@ -409,11 +451,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int j = 0; j < 8; ++j) {
                     const float rs = __fsub_rn(v0[j], v1[j]);
                     v1[j] = __fadd_rn(v0[j], v1[j]);
-                    const float nr = seg == 0 ? rs : __fadd_rn(re[cb + j], rs);
-                    if constexpr (PATH) {
-                        ir[cb + j] = risk_step(seg == 0 ? 0.0f : ir[cb + j], seg == 0 ? 0.0f : re[cb + j], nr, w);
-                    }
-                    re[cb + j] = nr;
+                    re[cb + j] = seg == 0 ? rs : __fadd_rn(re[cb + j], rs);
                 }
                 tmem_st8(spare + (uint32_t)cb, v1);
             }
@@ -438,11 +476,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const float is = __fsub_rn(v2[j], u[j]);
-                    const float ni = seg == 0 ? is : __fadd_rn(im[cb + j], is);
-                    if constexpr (PATH) {
-                        ii[cb + j] = risk_step(seg == 0 ? 0.0f : ii[cb + j], seg == 0 ? 0.0f : im[cb + j], ni, w);
-                    }
-                    im[cb + j] = ni;
+                    im[cb + j] = seg == 0 ? is : __fadd_rn(im[cb + j], is);
                 }
             }
             tc_fence_before();
@@ -459,9 +493,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if (p.parts == 1) {
                         float2* cp = p.C + (size_t)col * p.ldc + row;
                         *cp = epilogue_value(re[j], im[j], p.epi, cp);
-                        if constexpr (PATH) {
-                            p.path[(size_t)col * p.ldc + row] = ir[j] > ii[j] ? ir[j] : ii[j];
-                        }
                     } else {
                         const size_t o = (size_t)col * p.ppitch + row;
                         p.partial[(size_t)(2 * part) * p.pplane + o] = re[j];
@@ -475,6 +506,241 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 1) {
         tc_fence_after();
         tmem_dealloc(tmem, G::TMEM_COLS);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Risk path of the tensor-core forms' rounding pass: one CTA per 128 x 128
+// output tile over the leading split plane of the real and imaginary
+// components only (the sum planes are not read).  Per K-block one ring stage
+// holds A_re, A_im, B_re, B_im (16 KB each) and one thread issues, per 32-byte
+// K step,
+//   Re += A_re B_re + (-A_im) B_im   (the second with the negate-A bit)
+//   Im += A_re B_im + A_im B_re
+// into TMEM columns [0, 128) and [128, 256); the running sums live in columns
+// [256, 384) and [384, 512).  After every K segment the epilogue merges Re_s
+// and Im_s into the running sums with round-to-nearest FP32 and advances both
+// risk integrals of its 32 outputs (registers) by d/9 (s_old^2 + s_old s_new
+// + s_new^2), as MergeProductsWithPath does (cgemm_compute_kernel.cpp:432-474).
+// The four-multiplication products read 2.25x fewer operand bytes per output
+// than the three-multiplication ones over 128 x 64 tiles (the register-resident
+// running state of that form caps its tile width), and the risk estimate,
+// which needs a few significant bits of the running sums, does not tell the
+// two apart.  The K range is never partitioned: the risk plane needs the whole
+// chain.  C receives the leading-plane product (its finiteness is all the
+// selection reads).
+constexpr int kLeadBN = 128;
+// 16 epilogue warps (four per TMEM lane quadrant, 32 columns each) hide the
+// TMEM load latency four ways per sub-partition; 18 warps launch at up to 96
+// registers a thread (five warps on the busiest sub-partition's 16K).
+constexpr int kLeadEpiWarps = 16;
+constexpr int kLeadThreads = (2 + kLeadEpiWarps) * 32;
+constexpr int kLeadStage = 4 * A_PLANE;                 // 64 KB
+constexpr int kLeadStages = RING_BYTES / kLeadStage;    // 3
+constexpr size_t kLeadSmem = (size_t)kLeadStages * kLeadStage + 1024 + 256;
+constexpr uint32_t kNegateA = 1u << 13;                 // instruction descriptor: negate the A operand
+
+template <int LEAD>
+__global__ void __launch_bounds__(kLeadThreads, 1)
+    gemm3m_lead_path_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                            const TcParams p)
+{
+    using Cfg = TcCfg<LEAD>;
+    constexpr int KSTEPS = ROW_BYTES / 32;
+    constexpr int COLS = kLeadBN / (kLeadEpiWarps / 4);  // columns per epilogue thread
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* ring = align_shared<1024>(smem_raw);
+    uint64_t* full = reinterpret_cast<uint64_t*>(ring + kLeadStages * kLeadStage);
+    uint64_t* empty = full + kLeadStages;
+    uint64_t* acc_full = empty + kLeadStages;  // MMA -> epilogue: Re_s and Im_s of the segment are in TMEM
+    uint64_t* acc_free = acc_full + 1;         // epilogue -> MMA: both may be overwritten
+    uint64_t* mma_done = acc_free + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+
+    constexpr int GM = 8;
+    const int pid = blockIdx.x;
+    const int in_group = GM * p.tiles_n;
+    const int first_m = (pid / in_group) * GM;
+    const int gsz = min(p.tiles_m - first_m, GM);
+    const int tm = first_m + (pid % in_group) % gsz;
+    const int tn = (pid % in_group) / gsz;
+    const int m0 = tm * TILE_M, n0 = tn * kLeadBN;
+    const int kblocks = (p.k + Cfg::BK - 1) / Cfg::BK;
+    const int seg_blocks = p.seg_blocks;
+    const int segments = (kblocks + seg_blocks - 1) / seg_blocks;
+
+    if (tid == 0) {
+        for (int s = 0; s < kLeadStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(acc_free, kLeadEpiWarps);
+        mbar_init(mma_done, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, 512);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ---------------- TMA producer: one stage per K-block ----------------
+        if (lane == 0) {
+            tma_prefetch_desc(&tmA);
+            tma_prefetch_desc(&tmB);
+            int it = 0;
+            for (; it < kblocks; ++it) {
+                const int s = it % kLeadStages;
+                if ((it >= kLeadStages && !mbar_wait(&empty[s], ((it / kLeadStages) - 1) & 1, p.status)) ||
+                    *abort_flag) {
+                    *abort_flag = 1;
+                    break;
+                }
+                uint8_t* st = ring + s * kLeadStage;
+                const int k = it * Cfg::BK;
+                mbar_arrive_expect_tx(&full[s], kLeadStage);
+                tma_load_3d(st, &tmA, &full[s], k, m0, 0);
+                tma_load_3d(st + A_PLANE, &tmA, &full[s], k, m0, Cfg::ZS);
+                tma_load_3d(st + 2 * A_PLANE, &tmB, &full[s], k, n0, 0);
+                tma_load_3d(st + 3 * A_PLANE, &tmB, &full[s], k, n0, Cfg::ZS);
+            }
+            for (int j = it > kLeadStages ? it - kLeadStages : 0; j < it; ++j) {
+                mbar_wait(&full[j % kLeadStages], (j / kLeadStages) & 1, p.status);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc<Cfg::FMT, kLeadBN>();
+            const uint32_t idesc_neg = idesc | kNegateA;
+            const uint32_t d_re = tmem, d_im = tmem + (uint32_t)kLeadBN;
+            int it = 0;
+            bool stop = false;
+            for (int seg = 0; seg < segments && !stop; ++seg) {
+                if (seg > 0) {
+                    if (!mbar_wait(acc_free, (seg - 1) & 1, p.status)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                }
+                const int kb0 = seg * seg_blocks, kb1 = min(kblocks, kb0 + seg_blocks);
+                for (int kb = kb0; kb < kb1; ++kb, ++it) {
+                    const int s = it % kLeadStages;
+                    if (!mbar_wait(&full[s], (it / kLeadStages) & 1, p.status)) {
+                        *abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t base = smem_u32(ring + s * kLeadStage);
+#pragma unroll
+                    for (int kk = 0; kk < KSTEPS; ++kk) {
+                        const uint64_t a_re = smem_desc(base + kk * 32);
+                        const uint64_t a_im = smem_desc(base + A_PLANE + kk * 32);
+                        const uint64_t b_re = smem_desc(base + 2 * A_PLANE + kk * 32);
+                        const uint64_t b_im = smem_desc(base + 3 * A_PLANE + kk * 32);
+                        const uint32_t acc = (kb > kb0 || kk > 0) ? 1u : 0u;
+                        if constexpr (Cfg::FMT == 2) {
+                            umma_tf32(d_re, a_re, b_re, idesc, acc);
+                            umma_tf32(d_re, a_im, b_im, idesc_neg, 1u);
+                            umma_tf32(d_im, a_re, b_im, idesc, acc);
+                            umma_tf32(d_im, a_im, b_re, idesc, 1u);
+                        } else {
+                            umma_f16(d_re, a_re, b_re, idesc, acc);
+                            umma_f16(d_re, a_im, b_im, idesc_neg, 1u);
+                            umma_f16(d_im, a_re, b_im, idesc, acc);
+                            umma_f16(d_im, a_im, b_re, idesc, 1u);
+                        }
+                    }
+                    umma_commit(&empty[s]);
+                }
+                if (!stop) {
+                    umma_commit(acc_full);
+                }
+            }
+            umma_commit(mma_done);
+            mbar_wait(mma_done, 0, p.status);  // nothing may still write TMEM when it is freed
+        }
+    } else {
+        // ---------------- epilogue warps 2.. ----------------
+        // TMEM lane quadrant = warp % 4; warps 2-5 take the first COLS columns
+        // of the tile, warps 6-9 the next, and so on.
+        const int quad = warp & 3;
+        const int group = (warp - 2) >> 2;
+        const int row = m0 + quad * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(group * COLS);
+        const uint32_t seg_re = lane_addr, seg_im = lane_addr + kLeadBN;
+        const uint32_t run_re = lane_addr + 2 * kLeadBN, run_im = lane_addr + 3 * kLeadBN;
+        // Risk integrals by parts: with s_0 = 0 and equal weights w = d/9 on
+        // the full segments,
+        //   sum_{k<K} w (s_{k-1}^2 + s_{k-1} s_k + s_k^2)
+        //     = w (sum_{k<K} s_k (2 s_k + s_{k-1}) - s_{K-1}^2),
+        // so a full segment costs two FMAs per part and the last one (of depth
+        // d_K <= d) closes the sum with the whole step of weight d_K / 9.
+        float ir[COLS], ii[COLS];
+        const float wfull = __fdiv_rn((float)(seg_blocks * Cfg::BK), 9.0f);
+        bool go = true;
+        for (int seg = 0; seg < segments && go; ++seg) {
+            const int t0 = seg * seg_blocks * Cfg::BK;
+            const int depth = min(p.k, t0 + seg_blocks * Cfg::BK) - t0;
+            const float w = __fdiv_rn((float)depth, 9.0f);
+            const bool last = seg == segments - 1;
+            const bool ready = mbar_wait(acc_full, seg & 1, p.status);
+            tc_fence_after();
+            go = __all_sync(0xffffffffu, ready && !*abort_flag);
+            if (!go) {
+                break;
+            }
+            if (last) {
+                lead_drain<COLS, 2>(seg_re, seg_im, run_re, run_im, seg == 0, w, wfull, ir, ii);
+            } else if (seg == 0) {
+                lead_drain<COLS, 0>(seg_re, seg_im, run_re, run_im, true, w, wfull, ir, ii);
+            } else {
+                lead_drain<COLS, 1>(seg_re, seg_im, run_re, run_im, false, w, wfull, ir, ii);
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(acc_free);
+            }
+        }
+        if (go) {
+#pragma unroll
+            for (int cb = 0; cb < COLS; cb += 8) {
+                float re[8], im[8];
+                tmem_ld8x2(run_re + (uint32_t)cb, run_im + (uint32_t)cb, re, im);
+                if (row < p.m) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int col = n0 + group * COLS + cb + j;
+                        if (col < p.n) {
+                            float2* cp = p.C + (size_t)col * p.ldc + row;
+                            *cp = epilogue_value(re[j], im[j], p.epi, cp);
+                            p.path[(size_t)col * p.ldc + row] = ir[cb + j] > ii[cb + j] ? ir[cb + j] : ii[cb + j];
+                        }
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 512);
     }
 }
 
@@ -911,8 +1177,8 @@ cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan
     return err != cudaSuccess ? err : cudaGetLastError();
 }
 
-template <int FORM, int BN, bool PATH>
-cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status, float* path)
+template <int FORM, int BN>
+cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status)
 {
     using Cfg = TcCfg<FORM>;
     using G = TcGeom<FORM, BN>;
@@ -956,14 +1222,65 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
     if (p.seg_blocks < 1) {
         p.seg_blocks = 1;
     }
-    p.path = path;
-    auto kernel = gemm3m_tc_kernel<FORM, BN, PATH>;
+    auto kernel = gemm3m_tc_kernel<FORM, BN>;
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
     if (err != cudaSuccess) {
         return err;
     }
     const dim3 grid((unsigned)(p.tiles_m * p.tiles_n), (unsigned)plan.parts);
     kernel<<<grid, kThreads, G::SMEM, stream>>>(ta, tb, p);
+    return cudaGetLastError();
+}
+
+template <int LEAD>
+cudaError_t launch_lead_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status,
+                             float* path)
+{
+    using Cfg = TcCfg<LEAD>;
+    const bool bf16 = Cfg::FMT == 1;
+    const size_t elem = bf16 ? 2 : 4;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    CUtensorMap ta, tb;
+    const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.m, (uint64_t)(3 * Cfg::ZS)};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_a * elem, (uint64_t)plan.plane_a_elems * elem};
+        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)TILE_M, 1u};
+        if (!encode_tensor_map(&ta, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_a_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    {
+        const uint64_t dims[3] = {(uint64_t)pr.k, (uint64_t)pr.n, (uint64_t)(3 * Cfg::ZS)};
+        const uint64_t strides[2] = {(uint64_t)plan.pitch_b * elem, (uint64_t)plan.plane_b_elems * elem};
+        const uint32_t box[3] = {(uint32_t)Cfg::BK, (uint32_t)kLeadBN, 1u};
+        if (!encode_tensor_map(&tb, dt, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B, w + plan.planes_b_off)) {
+            return cudaErrorInvalidValue;
+        }
+    }
+    TcParams p{};
+    p.m = pr.m;
+    p.n = pr.n;
+    p.k = pr.k;
+    p.span = pr.k;
+    p.parts = 1;
+    p.tiles_m = ceil_div(pr.m, TILE_M);
+    p.tiles_n = ceil_div(pr.n, kLeadBN);
+    p.epi = EpiParams{pr.ar, pr.ai, pr.br, pr.bi, plan.unit ? 1 : 0, plan.beta_zero ? 1 : 0};
+    p.C = static_cast<float2*>(pr.C);
+    p.ldc = pr.ldc;
+    p.status = status;
+    p.seg_blocks = plan.tc_segment > 0 ? (plan.tc_segment + Cfg::BK - 1) / Cfg::BK : 64 / Cfg::BK;
+    if (p.seg_blocks < 1) {
+        p.seg_blocks = 1;
+    }
+    p.path = path;
+    auto kernel = gemm3m_lead_path_kernel<LEAD>;
+    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLeadSmem);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    kernel<<<(unsigned)(p.tiles_m * p.tiles_n), kLeadThreads, kLeadSmem, stream>>>(ta, tb, p);
     return cudaGetLastError();
 }
 
@@ -986,9 +1303,9 @@ cudaError_t launch_gemm_tc(cudaStream_t stream, const Problem& pr, const Plan& p
         }
     }
     switch (plan.form) {
-        case CG3M_FORM_TF32X3: return launch_form<CG3M_FORM_TF32X3, 128, false>(stream, pr, plan, ws, status, nullptr);
-        case CG3M_FORM_BF16X6: return launch_form<CG3M_FORM_BF16X6, 128, false>(stream, pr, plan, ws, status, nullptr);
-        case CG3M_FORM_BF16X9: return launch_form<CG3M_FORM_BF16X9, 128, false>(stream, pr, plan, ws, status, nullptr);
+        case CG3M_FORM_TF32X3: return launch_form<CG3M_FORM_TF32X3, 128>(stream, pr, plan, ws, status);
+        case CG3M_FORM_BF16X6: return launch_form<CG3M_FORM_BF16X6, 128>(stream, pr, plan, ws, status);
+        case CG3M_FORM_BF16X9: return launch_form<CG3M_FORM_BF16X9, 128>(stream, pr, plan, ws, status);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -997,9 +1314,9 @@ cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Pl
                                 int* status)
 {
     switch (plan.form) {
-        case CG3M_FORM_TF32X3: return launch_form<kLeadTf32, 64, true>(stream, pr, plan, ws, status, path);
+        case CG3M_FORM_TF32X3: return launch_lead_path<kLeadTf32>(stream, pr, plan, ws, status, path);
         case CG3M_FORM_BF16X6:
-        case CG3M_FORM_BF16X9: return launch_form<kLeadBf16, 64, true>(stream, pr, plan, ws, status, path);
+        case CG3M_FORM_BF16X9: return launch_lead_path<kLeadBf16>(stream, pr, plan, ws, status, path);
         default: return cudaErrorInvalidValue;
     }
 }

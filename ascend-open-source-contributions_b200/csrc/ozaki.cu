@@ -18,18 +18,19 @@
 //      beta = 47, and the row counts its parts for which a != x 2^(beta - E)
 //      (cA_i; cB_j for the columns).  The planes hold a mod p_m for the
 //      kOzMods = 14 moduli p_m <= 256 (pairwise coprime, product M ~ 2^110.2)
-//      as int8 in [-(p-1)/2, (p-1)/2] ([-128, 127] for 256); the op(A)
-//      residues are multiplied by u_m = (M / p_m)^-1 mod p_m on the way.
+//      as int8 in [-(p-1)/2, (p-1)/2] ([-128, 127] for 256).
 //   2. ozaki_pair_kernel: for each modulus the int8 products
 //        Re_m = sum Ar Br + Ai (-Bi),  Im_m = sum Ar Bi + Ai Br
 //      are exact in the int32 TMEM accumulators (|sum| <= 2 * 4096 * 128^2
 //      < 2^31); the epilogue stores y_m = sum mod p_m in [0, p_m) as one byte
-//      per output and part.  By construction y_m = u_m x mod p_m, x the exact
-//      integer product of the rounded parts.
-//   3. ozaki_crt_kernel: x = sum_m y_m (M / p_m) - k M with k the nearest
-//      integer to sum_m y_m / p_m (|x| <= 2 n 2^(2 beta) <= 2^107 < M / 8,
-//      so k is never in doubt), evaluated exactly in three 40-bit limbs of
-//      FP64.  Rounding a part moves each real product by at most 2^(beta - 1),
+//      per output and part: y_m = x mod p_m, x the exact integer product of
+//      the rounded parts.
+//   3. ozaki_crt_kernel: x = sum_m y_m w_m - k M with w_m = u_m (M / p_m)
+//      mod M, u_m = (M / p_m)^-1 mod p_m (so w_m = 1 mod p_m, 0 mod the other
+//      moduli), and k the nearest integer to sum_m y_m w_m / M
+//      (|x| <= 2 n 2^(2 beta) <= 2^107 < M / 8, so k is never in doubt),
+//      evaluated exactly in three 40-bit limbs of FP64.  The factor u_m lives
+//      in the constants w_m, so the residue kernel does no multiplication.  Rounding a part moves each real product by at most 2^(beta - 1),
 //      so
 //        |error| <= (cA_i + cB_j) 2^(beta - 1)   (units of 2^(E_i + F_j - 2 beta)),
 //      zero for rows and columns that scaled exactly.  Every output of a tile
@@ -86,13 +87,13 @@ constexpr int kOzModuli[kOzMods] = {256, 255, 253, 251, 247, 241, 239, 233, 229,
 // Constants of the moduli (host-computed once, passed by value).
 struct OzCrt {
     int p[kOzMods];
-    int u[kOzMods];          // (M / p)^-1 mod p, in [-(p-1)/2, (p-1)/2] ([-128, 127] for 256)
     int c16[kOzMods];        // 2^16 mod p
     float pf[kOzMods];
     float inv_pf[kOzMods];   // rn(1 / p)
+    float wf[kOzMods];       // rn(w / M)
     double pd[kOzMods];
     double inv_pd[kOzMods];  // rn(1 / p)
-    double w[kOzMods][3];    // M / p in 40-bit limbs, low first
+    double w[kOzMods][3];    // w = u (M / p) mod M, u = (M / p)^-1 mod p, in 40-bit limbs, low first
     double m[3];             // M in 40-bit limbs, low first
 };
 
@@ -138,22 +139,12 @@ __device__ __forceinline__ int mod_odd_d(double t, double tm, double pd, double 
     return __double2loint(__fma_rn(-q, pd, tm));
 }
 
-// v mod p in [-(p-1)/2, (p-1)/2] for odd p >= 199 and |v| <= 127^2 (|v / p| is
-// off by < 2^-17 in FP32, against a distance >= 1 / 2p to a half-integer).
-__device__ __forceinline__ int mod_odd_f(int v, float pf, float inv_pf)
-{
-    const float vf = __fsub_rn(__int_as_float(0x4B400000 + v), kMagicF);  // exact: v as a float
-    const float q = __fsub_rn(__fmaf_rn(vf, inv_pf, kMagicF), kMagicF);
-    const float r = __fmaf_rn(-q, pf, vf);
-    return __float_as_int(__fadd_rn(r, kMagicF)) - 0x4B400000;
-}
-
 // ---- 1. residues -------------------------------------------------------------------
 
 // One block per op(A) row (blockIdx.x < n) or op(B) column.  Plane layout:
 // [plane][row][kpitch] int8, A planes 2m + {0 re, 1 im}, B planes
 // 3m + {0 re, 1 im, 2 -im}.
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
     ozaki_split_kernel(int n, int pitch, const float2* __restrict__ rows_a, const float2* __restrict__ rows_b,
                        int8_t* __restrict__ pa, int8_t* __restrict__ pb, int kpitch, size_t plane_bytes,
                        int* __restrict__ E, int* __restrict__ F, int* __restrict__ CA, int* __restrict__ CB,
@@ -198,6 +189,7 @@ __global__ void __launch_bounds__(256, 3)
     const int planes_per_mod = is_a ? 2 : 3;
     int rounded = 0;
     // Four consecutive K terms per thread: 4-byte stores into every plane.
+#pragma unroll 1
     for (int k0 = tid * 4; k0 < n; k0 += 256 * 4) {
         // The real parts, then the imaginary parts, of four consecutive terms.
 #pragma unroll 1
@@ -222,10 +214,6 @@ __global__ void __launch_bounds__(256, 3)
                         v[q] = (int)(signed char)(__double2loint(tm[q]) & 0xFF);
                     } else {
                         v[q] = mod_odd_d(t[q], tm[q], crt.pd[mi], crt.inv_pd[mi]);
-                    }
-                    if (is_a) {
-                        const int w = v[q] * crt.u[mi];
-                        v[q] = mi == 0 ? (int)(signed char)(w & 0xFF) : mod_odd_f(w, crt.pf[mi], crt.inv_pf[mi]);
                     }
                 }
                 int8_t* plane = dst + (size_t)(planes_per_mod * mi + part) * plane_bytes;
@@ -568,12 +556,13 @@ __device__ __forceinline__ void crt_part2(const OzCrt& crt, const uint32_t* word
             s[c][0] = __fma_rn(yd, crt.w[mi][0], s[c][0]);
             s[c][1] = __fma_rn(yd, crt.w[mi][1], s[c][1]);
             s[c][2] = __fma_rn(yd, crt.w[mi][2], s[c][2]);
-            ks[c] = __fmaf_rn(yf, crt.inv_pf[mi], ks[c]);
+            ks[c] = __fmaf_rn(yf, crt.wf[mi], ks[c]);
         }
     }
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-        // sum y / p = k + x / M with |x / M| < 1/8; the FP32 sum is off by < 2^-15
+        // sum y w / M = k + x / M with |x / M| < 1/8; the FP32 sum (14 terms of at
+        // most 255, k <= 3570) is off by < 2^-8
         const double k = (double)rintf(ks[c]);
         const double d0 = __fma_rn(-k, crt.m[0], s[c][0]);  // exact integers below 2^53
         const double d1 = __fma_rn(-k, crt.m[1], s[c][1]);
@@ -678,14 +667,15 @@ OzCrt make_crt()
                 break;
             }
         }
+        const unsigned __int128 w = (W * (unsigned)u) % M;  // W u < M p < 2^119: no overflow
         c.p[mi] = p;
-        c.u[mi] = u > p / 2 ? u - p : u;
         c.c16[mi] = (1 << 16) % p;
         c.pf[mi] = (float)p;
         c.inv_pf[mi] = 1.0f / (float)p;
+        c.wf[mi] = (float)((double)w / (double)M);
         c.pd[mi] = (double)p;
         c.inv_pd[mi] = 1.0 / (double)p;
-        limbs(W, c.w[mi]);
+        limbs(w, c.w[mi]);
     }
     limbs(M, c.m);
     return c;

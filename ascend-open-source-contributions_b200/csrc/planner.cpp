@@ -287,6 +287,12 @@ bool make_plan(const Problem& p, const cg3mOptions& opts, int sm_count, Plan* pl
     if (opts.k_partitions <= 0 && !tc && p.k >= 1024 && std::min(p.m, p.n) <= 16 && std::max(p.m, p.n) <= 32) {
         best_parts = std::max(best_parts, 8);
     }
+    // The tensor-core forms' rounding pass runs its products over the whole K:
+    // the risk plane needs the whole chain and the form's products on the
+    // tiles the exact recompute does not take run unsplit.
+    if (tc && out.rounding) {
+        best_parts = 1;
+    }
     out.tile_m = best_tile.bm;
     out.tile_n = best_tile.bn;
     out.parts = best_parts;

@@ -233,6 +233,20 @@ def test_rounding_gate(cg3m):
     assert cg3m.plan("N", "N", 2048, 2048, 2048, rounding="off")["rounding"] == 0
 
 
+def test_tc_rounding_pass_runs_unsplit(cg3m):
+    """A requested K split does not reach the tensor-core forms' rounding pass,
+    whose risk plane and form products run over the whole K; with the pass off
+    (or for the FP32 form, whose split is part of the reference's arithmetic)
+    the request stands."""
+    for form in ("tf32x3", "bf16x6", "bf16x9"):
+        on = cg3m.plan("N", "N", 2048, 2048, 2048, form=form, k_partitions=4)
+        assert on["rounding"] == 1 and on["k_partitions"] == 1
+        off = cg3m.plan("N", "N", 2048, 2048, 2048, form=form, k_partitions=4, rounding="off")
+        assert off["k_partitions"] == 4
+    fp32 = cg3m.plan("N", "N", 2048, 2048, 2048, form="fp32", k_partitions=4)
+    assert fp32["rounding"] == 1 and fp32["k_partitions"] == 4
+
+
 def test_batch_plan_validation_without_device(cg3m):
     """Argument errors of cg3mBatchPlanCreate come from the host-side
     validation, per problem in order, before any device work."""

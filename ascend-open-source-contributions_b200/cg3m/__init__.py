@@ -349,11 +349,15 @@ def stage_names(info):
         return ["onchip"][:k]
     if info["rounding"]:
         fp32 = info["form"] == FORM["fp32"]
-        prep = ["pack_rows", "energy"] + ([] if fp32 else ["exact_split"])
-        tail = ["select", "replay_tiles", "lanes_needed", "lane_major", "replay_outputs"] if fp32 else \
-            ["select", "gemm_form_tiles", "exact_tiles", "exact_crt", "lanes_needed", "lane_major",
-             "recompute_fp64_outputs", "fallback_fp64"]
-        names = ["pack", "gemm_path"] + prep + tail
+        if fp32:
+            names = ["pack", "gemm_path", "pack_rows", "energy", "select", "replay_tiles", "lanes_needed",
+                     "lane_major", "replay_outputs"]
+        else:
+            # packed rows with the leading planes first; the rest of the planes
+            # only for the bands the form's products read
+            names = ["pack_rows", "gemm_path", "energy", "exact_split", "select", "band_need", "pack_rest",
+                     "gemm_form_tiles", "exact_tiles", "exact_crt", "lanes_needed", "lane_major",
+                     "recompute_fp64_outputs", "fallback_fp64"]
     else:
         names = ["pack", "gemm", "merge"]
     names = names[:k]

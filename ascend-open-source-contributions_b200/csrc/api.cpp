@@ -246,7 +246,10 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
     int count = 0;
     {
         auto mark = run_marks(0, main_len, s);
-        err = launch_pack(s, p, plan, ws);
+        // tensor-core forms in the rounding pass: packed rows with the leading
+        // planes; the rest of the planes is packed after the selection
+        err = plan.rounding && plan.form != CG3M_FORM_FP32 ? launch_rounding_pack(s, p, plan, ws)
+                                                           : launch_pack(s, p, plan, ws);
         mark(++count);
         if (err == cudaSuccess) {
             if (plan.rounding) {
@@ -875,7 +878,7 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
     info->k_span = plan.span;
     info->rounding = plan.rounding ? 1 : 0;
     info->kernels =
-        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? (plan.form == CG3M_FORM_FP32 ? 7 : 11) : 0);
+        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? (plan.form == CG3M_FORM_FP32 ? 7 : 12) : 0);
     info->workspace_bytes = plan.total;
     return CG3M_STATUS_SUCCESS;
 }

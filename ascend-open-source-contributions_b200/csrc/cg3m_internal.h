@@ -92,15 +92,24 @@ bool encode_tensor_map(CUtensorMap* map, CUtensorMapDataType type, int rank, con
 
 // ---- kernel launchers (return cudaSuccess or the launch error) -------------
 cudaError_t launch_beta_scale(cudaStream_t s, int m, int n, float br, float bi, void* C, int ldc);
-cudaError_t launch_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws);
+// band_a / band_b (tensor-core forms' rounding pass): pack only the planes the
+// packed rows did not (all but the leading term of re and im), and only for the
+// 256-row bands of op(A) rows / op(B) columns whose byte is nonzero.
+cudaError_t launch_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, const uint8_t* band_a = nullptr,
+                        const uint8_t* band_b = nullptr);
 cudaError_t launch_gemm_fp32(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
 cudaError_t launch_gemm_tc(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status);
 cudaError_t launch_merge(cudaStream_t s, const Problem& p, const Plan& plan, void* ws);
-// The rounding-correction pass in two halves: the preparation reads only
-// op(A) and op(B) (packed rows, energies, lane-major copies and, for the
-// tensor-core forms, the residues of the exact recompute); the finish needs
-// the GEMM's C and risk plane (selection, then the recomputes).  mark(i) is
-// called after the i-th kernel of each half (1-based) is enqueued.
+// The rounding-correction pass.  Tensor-core forms start the call with the
+// packed rows, which also write the leading split planes the risk-plane GEMM
+// reads (launch_rounding_pack, instead of the full pack).  Then two halves:
+// the preparation reads only op(A) and op(B) (packed rows for the FP32 form,
+// energies and, for the tensor-core forms, the residues of the exact
+// recompute); the finish needs the GEMM's C and risk plane (selection, then
+// the recomputes; the tensor-core forms pack the rest of their planes there,
+// for the bands whose tiles the exact recompute leaves to the form).  mark(i)
+// is called after the i-th kernel of each half (1-based) is enqueued.
+cudaError_t launch_rounding_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws);
 int rounding_prep_kernels(int form);
 cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* launched,
                                  const std::function<void(int)>& mark);

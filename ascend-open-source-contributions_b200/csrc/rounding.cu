@@ -38,7 +38,8 @@
 
 namespace cg3m {
 
-cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a, void* rows_b, int pitch);
+cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a, void* rows_b, int pitch,
+                             const Plan* lead_plan = nullptr, void* ws = nullptr);
 cudaError_t launch_gemm_fp32_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, float* path,
                                   int* status);
 cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, float* path,
@@ -152,6 +153,25 @@ __global__ void select_kernel(int n, const float2* __restrict__ C, const float* 
     local = __reduce_add_sync(0xffffffffu, local);
     if (lane == 0 && local != 0) {
         atomicAdd(&stats[kStatFlagged], local);
+    }
+}
+
+// Per 256 x 256 tile (blockIdx.x: op(A) row band, blockIdx.y: op(B) column
+// band): when none of its 16 x 16 count tiles holds more than kSparseMax
+// flagged outputs (the exact recompute's and the pair kernel's own test), the
+// form's products run there and read that row band of op(A) and column band
+// of op(B), so both bands are marked for the rest of the pack.
+static_assert(kOzakiTile / kTile == 16, "16 x 16 count tiles per exact tile");
+__global__ void __launch_bounds__(256) band_need_kernel(int n, const uint32_t* __restrict__ tile_count,
+                                                         uint8_t* __restrict__ band_a, uint8_t* __restrict__ band_b)
+{
+    const int g16 = (n + kTile - 1) / kTile;
+    const int gi = blockIdx.x * 16 + threadIdx.x % 16;
+    const int gj = blockIdx.y * 16 + threadIdx.x / 16;
+    const bool dense = gi < g16 && gj < g16 && tile_count[(size_t)gj * g16 + gi] > kSparseMax;
+    if (!__syncthreads_or(dense) && threadIdx.x == 0) {
+        band_a[blockIdx.x] = 1;
+        band_b[blockIdx.y] = 1;
     }
 }
 
@@ -874,12 +894,16 @@ struct RoundLayout {
     uint32_t* stats;
     uint32_t* fallback_bits;
     uint8_t* need;      // rows of op(A), then columns of op(B), the per-output kernels read
-    size_t zero_bytes;  // tile_count + stats + fallback_bits + need, one memset
+    uint8_t* band;      // [kMaxBands] op(A) row bands, then [kMaxBands] op(B) column bands, of 256
+                        // whose tiles the form's products read (tensor-core forms)
+    size_t zero_bytes;  // tile_count + stats + fallback_bits + need + band, one memset
     OzLayout oz;
 };
 
 static size_t flag_words(int n) { return ((size_t)n * n + 31) / 32; }
 static size_t need_words(int n) { return ((size_t)2 * n + 3) / 4; }
+constexpr int kMaxBands = 16;  // 256-row bands of the largest gated order, 4096
+static size_t band_words() { return (size_t)2 * kMaxBands / 4; }
 static size_t tile_words(int n)
 {
     const size_t t = (size_t)(n + kTile - 1) / kTile;
@@ -916,7 +940,8 @@ static RoundOffsets round_offsets(int n, int form, std::vector<size_t>* guards)
     o.energy = off;
     off = next_region(off, (size_t)2 * n * 4, guards);
     o.flags = off;
-    off = next_region(off, (2 * flag_words(n) + tile_words(n) + kStatWords + need_words(n)) * 4, guards);
+    off = next_region(off, (2 * flag_words(n) + tile_words(n) + kStatWords + need_words(n) + band_words()) * 4,
+                      guards);
     o.oz = off;
     if (form != CG3M_FORM_FP32) {
         std::vector<size_t> inner;
@@ -947,7 +972,8 @@ static RoundLayout round_layout(const Plan& plan, void* ws, int n)
     L.stats = L.tile_count + tile_words(n);
     L.fallback_bits = L.stats + kStatWords;
     L.need = reinterpret_cast<uint8_t*>(L.fallback_bits + flag_words(n));
-    L.zero_bytes = (tile_words(n) + kStatWords + flag_words(n) + need_words(n)) * 4;
+    L.band = L.need + need_words(n) * 4;
+    L.zero_bytes = (tile_words(n) + kStatWords + flag_words(n) + need_words(n) + band_words()) * 4;
     if (plan.form != CG3M_FORM_FP32) {
         L.oz = oz_layout(n, b + o.oz);
     }
@@ -1007,7 +1033,14 @@ static cudaError_t launch_replay(cudaStream_t s, int n, int span, const RoundLay
 
 int rounding_prep_kernels(int form)
 {
-    return form == CG3M_FORM_FP32 ? 2 : 3;
+    (void)form;
+    return 2;  // FP32: packed rows, energies; tensor-core forms: energies, residues
+}
+
+cudaError_t launch_rounding_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws)
+{
+    const RoundLayout L = round_layout(plan, ws, p.n);
+    return launch_pack_rows(s, p, L.rows_a, L.rows_b, row_pitch(p.n), &plan, ws);
 }
 
 cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* launched,
@@ -1018,8 +1051,11 @@ cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& p
     const RoundLayout L = round_layout(plan, ws, n);
     const int span = ((n + kLanes - 1) / kLanes) | 1;
     int count = 0;
-    cudaError_t err = launch_pack_rows(s, p, L.rows_a, L.rows_b, pitch);
-    mark(++count);
+    cudaError_t err = cudaSuccess;
+    if (plan.form == CG3M_FORM_FP32) {  // the tensor-core forms packed their rows first
+        err = launch_pack_rows(s, p, L.rows_a, L.rows_b, pitch);
+        mark(++count);
+    }
     if (err == cudaSuccess) {
         energy_kernel<<<2 * n, kLanes, 0, s>>>(L.rows_a, L.rows_b, n, pitch, span,
                                                                         L.energy);
@@ -1094,6 +1130,20 @@ cudaError_t launch_rounding_finish(cudaStream_t s, const Problem& p, const Plan&
         // The path GEMM's C came from the leading split planes alone: the
         // form's own products now run on every tile the exact recompute does
         // not take, and the exact recompute writes every output of its tiles.
+        // The rest of the form's planes is packed for the bands those tiles read.
+        const int bands = (n + kOzakiTile - 1) / kOzakiTile;
+        if (err == cudaSuccess && bands > kMaxBands) {
+            err = cudaErrorInvalidValue;  // beyond the gated orders
+        }
+        if (err == cudaSuccess) {
+            band_need_kernel<<<dim3(bands, bands), 256, 0, s>>>(n, L.tile_count, L.band, L.band + kMaxBands);
+            err = cudaGetLastError();
+            mark(++count);
+        }
+        if (err == cudaSuccess) {
+            err = launch_pack(s, p, plan, ws, L.band, L.band + kMaxBands);
+            mark(++count);
+        }
         if (err == cudaSuccess) {
             err = launch_gemm_tc_tiles(s, p, plan, ws, status, L.tile_count);
             mark(++count);

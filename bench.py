@@ -583,20 +583,22 @@ def kernel_roofline(name, ms, n, form, sm_count, sgemm, stats, mhz):
     pk, src = peaks()
     p = PASSES[form]
     if name in ("gemm", "gemm_path", "gemm_form_tiles"):
-        # the tensor-core forms' path GEMM is one pass over the leading split
-        # planes; their form products then cover only the tiles the exact
-        # recompute does not take
+        # the tensor-core forms' path GEMM is one pass of the four real products
+        # (8 n^3 flop) over the leading split planes of re and im; their form
+        # products then cover only the tiles the exact recompute does not take
         cover = 1.0
+        per = 6.0
         if name == "gemm_path" and form != "fp32":
-            p = 1
+            p, per = 1, 8.0
         if name == "gemm_form_tiles":
             cover = 1.0 - (float(stats.get("exact_positions", 0)) / float(n * n) if stats else 0.0)
-        work = 6.0 * n ** 3 * p * cover
+        work = per * n ** 3 * p * cover
         peak, peak_src = pipe_peak(form, sm_count, sgemm)
         return {"bound": "tensor" if form != "fp32" else "fp32-pipe",
                 "achieved": work / (ms * 1e-3) / 1e12 if ms > 0 else 0.0,
                 "peak": peak, "unit": "TFLOP/s", "work_per_launch": work,
-                "work_model": f"6*n^3 real flop x {p} pass(es) x {cover:.3f} of the outputs", "peak_source": peak_src}
+                "work_model": f"{per:.0f}*n^3 real flop x {p} pass(es) x {cover:.3f} of the outputs",
+                "peak_source": peak_src}
     if name == "exact_tiles":
         positions = float(stats.get("exact_positions", 0)) if stats else 0.0
         work = 2.0 * 14 * 4 * positions * n  # int8 ops: 14 moduli x 4 real products per output and term

@@ -63,8 +63,10 @@ typedef enum { CG3M_FORM_FP32 = 0, CG3M_FORM_TF32X3 = 1, CG3M_FORM_BF16X6 = 2, C
  *   AUTO -- as the reference: only for m==n==k in [2048,4096], lda==ldb==ldc==m,
  *           alpha==1, beta==0.  FP32 form: flagged outputs are recomputed in
  *           FP32 fixed order (the reference's replay bit for bit).  Tensor-core
- *           forms: the risk plane comes from one tensor pass over the leading
- *           split planes; every output of a 256 x 256 tile holding a 16 x 16
+ *           forms: the risk plane comes from one tensor pass (four real
+ *           products) over the leading split planes of the real and imaginary
+ *           parts, and the call runs unsplit over K whatever k_partitions asks;
+ *           every output of a 256 x 256 tile holding a 16 x 16
  *           tile with more than 64 flagged outputs is computed to within one
  *           FP32 rounding of the exact product (exact int8 products by residues
  *           on the tensor cores, FP64 where their bound does not certify it);
@@ -84,7 +86,8 @@ typedef struct cg3mContext* cg3mHandle_t;
 typedef struct {
     cg3mForm_t form;
     cg3mRounding_t rounding;
-    int k_partitions; /* 0 = planner's choice; else force this many K partitions (1..64) */
+    int k_partitions; /* 0 = planner's choice; else force this many K partitions (1..64; the
+                         tensor-core forms' rounding pass runs unsplit) */
     int tc_segment;   /* tensor-core forms: K terms accumulated in TMEM before each round-to-nearest
                          FP32 merge (0 = planner: 128 for k >= 2048, 64 for k > 1024, else 32;
                          rounded up to the kernel's K-block of 32 or 64) */

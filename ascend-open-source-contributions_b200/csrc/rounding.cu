@@ -646,11 +646,6 @@ __device__ __forceinline__ bool ozaki_tile_dense(const uint32_t* tile_count, int
 //     sums are reduced in FP64 and the result is rounded once to FP32.
 enum { kSparseFp32 = 0, kSparseFp64 = 1, kFallbackFp64 = 2 };
 
-// One tile per block: several consecutive tiles per block (4, or a grid-
-// stride walk) saved ~0.02 ms of block launches where no tile has work but
-// made the reference's data (~7 flagged outputs per tile) 1.6-2.5x slower.
-constexpr int kSparseTilesPerBlock = 1;
-
 template <int MODE>
 __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int span,
                                                           const float2* __restrict__ lanes_a,
@@ -669,24 +664,19 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int span,
     // Tiles in bands of kSparseBand tile rows, rows fastest within a band: the
     // op(A) rows of a band (1024 rows, 32 MB at n = 4096) stay in L2 while the
     // band's columns go by, so each staged row comes from L2, not HBM.
-    // A block takes kSparseTilesPerBlock consecutive tiles of that order.
     constexpr int kSparseBand = 64;
     const int tiles = (n + kTile - 1) / kTile;
-    const int l = threadIdx.x;
-    const int kbeg = min(n, l * span), cnt = min(n, kbeg + span) - kbeg;
-    const int t_end = min(tiles * tiles, (int)(blockIdx.x + 1) * kSparseTilesPerBlock);
-    for (int t = blockIdx.x * kSparseTilesPerBlock; t < t_end; ++t) {
-    __syncthreads();  // the previous tile's list is no longer read
-    const int band = t / (kSparseBand * tiles), first = band * kSparseBand;
-    const int rows_in_band = min(kSparseBand, tiles - first), in_band = t - band * kSparseBand * tiles;
+    const int band = blockIdx.x / (kSparseBand * tiles), first = band * kSparseBand;
+    const int rows_in_band = min(kSparseBand, tiles - first), in_band = blockIdx.x - band * kSparseBand * tiles;
     const int gi = first + in_band % rows_in_band, gj = in_band / rows_in_band;
     const uint32_t count = tile_count[(size_t)gj * tiles + gi];
     if (count == 0) {
-        continue;
+        return;
     }
     if (MODE != kFallbackFp64 && count > kSparseMax) {
-        continue;
+        return;
     }
+    const int l = threadIdx.x;
     const int i0 = gi * kTile, j0 = gj * kTile;
     if (MODE == kFallbackFp64) {
         // Fallback bits are only ever set inside the exact recompute's tiles:
@@ -699,12 +689,12 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int span,
             }
         }
         if (!__syncthreads_or(any)) {
-            continue;
+            return;
         }
     }
     // The exact recompute writes (or marks) every flagged output of its tiles.
     if (MODE == kSparseFp64 && ozaki_tile_dense(tile_count, tiles, gi, gj, exact_gn)) {
-        continue;
+        return;
     }
     if (l == 0) {
         listed = 0;
@@ -719,7 +709,7 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int span,
     __syncthreads();
     const int outputs = listed;
     if (outputs == 0) {
-        continue;
+        return;
     }
     if (l == 0 && MODE != kFallbackFp64) {
         atomicAdd(&stats[kStatSparseOutputs], (uint32_t)outputs);
@@ -727,6 +717,7 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int span,
     // Lane l's terms, read from the lane-major copies (element s of lane l at
     // s * 64 + l): every warp load is 256 contiguous bytes, and no shared
     // memory is staged, so many blocks share an SM.
+    const int kbeg = min(n, l * span), cnt = min(n, kbeg + span) - kbeg;
     for (int u = 0; u < outputs; ++u) {
         const int o = list[u];
         const int i = i0 + o % kTile, j = j0 + o / kTile;
@@ -866,7 +857,6 @@ __global__ void __launch_bounds__(kLanes) recompute_sparse(int n, int span,
             }
         }
         __syncthreads();  // every read of this output's staged vectors and sums is done
-    }
     }
 }
 
@@ -1119,8 +1109,11 @@ cudaError_t launch_rounding_finish(cudaStream_t s, const Problem& p, const Plan&
         return e;
     };
     auto sparse = [&](auto kernel, const uint32_t* bits) {
-        const int blocks = (tiles16 * tiles16 + kSparseTilesPerBlock - 1) / kSparseTilesPerBlock;
-        kernel<<<blocks, kLanes, 0, s>>>(n, span, L.lanes_a, L.lanes_b, bits, L.tile_count, L.stats, C, exact_gn);
+        // one block per 16 x 16 tile: several tiles per block (4, or a grid-
+        // stride walk) saved ~0.02 ms of block launches where no tile has work
+        // but made the reference's data (~7 flagged outputs per tile) 1.6-2.5x slower
+        kernel<<<tiles16 * tiles16, kLanes, 0, s>>>(n, span, L.lanes_a, L.lanes_b, bits, L.tile_count, L.stats, C,
+                                                    exact_gn);
         const cudaError_t e = cudaGetLastError();
         mark(++count);
         return e;

@@ -27,7 +27,8 @@
 //      the rounded parts.
 //   3. ozaki_crt_kernel: x = sum_m y_m w_m - k M with w_m = u_m (M / p_m)
 //      mod M, u_m = (M / p_m)^-1 mod p_m (so w_m = 1 mod p_m, 0 mod the other
-//      moduli), and k the nearest integer to sum_m y_m w_m / M
+//      moduli), and k the nearest integer to sum_m y_m w_m / M (from the
+//      exact limb sums)
 //      (|x| <= 2 n 2^(2 beta) <= 2^107 < M / 8, so k is never in doubt),
 //      evaluated exactly in three 40-bit limbs of FP64.  The factor u_m lives
 //      in the constants w_m, so the residue kernel does no multiplication.  Rounding a part moves each real product by at most 2^(beta - 1),
@@ -90,11 +91,11 @@ struct OzCrt {
     int c16[kOzMods];        // 2^16 mod p
     float pf[kOzMods];
     float inv_pf[kOzMods];   // rn(1 / p)
-    float wf[kOzMods];       // rn(w / M)
     double pd[kOzMods];
     double inv_pd[kOzMods];  // rn(1 / p)
     double w[kOzMods][3];    // w = u (M / p) mod M, u = (M / p)^-1 mod p, in 40-bit limbs, low first
     double m[3];             // M in 40-bit limbs, low first
+    double k2, k1;           // rn(2^80 / M), rn(2^40 / M): k from the limb sums
 };
 
 struct OzParams {
@@ -536,34 +537,28 @@ __device__ __forceinline__ double pow2d(int e)
 __device__ __forceinline__ void crt_part2(const OzCrt& crt, const uint32_t* words, int c0, double* x)
 {
     double s[2][3];
-    float ks[2];
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
         s[c][0] = s[c][1] = s[c][2] = 0.0;
-        ks[c] = 0.0f;
     }
 #pragma unroll
     for (int mi = 0; mi < kOzMods; ++mi) {
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            // byte c0 + c of the word as the low byte of 2^52 + y (FP64) and 2^23 + y (FP32)
-            const unsigned sel = (unsigned)(c0 + c);
-            const int lo = (int)__byte_perm(words[mi], 0u, 0x4440u + sel);
-            const int fb = (int)__byte_perm(words[mi], 0x4B000000u, 0x7440u + sel);
+            // byte c0 + c of the word as the low byte of 2^52 + y
+            const int lo = (int)__byte_perm(words[mi], 0u, 0x4440u + (unsigned)(c0 + c));
             const double yd = __dsub_rn(__hiloint2double(0x43300000, lo), 4503599627370496.0);  // exact
-            const float yf = __fsub_rn(__int_as_float(fb), 8388608.0f);                         // exact
             // every product and partial sum stays below 2^52: exact
             s[c][0] = __fma_rn(yd, crt.w[mi][0], s[c][0]);
             s[c][1] = __fma_rn(yd, crt.w[mi][1], s[c][1]);
             s[c][2] = __fma_rn(yd, crt.w[mi][2], s[c][2]);
-            ks[c] = __fmaf_rn(yf, crt.wf[mi], ks[c]);
         }
     }
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-        // sum y w / M = k + x / M with |x / M| < 1/8; the FP32 sum (14 terms of at
-        // most 255, k <= 3570) is off by < 2^-8
-        const double k = (double)rintf(ks[c]);
+        // S / M = k + x / M with |x / M| < 1/8, S = (s2 2^40 + s1) 2^40 + s0;
+        // s2 rn(2^80 / M) + s1 rn(2^40 / M) is off S / M by < 2^-40 (S / M < 3570)
+        const double k = rint(__fma_rn(s[c][2], crt.k2, __dmul_rn(s[c][1], crt.k1)));
         const double d0 = __fma_rn(-k, crt.m[0], s[c][0]);  // exact integers below 2^53
         const double d1 = __fma_rn(-k, crt.m[1], s[c][1]);
         const double d2 = __fma_rn(-k, crt.m[2], s[c][2]);
@@ -672,12 +667,13 @@ OzCrt make_crt()
         c.c16[mi] = (1 << 16) % p;
         c.pf[mi] = (float)p;
         c.inv_pf[mi] = 1.0f / (float)p;
-        c.wf[mi] = (float)((double)w / (double)M);
         c.pd[mi] = (double)p;
         c.inv_pd[mi] = 1.0 / (double)p;
         limbs(w, c.w[mi]);
     }
     limbs(M, c.m);
+    c.k2 = (double)((long double)((unsigned __int128)1 << 80) / (long double)M);
+    c.k1 = (double)((long double)((unsigned __int128)1 << 40) / (long double)M);
     return c;
 }
 

@@ -248,6 +248,54 @@ def test_tc_pass_tiles_taken_and_form_products(cg3m, oracle, cuda, h, form):
 
 
 @pytest.mark.parametrize("form", ["tf32x3", "bf16x6"])
+def test_tc_pass_row_band_taken(cg3m, oracle, cuda, h, form):
+    """The transposed layout: six adjacent op(A) rows scaled by 1024 make every
+    tile of the first 256-row band dense, so the exact recompute takes that
+    band across all columns and the rest of the form's planes is packed for
+    the other op(A) row bands only.  Outside the band the unflagged outputs are
+    the form's own products byte for byte and the scaled columns' outputs are
+    within one FP32 rounding; inside it every output is within one rounding."""
+    import torch
+
+    n = 2048
+    a = oracle.make_matrix(n, n, n, "UNIFORM_1", 93)
+    b = oracle.make_matrix(n, n, n, "UNIFORM_1", 94)
+    srows = list(range(160, 166))
+    scols = [7, 300, 1201, n - 2]
+    A = a.reshape(n, n)  # [col][row]
+    B = b.reshape(n, n)
+    for r in srows:
+        A[:, r] *= np.float32(1024.0)
+    for c in scols:
+        B[c, :] *= np.float32(1024.0)
+    c0 = np.zeros(n * n, np.complex64)
+    on, info = run(cg3m, h, torch, cuda, "N", "N", n, n, n, 1.0, a, n, b, n, 0.0, c0, n, form=form)
+    assert info["rounding"] == 1
+    st = h.rounding_stats()
+    assert st["exact_tiles"] == n // 256 and st["exact_positions"] == 256 * n
+    off, _ = run(cg3m, h, torch, cuda, "N", "N", n, n, n, 1.0, a, n, b, n, 0.0, c0, n, form=form,
+                 rounding="off", k_partitions=1)
+    On = oracle.unpack(on, n, n, n)
+    Off = oracle.unpack(off, n, n, n)
+    opa = oracle.op_matrix(a, n, "N", n, n).astype(np.complex128)
+    opb = oracle.op_matrix(b, n, "N", n, n).astype(np.complex128)
+
+    def within_one_rounding(x, z):
+        x = x.astype(np.complex128)
+        sr = np.spacing(np.abs(z.real).astype(np.float32)).astype(np.float64)
+        si = np.spacing(np.abs(z.imag).astype(np.float32)).astype(np.float64)
+        return np.all(np.abs(x.real - z.real) <= sr) and np.all(np.abs(x.imag - z.imag) <= si)
+
+    # taken band: all 256 rows, sampled columns (scaled and plain)
+    cols = np.r_[0:8, scols, 1000:1008, n - 8:n]
+    assert within_one_rounding(On[0:256][:, cols], opa[0:256, :] @ opb[:, cols])
+    # outside it: plain columns keep the form's products exactly, scaled columns are recomputed
+    plain = np.setdiff1d(np.arange(n), scols)
+    assert On[np.ix_(np.arange(256, n), plain)].tobytes() == Off[np.ix_(np.arange(256, n), plain)].tobytes()
+    assert within_one_rounding(On[256:, :][:, scols], opa[256:, :] @ opb[:, scols])
+
+
+@pytest.mark.parametrize("form", ["tf32x3", "bf16x6"])
 def test_tc_pass_odd_order_edges(cg3m, oracle, cuda, h, form):
     """Order 2077 (a rounding-gated size of the reference's performance table,
     not a multiple of the 256 x 256 exact tile): the last row and column of

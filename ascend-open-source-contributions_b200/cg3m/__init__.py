@@ -353,9 +353,10 @@ def stage_names(info):
             names = ["pack", "gemm_path", "pack_rows", "energy", "select", "replay_tiles", "lanes_needed",
                      "lane_major", "replay_outputs"]
         else:
-            # packed rows with the leading planes first; the rest of the planes
-            # only for the bands the form's products read
-            names = ["pack_rows", "gemm_path", "energy", "exact_split", "select", "band_need", "pack_rest",
+            # packed rows with the leading planes and the energies first; the
+            # risk-plane GEMM selects; the rest of the planes only for the bands
+            # the form's products read
+            names = ["pack_rows", "energy", "gemm_path", "exact_split", "band_need", "pack_rest",
                      "gemm_form_tiles", "exact_tiles", "exact_crt", "lanes_needed", "lane_major",
                      "recompute_fp64_outputs", "fallback_fp64"]
     else:

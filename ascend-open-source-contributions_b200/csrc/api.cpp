@@ -239,18 +239,23 @@ cudaError_t enqueue(cudaStream_t s, const Problem& p, const Plan& plan, void* ws
         }
         return e;
     }
-    const int main_len = 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0);
+    // tensor-core forms in the rounding pass: packed rows with the leading
+    // planes and the energies precede the risk-plane GEMM, which selects
+    const bool tc_round = plan.rounding && plan.form != CG3M_FORM_FP32;
+    const int main_len = 2 + (tc_round ? 1 : 0) + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0);
     const int prep_len = plan.rounding ? rounding_prep_kernels(plan.form) : 0;
     cudaError_t err = cudaSuccess;
     int prep_launched = 0;
     int count = 0;
     {
         auto mark = run_marks(0, main_len, s);
-        // tensor-core forms in the rounding pass: packed rows with the leading
-        // planes; the rest of the planes is packed after the selection
-        err = plan.rounding && plan.form != CG3M_FORM_FP32 ? launch_rounding_pack(s, p, plan, ws)
-                                                           : launch_pack(s, p, plan, ws);
-        mark(++count);
+        if (tc_round) {
+            // the rest of the planes is packed after the selection
+            err = launch_rounding_pack(s, p, plan, ws, [&]() { mark(++count); });
+        } else {
+            err = launch_pack(s, p, plan, ws);
+            mark(++count);
+        }
         if (err == cudaSuccess) {
             if (plan.rounding) {
                 err = launch_gemm_with_path(s, p, plan, ws, status);
@@ -878,7 +883,7 @@ cg3mStatus_t cg3mPlan(cg3mOperation_t transa, cg3mOperation_t transb, int m, int
     info->k_span = plan.span;
     info->rounding = plan.rounding ? 1 : 0;
     info->kernels =
-        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? (plan.form == CG3M_FORM_FP32 ? 7 : 12) : 0);
+        plan.engine == 2 ? 1 : 2 + (plan.parts > 1 && !plan.cluster_merge ? 1 : 0) + (plan.rounding ? (plan.form == CG3M_FORM_FP32 ? 7 : 11) : 0);
     info->workspace_bytes = plan.total;
     return CG3M_STATUS_SUCCESS;
 }

@@ -109,7 +109,17 @@ cudaError_t launch_merge(cudaStream_t s, const Problem& p, const Plan& plan, voi
 // the recomputes; the tensor-core forms pack the rest of their planes there,
 // for the bands whose tiles the exact recompute leaves to the form).  mark(i)
 // is called after the i-th kernel of each half (1-based) is enqueued.
-cudaError_t launch_rounding_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws);
+cudaError_t launch_rounding_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws,
+                                 const std::function<void()>& mark);
+// The tensor-core forms' risk-plane GEMM applies the selection in its
+// epilogue: these are the selection's inputs and outputs.
+struct LeadSelect {
+    const float* energy;  // [n] op(A) rows, then [n] op(B) columns
+    float bridge, conf2;
+    uint32_t* flag_bits;
+    uint32_t* tile_count;
+    uint32_t* stats;
+};
 int rounding_prep_kernels(int form);
 cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* launched,
                                  const std::function<void(int)>& mark);

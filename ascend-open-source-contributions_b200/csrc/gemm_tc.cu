@@ -166,11 +166,16 @@ struct TcParams {
     size_t pplane;
     int* status;
     int seg_blocks;  // K-blocks per accumulation segment
-    float* path;     // risk plane (gemm3m_lead_path_kernel), ld = ldc
     int cluster_merge;  // pair kernel: the `parts` pairs of a tile form one cluster and merge on chip
     // pair kernel in the rounding pass: the per-16 x 16 flagged counts; pair
     // tiles inside a 256 x 256 tile the exact recompute takes are skipped
     const uint32_t* skip_count;
+    // gemm3m_lead_path_kernel: the rounding pass's selection in its epilogue
+    const float* energy;   // [n] op(A) rows, then [n] op(B) columns
+    float bridge, conf2;
+    uint32_t* flag_bits;   // one bit per output (column-major index), zeroed beforehand
+    uint32_t* tile_count;  // flagged outputs per 16 x 16 tile, zeroed beforehand
+    uint32_t* stats;
 };
 
 // Loads from a shared::cluster address (a peer block's shared memory).
@@ -527,8 +532,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 // running state of that form caps its tile width), and the risk estimate,
 // which needs a few significant bits of the running sums, does not tell the
 // two apart.  The K range is never partitioned: the risk plane needs the whole
-// chain.  C receives the leading-plane product (its finiteness is all the
-// selection reads).
+// chain.  The epilogue then applies the selection itself (flag words, 16 x
+// 16 tile counts, the flagged total); C and the risk plane are not written.
 constexpr int kLeadBN = 128;
 // 16 epilogue warps (four per TMEM lane quadrant, 32 columns each) hide the
 // TMEM load latency four ways per sub-partition; 18 warps launch at up to 96
@@ -718,21 +723,60 @@ __global__ void __launch_bounds__(kLeadThreads, 1)
             }
         }
         if (go) {
+            // The selection (select_kernel's predicate on this product's sums and
+            // risk plane): C and the risk plane are not written, as the form's
+            // products or the exact recompute overwrite every output later.
+            const bool row_ok = row < p.m;
+            const float ei = row_ok ? __ldg(p.energy + row) : 0.0f;
+            const int rbase = m0 + quad * 32;          // the warp's 32 rows
+            const int cbase = n0 + group * COLS;       // this thread's 32 columns
+            const bool words = (p.n & 31) == 0;        // then the warp's rows of a column are one flag word
+            uint32_t cnt00 = 0, cnt01 = 0, cnt10 = 0, cnt11 = 0, total = 0;  // [row tile][column tile]
 #pragma unroll
             for (int cb = 0; cb < COLS; cb += 8) {
                 float re[8], im[8];
                 tmem_ld8x2(run_re + (uint32_t)cb, run_im + (uint32_t)cb, re, im);
-                if (row < p.m) {
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const int col = n0 + group * COLS + cb + j;
-                        if (col < p.n) {
-                            float2* cp = p.C + (size_t)col * p.ldc + row;
-                            *cp = epilogue_value(re[j], im[j], p.epi, cp);
-                            p.path[(size_t)col * p.ldc + row] = ir[cb + j] > ii[cb + j] ? ir[cb + j] : ii[cb + j];
-                        }
+                for (int j = 0; j < 8; ++j) {
+                    const int col = cbase + cb + j;
+                    bool sel = false;
+                    if (row_ok && col < p.n) {
+                        const float ar = fabsf(re[j]), ai = fabsf(im[j]);
+                        const float magnitude = ar > ai ? ar : ai;
+                        const float risk = ir[cb + j] > ii[cb + j] ? ir[cb + j] : ii[cb + j];
+                        const float ej = __ldg(p.energy + p.n + col);
+                        const float variance =
+                            __fmul_rn(0x1p-48f, __fadd_rn(risk, __fmul_rn(__fmul_rn(ei, ej), p.bridge)));
+                        sel = !isfinite(magnitude) || !isfinite(variance) || __fmul_rn(p.conf2, variance) >= 0.0001f;
                     }
+                    const uint32_t word = __ballot_sync(0xffffffffu, sel);
+                    if (words) {
+                        if (lane == 0 && col < p.n && rbase < p.m) {
+                            p.flag_bits[((size_t)col * p.n + rbase) >> 5] = word;
+                        }
+                    } else if (sel) {
+                        const size_t idx = (size_t)col * p.n + row;
+                        atomicOr(&p.flag_bits[idx >> 5], 1u << (idx & 31));
+                    }
+                    const uint32_t lo = (uint32_t)__popc(word & 0xFFFFu), hi = (uint32_t)__popc(word >> 16);
+                    if ((cb + j) < 16) {
+                        cnt00 += lo;
+                        cnt10 += hi;
+                    } else {
+                        cnt01 += lo;
+                        cnt11 += hi;
+                    }
+                    total += lo + hi;
                 }
+            }
+            if (lane == 0 && total != 0) {
+                const int g16 = (p.n + 15) / 16;
+                const size_t ti = (size_t)(rbase >> 4), tj = (size_t)(cbase >> 4);
+                if (cnt00) atomicAdd(&p.tile_count[tj * g16 + ti], cnt00);
+                if (cnt10) atomicAdd(&p.tile_count[tj * g16 + ti + 1], cnt10);
+                if (cnt01) atomicAdd(&p.tile_count[(tj + 1) * g16 + ti], cnt01);
+                if (cnt11) atomicAdd(&p.tile_count[(tj + 1) * g16 + ti + 1], cnt11);
+                atomicAdd(&p.stats[kStatFlagged], total);
             }
         }
     }
@@ -1148,7 +1192,6 @@ cudaError_t launch_pair(cudaStream_t stream, const Problem& pr, const Plan& plan
     if (p.seg_blocks < 1) {
         p.seg_blocks = 1;
     }
-    p.path = nullptr;
     p.skip_count = skip_count;
     p.cluster_merge = plan.cluster_merge ? 1 : 0;
     if (p.cluster_merge && (plan.parts < 2 || plan.parts > 4)) {
@@ -1234,7 +1277,7 @@ cudaError_t launch_form(cudaStream_t stream, const Problem& pr, const Plan& plan
 
 template <int LEAD>
 cudaError_t launch_lead_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, int* status,
-                             float* path)
+                             const LeadSelect& sel)
 {
     using Cfg = TcCfg<LEAD>;
     const bool bf16 = Cfg::FMT == 1;
@@ -1274,7 +1317,12 @@ cudaError_t launch_lead_path(cudaStream_t stream, const Problem& pr, const Plan&
     if (p.seg_blocks < 1) {
         p.seg_blocks = 1;
     }
-    p.path = path;
+    p.energy = sel.energy;
+    p.bridge = sel.bridge;
+    p.conf2 = sel.conf2;
+    p.flag_bits = sel.flag_bits;
+    p.tile_count = sel.tile_count;
+    p.stats = sel.stats;
     auto kernel = gemm3m_lead_path_kernel<LEAD>;
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLeadSmem);
     if (err != cudaSuccess) {
@@ -1310,13 +1358,13 @@ cudaError_t launch_gemm_tc(cudaStream_t stream, const Problem& pr, const Plan& p
     }
 }
 
-cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, float* path,
-                                int* status)
+cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws,
+                                const LeadSelect& sel, int* status)
 {
     switch (plan.form) {
-        case CG3M_FORM_TF32X3: return launch_lead_path<kLeadTf32>(stream, pr, plan, ws, status, path);
+        case CG3M_FORM_TF32X3: return launch_lead_path<kLeadTf32>(stream, pr, plan, ws, status, sel);
         case CG3M_FORM_BF16X6:
-        case CG3M_FORM_BF16X9: return launch_lead_path<kLeadBf16>(stream, pr, plan, ws, status, path);
+        case CG3M_FORM_BF16X9: return launch_lead_path<kLeadBf16>(stream, pr, plan, ws, status, sel);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -42,8 +42,8 @@ cudaError_t launch_pack_rows(cudaStream_t stream, const Problem& p, void* rows_a
                              const Plan* lead_plan = nullptr, void* ws = nullptr);
 cudaError_t launch_gemm_fp32_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, float* path,
                                   int* status);
-cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws, float* path,
-                                int* status);
+cudaError_t launch_gemm_tc_path(cudaStream_t stream, const Problem& pr, const Plan& plan, void* ws,
+                                const LeadSelect& sel, int* status);
 
 namespace {
 
@@ -987,8 +987,12 @@ size_t rounding_bytes(int n, int form, std::vector<size_t>* guards) { return rou
 cudaError_t launch_gemm_with_path(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* status)
 {
     const RoundLayout L = round_layout(plan, ws, p.n);
-    return plan.form == CG3M_FORM_FP32 ? launch_gemm_fp32_path(s, p, plan, ws, L.path, status)
-                                       : launch_gemm_tc_path(s, p, plan, ws, L.path, status);
+    if (plan.form == CG3M_FORM_FP32) {
+        return launch_gemm_fp32_path(s, p, plan, ws, L.path, status);
+    }
+    const LeadSelect sel{L.energy, bridge_term(p.n), kConfidence * kConfidence, L.flag_bits,
+                         L.tile_count, L.stats};
+    return launch_gemm_tc_path(s, p, plan, ws, sel, status);
 }
 
 // The replay's staging copies: op(A) rows or op(B) columns as an n x n array of
@@ -1033,14 +1037,31 @@ static cudaError_t launch_replay(cudaStream_t s, int n, int span, const RoundLay
 
 int rounding_prep_kernels(int form)
 {
-    (void)form;
-    return 2;  // FP32: packed rows, energies; tensor-core forms: energies, residues
+    return form == CG3M_FORM_FP32 ? 2 : 1;  // FP32: packed rows, energies; tensor-core forms: residues
 }
 
-cudaError_t launch_rounding_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws)
+// Tensor-core forms: zero the selection's outputs (its flag words too, which
+// take per-bit atomics when n is not a multiple of 32), then the packed rows
+// with the leading planes and the energies, all before the risk-plane GEMM
+// that applies the selection.
+cudaError_t launch_rounding_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws,
+                                 const std::function<void()>& mark)
 {
-    const RoundLayout L = round_layout(plan, ws, p.n);
-    return launch_pack_rows(s, p, L.rows_a, L.rows_b, row_pitch(p.n), &plan, ws);
+    const int n = p.n;
+    const RoundLayout L = round_layout(plan, ws, n);
+    const int pitch = row_pitch(n);
+    cudaError_t err = cudaMemsetAsync(L.flag_bits, 0, L.zero_bytes + flag_words(n) * 4, s);
+    if (err == cudaSuccess) {
+        err = launch_pack_rows(s, p, L.rows_a, L.rows_b, pitch, &plan, ws);
+        mark();
+    }
+    if (err == cudaSuccess) {
+        const int span = ((n + kLanes - 1) / kLanes) | 1;
+        energy_kernel<<<2 * n, kLanes, 0, s>>>(L.rows_a, L.rows_b, n, pitch, span, L.energy);
+        err = cudaGetLastError();
+        mark();
+    }
+    return err;
 }
 
 cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& plan, void* ws, int* launched,
@@ -1052,11 +1073,11 @@ cudaError_t launch_rounding_prep(cudaStream_t s, const Problem& p, const Plan& p
     const int span = ((n + kLanes - 1) / kLanes) | 1;
     int count = 0;
     cudaError_t err = cudaSuccess;
-    if (plan.form == CG3M_FORM_FP32) {  // the tensor-core forms packed their rows first
+    if (plan.form == CG3M_FORM_FP32) {  // the tensor-core forms packed their rows and energies first
         err = launch_pack_rows(s, p, L.rows_a, L.rows_b, pitch);
         mark(++count);
     }
-    if (err == cudaSuccess) {
+    if (err == cudaSuccess && plan.form == CG3M_FORM_FP32) {
         energy_kernel<<<2 * n, kLanes, 0, s>>>(L.rows_a, L.rows_b, n, pitch, span,
                                                                         L.energy);
         err = cudaGetLastError();
@@ -1079,8 +1100,11 @@ cudaError_t launch_rounding_finish(cudaStream_t s, const Problem& p, const Plan&
     const RoundLayout L = round_layout(plan, ws, n);
     const int span = ((n + kLanes - 1) / kLanes) | 1;
     int count = 0;
-    cudaError_t err = cudaMemsetAsync(L.tile_count, 0, L.zero_bytes, s);
-    if (err == cudaSuccess) {
+    cudaError_t err = cudaSuccess;
+    if (plan.form == CG3M_FORM_FP32) {  // the tensor-core forms' risk-plane GEMM selected already
+        err = cudaMemsetAsync(L.tile_count, 0, L.zero_bytes, s);
+    }
+    if (err == cudaSuccess && plan.form == CG3M_FORM_FP32) {
         select_kernel<<<148 * 8, 256, 0, s>>>(n, static_cast<const float2*>(p.C), L.energy, L.path, bridge_term(n),
                                               L.flag_bits, L.tile_count, L.stats);
         err = cudaGetLastError();

@@ -250,16 +250,18 @@ def test_tc_rounding_pass_runs_unsplit(cg3m):
 def test_rounding_stage_names_match_kernel_count(cg3m):
     """The names cg3mSetStageEvents' brackets are reported under cover exactly
     the kernels a rounding call launches: the FP32 form's pack, path GEMM and
-    replay (9), the tensor-core forms' packed rows with the leading planes
-    first, the banded rest of the planes after the selection (14)."""
+    replay (9), the tensor-core forms' packed rows with the leading planes and
+    the energies first, the selection inside the risk-plane GEMM and the banded
+    rest of the planes after it (13)."""
     fp32 = cg3m.plan("N", "N", 4096, 4096, 4096, form="fp32")
     names = cg3m.stage_names(fp32)
     assert fp32["kernels"] == 9 and len(names) == 9 and names[:2] == ["pack", "gemm_path"]
     for form in ("tf32x3", "bf16x6", "bf16x9"):
         tc = cg3m.plan("N", "N", 4096, 4096, 4096, form=form)
         names = cg3m.stage_names(tc)
-        assert tc["kernels"] == 14 and len(names) == 14, (form, tc, names)
-        assert names[:2] == ["pack_rows", "gemm_path"] and "kernel" not in "".join(names)
+        assert tc["kernels"] == 13 and len(names) == 13, (form, tc, names)
+        assert names[:3] == ["pack_rows", "energy", "gemm_path"] and "kernel" not in "".join(names)
+        assert "select" not in names
         assert names.index("band_need") < names.index("pack_rest") < names.index("gemm_form_tiles")
 
 

@@ -105,10 +105,11 @@ cudaError_t launch_merge(cudaStream_t s, const Problem& p, const Plan& plan, voi
 // reads (launch_rounding_pack, instead of the full pack).  Then two halves:
 // the preparation reads only op(A) and op(B) (packed rows for the FP32 form,
 // energies and, for the tensor-core forms, the residues of the exact
-// recompute); the finish needs the GEMM's C and risk plane (selection, then
-// the recomputes; the tensor-core forms pack the rest of their planes there,
-// for the bands whose tiles the exact recompute leaves to the form).  mark(i)
-// is called after the i-th kernel of each half (1-based) is enqueued.
+// recompute); the finish needs the GEMM's C and risk plane (FP32: selection,
+// then the recomputes; the tensor-core forms' risk-plane GEMM selected in its
+// epilogue, and they pack the rest of their planes in the finish, for the
+// bands whose tiles the exact recompute leaves to the form).  mark(i) is
+// called after the i-th kernel of each half (1-based) is enqueued.
 cudaError_t launch_rounding_pack(cudaStream_t s, const Problem& p, const Plan& plan, void* ws,
                                  const std::function<void()>& mark);
 // The tensor-core forms' risk-plane GEMM applies the selection in its
